@@ -1,0 +1,165 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes driver for the oracle's C restatement (gpl_oracle.c).
+
+Same method set as ``oracle.refcpu.RefModel`` and the product's ``gaspacho2_b200.GPLVM`` so a
+test can run one sequence of phases through all three. Only tests, ``smoke()`` and
+bench.py's CPU legs may load this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libgpl_oracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(ORACLE_SO)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{ORACLE_SO} is not built (make -C oracle oracle)")
+        L = ctypes.CDLL(ORACLE_SO)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, _ip, _ip, _dp, ctypes.c_int, _ip, _ip,
+                                 ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_dims.argtypes = [ctypes.c_void_p, _ip]
+        L.orc_init_params.argtypes = [ctypes.c_void_p]
+        L.orc_set_params.argtypes = [ctypes.c_void_p] + [_dp] * 6
+        L.orc_set_beta.argtypes = [ctypes.c_void_p, _dp]
+        for name in ("orc_kernel_mats", "orc_glm_init", "orc_expand_delta", "orc_beta_from_tilde"):
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+        L.orc_irls_sweep.restype = ctypes.c_double
+        L.orc_irls_sweep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_irls.restype = ctypes.c_int
+        L.orc_irls.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_objective_after_irls.restype = ctypes.c_double
+        L.orc_objective_after_irls.argtypes = [ctypes.c_void_p]
+        L.orc_gradient.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_objective.restype = ctypes.c_double
+        L.orc_objective.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_lbfgs_update.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_downdate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.orc_fit.restype = ctypes.c_int
+        L.orc_fit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]
+        L.orc_get.restype = ctypes.c_long
+        L.orc_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _dptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+class OracleModel:
+    def __init__(self, y, z, ls, X0, M: int, Q: int):
+        L = lib()
+        self._ci = np.ascontiguousarray(y.i, np.int32)
+        self._gp = np.ascontiguousarray(y.p, np.int32)
+        self._cx = np.ascontiguousarray(y.x, np.float64)
+        self._c = np.ascontiguousarray(z.c, np.int32)
+        self._v = np.ascontiguousarray(z.v, np.int32)
+        body = z.body_bytes()
+        self._body = ctypes.create_string_buffer(body, len(body) or 1)
+        self._ls = np.ascontiguousarray(ls, np.float64)
+        self._X0 = np.ascontiguousarray(np.asarray(X0, np.float64).ravel(order="F"))
+        self.h = L.orc_create(y.N, y.J, y.L, self._ci.ctypes.data_as(_ip), self._gp.ctypes.data_as(_ip),
+                              _dptr(self._cx), z.n_var, self._c.ctypes.data_as(_ip), self._v.ctypes.data_as(_ip),
+                              ctypes.cast(self._body, ctypes.c_void_p), len(body), int(M), int(Q), _dptr(self._ls),
+                              _dptr(self._X0))
+        if not self.h:
+            raise ValueError("oracle rejected the inputs")
+        d = (ctypes.c_int * 6)()
+        L.orc_dims(self.h, d)
+        self.N, self.J, self.M, self.P, self.p, self.Q = list(d)
+
+    @classmethod
+    def from_dataset(cls, ds) -> "OracleModel":
+        return cls(ds.y, ds.z, ds.ls, ds.X0, ds.M, ds.Q)
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, prm) -> None:
+        flat = [np.ascontiguousarray(a, dtype=np.float64) for a in prm.flat()]
+        lib().orc_set_params(self.h, *[_dptr(a) for a in flat])
+
+    def set_beta(self, beta: np.ndarray) -> None:
+        b = np.ascontiguousarray(np.asarray(beta, np.float64).ravel(order="F"))
+        lib().orc_set_beta(self.h, _dptr(b))
+
+    def kernel_mats(self):
+        lib().orc_kernel_mats(self.h)
+
+    def glm_init(self):
+        lib().orc_glm_init(self.h)
+
+    def expand_delta(self):
+        lib().orc_expand_delta(self.h)
+
+    def irls_sweep(self, itr: int, jtr: int) -> float:
+        return lib().orc_irls_sweep(self.h, jtr)
+
+    def irls(self, itr: int, jtr_max: int) -> int:
+        return lib().orc_irls(self.h, jtr_max)
+
+    def objective_after_irls(self, itr: int = 0) -> float:
+        return lib().orc_objective_after_irls(self.h)
+
+    def objective(self, itr: int, slot: int) -> float:
+        return lib().orc_objective(self.h, slot)
+
+    def gradient(self) -> np.ndarray:
+        n = self.N + self.p + self.N * self.Q + self.M * self.Q + self.Q
+        g = np.zeros(n)
+        lib().orc_gradient(self.h, _dptr(g))
+        return g
+
+    def lbfgs_update(self, jtr: int, rhoflag: int):
+        lib().orc_lbfgs_update(self.h, jtr, rhoflag)
+
+    def downdate(self, jtr: int, sr: float, rhoflag: int):
+        lib().orc_downdate(self.h, jtr, sr, rhoflag)
+
+    def beta_from_tilde(self):
+        lib().orc_beta_from_tilde(self.h)
+
+    def fit(self, itr_max: int, lbfgs_budget: int, trace_cap: int = 100000):
+        st = (ctypes.c_int * 4)()
+        tr = np.zeros(trace_cap)
+        rc = lib().orc_fit(self.h, itr_max, lbfgs_budget, st, _dptr(tr), trace_cap)
+        stats = dict(outer=st[0], irls=st[1], lbfgs=st[2], evals=st[3])
+        return rc, stats, tr[:stats["outer"] + stats["lbfgs"]].copy()
+
+    def get(self, name: str) -> np.ndarray:
+        n = lib().orc_get(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        lib().orc_get(self.h, name.encode(), _dptr(out))
+        return out

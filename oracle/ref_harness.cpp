@@ -1,0 +1,448 @@
+/*
+ * ref_harness.cpp -- TEST INFRASTRUCTURE ONLY: drives the reference's own kernels,
+ * compiled for the host through ref_shim.h, in the order the reference driver calls
+ * them (ggplvm.cu:951-1354, `main`). Built by oracle/Makefile into oracle/_ref/.
+ *
+ * Nothing here computes model arithmetic: every number comes from the reference
+ * kernels (kernel_funcs.cu, chol.cu, util_cuda.cu, init.cu, ggplvm.cu:1-935). The
+ * harness only allocates the buffers main allocates (ggplvm.cu:1024-1060), launches
+ * the kernels with main's grid/block shapes (ggplvm.cu:1068-1095), and exposes the
+ * phases as C functions so tests can compare the product path with the reference
+ * step by step. ITRMAX/JTRMAX are hard-coded in main; ref_fit takes them as budgets.
+ *
+ * Deviations from main, all forced by running without GSL or a GPU:
+ *   - initTaWithPer (util.c:73-87, GSL MT19937) is not available: dim 0 of T gets
+ *     main's equispaced grid and dims >= 1 start at zero; callers always pass T
+ *     through ref_set_params (the --init-params path, ggplvm.cu:1103-1106).
+ *   - device memory is calloc'd, so zeta and the unused tail of ss read as zero.
+ *   - the per-iteration text dumps (X9.gz, phi.gz, Params9.bin; ggplvm.cu:1302-1315)
+ *     are not written.
+ */
+#include <vector>
+#include <string>
+#include <cstring>
+
+#include "SparseMat.cuh"
+#include "util_cuda.cuh"
+#include "init.cuh"
+#include "kernel_funcs.cuh"
+
+extern "C" int ref_verbose = 0;
+
+/* kernels defined in ggplvm.cu (no header in the reference) */
+extern double wt, igap1, igb;
+void solvePsi(int J, int P, double* IdenP, double* Psi);
+void getC2(int J, DataFrame* Z, double* Psi, double* W, double* delta, double* tBeta, double* phi, double* K,
+           double* Kinv, double* KinvKmn, double wt, double* Work, double* C2);
+void getGradTau(int Q, DataFrame* Z, double* Xi, double* Ta, double* rho, double* C1, double* C2, double* grad);
+void collectGradLogRho(int Q, DataFrame* Z, double* gradLogRhoTmp, double* grad);
+void getGradLogRho(int Q, DataFrame* Z, double* Xi, double* Ta, double* rho, double* C1, double* C2,
+                   double* gradLogRhoTmp);
+void getGradLogDelta(int J, DataFrame* Z, double* DeltaInv, double* delta, double* K, double* Psi, double* tBeta,
+                     double* phi, double* Work, double* gradDeltaTmp);
+void collectGradLogDelta(int J, DataFrame* Z, double* delta, double* gradDeltaTmp, double* W, double* titsias,
+                         double wt, double* grad);
+void getOinvt(int N, int J, double* Omega, double* W);
+void getGradLogOmega(int J, int Q, DataFrame* Z, double* Omega, double* delta, double* phi, double* Nu, double* Psi,
+                     double* W, double* tBeta, double* Xi, double* Ta, double* rho, double* KinvKmn,
+                     double* titsias, double wt, double igap1, double igb, double* Work, double* C1, double* grad);
+void getBetaFromTildeBeta(int J, DataFrame* Z, double* tBeta, double* zeta, double* Beta);
+void getTildeBeta(int J, DataFrame* Z, double* ls, double* Psi, double* Omega, double* Nu, double* W, double* Work,
+                  double* tBeta);
+void getBetaPhi(int J, DataFrame* Z, double* ls, double* Psi, double* Omega, double* zeta, double* Nu, double* W,
+                double* Work, int jtr, double* Beta, double* phi);
+void getWForBeta(SparseMat* Y, DataFrame* Z, double* ls, double* Beta, double* zeta, double* delta, double* titsias,
+                 double wt, double* W, double* Nu);
+void getPsi(int J, DataFrame* Z, double* Omega, double* DeltaInv, double* W, double* Psi, int jtr);
+void cholPsi(int J, int P, double* Psi);
+void cholDeltaInv(int P, double* DeltaInv);
+void getLkhdPois(SparseMat* Y, DataFrame* Z, double* W, double* delta, double* titsias, double wt, double* lkhds);
+void getLkhd(int J, DataFrame* Z, double* Omega, double* DeltaInv, double* phi, double* Nu, double* Psi, double* W,
+             double* Work, double* lkhds);
+void collectLkhd(int N, int J, int Q, double* Omega, double* lkhds, int itr, int jtr, DataFrame* Z, double* delta,
+                 double* Xi, double* Ta, double* W, double* titsias, double wt, double igap1, double igb,
+                 double* lkhd_d);
+void Downdate(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K, double* Xi, double* Ta,
+              double* rho, double* grad, double* grad0, double* SS, double* XX, double* ss, double r, int rhoflag);
+void LBFGS(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K, double* Xi, double* Ta, double* rho,
+           double* grad, double* grad0, double* SS, double* XX, double* ss, double* Work, int rhoflag);
+
+namespace {
+
+struct RefCtx {
+  int N, J, M, Q, P, p;
+  SparseMat *Y_h, *Y;
+  DataFrame *Z_h, *Z;
+  double *Omega, *DeltaInv, *delta, *zeta, *ls, *phi, *Psi, *W, *Nu, *Beta, *tBeta, *lkhds, *lkhd_d;
+  double *grad, *grad0, *SS, *XX, *ss, *gradDeltaTmp, *gradLogRhoTmp, *Work;
+  double *rho, *Xi, *Ta, *K, *Kinv, *KinvKmn, *C1, *C2, *IdenP, *titsias;
+  dim3 gridJ, gridJP, gridPsi, blockPsi, gridPP, gridN, blockN, gridDel, block1, gridNpMM, gridMM, gridMQ, gridQ;
+  int rhoflag;
+  std::vector<double> lkhd_h;
+};
+
+double* dalloc(size_t n) {
+  void* p = nullptr;
+  cudaMalloc(&p, sizeof(double) * (n ? n : 1));
+  return (double*)p;
+}
+
+bool read_doubles(const char* path, double* dst, size_t n) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  size_t got = fread(dst, sizeof(double), n, f);
+  fclose(f);
+  return got == n;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Mirrors main up to the device boundary (ggplvm.cu:965-1101): reference loaders,
+ * main's allocations and grid shapes, then initParams. Returns NULL on a file error. */
+void* ref_open(const char* y_path, const char* z_path, const char* ls_path, const char* xi_path, int M, int Q) {
+  FILE* probe;
+  for (const char* pth : {y_path, z_path, ls_path, xi_path}) {
+    if (!(probe = fopen(pth, "rb"))) return nullptr;
+    fclose(probe);
+  }
+  RefCtx* c = new RefCtx();
+  std::string yp(y_path), zp(z_path);
+  c->Y_h = loadSparseMat(&yp[0]);
+  c->N = c->Y_h->N;
+  c->J = c->Y_h->J;
+  c->Y = newSparseMatOnDevice(c->Y_h);
+  c->M = M;
+  c->Q = Q;
+  c->Z_h = loadDataFrame(&zp[0], M);
+  c->Z = newDataFrameOnDevice(c->Z_h);
+  c->P = c->Z_h->P;
+  c->p = c->Z_h->p;
+  const int N = c->N, J = c->J, P = c->P, p = c->p;
+
+  c->Psi = dalloc((size_t)J * P * P * 2);
+  c->W = dalloc((size_t)N * (J + 1));
+  c->Nu = dalloc((size_t)N * J);
+  c->grad = dalloc(N + p + (size_t)(N + M + 1) * Q);
+  c->grad0 = dalloc(N + p + (size_t)(N + M + 1) * Q);
+  c->SS = dalloc((N + p + (size_t)(N + M + 1) * Q) * 10);
+  c->XX = dalloc((N + p + (size_t)(N + M + 1) * Q) * 10);
+  c->ss = dalloc(N + p + (size_t)(N + M + 1) * Q);
+  size_t lwork = (size_t)(N < M * M ? M * M : N);
+  if (lwork < (size_t)J * P) lwork = (size_t)J * P;
+  lwork *= (2 * P);
+  c->Work = dalloc(lwork);
+  c->C1 = dalloc((size_t)N * M);
+  c->C2 = dalloc((size_t)M * M);
+  c->IdenP = dalloc((size_t)P * P);
+  c->ls = dalloc(N);
+  c->Omega = dalloc((size_t)N * 2);
+  c->DeltaInv = dalloc((size_t)P * P);
+  c->delta = dalloc((size_t)p * 2);
+  c->phi = dalloc(J);
+  c->gradDeltaTmp = dalloc((size_t)P * J);
+  c->gradLogRhoTmp = dalloc((size_t)M * Q);
+  c->zeta = dalloc(P);
+  c->Beta = dalloc((size_t)P * J);
+  c->tBeta = dalloc((size_t)P * J);
+  c->lkhds = dalloc(J);
+  c->lkhd_d = dalloc(50000);
+  c->rho = dalloc((size_t)Q * 2);
+  c->Xi = dalloc((size_t)N * Q * 2);
+  c->Ta = dalloc((size_t)M * Q * 2);
+  c->K = dalloc((size_t)M * M);
+  c->Kinv = dalloc((size_t)M * M);
+  c->KinvKmn = dalloc((size_t)N * M);
+  c->titsias = dalloc(N);
+  c->lkhd_h.assign(50000, 0.0);
+
+  if (!read_doubles(xi_path, c->Xi, (size_t)N * Q) || !read_doubles(ls_path, c->ls, N)) {
+    delete c;
+    return nullptr;
+  }
+  for (int i = 0; i < M; i++) c->Ta[i] = ((double)(i + 1) / (double)(M + 1)) * 2.0 * 3.14159265358979;
+
+  int sN = (int)(sqrt((double)N) / 4) + 1;
+  c->gridJ = dim3(J, 1);
+  c->gridJP = dim3(J, P);
+  c->gridPsi = dim3(J, P);
+  c->blockPsi = dim3(1, P);
+  c->gridPP = dim3(P, P);
+  c->gridN = dim3(sN, sN);
+  c->blockN = dim3(4, 4);
+  c->gridDel = dim3(p, 1);
+  c->block1 = dim3(1, 1);
+  c->gridNpMM = dim3(N + M, M);
+  c->gridMM = dim3(M, M);
+  c->gridMQ = dim3(M, Q);
+  c->gridQ = dim3(Q, 1);
+  c->rhoflag = 0;
+
+  ref_launch(dim3(1), dim3(1), [&] { initParams(N, J, P, p, Q, c->delta, c->Omega, c->phi, c->rho, c->IdenP); });
+  return c;
+}
+
+void ref_close(void* h) {
+  /* buffers are left to process exit: the reference never frees most of them either */
+  delete (RefCtx*)h;
+}
+
+void ref_dims(void* h, int* out) {
+  RefCtx* c = (RefCtx*)h;
+  out[0] = c->N; out[1] = c->J; out[2] = c->M; out[3] = c->P; out[4] = c->p; out[5] = c->Q;
+}
+
+/* readParams (util_cuda.cu:520-544) without the file: any NULL argument keeps the current value. */
+void ref_set_params(void* h, const double* Omega, const double* delta, const double* X, const double* T,
+                    const double* rho, const double* phi) {
+  RefCtx* c = (RefCtx*)h;
+  if (Omega) memcpy(c->Omega, Omega, sizeof(double) * c->N);
+  if (delta) memcpy(c->delta, delta, sizeof(double) * c->p);
+  if (X) memcpy(c->Xi, X, sizeof(double) * c->N * c->Q);
+  if (T) memcpy(c->Ta, T, sizeof(double) * c->M * c->Q);
+  if (rho) memcpy(c->rho, rho, sizeof(double) * c->Q);
+  if (phi) memcpy(c->phi, phi, sizeof(double) * c->J);
+}
+
+void ref_set_beta(void* h, const double* beta) {
+  RefCtx* c = (RefCtx*)h;
+  memcpy(c->Beta, beta, sizeof(double) * (size_t)c->P * c->J);
+}
+
+/* ggplvm.cu:1111-1113 */
+void ref_kernel_mats(void* h) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(c->gridNpMM, c->block1, [&] { getKernelMats(c->Q, c->Xi, c->Ta, c->rho, c->Z, c->K, c->Kinv, c->KinvKmn); });
+  ref_launch(dim3(1), dim3(1), [&] { cholKmm(c->M, c->Kinv); });
+  ref_launch(c->gridN, c->blockN, [&] { getKinvKmn(c->Kinv, c->Z, c->KinvKmn, c->titsias); });
+}
+
+/* ggplvm.cu:1134-1137 (GLM initialisation) */
+void ref_glm_init(void* h) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(dim3(1), dim3(1), [&] { expandDelta_k(c->Z, c->delta, c->K, c->DeltaInv); });
+  ref_launch(c->gridPP, c->block1, [&] { initPsi(c->Z, c->DeltaInv, c->Psi); });
+  ref_launch(dim3(1), dim3(1), [&] { initPsi2(c->P, c->Psi); });
+  ref_launch(c->gridJ, c->block1, [&] { initBeta(c->Y, c->ls, c->Z, c->Psi, c->Work, c->Beta); });
+}
+
+void ref_expand_delta(void* h) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(dim3(1), dim3(1), [&] { expandDelta_k(c->Z, c->delta, c->K, c->DeltaInv); });
+}
+
+/* One IRLS sweep, ggplvm.cu:1156-1181; returns lkhd_d[jtr] (the Poisson log-likelihood sum). */
+double ref_irls_sweep(void* h, int itr, int jtr) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(c->gridJ, c->block1,
+             [&] { getWForBeta(c->Y, c->Z, c->ls, c->Beta, c->zeta, c->delta, c->titsias, wt, c->W, c->Nu); });
+  ref_launch(c->gridPsi, c->blockPsi, [&] { getPsi(c->J, c->Z, c->Omega, c->DeltaInv, c->W, c->Psi, jtr + 1); });
+  ref_launch(c->gridJ, c->block1, [&] { cholPsi(c->J, c->P, c->Psi); });
+  ref_launch(c->gridJ, c->block1, [&] {
+    getBetaPhi(c->J, c->Z, c->ls, c->Psi, c->Omega, c->zeta, c->Nu, c->W, c->Work, jtr, c->Beta, c->phi);
+  });
+  ref_launch(c->gridJ, c->block1, [&] { getLkhdPois(c->Y, c->Z, c->W, c->delta, c->titsias, wt, c->lkhds); });
+  ref_launch(dim3(1), dim3(1), [&] {
+    collectLkhd(0, c->J, 0, c->Omega, c->lkhds, itr, jtr, c->Z, c->delta, c->Xi, c->Ta, c->W, c->titsias, wt, igap1,
+                igb, c->lkhd_d);
+  });
+  c->lkhd_h[jtr] = c->lkhd_d[jtr];
+  return c->lkhd_d[jtr];
+}
+
+/* The IRLS loop with main's stopping rule (ggplvm.cu:1152-1189). Returns the number of
+ * sweeps run, or -1 when main would exit on a NaN likelihood (ggplvm.cu:1182). */
+int ref_irls(void* h, int itr, int jtr_max) {
+  RefCtx* c = (RefCtx*)h;
+  int jtr;
+  for (jtr = 0; jtr < jtr_max; jtr++) {
+    ref_irls_sweep(h, itr, jtr);
+    double* l = c->lkhd_h.data();
+    if (jtr > 0) {
+      if (std::isnan(l[jtr])) return -1;
+      if (jtr == (jtr_max - 1) || fabs(l[jtr - 1] - l[jtr]) / fabs(l[jtr]) < 1e-7) { jtr++; break; }
+    }
+  }
+  return jtr;
+}
+
+/* ggplvm.cu:1205-1211: objective at the IRLS solution, stored in lkhd_d[0]. */
+double ref_objective_after_irls(void* h, int itr) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(c->gridN, c->blockN, [&] { getOinvt(c->N, c->J, c->Omega, c->W); });
+  ref_launch(dim3(1), dim3(1), [&] { cholDeltaInv(c->P, c->DeltaInv); });
+  ref_launch(c->gridJ, c->block1, [&] {
+    getLkhd(c->J, c->Z, c->Omega, c->DeltaInv, c->phi, c->Nu, c->Psi, c->W, c->Work, c->lkhds);
+  });
+  ref_launch(dim3(1), dim3(1), [&] {
+    collectLkhd(c->N, c->J, c->Q, c->Omega, c->lkhds, itr, 0, c->Z, c->delta, c->Xi, c->Ta, c->W, c->titsias, wt,
+                igap1, igb, c->lkhd_d);
+  });
+  c->lkhd_h[0] = c->lkhd_d[0];
+  return c->lkhd_d[0];
+}
+
+/* One gradient evaluation, ggplvm.cu:1215-1240. Writes the N+p+N*Q+M*Q+Q vector. */
+void ref_gradient(void* h, double* grad_out) {
+  RefCtx* c = (RefCtx*)h;
+  const int N = c->N, J = c->J, M = c->M, Q = c->Q, P = c->P, p = c->p;
+  ref_launch(dim3(1), dim3(1), [&] { expandDelta_k(c->Z, c->delta, c->K, c->DeltaInv); });
+  ref_launch(c->gridN, c->blockN, [&] { getOinvt(N, J, c->Omega, c->W); });
+  ref_launch(c->gridJ, c->block1,
+             [&] { getTildeBeta(J, c->Z, c->ls, c->Psi, c->Omega, c->Nu, c->W, c->Work, c->tBeta); });
+  ref_launch(c->gridJP, c->block1, [&] {
+    getGradLogDelta(J, c->Z, c->DeltaInv, c->delta, c->K, c->Psi, c->tBeta, c->phi, c->Work, c->gradDeltaTmp);
+  });
+  ref_launch(c->gridDel, c->block1,
+             [&] { collectGradLogDelta(J, c->Z, c->delta, c->gradDeltaTmp, c->W, c->titsias, wt, c->grad); });
+  ref_launch(c->gridN, c->blockN, [&] {
+    getGradLogOmega(J, Q, c->Z, c->Omega, c->delta, c->phi, c->Nu, c->Psi, c->W, c->tBeta, c->Xi, c->Ta, c->rho,
+                    c->KinvKmn, c->titsias, wt, igap1, igb, c->Work, c->C1, c->grad);
+  });
+  ref_launch(c->gridJP, c->block1, [&] { solvePsi(J, P, c->IdenP, c->Psi); });
+  ref_launch(c->gridMM, c->block1, [&] {
+    getC2(J, c->Z, c->Psi, c->W, c->delta, c->tBeta, c->phi, c->K, c->Kinv, c->KinvKmn, wt, c->Work, c->C2);
+  });
+  ref_launch(c->gridMQ, c->block1, [&] { getGradTau(Q, c->Z, c->Xi, c->Ta, c->rho, c->C1, c->C2, c->grad); });
+  ref_launch(c->gridMQ, c->block1,
+             [&] { getGradLogRho(Q, c->Z, c->Xi, c->Ta, c->rho, c->C1, c->C2, c->gradLogRhoTmp); });
+  ref_launch(c->gridQ, c->block1, [&] { collectGradLogRho(Q, c->Z, c->gradLogRhoTmp, c->grad); });
+  if (grad_out) memcpy(grad_out, c->grad, sizeof(double) * ((size_t)N + p + (size_t)N * Q + (size_t)M * Q + Q));
+}
+
+/* One line-search evaluation of the objective, ggplvm.cu:1258-1277; stores lkhd_d[slot]. */
+double ref_objective(void* h, int itr, int slot) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(c->gridN, c->blockN, [&] { getOinvt(c->N, c->J, c->Omega, c->W); });
+  ref_launch(c->gridNpMM, c->block1,
+             [&] { getKernelMats(c->Q, c->Xi, c->Ta, c->rho, c->Z, c->K, c->Kinv, c->KinvKmn); });
+  ref_launch(dim3(1), dim3(1), [&] { expandDelta_k(c->Z, c->delta, c->K, c->DeltaInv); });
+  ref_launch(dim3(1), dim3(1), [&] { cholKmm(c->M, c->Kinv); });
+  ref_launch(c->gridN, c->blockN, [&] { getKinvKmn(c->Kinv, c->Z, c->KinvKmn, c->titsias); });
+  ref_launch(c->gridPsi, c->blockPsi,
+             [&] { getPsi(c->J, c->Z, c->Omega, c->DeltaInv, c->W, c->Psi, slot); });
+  ref_launch(c->gridJ, c->block1, [&] { cholPsi(c->J, c->P, c->Psi); });
+  ref_launch(dim3(1), dim3(1), [&] { cholDeltaInv(c->P, c->DeltaInv); });
+  ref_launch(c->gridJ, c->block1, [&] {
+    getLkhd(c->J, c->Z, c->Omega, c->DeltaInv, c->phi, c->Nu, c->Psi, c->W, c->Work, c->lkhds);
+  });
+  ref_launch(dim3(1), dim3(1), [&] {
+    collectLkhd(c->N, c->J, c->Q, c->Omega, c->lkhds, itr, slot, c->Z, c->delta, c->Xi, c->Ta, c->W, c->titsias, wt,
+                igap1, igb, c->lkhd_d);
+  });
+  c->lkhd_h[slot] = c->lkhd_d[slot];
+  return c->lkhd_d[slot];
+}
+
+/* ggplvm.cu:1251 */
+void ref_lbfgs_update(void* h, int jtr, int rhoflag) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(dim3(1), dim3(1), [&] {
+    LBFGS(jtr, c->Q, c->Z, c->Omega, c->delta, c->K, c->Xi, c->Ta, c->rho, c->grad, c->grad0, c->SS, c->XX, c->ss,
+          c->Work, rhoflag);
+  });
+}
+
+/* ggplvm.cu:1289 */
+void ref_downdate(void* h, int jtr, double sr, int rhoflag) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(dim3(1), dim3(1), [&] {
+    Downdate(jtr, c->Q, c->Z, c->Omega, c->delta, c->K, c->Xi, c->Ta, c->rho, c->grad, c->grad0, c->SS, c->XX, c->ss,
+             sr, rhoflag);
+  });
+}
+
+/* ggplvm.cu:1324 */
+void ref_beta_from_tilde(void* h) {
+  RefCtx* c = (RefCtx*)h;
+  ref_launch(c->gridJ, dim3(1), [&] { getBetaFromTildeBeta(c->J, c->Z, c->tBeta, c->zeta, c->Beta); });
+}
+
+/* The outer fit loop of main (ggplvm.cu:1146-1330) with its schedule, stopping rules and
+ * line search, under explicit budgets: at most itr_max outer iterations and at most
+ * lbfgs_budget L-BFGS steps in total (<= 0: no budget). stats[0..3] receive outer
+ * iterations, total IRLS sweeps, total L-BFGS steps, total objective evaluations.
+ * Returns 0, or 1 where main would exit on a NaN IRLS likelihood. */
+int ref_fit(void* h, int itr_max, int lbfgs_budget, int* stats, double* lkhd_trace, int trace_cap) {
+  RefCtx* c = (RefCtx*)h;
+  int JTRMAX = 1000, itr, jtr, total_lbfgs = 0, total_irls = 0, total_evals = 0, ntrace = 0;
+  int rhoflag = 0;
+  int rc = 0;
+  bool budget_hit = false;
+  for (itr = 0; itr < itr_max && !budget_hit; itr++) {
+    JTRMAX = (itr == 0) ? 200 : 100;
+    int n = ref_irls(h, itr, JTRMAX);
+    if (n < 0) { rc = 1; itr++; break; }
+    total_irls += n;
+    double l0 = ref_objective_after_irls(h, itr);
+    total_evals++;
+    if (lkhd_trace && ntrace < trace_cap) lkhd_trace[ntrace++] = l0;
+    if (itr > 20) rhoflag = 1;
+    if (itr == 30) JTRMAX = 10000;
+    for (jtr = 0; jtr < JTRMAX; jtr++) {
+      ref_gradient(h, nullptr);
+      ref_lbfgs_update(h, jtr, rhoflag);
+      double sr = 1.0;
+      double* l = c->lkhd_h.data();
+      for (int ktr = 1; ktr < 8; ktr++) {
+        ref_objective(h, itr, jtr + 1);
+        total_evals++;
+        if (l[jtr + 1] > l[jtr] || ktr == 7) break;
+        else if (std::isnan(l[jtr + 1]) || std::isinf(l[jtr + 1])) sr *= 0.01;
+        else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
+        ref_downdate(h, jtr, sr, rhoflag);
+      }
+      total_lbfgs++;
+      if (lkhd_trace && ntrace < trace_cap) lkhd_trace[ntrace++] = l[jtr + 1];
+      if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
+      if (lbfgs_budget > 0 && total_lbfgs >= lbfgs_budget) { budget_hit = true; break; }
+    }
+    ref_expand_delta(h);
+    ref_beta_from_tilde(h);
+  }
+  c->rhoflag = rhoflag;
+  if (stats) { stats[0] = itr; stats[1] = total_irls; stats[2] = total_lbfgs; stats[3] = total_evals; }
+  return rc;
+}
+
+/* Copies a named buffer out (element counts follow main's allocations). Returns the
+ * number of doubles written, or -1 for an unknown name. */
+long ref_get(void* h, const char* name, double* out) {
+  RefCtx* c = (RefCtx*)h;
+  const size_t N = c->N, J = c->J, M = c->M, Q = c->Q, P = c->P, p = c->p;
+  struct Item { const char* n; const double* ptr; size_t len; };
+  DataFrame* Zd = c->Z;
+  const Item items[] = {
+      {"Omega", c->Omega, N},        {"delta", c->delta, p},         {"X", c->Xi, N * Q},
+      {"T", c->Ta, M * Q},           {"rho", c->rho, Q},             {"phi", c->phi, J},
+      {"Beta", c->Beta, P * J},      {"tBeta", c->tBeta, P * J},     {"Knm", Zd->Knm, N * M},
+      {"Kmm", c->K, M * M},          {"Kinv", c->Kinv, M * M},       {"KinvKmn", c->KinvKmn, N * M},
+      {"titsias", c->titsias, N},    {"W", c->W, N * (J + 1)},       {"Nu", c->Nu, N * J},
+      {"Psi", c->Psi, J * P * P},    {"PsiInv", c->Psi + J * P * P, J * P * P},
+      {"DeltaInv", c->DeltaInv, P * P}, {"lkhds", c->lkhds, J},     {"C1", c->C1, N * M},
+      {"C2", c->C2, M * M},          {"grad", c->grad, N + p + N * Q + M * Q + Q},
+      {"ss", c->ss, N + p + N * Q + M * Q + Q},
+      {"lkhd", c->lkhd_d, 50000},    {"zeta", c->zeta, P},
+  };
+  for (const Item& it : items) {
+    if (strcmp(it.n, name) == 0) {
+      if (out) memcpy(out, it.ptr, sizeof(double) * it.len);
+      return (long)it.len;
+    }
+  }
+  return -1;
+}
+
+/* Model-matrix column metadata from the reference loader (DataFrame.cu:88-149). */
+void ref_model_meta(void* h, int* nh_out, int* mc_out, int* mv_out, int* mk_out) {
+  RefCtx* c = (RefCtx*)h;
+  if (nh_out) memcpy(nh_out, c->Z_h->nh, sizeof(int) * (c->p + 1));
+  if (mc_out) memcpy(mc_out, c->Z_h->mc, sizeof(int) * c->P);
+  if (mv_out) memcpy(mv_out, c->Z_h->mv, sizeof(int) * c->P);
+  if (mk_out) memcpy(mk_out, c->Z_h->mk, sizeof(int) * c->P);
+}
+
+void ref_set_verbose(int v) { ref_verbose = v; }
+
+}  // extern "C"

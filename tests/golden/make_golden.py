@@ -1,0 +1,139 @@
+"""Generates the golden vectors in tests/golden/ from the reference's own kernels.
+
+The reference publishes no test vectors, so these fixtures are produced by running the
+reference source itself (compiled for the host by ``make -C oracle ref`` from the
+reference checkout) on small seeded inputs, phase by phase in the reference driver's
+order (ggplvm.cu:1101-1330). Each fixture stores its inputs too, so tests do not depend
+on the generator's random streams. Run from the repository root:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from gaspacho2_b200 import synth  # noqa: E402
+from gaspacho2_b200.formats import Counts  # noqa: E402
+from oracle import refcpu  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def edge_counts(ds):
+    """Adds the count-handling edge cases the reference's merge walk defines
+    (ggplvm.cu:505-511): an all-zero gene, a gene with every cell nonzero, a gene whose
+    entries go out of order (the walk stops at the first non-increasing index) and a
+    gene with a duplicated index."""
+    y = ds.y
+    N = y.N
+    genes_i = [y.i[y.p[j]:y.p[j + 1]] for j in range(y.J)]
+    genes_x = [y.x[y.p[j]:y.p[j + 1]] for j in range(y.J)]
+    genes_i[0] = np.zeros(0, np.int32)
+    genes_x[0] = np.zeros(0)
+    genes_i[1] = np.arange(N, dtype=np.int32)
+    genes_x[1] = (np.arange(N) % 5 + 1).astype(np.float64)
+    sizes = [g.shape[0] for g in genes_i]
+    swap_gene = next(j for j in range(2, y.J) if sizes[j] >= 6)
+    dup_gene = next(j for j in range(swap_gene + 1, y.J) if sizes[j] >= 4)
+    gi = genes_i[swap_gene].copy()
+    gi[3], gi[4] = gi[4], gi[3]
+    genes_i[swap_gene] = gi
+    gi = genes_i[dup_gene].copy()
+    gi[2] = gi[1]
+    genes_i[dup_gene] = gi
+    ds.edge_genes = (swap_gene, dup_gene)
+    p = np.zeros(y.J + 1, np.int64)
+    p[1:] = np.cumsum([g.shape[0] for g in genes_i])
+    ds.y = Counts(N, y.J, np.concatenate(genes_i).astype(np.int32), p.astype(np.int32), np.concatenate(genes_x))
+    return ds
+
+
+CASES = {
+    "c0_small": dict(config=0, seed=1, N=300, G=40, M=8, Q=2),
+    "c2_cats": dict(config=2, seed=2, N=400, G=30, M=10, Q=3),
+    "edges": dict(config=1, seed=3, N=250, G=24, M=6, Q=2),
+}
+
+
+def make_case(name: str, spec: dict) -> dict:
+    kw = dict(spec)
+    cfg = kw.pop("config")
+    seed = kw.pop("seed")
+    ds = synth.make(cfg, seed, **kw)
+    if name == "c2_cats":
+        # leave one donor level without cells (an all-zero column of the model matrix)
+        donor = ds.z.columns[-1]
+        donor[donor == 3] = 4
+    if name == "edges":
+        ds = edge_counts(ds)
+    m = refcpu.RefModel.from_dataset(ds)
+    extra = {"edge_genes": np.array(ds.edge_genes)} if name == "edges" else {}
+    out = {
+        "in_N": np.array(ds.y.N), "in_J": np.array(ds.y.J), "in_M": np.array(ds.M), "in_Q": np.array(ds.Q),
+        "in_y_i": ds.y.i, "in_y_p": ds.y.p, "in_y_x": ds.y.x, "in_z_c": ds.z.c, "in_z_v": ds.z.v,
+        "in_z_body": np.frombuffer(ds.z.body_bytes(), np.uint8), "in_ls": ds.ls, "in_X0": ds.X0,
+    }
+    for k, a in zip(("Omega", "delta", "X", "T", "rho", "phi"), ds.init.flat()):
+        out["in_init_" + k] = a
+    m.set_params(ds.init)
+    m.kernel_mats()
+    for k in ("Knm", "Kmm", "Kinv", "KinvKmn", "titsias"):
+        out["kmats_" + k] = m.get(k)
+    m.glm_init()
+    out["init_Beta"] = m.get("Beta")
+    out["sweep0_lkhd"] = np.array(m.irls_sweep(0, 0))
+    P = m.P
+    out["sweep0_Psi3"] = m.get("Psi")[:3 * P * P]
+    for k in ("Beta", "phi", "lkhds"):
+        out["sweep0_" + k] = m.get(k)
+    out["sweep0_W"] = m.get("W")[: m.N * m.J]
+    out["sweep0_Nu"] = m.get("Nu")
+    n = m.irls(0, 200)
+    out["irls_n"] = np.array(n)
+    out["irls_lkhd"] = m.get("lkhd")[:n]
+    for k in ("Beta", "phi"):
+        out["irls_" + k] = m.get(k)
+    out["obj0"] = np.array(m.objective_after_irls(0))
+    out["obj0_lkhds"] = m.get("lkhds")
+    out["grad0"] = m.gradient()
+    for k in ("tBeta", "C1", "C2"):
+        out["grad0_" + k] = m.get(k)
+    m.lbfgs_update(0, 0)
+    out["obj1"] = np.array(m.objective(0, 1))
+    for k in ("Omega", "delta", "X", "T", "rho"):
+        out["step1_" + k] = m.get(k)
+    out.update(extra)
+    m.close()
+    # an independent fit from the start with a budget of 12 L-BFGS steps
+    m = refcpu.RefModel.from_dataset(ds)
+    m.set_params(ds.init)
+    m.kernel_mats()
+    m.glm_init()
+    rc, st, tr = m.fit(1, 12)
+    out["fit_rc"] = np.array(rc)
+    out["fit_stats"] = np.array([st["outer"], st["irls"], st["lbfgs"], st["evals"]])
+    out["fit_trace"] = tr
+    for k in ("Omega", "delta", "X", "T", "rho", "phi", "Beta"):
+        out["fit_" + k] = m.get(k)
+    return out
+
+
+def main():
+    if not refcpu.available():
+        raise SystemExit("build the reference first: make -C oracle ref")
+    for name, spec in CASES.items():
+        out = make_case(name, spec)
+        path = os.path.join(OUT, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, irls sweeps {int(out['irls_n'])}, "
+              f"fit {out['fit_stats'].tolist()}")
+
+
+if __name__ == "__main__":
+    main()
