@@ -1,0 +1,371 @@
+"""Throughput benchmark: objective+gradient evaluations per second of the sparse GP-LVM fit.
+
+One step = one evaluation of the objective and its full gradient at fixed IRLS weights
+(kernel matrices, prior, per-gene Gram, batched Cholesky, likelihood, tilde-beta and every
+gradient block: d/dlog Omega, d/dlog delta, d/dX, d/dT, d/dlog rho), the unit that the
+reference's L-BFGS loop repeats (ggplvm.cu:1215-1277).
+
+Workload (default): 100,000 cells x 10,000 genes, M=128 inducing points, Q=10 latent
+dimensions, covariates of the 100-donor configuration (P=236 model columns), seeded
+synthetic counts. W and nu (8 GB each) exceed the 126 MB L2, so no flush is needed
+between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU (the fit does
+not shard across GPUs: one evaluation per rank, no collective on the data path); rank 0
+prints one JSON line with the whole-job rate and the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "obj+grad evals/s (100K cells x 10K genes, M=128, Q=10)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--N", type=int, default=None)
+    ap.add_argument("--G", type=int, default=None)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
+    ap.add_argument("--irls-sweeps", type=int, default=2)
+    ap.add_argument("--cpu-genes", type=int, default=6, help="genes in the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---- clocks ------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def fp64_peak_tflops(torch) -> float:
+    """Dense FP64 GEMM rate on this GPU (torch.matmul float64 8192^3, best of 5), the FP64
+    counterpart of the bf16 figure in MEASURED_PEAKS.json, which has no FP64 entry."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def flops_table(N, J, M, P, n_dense):
+    """Algorithmic flops per launch of the dominant kernels (2 flops per multiply-add)."""
+    return {
+        # Gram: unique upper-triangle entries of the dense GP block (N*G*M*(M+1) flops)
+        "gram": float(N) * J * M * (M + 1),
+        # gradient contraction over genes of S_j z_i, dense-model-matrix form: 2*N*J*P^2
+        "uq": 2.0 * N * J * P * P,
+    }
+
+
+# ---- CPU legs: bounded samples of the same workload --------------------------------------------
+class CpuSample:
+    """A bounded sample of the workload on the host cores: the first `genes` genes with all
+    cells, through the reference's own kernels built for the host (oracle/_ref, "reference")
+    or, where that build is absent, the oracle's restatement ("port"). One step is one
+    objective + gradient evaluation; its time is scaled to all genes (every per-gene and
+    per-cell-over-genes kernel is linear in the number of genes)."""
+
+    def __init__(self, ds, genes: int):
+        from gaspacho2_b200 import synth
+        from oracle import port, refcpu
+
+        sub = synth.gene_subset(ds, genes)
+        self.threads = os.cpu_count() or 1
+        if refcpu.available():
+            self.m = refcpu.RefModel.from_dataset(sub)
+            self.kind = "reference"
+        else:
+            port.set_threads(self.threads)
+            self.m = port.OracleModel.from_dataset(sub)
+            self.kind = "port"
+        m = self.m
+        m.set_params(sub.init)
+        m.kernel_mats()
+        m.glm_init()
+        m.irls_sweep(0, 0)
+        m.objective_after_irls(0)
+        self.scale = ds.J / float(genes)
+        self.slot = 1
+        self.desc = (f"{genes} of {ds.J} genes with all {ds.N} cells, one objective+gradient evaluation per step "
+                     f"on {self.threads} host threads, time scaled by {self.scale:.0f} to all genes")
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        self.m.gradient()
+        self.m.objective(0, self.slot)
+        self.slot += 1
+        return (time.perf_counter() - t0) * self.scale
+
+
+def dataset(args):
+    from gaspacho2_b200 import synth
+
+    kw = {}
+    if args.N:
+        kw["N"] = args.N
+    if args.G:
+        kw["G"] = args.G
+    return synth.make(args.config, 0, init=False, **kw)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ds = dataset(args)
+    cs = CpuSample(ds, args.cpu_genes)
+    per_eval = []
+    for i in range(args.warmup + args.steps):
+        t = cs.step()
+        if i >= args.warmup:
+            per_eval.append(t)
+    kind, threads, desc = cs.kind, cs.threads, cs.desc
+    t = statistics.mean(per_eval)
+    value = 1.0 / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(ds, args, "fp64"),
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(ds, args, precision):
+    p = ds.z.n_var + 2
+    M, Q = ds.M, ds.Q
+    P = 1 + int(sum(int(c) * int(v) for c, v in zip(ds.z.c, ds.z.v))) + M
+    return {"workload": f"config {args.config}: N={ds.N} cells, G={ds.J} genes, M={M}, Q={Q}, P={P}, p={p}",
+            "N": ds.N, "G": ds.J, "M": M, "Q": Q, "P": P, "precision": precision,
+            "l2": "inputs larger than L2 (W and nu are N*G doubles each)", "parallelism": f"replicas{args.gpus}",
+            "global_batch": ds.N, "seq_len": None}
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from gaspacho2_b200 import GPLVM
+
+    ds = dataset(args)
+    # a dedicated stream: the library runs every kernel on it and the CUDA events below are
+    # recorded on it (torch's default stream has handle 0, which the C ABI reads as "own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    m = GPLVM.from_dataset(ds, device=local, stream=stream.cuda_stream, precision=args.precision)
+    m.set_params(ds.init)
+    m.kernel_mats()
+    m.glm_init()
+    for j in range(args.irls_sweeps):
+        m.irls_sweep(0, j)
+    m.objective_after_irls(0)
+    for _ in range(args.warmup):
+        m.evaluate_device()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # device-resident throughput
+    m.profile(True)
+    m.profile_reset()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = m.launches()
+    barrier()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        m.evaluate_device()
+    e.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    dt = s.elapsed_time(e) / 1e3
+    launches = m.launches() - l0
+    ck = clocks.stop()
+    prof = {}
+    for name in ("gram", "uq", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
+                 "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
+                 "expand_delta", "chol_small"):
+        ms, n = m.profile_read(name)
+        if n:
+            prof[name] = (ms, n)
+    m.profile(False)
+    t_max = dt
+    if dist is not None:
+        tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * args.steps / t_max
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    n_par = m.n_params()
+    params = torch.empty(n_par, dtype=torch.float64, pin_memory=True).numpy()
+    params[:] = m.params_vector()
+    grad = torch.empty(n_par, dtype=torch.float64, pin_memory=True).numpy()
+    barrier()
+    torch.cuda.synchronize()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        m.evaluate(params, grad)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    dt2 = s2.elapsed_time(e2) / 1e3
+    if dist is not None:
+        tt = torch.tensor([dt2], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dt2 = float(tt.item())
+    e2e = {"value": world * args.steps / dt2, "unit": "evals/s", "h2d_bytes_per_step": int(params.nbytes),
+           "d2h_bytes_per_step": int(grad.nbytes + 8)}
+
+    line = None
+    if rank == 0:
+        total_prof = sum(v[0] for v in prof.values())
+        dom = max(prof, key=lambda k: prof[k][0])
+        P = m.P
+        ft = flops_table(m.N, m.J, m.M, P, 0)
+        peaks = measured_peaks()
+        if dom in ft:
+            f64 = fp64_peak_tflops(torch)
+            avg_s = prof[dom][0] / prof[dom][1] / 1e3
+            achieved = ft[dom] / avg_s / 1e12
+            roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": f64, "unit": "TFLOP/s",
+                    "frac": achieved / f64, "traffic": None,
+                    "peak_source": "measured in this run: torch.matmul float64 8192^3 best of 5 "
+                                   "(MEASURED_PEAKS.json has no FP64 entry)",
+                    "flops_per_launch": ft[dom], "avg_launch_ms": avg_s * 1e3,
+                    "share_of_step": prof[dom][0] / max(total_prof, 1e-30)}
+        else:
+            roof = {"kernel": dom, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
+                    "traffic": None}
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3+f64",
+            "data": "synthetic", "config": workload_config(ds, args, args.precision), "e2e": e2e,
+            "gpu_launches": int(launches), "roofline": roof, "clocks": ck,
+            "phase_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "hbm_gbs_measured": peaks.get("hbm_gbs"), "bf16_tflops_measured": peaks.get("bf16_tflops"),
+        }
+    m.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cs = CpuSample(ds, args.cpu_genes)
+        t = cs.step()
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "evals/s", "cores": cs.threads, "kind": cs.kind,
+                                "sample": cs.desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,833 @@
+// C ABI of libgpl_b200: context management, data loading and the phase drivers that follow
+// the reference driver's call order (ggplvm.cu:951-1354). See include/gpl.h.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+bool check(Ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+ProfScope::ProfScope(Ctx* c_, const char* n) : c(c_), name(n) {
+  if (!c->prof) return;
+  if (c->event_pool.size() < 2) {
+    for (int k = 0; k < 64; k++) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) == cudaSuccess) c->event_pool.push_back(e);
+    }
+  }
+  if (c->event_pool.size() < 2) return;
+  a = c->event_pool.back();
+  c->event_pool.pop_back();
+  b = c->event_pool.back();
+  c->event_pool.pop_back();
+  cudaEventRecord(a, c->stream);
+}
+
+ProfScope::~ProfScope() {
+  if (!a) return;
+  cudaEventRecord(b, c->stream);
+  c->prof_pending.push_back({name, a, b});
+  if (c->prof_pending.size() > 4096) {  // drain to bound the number of live events
+    cudaEventSynchronize(b);
+    for (auto& r : c->prof_pending) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      bool found = false;
+      for (auto& t : c->prof_total)
+        if (t.first == r.name) { t.second.first += ms; t.second.second++; found = true; break; }
+      if (!found) c->prof_total.push_back({r.name, {ms, 1}});
+      c->event_pool.push_back(r.a);
+      c->event_pool.push_back(r.b);
+    }
+    c->prof_pending.clear();
+  }
+}
+
+static void drain_profile(Ctx* c) {
+  if (c->prof_pending.empty()) return;
+  cudaEventSynchronize(c->prof_pending.back().b);
+  for (auto& r : c->prof_pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    bool found = false;
+    for (auto& t : c->prof_total)
+      if (t.first == r.name) { t.second.first += ms; t.second.second++; found = true; break; }
+    if (!found) c->prof_total.push_back({r.name, {ms, 1}});
+    c->event_pool.push_back(r.a);
+    c->event_pool.push_back(r.b);
+  }
+  c->prof_pending.clear();
+}
+
+template <class T>
+static int dalloc(Ctx* c, T** p, size_t n, const char* what) {
+  if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = std::string("device allocation failed: ") + what + " (" + std::to_string(sizeof(T) * n) + " bytes)";
+    return GPL_ERR_ALLOC;
+  }
+  return GPL_OK;
+}
+
+static void free_state(Ctx* c) {
+  void* bufs[] = {c->Z,      c->W,      c->Nu,      c->Psi,     c->PsiInv, c->Beta,   c->tBeta,  c->scratch,
+                  c->U,      c->Kmm,    c->Kinv,    c->KinvKmn, c->titsias, c->DeltaInv, c->Omega, c->delta,
+                  c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
+                  c->grad0,  c->ss,     c->SS,      c->XX,      c->gdtmp,  c->C1,     c->C2,     c->grtmp,
+                  c->KmmInv, c->bvec,   c->sol,     c->red,     c->lb_work, c->mc_d,  c->mv_d,   c->mk_d,
+                  c->nh_d};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  c->Z = c->W = c->Nu = c->Psi = c->PsiInv = c->Beta = c->tBeta = c->scratch = c->U = nullptr;
+  c->Kmm = c->Kinv = c->KinvKmn = c->titsias = c->DeltaInv = c->Omega = c->delta = c->X = c->T = nullptr;
+  c->rho = c->phi = c->ls = c->lkhds = c->lkhd_dev = c->grad = c->grad0 = c->ss = c->SS = c->XX = nullptr;
+  c->gdtmp = c->C1 = c->C2 = c->grtmp = c->KmmInv = c->bvec = c->sol = c->red = c->lb_work = nullptr;
+  c->mc_d = c->mv_d = c->mk_d = c->nh_d = nullptr;
+  c->have_design = false;
+}
+
+static void free_counts(Ctx* c) {
+  if (c->cell) cudaFree(c->cell);
+  if (c->gptr) cudaFree(c->gptr);
+  if (c->gvalid) cudaFree(c->gvalid);
+  if (c->cnt) cudaFree(c->cnt);
+  c->cell = nullptr;
+  c->gptr = nullptr;
+  c->gvalid = nullptr;
+  c->cnt = nullptr;
+  c->have_counts = false;
+}
+
+static int need_state(Ctx* c) {
+  if (!c->have_counts || !c->have_design) {
+    c->err = "counts and design must be loaded first";
+    return GPL_ERR_STATE;
+  }
+  return GPL_OK;
+}
+
+#define GPL_RUN(expr)          \
+  do {                         \
+    int rc_ = (expr);          \
+    if (rc_ != GPL_OK) return rc_; \
+  } while (0)
+
+static int read_slot(Ctx* c, int slot, double* out) {
+  double v = 0.0;
+  GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + slot, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  c->lkhd[slot] = v;
+  if (out) *out = v;
+  return GPL_OK;
+}
+
+// ---- phases -------------------------------------------------------------------------------
+static int irls_sweep(Ctx* c, int jtr, double* lk) {
+  GPL_RUN(launch_w_nu(c));
+  GPL_RUN(launch_gram(c, false));
+  GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, (int64_t)c->P * c->P));
+  GPL_RUN(launch_zt_u(c, 0));
+  GPL_RUN(launch_beta_phi(c, jtr));
+  GPL_RUN(launch_lkhd_pois(c));
+  GPL_RUN(launch_collect_lkhd(c, 0, jtr));
+  return read_slot(c, jtr, lk);
+}
+
+static int irls(Ctx* c, int jtr_max, int* n_sweeps) {
+  int jtr;
+  for (jtr = 0; jtr < jtr_max; jtr++) {
+    GPL_RUN(irls_sweep(c, jtr, nullptr));
+    if (jtr > 0) {
+      const double a = c->lkhd[jtr - 1], b = c->lkhd[jtr];
+      if (isnan(b)) {
+        if (n_sweeps) *n_sweeps = jtr + 1;
+        c->err = "IRLS likelihood is NaN";
+        return GPL_ERR_NAN;
+      }
+      if (jtr == jtr_max - 1 || fabs(a - b) / fabs(b) < 1e-7) {
+        jtr++;
+        break;
+      }
+    }
+  }
+  if (n_sweeps) *n_sweeps = jtr;
+  return GPL_OK;
+}
+
+static int objective_after_irls(Ctx* c, double* lk) {
+  GPL_RUN(launch_oinvt(c));
+  GPL_RUN(launch_chol_single(c, c->DeltaInv, c->P));
+  GPL_RUN(launch_zt_u(c, 0));
+  GPL_RUN(launch_lkhd_genes(c));
+  GPL_RUN(launch_collect_lkhd(c, c->N, 0));
+  return read_slot(c, 0, lk);
+}
+
+static int objective_launch(Ctx* c, int slot) {
+  GPL_RUN(launch_oinvt(c));
+  GPL_RUN(launch_kernel_mats(c));
+  GPL_RUN(launch_expand_delta(c));
+  GPL_RUN(launch_gram(c, false));
+  GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, (int64_t)c->P * c->P));
+  GPL_RUN(launch_chol_single(c, c->DeltaInv, c->P));
+  GPL_RUN(launch_zt_u(c, 0));
+  GPL_RUN(launch_lkhd_genes(c));
+  GPL_RUN(launch_collect_lkhd(c, c->N, slot));
+  return GPL_OK;
+}
+
+static int gradient_launch(Ctx* c) {
+  GPL_RUN(launch_expand_delta(c));
+  GPL_RUN(launch_oinvt(c));
+  GPL_RUN(launch_zt_u(c, 0));
+  GPL_RUN(launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->tBeta, c->P, c->J));
+  GPL_RUN(launch_inverse_batched(c));
+  GPL_RUN(launch_grad_delta(c));
+  GPL_RUN(launch_grad_omega(c));
+  GPL_RUN(launch_c2(c));
+  GPL_RUN(launch_grad_tau_rho(c));
+  return GPL_OK;
+}
+
+static int glm_init(Ctx* c) {
+  GPL_RUN(launch_expand_delta(c));
+  GPL_RUN(launch_gram(c, true));
+  GPL_RUN(launch_chol_single(c, c->Psi, c->P));
+  GPL_RUN(launch_init_response(c));
+  GPL_RUN(launch_zt_u(c, 1));
+  GPL_RUN(launch_init_beta_solve(c));
+  return GPL_OK;
+}
+
+}  // namespace gpl
+
+using namespace gpl;
+
+static Ctx* C(gpl_ctx* h) { return &h->c; }
+
+extern "C" {
+
+int gpl_create(gpl_ctx** out, int device, void* stream) {
+  if (!out) return GPL_ERR_ARG;
+  *out = nullptr;
+  gpl_ctx* h = new (std::nothrow) gpl_ctx();
+  if (!h) return GPL_ERR_ALLOC;
+  Ctx* c = C(h);
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return GPL_ERR_CUDA;
+  }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return GPL_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  c->lkhd.assign(kLkhdSlots, 0.0);
+  *out = h;
+  return GPL_OK;
+}
+
+int gpl_destroy(gpl_ctx* h) {
+  if (!h) return GPL_OK;
+  Ctx* c = C(h);
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drain_profile(c);
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  free_state(c);
+  free_counts(c);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete h;
+  return GPL_OK;
+}
+
+const char* gpl_last_error(const gpl_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
+
+int gpl_set_precision(gpl_ctx* h, int precision) {
+  Ctx* c = C(h);
+  if (precision != GPL_PREC_FP64 && precision != GPL_PREC_BF16X3) {
+    c->err = "unknown precision";
+    return GPL_ERR_ARG;
+  }
+  c->precision = precision;
+  return GPL_OK;
+}
+
+int gpl_load_counts(gpl_ctx* h, int N, int J, int64_t nnz, const int32_t* cell_idx, const int32_t* gene_ptr,
+                    const double* counts) {
+  Ctx* c = C(h);
+  cudaSetDevice(c->device);
+  if (N <= 0 || J <= 0 || nnz < 0 || !gene_ptr || (nnz > 0 && (!cell_idx || !counts))) {
+    c->err = "bad counts arguments";
+    return GPL_ERR_ARG;
+  }
+  if (c->have_design && (N != c->N || J != c->J)) {
+    c->err = "counts sizes differ from the loaded design";
+    return GPL_ERR_ARG;
+  }
+  std::vector<int64_t> gp(J + 1);
+  std::vector<int32_t> gv(J);
+  for (int j = 0; j <= J; j++) gp[j] = gene_ptr[j];
+  for (int j = 0; j < J; j++) {
+    if (gp[j] < 0 || gp[j] > gp[j + 1] || gp[j + 1] > nnz) {
+      c->err = "gene offsets are not monotone within [0, nnz]";
+      return GPL_ERR_FORMAT;
+    }
+    // entries the reference's merge walk consumes (ggplvm.cu:505-511)
+    int last = -1;
+    int64_t l = gp[j];
+    for (; l < gp[j + 1]; l++) {
+      const int i = cell_idx[l];
+      if (i <= last || i >= N) break;
+      last = i;
+    }
+    gv[j] = (int32_t)(l - gp[j]);
+  }
+  free_counts(c);
+  GPL_RUN(dalloc(c, &c->cell, (size_t)nnz, "cells"));
+  GPL_RUN(dalloc(c, &c->gptr, (size_t)J + 1, "gene offsets"));
+  GPL_RUN(dalloc(c, &c->gvalid, (size_t)J, "gene valid lengths"));
+  GPL_RUN(dalloc(c, &c->cnt, (size_t)nnz, "counts"));
+  if (nnz) {
+    GPL_TRY(c, cudaMemcpy(c->cell, cell_idx, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->cnt, counts, sizeof(double) * nnz, cudaMemcpyHostToDevice));
+  }
+  GPL_TRY(c, cudaMemcpy(c->gptr, gp.data(), sizeof(int64_t) * (J + 1), cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->gvalid, gv.data(), sizeof(int32_t) * J, cudaMemcpyHostToDevice));
+  c->N = N;
+  c->J = J;
+  c->nnz = nnz;
+  c->have_counts = true;
+  return GPL_OK;
+}
+
+int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32_t* vv, const void* body,
+                    int64_t body_bytes, int M, int Q) {
+  Ctx* c = C(h);
+  cudaSetDevice(c->device);
+  if (!c->have_counts) {
+    c->err = "load the counts first";
+    return GPL_ERR_STATE;
+  }
+  if (N != c->N || n_var < 0 || M <= 0 || Q <= 0 || (n_var > 0 && (!cv || !vv))) {
+    c->err = "bad design arguments";
+    return GPL_ERR_ARG;
+  }
+  const int p = n_var + 2;
+  std::vector<int> vc(p), vvv(p), nh(p + 1, 0);
+  vc[0] = 1;
+  vvv[0] = 1;
+  for (int k = 0; k < n_var; k++) {
+    if (cv[k] < 1 || vv[k] < 1) {
+      c->err = "level counts and widths must be >= 1";
+      return GPL_ERR_FORMAT;
+    }
+    vc[k + 1] = cv[k];
+    vvv[k + 1] = vv[k];
+  }
+  vc[p - 1] = 1;
+  vvv[p - 1] = M;
+  int64_t need = 0;
+  for (int k = 0; k < n_var; k++) need += (int64_t)N * vv[k] * (cv[k] == 1 ? 8 : 4);
+  if (need != body_bytes || (need > 0 && !body)) {
+    c->err = "design body size does not match N, c and v";
+    return GPL_ERR_FORMAT;
+  }
+  for (int j = 0; j < p; j++) nh[j + 1] = nh[j] + vvv[j] * vc[j];
+  const int P = nh[p];
+  std::vector<int> mc(P), mv(P), mk(P);
+  for (int j = 0; j < p; j++)
+    for (int k = nh[j]; k < nh[j + 1]; k++) {
+      mc[k] = vc[j];
+      mv[k] = k - nh[j];
+      mk[k] = j;
+    }
+  free_state(c);
+  c->M = M;
+  c->Q = Q;
+  c->p = p;
+  c->P = P;
+  c->n_var = n_var;
+  c->vc = vc;
+  c->vv = vvv;
+  c->nh = nh;
+  c->mc = mc;
+  c->mv = mv;
+  c->mk = mk;
+  c->ldN = (N + 31) / 32 * 32;
+  const int J = c->J;
+  const size_t ldN = c->ldN;
+  // model matrix on the host: intercept, file variables, GP block left for getKernelMats
+  std::vector<double> Zh(ldN * P, 0.0);
+  for (int i = 0; i < N; i++) Zh[i] = 1.0;
+  const char* bp = (const char*)body;
+  int64_t off = 0;
+  for (int j = 1; j < p - 1; j++) {
+    const int64_t bytes = (int64_t)N * vvv[j] * (vc[j] == 1 ? 8 : 4);
+    if (vc[j] == 1) {
+      for (int m = 0; m < vvv[j]; m++) {
+        double* dst = &Zh[(size_t)(nh[j] + m) * ldN];
+        memcpy(dst, bp + off + (int64_t)m * N * 8, sizeof(double) * N);
+      }
+    } else {
+      std::vector<int32_t> codes(N);
+      memcpy(codes.data(), bp + off, sizeof(int32_t) * N);
+      const int ncol = vc[j] * vvv[j];
+      for (int i = 0; i < N; i++) {
+        if (codes[i] < 0 || codes[i] >= ncol) {
+          c->err = "categorical level code out of range in variable " + std::to_string(j);
+          return GPL_ERR_FORMAT;
+        }
+        Zh[(size_t)(nh[j] + codes[i]) * ldN + i] = 1.0;
+      }
+    }
+    off += bytes;
+  }
+  c->tot_max = tot_len(c, 1);
+  const size_t scratch_n = std::max({ldN * (size_t)J, (size_t)J * P * P, (size_t)c->tot_max, (size_t)M * M});
+  GPL_RUN(dalloc(c, &c->Z, ldN * P, "Z"));
+  GPL_RUN(dalloc(c, &c->W, ldN * (J + 1), "W"));
+  GPL_RUN(dalloc(c, &c->Nu, ldN * J, "Nu"));
+  GPL_RUN(dalloc(c, &c->Psi, (size_t)J * P * P, "Psi"));
+  GPL_RUN(dalloc(c, &c->PsiInv, (size_t)J * P * P, "PsiInv"));
+  GPL_RUN(dalloc(c, &c->Beta, (size_t)P * J, "Beta"));
+  GPL_RUN(dalloc(c, &c->tBeta, (size_t)P * J, "tBeta"));
+  GPL_RUN(dalloc(c, &c->bvec, (size_t)P * J, "bvec"));
+  GPL_RUN(dalloc(c, &c->sol, (size_t)P * J, "sol"));
+  GPL_RUN(dalloc(c, &c->scratch, scratch_n, "scratch"));
+  GPL_RUN(dalloc(c, &c->U, ldN * P, "U"));
+  GPL_RUN(dalloc(c, &c->Kmm, (size_t)M * M, "Kmm"));
+  GPL_RUN(dalloc(c, &c->Kinv, (size_t)M * M, "Kinv"));
+  GPL_RUN(dalloc(c, &c->KmmInv, (size_t)M * M, "KmmInv"));
+  GPL_RUN(dalloc(c, &c->KinvKmn, ldN * M, "KinvKmn"));
+  GPL_RUN(dalloc(c, &c->titsias, ldN, "titsias"));
+  GPL_RUN(dalloc(c, &c->DeltaInv, (size_t)P * P, "DeltaInv"));
+  GPL_RUN(dalloc(c, &c->Omega, 2 * (size_t)N, "Omega"));
+  GPL_RUN(dalloc(c, &c->delta, 2 * (size_t)p, "delta"));
+  GPL_RUN(dalloc(c, &c->X, 2 * (size_t)N * Q, "X"));
+  GPL_RUN(dalloc(c, &c->T, 2 * (size_t)M * Q, "T"));
+  GPL_RUN(dalloc(c, &c->rho, 2 * (size_t)Q, "rho"));
+  GPL_RUN(dalloc(c, &c->phi, (size_t)J, "phi"));
+  GPL_RUN(dalloc(c, &c->ls, (size_t)N, "ls"));
+  GPL_RUN(dalloc(c, &c->lkhds, (size_t)J, "lkhds"));
+  GPL_RUN(dalloc(c, &c->lkhd_dev, (size_t)kLkhdSlots, "lkhd"));
+  GPL_RUN(dalloc(c, &c->grad, (size_t)c->tot_max + Q, "grad"));
+  GPL_RUN(dalloc(c, &c->grad0, (size_t)c->tot_max + Q, "grad0"));
+  GPL_RUN(dalloc(c, &c->ss, (size_t)c->tot_max + Q, "ss"));
+  GPL_RUN(dalloc(c, &c->SS, (size_t)c->tot_max * kHist, "SS"));
+  GPL_RUN(dalloc(c, &c->XX, (size_t)c->tot_max * kHist, "XX"));
+  GPL_RUN(dalloc(c, &c->gdtmp, (size_t)P * J, "gdtmp"));
+  GPL_RUN(dalloc(c, &c->C1, ldN * M, "C1"));
+  GPL_RUN(dalloc(c, &c->C2, (size_t)M * M, "C2"));
+  GPL_RUN(dalloc(c, &c->grtmp, (size_t)M * Q, "grtmp"));
+  GPL_RUN(dalloc(c, &c->red, std::max((size_t)ldN, (size_t)4096), "reduction"));
+  GPL_RUN(dalloc(c, &c->lb_work, 64, "lbfgs scalars"));
+  GPL_RUN(dalloc(c, &c->mc_d, (size_t)P, "mc"));
+  GPL_RUN(dalloc(c, &c->mv_d, (size_t)P, "mv"));
+  GPL_RUN(dalloc(c, &c->mk_d, (size_t)P, "mk"));
+  GPL_RUN(dalloc(c, &c->nh_d, (size_t)p + 1, "nh"));
+  GPL_TRY(c, cudaMemcpy(c->Z, Zh.data(), sizeof(double) * ldN * P, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->mc_d, mc.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->mv_d, mv.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->mk_d, mk.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->nh_d, nh.data(), sizeof(int) * (p + 1), cudaMemcpyHostToDevice));
+  // freshly allocated reference buffers read as zero (the harness' calloc convention)
+  GPL_TRY(c, cudaMemset(c->W, 0, sizeof(double) * ldN * (J + 1)));
+  GPL_TRY(c, cudaMemset(c->Nu, 0, sizeof(double) * ldN * J));
+  GPL_TRY(c, cudaMemset(c->Psi, 0, sizeof(double) * (size_t)J * P * P));
+  GPL_TRY(c, cudaMemset(c->PsiInv, 0, sizeof(double) * (size_t)J * P * P));
+  GPL_TRY(c, cudaMemset(c->Beta, 0, sizeof(double) * (size_t)P * J));
+  GPL_TRY(c, cudaMemset(c->tBeta, 0, sizeof(double) * (size_t)P * J));
+  GPL_TRY(c, cudaMemset(c->ss, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
+  GPL_TRY(c, cudaMemset(c->grad, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
+  GPL_TRY(c, cudaMemset(c->grad0, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
+  GPL_TRY(c, cudaMemset(c->SS, 0, sizeof(double) * (size_t)c->tot_max * kHist));
+  GPL_TRY(c, cudaMemset(c->XX, 0, sizeof(double) * (size_t)c->tot_max * kHist));
+  GPL_TRY(c, cudaMemset(c->titsias, 0, sizeof(double) * ldN));
+  GPL_TRY(c, cudaMemset(c->X, 0, sizeof(double) * 2 * (size_t)N * Q));
+  GPL_TRY(c, cudaMemset(c->T, 0, sizeof(double) * 2 * (size_t)M * Q));
+  GPL_TRY(c, cudaMemset(c->lkhd_dev, 0, sizeof(double) * kLkhdSlots));
+  c->have_design = true;
+  std::vector<double> ones(N, 1.0);
+  GPL_TRY(c, cudaMemcpy(c->ls, ones.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  return gpl_init_params(h);
+}
+
+int gpl_set_size_factors(gpl_ctx* h, const double* ls) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (!ls) return GPL_ERR_ARG;
+  GPL_TRY(c, cudaMemcpy(c->ls, ls, sizeof(double) * c->N, cudaMemcpyHostToDevice));
+  return GPL_OK;
+}
+
+int gpl_dims(const gpl_ctx* h, int32_t* d) {
+  const Ctx* c = &h->c;
+  if (!d) return GPL_ERR_ARG;
+  d[0] = c->N; d[1] = c->J; d[2] = c->M; d[3] = c->P; d[4] = c->p; d[5] = c->Q;
+  return GPL_OK;
+}
+
+int gpl_init_params(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  std::vector<double> delta(c->p, 0.01), rho(c->Q, 10.0), Om(c->N, 1.0), phi(c->J, 1.0), T0(c->M);
+  delta[0] = 1.5;
+  delta[c->p - 1] = 0.3;
+  rho[0] = 5.0;
+  for (int i = 0; i < c->M; i++) T0[i] = ((double)(i + 1) / (double)(c->M + 1)) * 2.0 * 3.14159265358979;
+  GPL_TRY(c, cudaMemcpy(c->delta, delta.data(), sizeof(double) * c->p, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->rho, rho.data(), sizeof(double) * c->Q, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->Omega, Om.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->phi, phi.data(), sizeof(double) * c->J, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->T, T0.data(), sizeof(double) * c->M, cudaMemcpyHostToDevice));
+  return GPL_OK;
+}
+
+int gpl_set_params(gpl_ctx* h, const double* Omega, const double* delta, const double* X, const double* T,
+                   const double* rho, const double* phi) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  cudaSetDevice(c->device);
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  if (Omega) GPL_TRY(c, cudaMemcpy(c->Omega, Omega, sizeof(double) * c->N, cudaMemcpyHostToDevice));
+  if (delta) GPL_TRY(c, cudaMemcpy(c->delta, delta, sizeof(double) * c->p, cudaMemcpyHostToDevice));
+  if (X) GPL_TRY(c, cudaMemcpy(c->X, X, sizeof(double) * (size_t)c->N * c->Q, cudaMemcpyHostToDevice));
+  if (T) GPL_TRY(c, cudaMemcpy(c->T, T, sizeof(double) * (size_t)c->M * c->Q, cudaMemcpyHostToDevice));
+  if (rho) GPL_TRY(c, cudaMemcpy(c->rho, rho, sizeof(double) * c->Q, cudaMemcpyHostToDevice));
+  if (phi) GPL_TRY(c, cudaMemcpy(c->phi, phi, sizeof(double) * c->J, cudaMemcpyHostToDevice));
+  return GPL_OK;
+}
+
+int gpl_get_params(gpl_ctx* h, double* Omega, double* delta, double* X, double* T, double* rho, double* phi) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  if (Omega) GPL_TRY(c, cudaMemcpy(Omega, c->Omega, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  if (delta) GPL_TRY(c, cudaMemcpy(delta, c->delta, sizeof(double) * c->p, cudaMemcpyDeviceToHost));
+  if (X) GPL_TRY(c, cudaMemcpy(X, c->X, sizeof(double) * (size_t)c->N * c->Q, cudaMemcpyDeviceToHost));
+  if (T) GPL_TRY(c, cudaMemcpy(T, c->T, sizeof(double) * (size_t)c->M * c->Q, cudaMemcpyDeviceToHost));
+  if (rho) GPL_TRY(c, cudaMemcpy(rho, c->rho, sizeof(double) * c->Q, cudaMemcpyDeviceToHost));
+  if (phi) GPL_TRY(c, cudaMemcpy(phi, c->phi, sizeof(double) * c->J, cudaMemcpyDeviceToHost));
+  return GPL_OK;
+}
+
+int gpl_set_beta(gpl_ctx* h, const double* beta) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  GPL_TRY(c, cudaMemcpy(c->Beta, beta, sizeof(double) * (size_t)c->P * c->J, cudaMemcpyHostToDevice));
+  return GPL_OK;
+}
+
+int gpl_get_beta(gpl_ctx* h, double* beta) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  GPL_TRY(c, cudaMemcpy(beta, c->Beta, sizeof(double) * (size_t)c->P * c->J, cudaMemcpyDeviceToHost));
+  return GPL_OK;
+}
+
+int gpl_kernel_mats(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_RUN(launch_kernel_mats(c));
+  return GPL_OK;
+}
+
+int gpl_glm_init(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_RUN(glm_init(c));
+  return GPL_OK;
+}
+
+int gpl_expand_delta(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  return launch_expand_delta(c);
+}
+
+int gpl_irls_sweep(gpl_ctx* h, int jtr, double* lkhd) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (jtr < 0 || jtr >= kLkhdSlots) return GPL_ERR_ARG;
+  return irls_sweep(c, jtr, lkhd);
+}
+
+int gpl_irls(gpl_ctx* h, int jtr_max, int* n_sweeps) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (jtr_max < 1 || jtr_max >= kLkhdSlots) return GPL_ERR_ARG;
+  return irls(c, jtr_max, n_sweeps);
+}
+
+int gpl_objective_after_irls(gpl_ctx* h, double* lkhd) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  return objective_after_irls(c, lkhd);
+}
+
+int gpl_objective(gpl_ctx* h, int slot, double* lkhd) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (slot < 0 || slot >= kLkhdSlots) return GPL_ERR_ARG;
+  GPL_RUN(objective_launch(c, slot));
+  return read_slot(c, slot, lkhd);
+}
+
+int gpl_gradient(gpl_ctx* h, double* grad) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_RUN(gradient_launch(c));
+  if (grad) {
+    const int64_t n = tot_len(c, 0) + c->Q;
+    GPL_TRY(c, cudaMemcpyAsync(grad, c->grad, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  return GPL_OK;
+}
+
+int gpl_lbfgs_update(gpl_ctx* h, int jtr, int rhoflag) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  return launch_lbfgs_update(c, jtr, rhoflag ? 1 : 0);
+}
+
+int gpl_downdate(gpl_ctx* h, int jtr, double sr, int rhoflag) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  return launch_downdate(c, jtr, sr, rhoflag ? 1 : 0);
+}
+
+int gpl_beta_from_tilde(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  return launch_beta_from_tilde(c);
+}
+
+int gpl_fit(gpl_ctx* h, int itr_max, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  int itr, rhoflag = 0, total_lbfgs = 0, total_irls = 0, total_evals = 0, ntrace = 0, rc = GPL_OK;
+  bool budget_hit = false;
+  for (itr = 0; itr < itr_max && !budget_hit; itr++) {
+    int JTRMAX = (itr == 0) ? 200 : 100;
+    int n = 0;
+    rc = irls(c, JTRMAX, &n);
+    total_irls += n;
+    if (rc == GPL_ERR_NAN) {
+      itr++;
+      break;
+    }
+    if (rc) return rc;
+    double l0 = 0.0;
+    GPL_RUN(objective_after_irls(c, &l0));
+    total_evals++;
+    if (trace && ntrace < trace_cap) trace[ntrace++] = l0;
+    if (itr > 20) rhoflag = 1;
+    if (itr == 30) JTRMAX = 10000;
+    for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
+      GPL_RUN(gradient_launch(c));
+      GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
+      double sr = 1.0;
+      std::vector<double>& l = c->lkhd;
+      for (int ktr = 1; ktr < 8; ktr++) {
+        GPL_RUN(objective_launch(c, jtr + 1));
+        GPL_RUN(read_slot(c, jtr + 1, nullptr));
+        total_evals++;
+        if (l[jtr + 1] > l[jtr] || ktr == 7) break;
+        else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
+        else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
+        GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
+      }
+      total_lbfgs++;
+      if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
+      if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
+      if (lbfgs_budget > 0 && total_lbfgs >= lbfgs_budget) {
+        budget_hit = true;
+        break;
+      }
+    }
+    GPL_RUN(launch_expand_delta(c));
+    GPL_RUN(launch_beta_from_tilde(c));
+  }
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  if (stats) {
+    stats[0] = itr;
+    stats[1] = total_irls;
+    stats[2] = total_lbfgs;
+    stats[3] = total_evals;
+  }
+  return rc == GPL_ERR_NAN ? GPL_ERR_NAN : GPL_OK;
+}
+
+int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkhd, double* grad) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  const int64_t n = tot_len(c, 0) + c->Q;
+  if (!params || n_params != n) {
+    c->err = "params must hold N + p + N*Q + M*Q + Q values";
+    return GPL_ERR_ARG;
+  }
+  const double* p = params;
+  GPL_TRY(c, cudaMemcpyAsync(c->Omega, p, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+  p += c->N;
+  GPL_TRY(c, cudaMemcpyAsync(c->delta, p, sizeof(double) * c->p, cudaMemcpyHostToDevice, c->stream));
+  p += c->p;
+  GPL_TRY(c, cudaMemcpyAsync(c->X, p, sizeof(double) * (size_t)c->N * c->Q, cudaMemcpyHostToDevice, c->stream));
+  p += (size_t)c->N * c->Q;
+  GPL_TRY(c, cudaMemcpyAsync(c->T, p, sizeof(double) * (size_t)c->M * c->Q, cudaMemcpyHostToDevice, c->stream));
+  p += (size_t)c->M * c->Q;
+  GPL_TRY(c, cudaMemcpyAsync(c->rho, p, sizeof(double) * c->Q, cudaMemcpyHostToDevice, c->stream));
+  GPL_RUN(objective_launch(c, 1));
+  GPL_RUN(gradient_launch(c));
+  if (grad) GPL_TRY(c, cudaMemcpyAsync(grad, c->grad, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  double v = 0.0;
+  GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  c->lkhd[1] = v;
+  if (lkhd) *lkhd = v;
+  return GPL_OK;
+}
+
+int gpl_evaluate_device(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_RUN(objective_launch(c, 1));
+  GPL_RUN(gradient_launch(c));
+  return GPL_OK;
+}
+
+int gpl_get(gpl_ctx* h, const char* name, double* out, int64_t cap, int64_t* len) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (!name) return GPL_ERR_ARG;
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  const size_t N = c->N, J = c->J, M = c->M, Q = c->Q, P = c->P, p = c->p, ldN = c->ldN;
+  const int g0 = c->nh[c->p - 1];
+  std::string s(name);
+  auto plain = [&](const double* src, size_t n) -> int {
+    if (len) *len = (int64_t)n;
+    if (!out) return GPL_OK;
+    if ((int64_t)n > cap) { c->err = "output buffer too small"; return GPL_ERR_ARG; }
+    GPL_TRY(c, cudaMemcpy(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return GPL_OK;
+  };
+  // cell-fastest matrices with a padded leading dimension: copy column by column
+  auto cols = [&](const double* src, size_t ncol) -> int {
+    const size_t n = N * ncol;
+    if (len) *len = (int64_t)n;
+    if (!out) return GPL_OK;
+    if ((int64_t)n > cap) { c->err = "output buffer too small"; return GPL_ERR_ARG; }
+    GPL_TRY(c, cudaMemcpy2D(out, N * sizeof(double), src, ldN * sizeof(double), N * sizeof(double), ncol,
+                            cudaMemcpyDeviceToHost));
+    return GPL_OK;
+  };
+  if (s == "Omega") return plain(c->Omega, N);
+  if (s == "delta") return plain(c->delta, p);
+  if (s == "X") return plain(c->X, N * Q);
+  if (s == "T") return plain(c->T, M * Q);
+  if (s == "rho") return plain(c->rho, Q);
+  if (s == "phi") return plain(c->phi, J);
+  if (s == "Beta") return plain(c->Beta, P * J);
+  if (s == "tBeta") return plain(c->tBeta, P * J);
+  if (s == "Kmm") return plain(c->Kmm, M * M);
+  if (s == "Kinv") return plain(c->Kinv, M * M);
+  if (s == "titsias") return plain(c->titsias, N);
+  if (s == "Psi") return plain(c->Psi, J * P * P);
+  if (s == "PsiInv") return plain(c->PsiInv, J * P * P);
+  if (s == "DeltaInv") return plain(c->DeltaInv, P * P);
+  if (s == "lkhds") return plain(c->lkhds, J);
+  if (s == "C2") return plain(c->C2, M * M);
+  if (s == "grad") return plain(c->grad, N + p + N * Q + M * Q + Q);
+  if (s == "ss") return plain(c->ss, N + p + N * Q + M * Q + Q);
+  if (s == "zeta") {
+    if (len) *len = (int64_t)P;
+    if (out) memset(out, 0, sizeof(double) * P);
+    return GPL_OK;
+  }
+  if (s == "lkhd_dev") return plain(c->lkhd_dev, 2);
+  if (s == "lkhd") {
+    if (len) *len = kLkhdSlots;
+    if (out) {
+      if (cap < kLkhdSlots) return GPL_ERR_ARG;
+      memcpy(out, c->lkhd.data(), sizeof(double) * kLkhdSlots);
+    }
+    return GPL_OK;
+  }
+  if (s == "Knm") return cols(c->Z + (size_t)g0 * ldN, M);
+  if (s == "W") return cols(c->W, J + 1);
+  if (s == "Nu") return cols(c->Nu, J);
+  if (s == "C1") return cols(c->C1, M);
+  if (s == "Z") return cols(c->Z, P);
+  if (s == "KinvKmn") {  // reference layout M x N (k + i*M)
+    if (len) *len = (int64_t)(M * N);
+    if (!out) return GPL_OK;
+    if ((int64_t)(M * N) > cap) return GPL_ERR_ARG;
+    std::vector<double> tmp(N * M);
+    GPL_TRY(c, cudaMemcpy2D(tmp.data(), N * sizeof(double), c->KinvKmn, ldN * sizeof(double), N * sizeof(double), M,
+                            cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < N; i++)
+      for (size_t k = 0; k < M; k++) out[k + i * M] = tmp[i + k * N];
+    return GPL_OK;
+  }
+  c->err = "unknown buffer name: " + s;
+  return GPL_ERR_ARG;
+}
+
+int gpl_profile_enable(gpl_ctx* h, int on) {
+  C(h)->prof = on != 0;
+  return GPL_OK;
+}
+
+int gpl_profile_reset(gpl_ctx* h) {
+  Ctx* c = C(h);
+  drain_profile(c);
+  c->prof_total.clear();
+  return GPL_OK;
+}
+
+int gpl_profile_read(gpl_ctx* h, const char* name, double* total_ms, int64_t* launches) {
+  Ctx* c = C(h);
+  drain_profile(c);
+  for (auto& t : c->prof_total)
+    if (t.first == name) {
+      if (total_ms) *total_ms = t.second.first;
+      if (launches) *launches = t.second.second;
+      return GPL_OK;
+    }
+  if (total_ms) *total_ms = 0.0;
+  if (launches) *launches = 0;
+  return GPL_OK;
+}
+
+int gpl_launch_count(const gpl_ctx* h, int64_t* launches) {
+  if (!h || !launches) return GPL_ERR_ARG;
+  *launches = h->c.launches;
+  return GPL_OK;
+}
+
+int gpl_sync(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  return GPL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,186 @@
+// Internal state and helpers of libgpl_b200 (not part of the C ABI).
+//
+// Device data layout (HBM), all double precision unless noted; ldN = N rounded up to a
+// multiple of 32 so every column starts on a 256-byte boundary:
+//   Z        ldN x P   column-major model matrix [1 | covariates | Knm]; the last M columns
+//                      are Knm (getKernelMats writes them in place, as the reference does)
+//   W        ldN x (J+1) gene-major weights; column J holds Oinvt (ggplvm.cu:292)
+//   Nu       ldN x J   working responses
+//   Psi      J x (P x P) per-gene Gram, full symmetric, then Cholesky factor in the lower
+//                      triangle (the reference's in-place layout)
+//   PsiInv   J x (P x P) explicit inverses
+//   Beta, tBeta  P x J
+//   KinvKmn  M x N     (reference layout)
+//   scratch  ldN x J   per-(cell, gene) intermediates
+//   counts   CSR (int32 cells, int64 offsets, double values) + per-gene valid prefix length
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "gpl.h"
+
+namespace gpl {
+
+constexpr double kWt = 0.1;     // Titsias weight (ggplvm.cu:20)
+constexpr double kIgap1 = 100;  // inverse-gamma prior shape+1 on Omega (ggplvm.cu:21)
+constexpr double kIgb = 100;    // inverse-gamma prior scale on Omega (ggplvm.cu:22)
+constexpr int kHist = 10;       // L-BFGS memory (ggplvm.cu:872)
+constexpr int kLkhdSlots = 50000;
+
+struct Ctx;
+
+// Sum of a per-block partial array in a fixed order (deterministic reductions).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int precision = GPL_PREC_FP64;
+  std::string err;
+
+  // sizes
+  int N = 0, J = 0, M = 0, Q = 0, P = 0, p = 0, n_var = 0;
+  int ldN = 0;
+  int64_t nnz = 0;
+  bool have_counts = false, have_design = false;
+
+  // host copies of the model-matrix metadata (DataFrame.cu:96-134)
+  std::vector<int> vc, vv, nh, mc, mv, mk;
+
+  // device buffers
+  double *Z = nullptr, *W = nullptr, *Nu = nullptr, *Psi = nullptr, *PsiInv = nullptr;
+  double *Beta = nullptr, *tBeta = nullptr, *scratch = nullptr, *U = nullptr;
+  double *Kmm = nullptr, *Kinv = nullptr, *KinvKmn = nullptr, *titsias = nullptr, *DeltaInv = nullptr;
+  double *Omega = nullptr, *delta = nullptr, *X = nullptr, *T = nullptr, *rho = nullptr, *phi = nullptr;
+  double *ls = nullptr, *lkhds = nullptr, *lkhd_dev = nullptr;
+  double *grad = nullptr, *grad0 = nullptr, *ss = nullptr, *SS = nullptr, *XX = nullptr;
+  double *gdtmp = nullptr, *C1 = nullptr, *C2 = nullptr, *grtmp = nullptr, *KmmInv = nullptr;
+  double *bvec = nullptr;     // P x J right-hand sides Z^T diag(W/Omega) nu
+  double *sol = nullptr;      // P x J solutions Psi^{-1} bvec
+  double *red = nullptr;      // reduction partials
+  double *lb_work = nullptr;  // L-BFGS scalars
+  int *mc_d = nullptr, *mv_d = nullptr, *mk_d = nullptr, *nh_d = nullptr;
+  int32_t* cell = nullptr;    // CSR cell indices
+  int64_t* gptr = nullptr;    // CSR offsets (J+1)
+  int32_t* gvalid = nullptr;  // per gene: entries matched by the reference's merge walk
+  double* cnt = nullptr;      // CSR values
+  int64_t tot_max = 0;
+
+  // host mirror of the objective trace (lkhd_d in the reference, ggplvm.cu:1052)
+  std::vector<double> lkhd;
+
+  // profiling
+  bool prof = false;
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof_pending;
+  std::vector<std::pair<std::string, std::pair<double, int64_t>>> prof_total;
+  std::vector<cudaEvent_t> event_pool;
+  int64_t launches = 0;
+};
+
+// Throws-free error plumbing: every CUDA call goes through check().
+bool check(Ctx* c, cudaError_t e, const char* what);
+#define GPL_TRY(c, expr)                                    \
+  do {                                                      \
+    if (!::gpl::check((c), (expr), #expr)) return GPL_ERR_CUDA; \
+  } while (0)
+#define GPL_LAUNCHED(c, name)                                                          \
+  do {                                                                                 \
+    (c)->launches++;                                                                   \
+    if (!::gpl::check((c), cudaGetLastError(), name)) return GPL_ERR_CUDA;            \
+  } while (0)
+
+// Scoped profiling range on the context stream.
+struct ProfScope {
+  Ctx* c;
+  const char* name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(Ctx* c_, const char* n);
+  ~ProfScope();
+};
+
+inline int64_t tot_len(const Ctx* c, int rhoflag) {
+  return (int64_t)c->N + c->p + (int64_t)c->N * c->Q + (int64_t)c->M * c->Q + rhoflag;
+}
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// ---- launchers (one per kernel family; each returns GPL_OK or an error code) ----------
+// k_kmats.cu
+int launch_kernel_mats(Ctx* c);          // Knm into Z, Kmm, Kinv copy, chol(Kinv), KinvKmn, titsias
+int launch_expand_delta(Ctx* c);         // DeltaInv (upper + diag)
+int launch_chol_single(Ctx* c, double* A, int n);  // choldc on one n x n matrix
+// k_gemm.cu
+int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
+int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
+int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
+int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
+int launch_c1_tn(Ctx* c);                // C1 partial from tn/phi and tBeta GP block
+// k_gram.cu
+int launch_gram(Ctx* c, bool unweighted);  // Psi (full symmetric) = Z^T diag(W/Omega) Z + DeltaInv
+int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride);
+int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const double* B, int64_t bstride,
+                         double* X, int64_t xstride, int batch);
+int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
+int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
+// k_lkhd.cu
+int launch_oinvt(Ctx* c);
+int launch_beta_phi(Ctx* c, int jtr);
+int launch_lkhd_pois(Ctx* c);
+int launch_lkhd_genes(Ctx* c);
+int launch_collect_lkhd(Ctx* c, int n_cells, int slot);
+int launch_init_beta_solve(Ctx* c);
+// k_grad.cu
+int launch_grad_delta(Ctx* c);
+int launch_grad_omega(Ctx* c);
+int launch_c2(Ctx* c);
+int launch_grad_tau_rho(Ctx* c);
+// k_lbfgs.cu
+int launch_lbfgs_update(Ctx* c, int itr, int rhoflag);
+int launch_downdate(Ctx* c, int itr, double r, int rhoflag);
+int launch_beta_from_tilde(Ctx* c);
+
+}  // namespace gpl
+
+struct gpl_ctx {
+  gpl::Ctx c;
+};
+
+// ---- device helpers --------------------------------------------------------------------
+namespace gpl {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum (fixed shuffle tree, then fixed order over warps); all threads
+// of the block must call it; the result is valid in every thread. `sh` needs 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (wid == 0) {
+    t = lane < nw ? sh[lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) sh[0] = t;
+  }
+  __syncthreads();
+  return sh[0];
+}
+
+}  // namespace gpl

@@ -1,0 +1,272 @@
+// Double-precision (cell x gene) contractions of the IRLS and the gradient, all built on
+// one register-tiled FP64 GEMM (64x64 output tile, 16-deep K chunks in shared memory,
+// 4x4 accumulators per thread) with element-wise prologues and epilogues:
+//
+//   W / Nu     eta = Z beta_j for every cell and gene, then the getWForBeta epilogue
+//              (ggplvm.cu:468-514). The counts of the tile's genes are scattered into
+//              shared memory first: each gene's matched prefix is sorted by cell, so a
+//              binary search finds the tile's slice. Bound: FP64 FMA (N*J*P).
+//   bvec       Z^T diag(W_j/Omega) nu_j (getZtOinvjnj, util_cuda.cu:462-487) and the GLM
+//              initialisation right-hand sides Z^T y0_j (initBeta, init.cu:193-221).
+//   E          Z tBeta (cell x gene predictions used by the Omega/X gradient).
+//   C1 (part)  sum_j (tn_ij / phi_j) tBeta_j[GP] (ggplvm.cu:344).
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+namespace {
+constexpr int TM = 64, TN = 64, TK = 16;
+}
+
+// A(r, k) and B(k, c) loaders. kFastK: the K index is contiguous in memory (load K-fastest).
+struct LoadZ {  // A(r = cell, k = column) = Z[k*ldN + r]
+  static constexpr bool kFastK = false;
+  const double* Z;
+  int ldN, N, P;
+  __device__ double operator()(int r, int k) const { return (r < N && k < P) ? Z[(size_t)k * ldN + r] : 0.0; }
+};
+struct LoadZt {  // A(r = column, k = cell) = Z[r*ldN + k]
+  static constexpr bool kFastK = true;
+  const double* Z;
+  int ldN, N, P;
+  __device__ double operator()(int r, int k) const { return (r < P && k < N) ? Z[(size_t)r * ldN + k] : 0.0; }
+};
+struct LoadColMajor {  // B(k, c) = B[k + c*ld]
+  static constexpr bool kFastK = true;
+  const double* B;
+  int ld, K, C;
+  __device__ double operator()(int k, int c) const { return (k < K && c < C) ? B[k + (size_t)c * ld] : 0.0; }
+};
+struct LoadOinvNu {  // B(k = cell, c = gene) = W/Omega * Nu
+  static constexpr bool kFastK = true;
+  const double *W, *Nu, *Omega;
+  int ldN, N, J;
+  __device__ double operator()(int k, int c) const {
+    if (k >= N || c >= J) return 0.0;
+    const size_t e = (size_t)c * ldN + k;
+    return W[e] / Omega[k] * Nu[e];
+  }
+};
+struct LoadCellGene {  // B(k = cell, c = gene) = S[c*ldN + k]
+  static constexpr bool kFastK = true;
+  const double* S;
+  int ldN, N, J;
+  __device__ double operator()(int k, int c) const { return (k < N && c < J) ? S[(size_t)c * ldN + k] : 0.0; }
+};
+struct LoadTn {  // A(r = cell, k = gene) = tn / phi, tn = O*nu - O*E, O = W/Omega
+  static constexpr bool kFastK = false;
+  const double *W, *Nu, *E, *Omega, *phi;
+  int ldN, N, J;
+  __device__ double operator()(int r, int k) const {
+    if (r >= N || k >= J) return 0.0;
+    const size_t e = (size_t)k * ldN + r;
+    const double o = W[e] / Omega[r];
+    const double tn = o * Nu[e] - o * E[e];
+    return tn / phi[k];
+  }
+};
+struct LoadTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + a + k*P]
+  static constexpr bool kFastK = false;
+  const double* tB;
+  int P, g0, M, J;
+  __device__ double operator()(int k, int c) const { return (k < J && c < M) ? tB[g0 + c + (size_t)k * P] : 0.0; }
+};
+
+template <class LA, class LB>
+__device__ __forceinline__ void gemm_tile(int m0, int n0, int K, const LA& A, const LB& B, double (&acc)[4][4],
+                                          double (*As)[TM + 1], double (*Bs)[TN + 1]) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+  for (int k0 = 0; k0 < K; k0 += TK) {
+#pragma unroll
+    for (int t = 0; t < (TM * TK) / 256; t++) {
+      const int e = tid + t * 256;
+      int r, k;
+      if (LA::kFastK) { k = e % TK; r = e / TK; }
+      else { r = e % TM; k = e / TM; }
+      As[k][r] = A(m0 + r, k0 + k);
+    }
+#pragma unroll
+    for (int t = 0; t < (TN * TK) / 256; t++) {
+      const int e = tid + t * 256;
+      int k, cc;
+      if (LB::kFastK) { k = e % TK; cc = e / TK; }
+      else { cc = e % TN; k = e / TN; }
+      Bs[k][cc] = B(k0 + k, n0 + cc);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TK; k++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int x = 0; x < 4; x++) a[x] = As[k][tx + 16 * x];
+#pragma unroll
+      for (int y = 0; y < 4; y++) b[y] = Bs[k][ty + 16 * y];
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+    }
+    __syncthreads();
+  }
+}
+
+// ---- W / Nu -----------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int pvars, const double* __restrict__ Z,
+                                              const double* __restrict__ Beta, const double* __restrict__ ls,
+                                              const double* __restrict__ delta, const double* __restrict__ titsias,
+                                              const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
+                                              const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
+                                              double* __restrict__ W, double* __restrict__ Nu) {
+  // the GEMM tiles and the count tile are live at different times: overlay them
+  __shared__ __align__(16) unsigned char raw[TN * (TM + 1) * sizeof(double) + TN * TM];
+  double(*As)[TM + 1] = reinterpret_cast<double(*)[TM + 1]>(raw);
+  double(*Bs)[TN + 1] = reinterpret_cast<double(*)[TN + 1]>(raw + TK * (TM + 1) * sizeof(double));
+  double(*ys)[TM + 1] = reinterpret_cast<double(*)[TM + 1]>(raw);
+  unsigned char(*yf)[TM] = reinterpret_cast<unsigned char(*)[TM]>(raw + TN * (TM + 1) * sizeof(double));
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  double acc[4][4];
+  gemm_tile(m0, n0, P, LoadZ{Z, ldN, N, P}, LoadColMajor{Beta, P, P, J}, acc, As, Bs);
+  // counts of this tile
+  for (int e = threadIdx.x; e < TN * TM; e += 256) yf[e / TM][e % TM] = 0;
+  __syncthreads();
+  if (threadIdx.x < TN) {
+    const int j = n0 + threadIdx.x;
+    if (j < J) {
+      int64_t lo = gptr[j], hi = gptr[j] + gvalid[j];
+      while (lo < hi) {  // first entry with cell >= m0
+        const int64_t mid = (lo + hi) >> 1;
+        if (cell[mid] < m0) lo = mid + 1; else hi = mid;
+      }
+      const int64_t end = gptr[j] + gvalid[j];
+      for (int64_t l = lo; l < end && cell[l] < m0 + TM; l++) {
+        ys[threadIdx.x][cell[l] - m0] = cnt[l];
+        yf[threadIdx.x][cell[l] - m0] = 1;
+      }
+    }
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const double dgp = delta[pvars - 1];
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int r = tx + 16 * x, i = m0 + r;
+    if (i >= N) continue;
+    const double lsi = ls[i], tt = dgp * titsias[i] * kWt;
+    const double lls = log(lsi);
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const int cc = ty + 16 * y, j = n0 + cc;
+      if (j >= J) continue;
+      const double eta = acc[x][y];
+      const double logW = eta + lls + tt;
+      const double w = exp(eta) * lsi * exp(tt);
+      double nu;
+      if (yf[cc][r]) nu = eta + exp(log(ys[cc][r]) - logW) - 1.0;
+      else nu = eta - 1.0;
+      W[(size_t)j * ldN + i] = w;
+      Nu[(size_t)j * ldN + i] = nu;
+    }
+  }
+}
+
+int launch_w_nu(Ctx* c) {
+  ProfScope ps(c, "w_nu");
+  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+  k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->p, c->Z, c->Beta, c->ls, c->delta, c->titsias,
+                                   c->cell, c->gptr, c->gvalid, c->cnt, c->W, c->Nu);
+  GPL_LAUNCHED(c, "k_w_nu");
+  return GPL_OK;
+}
+
+// ---- generic GEMM with plain column-major store -----------------------------------------
+template <class LA, class LB>
+__global__ void __launch_bounds__(256) k_gemm_store(int m, int n, int K, LA A, LB B, double* __restrict__ out,
+                                                    int64_t ldo) {
+  __shared__ double As[TK][TM + 1];
+  __shared__ double Bs[TK][TN + 1];
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  double acc[4][4];
+  gemm_tile(m0, n0, K, A, B, acc, As, Bs);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int r = m0 + tx + 16 * x;
+    if (r >= m) continue;
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const int cc = n0 + ty + 16 * y;
+      if (cc < n) out[r + (size_t)cc * ldo] = acc[x][y];
+    }
+  }
+}
+
+// y0 for initBeta: log((y + 0.05)/ls) where a count is matched, log(0.05/ls) elsewhere.
+__global__ void k_init_response(int N, int ldN, int J, const double* __restrict__ ls, double* __restrict__ out) {
+  const int j = blockIdx.x;
+  for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < N; i += gridDim.y * blockDim.x)
+    out[(size_t)j * ldN + i] = log(0.05 / ls[i]);
+}
+__global__ void k_init_response_counts(int N, int ldN, int J, const double* __restrict__ ls,
+                                       const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
+                                       const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
+                                       double* __restrict__ out) {
+  const int j = blockIdx.x;
+  const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
+  for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
+    const int i = cell[l];
+    out[(size_t)j * ldN + i] = log((cnt[l] + 0.05) / ls[i]);
+  }
+}
+
+int launch_init_response(Ctx* c) {
+  ProfScope ps(c, "init_response");
+  dim3 g(c->J, div_up(c->N, 256) > 64 ? 64 : div_up(c->N, 256));
+  k_init_response<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->ls, c->scratch);
+  GPL_LAUNCHED(c, "k_init_response");
+  k_init_response_counts<<<c->J, 128, 0, c->stream>>>(c->N, c->ldN, c->J, c->ls, c->cell, c->gptr, c->gvalid,
+                                                     c->cnt, c->scratch);
+  GPL_LAUNCHED(c, "k_init_response_counts");
+  return GPL_OK;
+}
+
+int launch_zt_u(Ctx* c, int mode) {
+  ProfScope ps(c, "zt_u");
+  dim3 g(div_up(c->P, TM), div_up(c->J, TN));
+  LoadZt A{c->Z, c->ldN, c->N, c->P};
+  if (mode == 0) {
+    k_gemm_store<<<g, 256, 0, c->stream>>>(c->P, c->J, c->N, A, LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J},
+                                           c->bvec, (int64_t)c->P);
+  } else {
+    k_gemm_store<<<g, 256, 0, c->stream>>>(c->P, c->J, c->N, A, LoadCellGene{c->scratch, c->ldN, c->N, c->J},
+                                           c->bvec, (int64_t)c->P);
+  }
+  GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
+  return GPL_OK;
+}
+
+int launch_zbeta(Ctx* c, const double* B, double* out) {
+  ProfScope ps(c, "zbeta");
+  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+  k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->J, c->P, LoadZ{c->Z, c->ldN, c->N, c->P},
+                                         LoadColMajor{B, c->P, c->P, c->J}, out, (int64_t)c->ldN);
+  GPL_LAUNCHED(c, "k_gemm_store(zbeta)");
+  return GPL_OK;
+}
+
+// C1 <- sum_j (tn_ij/phi_j) tBeta_j[GP]   (stored cell-fastest, ld ldN)
+int launch_c1_tn(Ctx* c) {
+  ProfScope ps(c, "c1_tn");
+  const int g0 = c->nh[c->p - 1];
+  dim3 g(div_up(c->N, TM), div_up(c->M, TN));
+  k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->M, c->J,
+                                         LoadTn{c->W, c->Nu, c->scratch, c->Omega, c->phi, c->ldN, c->N, c->J},
+                                         LoadTBetaGP{c->tBeta, c->P, g0, c->M, c->J}, c->C1, (int64_t)c->ldN);
+  GPL_LAUNCHED(c, "k_gemm_store(c1_tn)");
+  return GPL_OK;
+}
+
+}  // namespace gpl

@@ -1,0 +1,116 @@
+// Kernel matrices of the sparse GP (replaces kernel_funcs.cu:61-162 and util_cuda.cu:249-269).
+//
+//   k_knm        Knm[i, m] = exp(-(sin^2((x_i0 - t_m0)/2)/rho_0 + sum_q>=1 (x_iq - t_mq)^2/(2 rho_q)))
+//                written into the model matrix's GP block (column-major, cell fastest).
+//                Bound: N*M*Q transcendental work, ~2% of one objective evaluation.
+//   k_kmm        Kmm (upper, unit diagonal, zero lower) and its copy Kinv.
+//   k_kinvkmn    per cell: x = Kmm^{-1} k_n by two triangular solves against the factor in
+//                Kinv's lower triangle (cholslg order), titsias_n = (1 - k_n . x)/2.
+//                One thread per cell; the factor is read by every thread at the same
+//                address (broadcast), the solution lives in a cell-fastest scratch so the
+//                per-step loads coalesce.
+//   k_expand     DeltaInv = blockdiag(1/delta_k I, Kmm/delta_GP), upper + diagonal.
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+__global__ void k_knm(int N, int ldN, int M, int Q, const double* __restrict__ X, const double* __restrict__ T,
+                      const double* __restrict__ rho, double* __restrict__ Knm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= N) return;
+  double sum = 0.0, t = sin((X[i] - T[j]) / 2.0);
+  sum += t * t / rho[0];
+  for (int k = 1; k < Q; k++) {
+    t = X[i + (size_t)k * N] - T[j + k * M];
+    sum += t * t / 2.0 / rho[k];
+  }
+  Knm[i + (size_t)j * ldN] = exp(-sum);
+}
+
+__global__ void k_kmm(int M, int Q, const double* __restrict__ T, const double* __restrict__ rho,
+                      double* __restrict__ K, double* __restrict__ Kinv) {
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (ii >= M) return;
+  double val;
+  if (ii == j) {
+    val = 1.0;
+  } else if (ii > j) {
+    val = 0.0;
+  } else {
+    double sum = 0.0, t = sin((T[ii] - T[j]) / 2.0);
+    sum += t * t / rho[0];
+    for (int k = 1; k < Q; k++) {
+      t = T[ii + k * M] - T[j + k * M];
+      sum += t * t / 2.0 / rho[k];
+    }
+    val = exp(-sum);
+  }
+  K[ii + j * M] = val;
+  Kinv[ii + j * M] = val;
+}
+
+// Two triangular solves per cell with the lower factor L (n x n, col-major) held in the
+// lower triangle of Kinv; Knm and the solution Y are cell-fastest (ld ldN).
+__global__ void k_kinvkmn(int N, int ldN, int M, const double* __restrict__ L, const double* __restrict__ Knm,
+                          double* __restrict__ Y, double* __restrict__ titsias) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int r = 0; r < M; r++) {
+    double sum = Knm[i + (size_t)r * ldN];
+    for (int k = r - 1; k >= 0; k--) sum -= L[r + k * M] * Y[i + (size_t)k * ldN];
+    Y[i + (size_t)r * ldN] = sum / L[r + r * M];
+  }
+  for (int r = M - 1; r >= 0; r--) {
+    double sum = Y[i + (size_t)r * ldN];
+    for (int k = r + 1; k < M; k++) sum -= L[k + r * M] * Y[i + (size_t)k * ldN];
+    Y[i + (size_t)r * ldN] = sum / L[r + r * M];
+  }
+  double d = 0.0;
+  for (int k = 0; k < M; k++) d += Knm[i + (size_t)k * ldN] * Y[i + (size_t)k * ldN];
+  titsias[i] = (1.0 - d) / 2.0;
+}
+
+__global__ void k_expand(int P, int p, int g0, int M, const int* __restrict__ mk, const double* __restrict__ delta,
+                         const double* __restrict__ K, double* __restrict__ D) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (r >= P) return;
+  double v = 0.0;
+  if (r <= col) {
+    if (r >= g0) v = K[(r - g0) + (col - g0) * M] / delta[p - 1];
+    else if (r == col) v = 1.0 / delta[mk[r]];
+  }
+  D[r + (size_t)col * P] = v;
+}
+
+int launch_kernel_mats(Ctx* c) {
+  const int g0 = c->nh[c->p - 1];
+  double* Knm = c->Z + (size_t)g0 * c->ldN;
+  {
+    ProfScope ps(c, "kernel_mats");
+    dim3 g(div_up(c->N, 128), c->M);
+    k_knm<<<g, 128, 0, c->stream>>>(c->N, c->ldN, c->M, c->Q, c->X, c->T, c->rho, Knm);
+    GPL_LAUNCHED(c, "k_knm");
+    dim3 g2(div_up(c->M, 64), c->M);
+    k_kmm<<<g2, 64, 0, c->stream>>>(c->M, c->Q, c->T, c->rho, c->Kmm, c->Kinv);
+    GPL_LAUNCHED(c, "k_kmm");
+  }
+  int rc = launch_chol_single(c, c->Kinv, c->M);
+  if (rc) return rc;
+  ProfScope ps(c, "kinvkmn");
+  k_kinvkmn<<<div_up(c->N, 128), 128, 0, c->stream>>>(c->N, c->ldN, c->M, c->Kinv, Knm, c->KinvKmn, c->titsias);
+  GPL_LAUNCHED(c, "k_kinvkmn");
+  return GPL_OK;
+}
+
+int launch_expand_delta(Ctx* c) {
+  ProfScope ps(c, "expand_delta");
+  dim3 g(div_up(c->P, 128), c->P);
+  k_expand<<<g, 128, 0, c->stream>>>(c->P, c->p, c->nh[c->p - 1], c->M, c->mk_d, c->delta, c->Kmm, c->DeltaInv);
+  GPL_LAUNCHED(c, "k_expand");
+  return GPL_OK;
+}
+
+}  // namespace gpl

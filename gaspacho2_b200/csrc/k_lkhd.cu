@@ -1,0 +1,188 @@
+// Per-gene likelihood pieces and the IRLS coefficient update (replaces getBetaPhi
+// ggplvm.cu:418-464, getLkhdPois :703-724, getLkhd/getLkhdj :744-784, collectLkhd :788-815,
+// getOinvt :284-294, initBeta init.cu:193-221). All reductions are block-deterministic:
+// a fixed shuffle tree per warp, then the warps in order.
+//
+//   k_oinvt       Oinvt_i = sum_j W_ij / Omega_i (thread per cell, genes in order) -> W column J
+//   k_beta_phi    per gene: damped beta <- (1-r) beta + r Psi^{-1} b, phi from the residual
+//                 quadratic form nu^T (W/Omega) nu - |L^T beta|^2, clamped as the reference
+//   k_lkhd_pois   per gene: sum over matched counts of (log W - delta_GP titsias wt) y, minus sum W
+//   k_lkhd_genes  per gene: the Laplace/PQL marginal l_j
+//   k_collect     sum_j l_j - wt delta_GP sum_i Oinvt_i titsias_i - inverse-gamma prior on Omega
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+__global__ void k_oinvt(int N, int ldN, int J, const double* __restrict__ Omega, double* __restrict__ W) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double om = Omega[i];
+  double s = 0.0;
+  for (int j = 0; j < J; j++) s += W[(size_t)j * ldN + i] / om;
+  W[(size_t)J * ldN + i] = s;
+}
+
+int launch_oinvt(Ctx* c) {
+  ProfScope ps(c, "oinvt");
+  k_oinvt<<<div_up(c->N, 256), 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->Omega, c->W);
+  GPL_LAUNCHED(c, "k_oinvt");
+  return GPL_OK;
+}
+
+// sol_j = Psi_j^{-1} b_j was solved beforehand.
+__global__ void __launch_bounds__(256) k_beta_phi(int N, int ldN, int P, double r, const double* __restrict__ W,
+                                                  const double* __restrict__ Nu, const double* __restrict__ Omega,
+                                                  const double* __restrict__ Psi, const double* __restrict__ sol,
+                                                  double* __restrict__ Beta, double* __restrict__ phi) {
+  __shared__ double sh[32];
+  extern __shared__ double sb[];  // P
+  const int j = blockIdx.x;
+  const double* Wj = W + (size_t)j * ldN;
+  const double* nj = Nu + (size_t)j * ldN;
+  double part = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) part += nj[i] * nj[i] * Wj[i] / Omega[i];
+  const double quad = block_sum(part, sh);
+  double* bj = Beta + (size_t)j * P;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    const double nb = bj[k] * (1 - r) + sol[(size_t)j * P + k] * r;
+    bj[k] = nb;
+    sb[k] = nb;
+  }
+  __syncthreads();
+  // |L^T beta|^2: row k of L^T is column k of L (rows >= k), one warp per k
+  const double* L = Psi + (size_t)j * P * P;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double sq = 0.0;
+  for (int k = wid; k < P; k += nw) {
+    double t = 0.0;
+    for (int i = k + lane; i < P; i += 32) t += L[i + (size_t)k * P] * sb[i];
+    t = warp_sum(t);
+    sq += t * t;
+  }
+  if (lane != 0) sq = 0.0;
+  const double s2 = block_sum(sq, sh);
+  if (threadIdx.x == 0) {
+    double ph = (quad - s2) / (double)N;
+    if (isnan(ph)) ph = 1.0;
+    if (ph < 0.0) ph = 1.0;
+    if (ph < 0.01) ph = 0.01;
+    if (ph > 1000.0) ph = 1000.0;
+    phi[j] = ph;
+  }
+}
+
+int launch_beta_phi(Ctx* c, int jtr) {
+  int rc = launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->sol, c->P, c->J);
+  if (rc) return rc;
+  double r = (double)(jtr + 1) / 100.0;
+  if (jtr > 100) r = 1.0;
+  ProfScope ps(c, "beta_phi");
+  k_beta_phi<<<c->J, 256, sizeof(double) * c->P, c->stream>>>(c->N, c->ldN, c->P, r, c->W, c->Nu, c->Omega, c->Psi,
+                                                              c->sol, c->Beta, c->phi);
+  GPL_LAUNCHED(c, "k_beta_phi");
+  return GPL_OK;
+}
+
+__global__ void __launch_bounds__(256) k_lkhd_pois(int N, int ldN, int pvars, const double* __restrict__ W,
+                                                   const double* __restrict__ delta, const double* __restrict__ titsias,
+                                                   const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
+                                                   const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
+                                                   double* __restrict__ lkhds) {
+  __shared__ double sh[32];
+  const int j = blockIdx.x;
+  const double* Wj = W + (size_t)j * ldN;
+  double part = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) part -= Wj[i];
+  const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
+  const double dgp = delta[pvars - 1];
+  for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
+    const int i = cell[l];
+    part += (log(Wj[i]) - dgp * titsias[i] * kWt) * cnt[l];
+  }
+  const double s = block_sum(part, sh);
+  if (threadIdx.x == 0) lkhds[j] = s;
+}
+
+int launch_lkhd_pois(Ctx* c) {
+  ProfScope ps(c, "lkhd_pois");
+  k_lkhd_pois<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->W, c->delta, c->titsias, c->cell, c->gptr,
+                                           c->gvalid, c->cnt, c->lkhds);
+  GPL_LAUNCHED(c, "k_lkhd_pois");
+  return GPL_OK;
+}
+
+// l_j = -N/2 log phi - sum_i log(Omega/W)/2 - sum_k log L_kk + sum_k log LD_kk
+//       - sum_i nu^2 (W/Omega) / (2 phi) + b^T Psi^{-1} b / (2 phi)
+__global__ void __launch_bounds__(256) k_lkhd_genes(int N, int ldN, int P, const double* __restrict__ W,
+                                                    const double* __restrict__ Nu, const double* __restrict__ Omega,
+                                                    const double* __restrict__ Psi, const double* __restrict__ LD,
+                                                    const double* __restrict__ bvec, const double* __restrict__ sol,
+                                                    const double* __restrict__ phi, double* __restrict__ lkhds) {
+  __shared__ double sh[32];
+  const int j = blockIdx.x;
+  const double* Wj = W + (size_t)j * ldN;
+  const double* nj = Nu + (size_t)j * ldN;
+  const double phij = phi[j];
+  double a = 0.0, q = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double om = Omega[i], w = Wj[i];
+    a += log(om / w);
+    q += nj[i] * nj[i] * (w / om);
+  }
+  const double* L = Psi + (size_t)j * P * P;
+  double ld = 0.0, bx = 0.0;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    ld += log(LD[k + (size_t)k * P]) - log(L[k + (size_t)k * P]);
+    bx += bvec[(size_t)j * P + k] * sol[(size_t)j * P + k];
+  }
+  const double sa = block_sum(a, sh);
+  const double sq = block_sum(q, sh);
+  const double sld = block_sum(ld, sh);
+  const double sbx = block_sum(bx, sh);
+  if (threadIdx.x == 0)
+    lkhds[j] = -((double)N) / 2.0 * log(phij) - sa / 2.0 + sld - sq / 2.0 / phij + sbx / 2.0 / phij;
+}
+
+int launch_lkhd_genes(Ctx* c) {
+  int rc = launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->sol, c->P, c->J);
+  if (rc) return rc;
+  ProfScope ps(c, "lkhd_genes");
+  k_lkhd_genes<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->W, c->Nu, c->Omega, c->Psi, c->DeltaInv, c->bvec,
+                                            c->sol, c->phi, c->lkhds);
+  GPL_LAUNCHED(c, "k_lkhd_genes");
+  return GPL_OK;
+}
+
+__global__ void __launch_bounds__(1024) k_collect(int J, int n, int ldN, int pvars, const double* __restrict__ lkhds,
+                                                  const double* __restrict__ W, const double* __restrict__ titsias,
+                                                  const double* __restrict__ Omega, const double* __restrict__ delta,
+                                                  double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  for (int k = threadIdx.x; k < J; k += blockDim.x) s1 += lkhds[k];
+  const double* Oinvt = W + (size_t)J * ldN;
+  const double dgp = delta[pvars - 1];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    s2 += kWt * dgp * Oinvt[i] * titsias[i];
+    s3 += kIgb / Omega[i] + kIgap1 * log(Omega[i]);
+  }
+  s1 = block_sum(s1, sh);
+  s2 = block_sum(s2, sh);
+  s3 = block_sum(s3, sh);
+  if (threadIdx.x == 0) out[0] = s1 - s2 - s3;
+}
+
+int launch_collect_lkhd(Ctx* c, int n_cells, int slot) {
+  ProfScope ps(c, "collect");
+  k_collect<<<1, 1024, 0, c->stream>>>(c->J, n_cells, c->ldN, c->p, c->lkhds, c->W, c->titsias, c->Omega, c->delta,
+                                       c->lkhd_dev + slot);
+  GPL_LAUNCHED(c, "k_collect");
+  return GPL_OK;
+}
+
+int launch_init_beta_solve(Ctx* c) {
+  // one factor (Psi slot 0) for every gene's right-hand side
+  return launch_solve_batched(c, c->Psi, c->P, 0, c->bvec, c->P, c->Beta, c->P, c->J);
+}
+
+}  // namespace gpl

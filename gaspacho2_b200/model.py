@@ -1,0 +1,197 @@
+"""Host-side mirror of the reference driver's phases over the C ABI (include/gpl.h).
+
+``GPLVM`` keeps the reference's vocabulary: the phases are the reference kernels' names
+(kernel matrices, GLM init, IRLS sweep, objective, gradient, L-BFGS update, downdate) and
+``get(name)`` returns the reference's buffers in the reference's layouts, so a test can
+run the same sequence through this class, the reference build (oracle/_ref) and the
+oracle and compare buffer by buffer.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+def _d(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class GPLVM:
+    """One fit context on a CUDA device: counts, design and the state of the fit."""
+
+    def __init__(self, y, z, ls, X0, M: int, Q: int, device: int = 0, stream: Optional[int] = None,
+                 precision: str = "fp64"):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        check(L.gpl_create(ctypes.byref(h), int(device), ctypes.c_void_p(stream) if stream else None), None,
+              "gpl_create")
+        self.h = h
+        self._L = L
+        ci = np.ascontiguousarray(y.i, np.int32)
+        gp = np.ascontiguousarray(y.p, np.int32)
+        cx = np.ascontiguousarray(y.x, np.float64)
+        check(L.gpl_load_counts(h, int(y.N), int(y.J), int(ci.shape[0]), ci.ctypes.data_as(_ip),
+                                gp.ctypes.data_as(_ip), _d(cx)), h, "gpl_load_counts")
+        c = np.ascontiguousarray(z.c, np.int32)
+        v = np.ascontiguousarray(z.v, np.int32)
+        body = z.body_bytes()
+        buf = ctypes.create_string_buffer(body, max(1, len(body)))
+        check(L.gpl_load_design(h, int(z.N), int(z.n_var), c.ctypes.data_as(_ip), v.ctypes.data_as(_ip),
+                                ctypes.cast(buf, ctypes.c_void_p), len(body), int(M), int(Q)), h, "gpl_load_design")
+        check(L.gpl_set_size_factors(h, _d(np.ascontiguousarray(ls, np.float64))), h, "gpl_set_size_factors")
+        X = np.ascontiguousarray(np.asarray(X0, np.float64).ravel(order="F"))
+        check(L.gpl_set_params(h, None, None, _d(X), None, None, None), h, "gpl_set_params")
+        d = (ctypes.c_int32 * 6)()
+        check(L.gpl_dims(h, d), h, "gpl_dims")
+        self.N, self.J, self.M, self.P, self.p, self.Q = list(d)
+        self.set_precision(precision)
+
+    @classmethod
+    def from_dataset(cls, ds, **kw) -> "GPLVM":
+        return cls(ds.y, ds.z, ds.ls, ds.X0, ds.M, ds.Q, **kw)
+
+    # -- lifetime ------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.gpl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc, what):
+        check(rc, self.h, what)
+
+    # -- parameters ----------------------------------------------------------------------------
+    def set_precision(self, precision: str):
+        self._c(self._L.gpl_set_precision(self.h, _lib.PREC[precision]), "gpl_set_precision")
+
+    def set_params(self, prm) -> None:
+        flat = [np.ascontiguousarray(a, dtype=np.float64) for a in prm.flat()]
+        self._keep = flat
+        self._c(self._L.gpl_set_params(self.h, *[_d(a) for a in flat]), "gpl_set_params")
+
+    def set_beta(self, beta: np.ndarray) -> None:
+        b = np.ascontiguousarray(np.asarray(beta, np.float64).ravel(order="F"))
+        self._c(self._L.gpl_set_beta(self.h, _d(b)), "gpl_set_beta")
+
+    def n_params(self) -> int:
+        return self.N + self.p + self.N * self.Q + self.M * self.Q + self.Q
+
+    # -- phases (reference driver order, ggplvm.cu:1101-1330) -------------------------------------
+    def kernel_mats(self):
+        self._c(self._L.gpl_kernel_mats(self.h), "gpl_kernel_mats")
+
+    def glm_init(self):
+        self._c(self._L.gpl_glm_init(self.h), "gpl_glm_init")
+
+    def expand_delta(self):
+        self._c(self._L.gpl_expand_delta(self.h), "gpl_expand_delta")
+
+    def irls_sweep(self, itr: int, jtr: int) -> float:
+        v = ctypes.c_double()
+        self._c(self._L.gpl_irls_sweep(self.h, int(jtr), ctypes.byref(v)), "gpl_irls_sweep")
+        return v.value
+
+    def irls(self, itr: int, jtr_max: int) -> int:
+        n = ctypes.c_int()
+        rc = self._L.gpl_irls(self.h, int(jtr_max), ctypes.byref(n))
+        if rc == -5:
+            return -1
+        self._c(rc, "gpl_irls")
+        return n.value
+
+    def objective_after_irls(self, itr: int = 0) -> float:
+        v = ctypes.c_double()
+        self._c(self._L.gpl_objective_after_irls(self.h, ctypes.byref(v)), "gpl_objective_after_irls")
+        return v.value
+
+    def objective(self, itr: int, slot: int) -> float:
+        v = ctypes.c_double()
+        self._c(self._L.gpl_objective(self.h, int(slot), ctypes.byref(v)), "gpl_objective")
+        return v.value
+
+    def gradient(self) -> np.ndarray:
+        g = np.zeros(self.n_params())
+        self._c(self._L.gpl_gradient(self.h, _d(g)), "gpl_gradient")
+        return g
+
+    def lbfgs_update(self, jtr: int, rhoflag: int):
+        self._c(self._L.gpl_lbfgs_update(self.h, int(jtr), int(rhoflag)), "gpl_lbfgs_update")
+
+    def downdate(self, jtr: int, sr: float, rhoflag: int):
+        self._c(self._L.gpl_downdate(self.h, int(jtr), float(sr), int(rhoflag)), "gpl_downdate")
+
+    def beta_from_tilde(self):
+        self._c(self._L.gpl_beta_from_tilde(self.h), "gpl_beta_from_tilde")
+
+    def fit(self, itr_max: int, lbfgs_budget: int, trace_cap: int = 100000):
+        st = (ctypes.c_int32 * 4)()
+        tr = np.zeros(trace_cap)
+        rc = self._L.gpl_fit(self.h, int(itr_max), int(lbfgs_budget), st, _d(tr), int(trace_cap))
+        if rc not in (0, -5):
+            self._c(rc, "gpl_fit")
+        stats = dict(outer=st[0], irls=st[1], lbfgs=st[2], evals=st[3])
+        return (1 if rc == -5 else 0), stats, tr[:stats["outer"] + stats["lbfgs"]].copy()
+
+    def evaluate(self, params: np.ndarray, grad_out: Optional[np.ndarray] = None):
+        """Objective and gradient at natural-scale params [Omega | delta | X | T | rho]."""
+        params = np.ascontiguousarray(params, np.float64)
+        g = grad_out if grad_out is not None else np.zeros(self.n_params())
+        v = ctypes.c_double()
+        self._c(self._L.gpl_evaluate(self.h, _d(params), int(params.shape[0]), ctypes.byref(v), _d(g)),
+                "gpl_evaluate")
+        return v.value, g
+
+    def evaluate_device(self):
+        """Enqueues one objective+gradient evaluation at the device-resident parameters."""
+        self._c(self._L.gpl_evaluate_device(self.h), "gpl_evaluate_device")
+
+    # -- state ---------------------------------------------------------------------------------
+    def get(self, name: str) -> np.ndarray:
+        n = ctypes.c_int64()
+        self._c(self._L.gpl_get(self.h, name.encode(), None, 0, ctypes.byref(n)), f"gpl_get({name})")
+        out = np.zeros(n.value)
+        self._c(self._L.gpl_get(self.h, name.encode(), _d(out), n.value, ctypes.byref(n)), f"gpl_get({name})")
+        return out
+
+    def params_vector(self) -> np.ndarray:
+        return np.concatenate([self.get(k) for k in ("Omega", "delta", "X", "T", "rho")])
+
+    def profile(self, on: bool = True):
+        self._c(self._L.gpl_profile_enable(self.h, int(on)), "gpl_profile_enable")
+
+    def profile_reset(self):
+        self._c(self._L.gpl_profile_reset(self.h), "gpl_profile_reset")
+
+    def profile_read(self, name: str):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self._c(self._L.gpl_profile_read(self.h, name.encode(), ctypes.byref(ms), ctypes.byref(n)),
+                "gpl_profile_read")
+        return ms.value, n.value
+
+    def launches(self) -> int:
+        n = ctypes.c_int64()
+        self._c(self._L.gpl_launch_count(self.h, ctypes.byref(n)), "gpl_launch_count")
+        return n.value
+
+    def sync(self):
+        self._c(self._L.gpl_sync(self.h), "gpl_sync")

@@ -1,0 +1,171 @@
+/*
+ * gpl.h -- C ABI of the B200 GASPACHO2 sparse GP-LVM fit (libgpl_b200.so).
+ *
+ * The reference (GASPACHO2, src/) has no library boundary: its driver `main`
+ * (ggplvm.cu:951-1354) reads four binary files, launches its kernels directly and
+ * writes params.bin. This header exposes the same path as plain C entry points so a
+ * C/C++ driver (the bundled `ggplvm` CLI), Python (ctypes) or any FFI can call it. Each
+ * function names the reference code it replaces.
+ *
+ * Conventions
+ *   - All arrays are HOST memory, in the reference's layouts (column-major, cell index
+ *     fastest, exactly as the reference files and kernels use them). The context owns
+ *     its device memory; nothing in the signatures is a device pointer or a torch type.
+ *   - Every function returns GPL_OK (0) or a negative GPL_ERR_* code; gpl_last_error()
+ *     gives the message. A context is used from one host thread at a time and runs its
+ *     kernels in order on one CUDA stream (its own, or one given at creation).
+ *   - Sizes: N cells, J genes, M inducing points, Q latent dimensions, p model variables
+ *     (intercept + file variables + the GP block), P model-matrix columns.
+ *   - The parameter vector of the optimiser ("grad" layout, ggplvm.cu:109,154,265,311)
+ *     is [log Omega (N) | log delta (p) | X (N*Q) | T (M*Q) | log rho (Q)].
+ */
+#ifndef GPL_H
+#define GPL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GPL_API __attribute__((visibility("default")))
+#else
+#define GPL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPL_OK 0
+#define GPL_ERR_ARG (-1)      /* bad argument or inconsistent sizes */
+#define GPL_ERR_CUDA (-2)     /* CUDA runtime error */
+#define GPL_ERR_ALLOC (-3)    /* device or host allocation failed */
+#define GPL_ERR_STATE (-4)    /* call out of order (e.g. counts not loaded) */
+#define GPL_ERR_NAN (-5)      /* NaN likelihood where the reference driver exits (ggplvm.cu:1182) */
+#define GPL_ERR_FORMAT (-6)   /* malformed input data (level code out of range, bad CSR offsets) */
+#define GPL_ERR_IO (-7)       /* file could not be read or written */
+
+#define GPL_PREC_FP64 0       /* plain double precision: the drop-in path */
+#define GPL_PREC_BF16X3 1     /* Gram-family contractions on tensor cores, BF16 hi/lo split, FP32 accumulation */
+
+typedef struct gpl_ctx gpl_ctx;
+
+/* Creates a context on CUDA device `device`. `stream` is a cudaStream_t to run on, or NULL
+ * for a context-owned stream. No reference counterpart (main's cudaMalloc block,
+ * ggplvm.cu:1024-1060, happens in gpl_load_design once sizes are known). */
+GPL_API int gpl_create(gpl_ctx** out, int device, void* stream);
+GPL_API int gpl_destroy(gpl_ctx* ctx);
+GPL_API const char* gpl_last_error(const gpl_ctx* ctx);
+GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
+
+/* Gene-major CSR counts: replaces loadSparseMat + newSparseMatOnDevice
+ * (SparseMat.cu:37-52,127-142). Gene j owns entries gene_ptr[j]..gene_ptr[j+1]-1.
+ * Count matching keeps the reference's merge-walk rule (ggplvm.cu:505-511): within a
+ * gene, entries are used in order while the cell index increases and stays below N; the
+ * first out-of-order, duplicated or out-of-range index ends that gene's counts. */
+GPL_API int gpl_load_counts(gpl_ctx* ctx, int N, int J, int64_t nnz, const int32_t* cell_idx, const int32_t* gene_ptr,
+                    const double* counts);
+
+/* Covariate DataFrame: replaces loadDataFrame(fname, M) + newDataFrameOnDevice
+ * (DataFrame.cu:88-191). `n_var` file variables with level counts c[] (1 = numeric) and
+ * widths v[], and the file body (numeric: double[N*v] column-major; categorical:
+ * int32[N] level codes). The intercept and the M-column Knm block are added as in the
+ * reference. Allocates the device state for N, J (counts must be loaded first), M, Q.
+ * Level codes outside 0..c*v-1 are rejected (GPL_ERR_FORMAT); the reference reads
+ * beyond the column block for them. */
+GPL_API int gpl_load_design(gpl_ctx* ctx, int N, int n_var, const int32_t* c, const int32_t* v, const void* body,
+                    int64_t body_bytes, int M, int Q);
+
+/* Size factors ls[N] (ggplvm.cu:1019-1022,1062). */
+GPL_API int gpl_set_size_factors(gpl_ctx* ctx, const double* ls);
+
+/* dims[6] = N, J, M, P, p, Q (ggplvm.cu:966-984). */
+GPL_API int gpl_dims(const gpl_ctx* ctx, int32_t* dims);
+
+/* initParams (init.cu:27-48): delta = (1.5, 0.01.., 0.3), Omega = 1, phi = 1, rho = (5, 10..);
+ * T dimension 0 equispaced on (0, 2 pi) as initTaWithPer (util.c:73-87), others 0. */
+GPL_API int gpl_init_params(gpl_ctx* ctx);
+
+/* readParams / writeParams without the file (util_cuda.cu:520-580): Omega[N], delta[p],
+ * X[N*Q], T[M*Q], rho[Q], phi[J]. A NULL pointer keeps (set) or skips (get) that block. */
+GPL_API int gpl_set_params(gpl_ctx* ctx, const double* Omega, const double* delta, const double* X, const double* T,
+                   const double* rho, const double* phi);
+GPL_API int gpl_get_params(gpl_ctx* ctx, double* Omega, double* delta, double* X, double* T, double* rho, double* phi);
+
+/* GLM coefficients beta[P*J] (column j = gene j). The reference never writes beta out
+ * (it is only printed, ggplvm.cu:1325); this is the added output. */
+GPL_API int gpl_set_beta(gpl_ctx* ctx, const double* beta);
+GPL_API int gpl_get_beta(gpl_ctx* ctx, double* beta);
+
+/* getKernelMats + cholKmm + getKinvKmn (ggplvm.cu:1111-1113, kernel_funcs.cu:61-162). */
+GPL_API int gpl_kernel_mats(gpl_ctx* ctx);
+
+/* expandDelta_k + initPsi + initPsi2 + initBeta (ggplvm.cu:1134-1137, init.cu:125-221). */
+GPL_API int gpl_glm_init(gpl_ctx* ctx);
+
+/* expandDelta_k alone (util_cuda.cu:249-269). */
+GPL_API int gpl_expand_delta(gpl_ctx* ctx);
+
+/* One IRLS sweep: getWForBeta, getPsi, cholPsi, getBetaPhi, getLkhdPois, collectLkhd
+ * (ggplvm.cu:1156-1180) with damping index jtr; *lkhd receives the Poisson sum. */
+GPL_API int gpl_irls_sweep(gpl_ctx* ctx, int jtr, double* lkhd);
+
+/* The IRLS loop with the driver's stopping rule (ggplvm.cu:1152-1189): up to jtr_max
+ * sweeps, stop at relative change < 1e-7. *n_sweeps gets the count. GPL_ERR_NAN where the
+ * reference exits on a NaN likelihood. */
+GPL_API int gpl_irls(gpl_ctx* ctx, int jtr_max, int* n_sweeps);
+
+/* getOinvt, cholDeltaInv, getLkhd, collectLkhd (ggplvm.cu:1205-1211). */
+GPL_API int gpl_objective_after_irls(gpl_ctx* ctx, double* lkhd);
+
+/* One line-search evaluation of the objective (ggplvm.cu:1258-1277) into slot `slot`. */
+GPL_API int gpl_objective(gpl_ctx* ctx, int slot, double* lkhd);
+
+/* One gradient evaluation (ggplvm.cu:1215-1240); grad may be NULL (kept on the device). */
+GPL_API int gpl_gradient(gpl_ctx* ctx, double* grad);
+
+/* LBFGS (ggplvm.cu:865-934, util_cuda.cu:187-232) and Downdate (ggplvm.cu:818-859). */
+GPL_API int gpl_lbfgs_update(gpl_ctx* ctx, int jtr, int rhoflag);
+GPL_API int gpl_downdate(gpl_ctx* ctx, int jtr, double sr, int rhoflag);
+
+/* getBetaFromTildeBeta (ggplvm.cu:394-402), with zeta = 0 (the driver never sets it). */
+GPL_API int gpl_beta_from_tilde(gpl_ctx* ctx);
+
+/* The driver's outer loop (ggplvm.cu:1146-1330): IRLS, objective, L-BFGS with backtracking
+ * line search, under budgets itr_max (outer iterations) and lbfgs_budget (total L-BFGS
+ * steps, <= 0 for none). stats[4] = outer iterations, IRLS sweeps, L-BFGS steps,
+ * objective evaluations; trace gets the accepted objective values (<= trace_cap). */
+GPL_API int gpl_fit(gpl_ctx* ctx, int itr_max, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap);
+
+/* One objective+gradient evaluation at host parameters (the unit of the throughput
+ * metric): params = [Omega (N) | delta (p) | X (N*Q) | T (M*Q) | rho (Q)] in natural
+ * scale (n_params = N + p + N*Q + M*Q + Q); the objective goes to *lkhd and the gradient
+ * (optimiser layout above, N + p + N*Q + M*Q + Q values) to grad. W, nu, phi and beta stay
+ * as the last IRLS phase left them, as inside the reference's L-BFGS loop. This is the
+ * line-search evaluation followed by the gradient (ggplvm.cu:1258-1277 then 1215-1240). */
+GPL_API int gpl_evaluate(gpl_ctx* ctx, const double* params, int64_t n_params, double* lkhd, double* grad);
+
+/* The same evaluation at the parameters already on the device, enqueued on the context's
+ * stream without host copies or synchronisation (device-resident throughput). The objective
+ * lands in slot 1 of the trace; read it with gpl_get("lkhd_dev") or the next evaluate. */
+GPL_API int gpl_evaluate_device(gpl_ctx* ctx);
+
+/* Copies a named state buffer out in the reference layout (names as the reference's
+ * variables: "Knm", "Kmm", "Kinv", "KinvKmn", "titsias", "W", "Nu", "Psi", "PsiInv",
+ * "DeltaInv", "Beta", "tBeta", "phi", "lkhds", "lkhd", "C1", "C2", "grad", "ss",
+ * "Omega", "delta", "X", "T", "rho"). *len gets the element count; out may be NULL. */
+GPL_API int gpl_get(gpl_ctx* ctx, const char* name, double* out, int64_t cap, int64_t* len);
+
+/* Per-kernel device time since the last reset: names[i] with total milliseconds and
+ * launch counts, recorded with CUDA events on the context's stream when enabled. */
+GPL_API int gpl_profile_enable(gpl_ctx* ctx, int on);
+GPL_API int gpl_profile_reset(gpl_ctx* ctx);
+GPL_API int gpl_profile_read(gpl_ctx* ctx, const char* name, double* total_ms, int64_t* launches);
+GPL_API int gpl_launch_count(const gpl_ctx* ctx, int64_t* launches);
+
+/* Synchronises the context's stream. */
+GPL_API int gpl_sync(gpl_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
