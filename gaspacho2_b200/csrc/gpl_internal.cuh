@@ -133,6 +133,7 @@ int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const 
                          double* X, int64_t xstride, int batch);
 int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
+int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA
 // k_lkhd.cu
 int launch_oinvt(Ctx* c);
 int launch_beta_phi(Ctx* c, int jtr);

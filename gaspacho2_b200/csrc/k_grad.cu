@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256) k_c2(int N, int ldN, int J, int P, int M,
 int launch_c2(Ctx* c) {
   ProfScope ps(c, "c2");
   // Kmm^{-1} from the factor in Kinv's lower triangle (column k = cholsl(Kinv, e_k))
-  int rc = launch_inverse_single(c, c->Kinv, c->M, c->scratch, c->KmmInv);
+  int rc = launch_cholinv_exact(c, c->Kinv, c->M, c->KmmInv);
   if (rc) return rc;
   const int np = c->M * (c->M + 1) / 2;
   k_c2<<<np, 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->P, c->M, c->nh[c->p - 1], c->p, c->KinvKmn, c->W, c->tBeta,

@@ -134,6 +134,61 @@ __global__ void __launch_bounds__(256) k_chol(double* __restrict__ A, int n, int
   }
 }
 
+// Single-matrix Cholesky in choldc's exact operation order (chol.cu:19-43): row i of the
+// factor is finished before row i+1, each entry's sum runs k = i-1 .. 0, and no multiply-add
+// is contracted, so identical inputs give the host reference's bits (sqrt and division are
+// correctly rounded on both). Used for the small, often ill-conditioned matrices: Kmm (no
+// jitter in the reference), the prior precision DeltaInv and the GLM initialisation Gram.
+// Reads the upper triangle, writes the factor into the lower one; zero-fills on a
+// non-positive pivot. One CTA.
+__global__ void __launch_bounds__(256) k_chol_exact(double* __restrict__ a, int n) {
+  __shared__ int fail;
+  if (threadIdx.x == 0) fail = 0;
+  __syncthreads();
+  for (int i = 0; i < n; i++) {
+    // sums for j = i .. n-1 (j = i is the pivot)
+    double sums[4];
+    int cnt = 0;
+    for (int j = i + threadIdx.x; j < n && cnt < 4; j += blockDim.x, cnt++) {
+      double sum = a[i + (size_t)j * n];
+      for (int k = i - 1; k >= 0; k--) sum = __dsub_rn(sum, __dmul_rn(a[i + (size_t)k * n], a[j + (size_t)k * n]));
+      sums[cnt] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (sums[0] <= 0.0) fail = 1;
+      else a[i + (size_t)i * n] = __dsqrt_rn(sums[0]);
+    }
+    __syncthreads();
+    if (fail) break;
+    const double lii = a[i + (size_t)i * n];
+    cnt = 0;
+    for (int j = i + threadIdx.x; j < n && cnt < 4; j += blockDim.x, cnt++)
+      if (j > i) a[j + (size_t)i * n] = __ddiv_rn(sums[cnt], lii);
+    __syncthreads();
+  }
+  if (fail)
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[e] = 0.0;
+}
+
+// Columns of (L L^T)^{-1} in cholsl's order (chol.cu:45-56), thread per column, no
+// contraction: the Kmm^{-1} of getC2 (ggplvm.cu:93-95). Y is an n x n scratch (col-major).
+__global__ void k_cholinv_exact(const double* __restrict__ a, int n, double* __restrict__ Y) {
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < n; col += gridDim.x * blockDim.x) {
+    double* x = Y + (size_t)col * n;
+    for (int i = 0; i < n; i++) {
+      double sum = (i == col) ? 1.0 : 0.0;
+      for (int k = i - 1; k >= 0; k--) sum = __dsub_rn(sum, __dmul_rn(a[i + (size_t)k * n], x[k]));
+      x[i] = __ddiv_rn(sum, a[i + (size_t)i * n]);
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double sum = x[i];
+      for (int k = i + 1; k < n; k++) sum = __dsub_rn(sum, __dmul_rn(a[k + (size_t)i * n], x[k]));
+      x[i] = __ddiv_rn(sum, a[i + (size_t)i * n]);
+    }
+  }
+}
+
 // (L L^T) x = b for `batch` systems, one warp each; y in shared memory.
 __global__ void k_solve(const double* __restrict__ L, int n, int64_t lstride, const double* __restrict__ B,
                         int64_t bstride, double* __restrict__ X, int64_t xstride, int batch) {
@@ -216,8 +271,19 @@ int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride) {
 
 int launch_chol_single(Ctx* c, double* A, int n) {
   ProfScope ps(c, "chol_small");
-  k_chol<<<1, 256, 0, c->stream>>>(A, n, 0, 1);
-  GPL_LAUNCHED(c, "k_chol");
+  if (n > 4 * 256) {  // wider than the exact kernel's per-thread row slots
+    k_chol<<<1, 256, 0, c->stream>>>(A, n, 0, 1);
+    GPL_LAUNCHED(c, "k_chol");
+    return GPL_OK;
+  }
+  k_chol_exact<<<1, 256, 0, c->stream>>>(A, n);
+  GPL_LAUNCHED(c, "k_chol_exact");
+  return GPL_OK;
+}
+
+int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out) {
+  k_cholinv_exact<<<div_up(n, 64), 64, 0, c->stream>>>(L, n, out);
+  GPL_LAUNCHED(c, "k_cholinv_exact");
   return GPL_OK;
 }
 

@@ -57,18 +57,20 @@ __global__ void k_kinvkmn(int N, int ldN, int M, const double* __restrict__ L, c
                           double* __restrict__ Y, double* __restrict__ titsias) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  // cholslg's order (chol.cu:86-97) without contracted multiply-adds: Kmm has no jitter in
+  // the reference and is often nearly singular, so the solve keeps the reference's rounding
   for (int r = 0; r < M; r++) {
     double sum = Knm[i + (size_t)r * ldN];
-    for (int k = r - 1; k >= 0; k--) sum -= L[r + k * M] * Y[i + (size_t)k * ldN];
-    Y[i + (size_t)r * ldN] = sum / L[r + r * M];
+    for (int k = r - 1; k >= 0; k--) sum = __dsub_rn(sum, __dmul_rn(L[r + k * M], Y[i + (size_t)k * ldN]));
+    Y[i + (size_t)r * ldN] = __ddiv_rn(sum, L[r + r * M]);
   }
   for (int r = M - 1; r >= 0; r--) {
     double sum = Y[i + (size_t)r * ldN];
-    for (int k = r + 1; k < M; k++) sum -= L[k + r * M] * Y[i + (size_t)k * ldN];
-    Y[i + (size_t)r * ldN] = sum / L[r + r * M];
+    for (int k = r + 1; k < M; k++) sum = __dsub_rn(sum, __dmul_rn(L[k + r * M], Y[i + (size_t)k * ldN]));
+    Y[i + (size_t)r * ldN] = __ddiv_rn(sum, L[r + r * M]);
   }
   double d = 0.0;
-  for (int k = 0; k < M; k++) d += Knm[i + (size_t)k * ldN] * Y[i + (size_t)k * ldN];
+  for (int k = 0; k < M; k++) d = __dadd_rn(d, __dmul_rn(Knm[i + (size_t)k * ldN], Y[i + (size_t)k * ldN]));
   titsias[i] = (1.0 - d) / 2.0;
 }
 

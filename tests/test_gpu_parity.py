@@ -68,7 +68,8 @@ def test_count_walk_on_device():
 
 
 def _sensitivity(ds, seeds=(0, 1)):
-    """The oracle's own change when the latent coordinates move by a fraction of an ulp:
+    """The oracle's own change when the latent and inducing coordinates move by a fraction of
+    an ulp:
     the rounding floor that any reordering of the same FP64 arithmetic can reach. With
     nearly singular Kmm (no jitter in the reference) this floor is far above 1e-8."""
     import dataclasses
@@ -78,7 +79,8 @@ def _sensitivity(ds, seeds=(0, 1)):
     for sd in seeds:
         rng = np.random.default_rng(sd)
         X2 = ds.init.X * (1 + 2e-16 * rng.standard_normal(ds.init.X.shape))
-        ds2 = dataclasses.replace(ds, init=dataclasses.replace(ds.init, X=X2))
+        T2 = ds.init.T * (1 + 2e-16 * rng.standard_normal(ds.init.T.shape))
+        ds2 = dataclasses.replace(ds, init=dataclasses.replace(ds.init, X=X2, T=T2))
         pert = gu.run_phases(port.OracleModel.from_dataset(ds2), ds2)
         for k in base:
             if k != "irls_n":
