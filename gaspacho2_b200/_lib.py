@@ -10,7 +10,8 @@ LIB_PATH = os.path.join(PKG, "libgpl_b200.so")
 
 GPL_OK = 0
 ERRORS = {-1: "GPL_ERR_ARG", -2: "GPL_ERR_CUDA", -3: "GPL_ERR_ALLOC", -4: "GPL_ERR_STATE", -5: "GPL_ERR_NAN",
-          -6: "GPL_ERR_FORMAT", -7: "GPL_ERR_IO"}
+          -6: "GPL_ERR_FORMAT", -7: "GPL_ERR_IO",
+          -8: "GPL_ERR_LIMIT"}
 PREC = {"fp64": 0, "bf16x3": 1}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -53,6 +54,8 @@ SIGNATURES = {
     "gpl_profile_read": (ctypes.c_int, [_vp, ctypes.c_char_p, _dp, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_sync": (ctypes.c_int, [_vp]),
+    "gpl_kernel_mats_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+                                               _vp, _vp]),
 }
 
 _lib = None

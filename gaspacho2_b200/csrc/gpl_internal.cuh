@@ -134,6 +134,9 @@ int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const 
 int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA
+void launch_chol_exact_raw(cudaStream_t st, double* A, int n);
+int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
+                           const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork);
 // k_lkhd.cu
 int launch_oinvt(Ctx* c);
 int launch_beta_phi(Ctx* c, int jtr);

@@ -281,6 +281,8 @@ int launch_chol_single(Ctx* c, double* A, int n) {
   return GPL_OK;
 }
 
+void launch_chol_exact_raw(cudaStream_t st, double* A, int n) { k_chol_exact<<<1, 256, 0, st>>>(A, n); }
+
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out) {
   k_cholinv_exact<<<div_up(n, 64), 64, 0, c->stream>>>(L, n, out);
   GPL_LAUNCHED(c, "k_cholinv_exact");

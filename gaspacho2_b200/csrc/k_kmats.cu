@@ -115,4 +115,18 @@ int launch_expand_delta(Ctx* c) {
   return GPL_OK;
 }
 
+// The kernel-matrix sequence on caller-supplied buffers, without a context: Knm and the
+// cell-fastest Kmm^{-1} k_n (both N x M, ld N), titsias (N), and an M x M work matrix that
+// receives Kmm and then its factor. Returns a cudaError_t.
+int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
+                           const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork) {
+  dim3 g(div_up(N, 128), M);
+  k_knm<<<g, 128, 0, st>>>(N, N, M, Q, X, T, rho, Knm);
+  dim3 g2(div_up(M, 64), M);
+  k_kmm<<<g2, 64, 0, st>>>(M, Q, T, rho, Lwork, Lwork);
+  launch_chol_exact_raw(st, Lwork, M);
+  k_kinvkmn<<<div_up(N, 128), 128, 0, st>>>(N, N, M, Lwork, Knm, KinvKmn, titsias);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace gpl

@@ -43,6 +43,7 @@ extern "C" {
 #define GPL_ERR_NAN (-5)      /* NaN likelihood where the reference driver exits (ggplvm.cu:1182) */
 #define GPL_ERR_FORMAT (-6)   /* malformed input data (level code out of range, bad CSR offsets) */
 #define GPL_ERR_IO (-7)       /* file could not be read or written */
+#define GPL_ERR_LIMIT (-8)    /* size beyond a fixed limit of the allocation-free entry point */
 
 #define GPL_PREC_FP64 0       /* plain double precision: the drop-in path */
 #define GPL_PREC_BF16X3 1     /* Gram-family contractions on tensor cores, BF16 hi/lo split, FP32 accumulation */
@@ -161,6 +162,21 @@ GPL_API int gpl_profile_enable(gpl_ctx* ctx, int on);
 GPL_API int gpl_profile_reset(gpl_ctx* ctx);
 GPL_API int gpl_profile_read(gpl_ctx* ctx, const char* name, double* total_ms, int64_t* launches);
 GPL_API int gpl_launch_count(const gpl_ctx* ctx, int64_t* launches);
+
+/* Kernel matrices without any device allocation. This entry point has no counterpart in the
+ * reference; it serves callers that cannot allocate device memory: code enqueueing work while
+ * a stream is captured into a CUDA graph, real-time loops that forbid allocation after
+ * start-up, and plugins whose host framework owns all device memory. Every pointer is DEVICE
+ * memory owned by the caller: X (N x Q), T (M x Q), rho (Q) in, Knm (N x M, cell fastest),
+ * KinvKmn (N x M, cell fastest: the transpose of the reference's M x N buffer) and titsias (N)
+ * out, computed as gpl_kernel_mats computes them. The M x M work matrix lives in a fixed
+ * 512 KiB array inside the library (M <= GPL_NOALLOC_MAX_M, else GPL_ERR_LIMIT), shared by all
+ * calls on a device: calls that overlap on the GPU race, so serialise them. The first call on
+ * a device looks the array up (make it before any stream capture). stream: a cudaStream_t or
+ * NULL for the default stream; the call only enqueues work. */
+#define GPL_NOALLOC_MAX_M 256
+GPL_API int gpl_kernel_mats_noalloc(int N, int M, int Q, const double* X, const double* T, const double* rho,
+                                    double* Knm, double* KinvKmn, double* titsias, void* stream);
 
 /* Synchronises the context's stream. */
 GPL_API int gpl_sync(gpl_ctx* ctx);
