@@ -134,8 +134,8 @@ def flops_table(N, J, M, P, n_dense):
     return {
         # Gram: unique upper-triangle entries of the dense GP block (N*G*M*(M+1) flops)
         "gram": float(N) * J * M * (M + 1),
-        # gradient contraction over genes of S_j z_i, dense-model-matrix form: 2*N*J*P^2
-        "uq": 2.0 * N * J * P * P,
+        # gradient contraction over genes of S_j[DD] d_i over the n_d dense columns: 2*N*J*n_d^2
+        "uq": 2.0 * N * J * n_dense * n_dense,
     }
 
 
@@ -283,7 +283,7 @@ def run_ours(args):
     prof = {}
     for name in ("gram", "uq", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
                  "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
-                 "expand_delta", "chol_small"):
+                 "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk"):
         ms, n = m.profile_read(name)
         if n:
             prof[name] = (ms, n)
@@ -322,7 +322,7 @@ def run_ours(args):
         total_prof = sum(v[0] for v in prof.values())
         dom = max(prof, key=lambda k: prof[k][0])
         P = m.P
-        ft = flops_table(m.N, m.J, m.M, P, 0)
+        ft = flops_table(m.N, m.J, m.M, P, m.n_dense())
         peaks = measured_peaks()
         if dom in ft:
             f64 = fp64_peak_tflops(torch)

@@ -80,6 +80,14 @@ static int dalloc(Ctx* c, T** p, size_t n, const char* what) {
 }
 
 static void free_state(Ctx* c) {
+  void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
+                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d};
+  for (void* q : extra)
+    if (q) cudaFree(q);
+  c->Dm = c->gsum = c->gT = c->HK = nullptr;
+  c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
+  c->hk_tiles_d = nullptr;
+  c->n_grp = c->n_cv = 0;
   void* bufs[] = {c->Z,      c->W,      c->Nu,      c->Psi,     c->PsiInv, c->Beta,   c->tBeta,  c->scratch,
                   c->U,      c->Kmm,    c->Kinv,    c->KinvKmn, c->titsias, c->DeltaInv, c->Omega, c->delta,
                   c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
@@ -358,6 +366,81 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
       mv[k] = k - nh[j];
       mk[k] = j;
     }
+  const int J = c->J;
+  const size_t ldN = (size_t)((N + 31) / 32 * 32);
+  // variable data from the body (numeric: N x v doubles; categorical: N level codes)
+  const char* bp = (const char*)body;
+  std::vector<int64_t> voff(p, -1);
+  {
+    int64_t off = 0;
+    for (int j = 1; j < p - 1; j++) {
+      voff[j] = off;
+      off += (int64_t)N * vvv[j] * (vc[j] == 1 ? 8 : 4);
+    }
+  }
+  std::vector<int> catv;  // categorical variables (model variable index)
+  std::vector<std::vector<int32_t>> codes;
+  for (int j = 1; j < p - 1; j++) {
+    if (vc[j] == 1) continue;
+    std::vector<int32_t> cd(N);
+    memcpy(cd.data(), bp + voff[j], sizeof(int32_t) * N);
+    const int ncol = vc[j] * vvv[j];
+    for (int i = 0; i < N; i++)
+      if (cd[i] < 0 || cd[i] >= ncol) {
+        c->err = "categorical level code out of range in variable " + std::to_string(j);
+        return GPL_ERR_FORMAT;
+      }
+    catv.push_back(j);
+    codes.push_back(std::move(cd));
+  }
+  // cell groups: cells sorted (stably) by their tuple of levels; runs of equal tuples
+  std::vector<int32_t> order(N);
+  for (int i = 0; i < N; i++) order[i] = i;
+  const int ncat = (int)catv.size();
+  std::vector<int32_t> gstart, glev;
+  int n_grp = 0;
+  if (ncat > 0) {
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+      for (int v = 0; v < ncat; v++)
+        if (codes[v][a] != codes[v][b]) return codes[v][a] < codes[v][b];
+      return false;
+    });
+    for (int k = 0; k < N; k++) {
+      bool fresh = k == 0;
+      for (int v = 0; v < ncat && !fresh; v++) fresh = codes[v][order[k]] != codes[v][order[k - 1]];
+      if (fresh) {
+        gstart.push_back(k);
+        for (int v = 0; v < ncat; v++) glev.push_back(codes[v][order[k]]);
+      }
+    }
+    gstart.push_back(N);
+    n_grp = (int)gstart.size() - 1;
+  }
+  // dense columns: every numeric column; categorical one-hots too when grouping does not pay
+  int n_dense_est = 1 + M;
+  for (int j = 1; j < p - 1; j++)
+    if (vc[j] == 1) n_dense_est += vvv[j];
+  const double gsum_bytes = (double)J * n_grp * (n_dense_est + 1) * 8.0;
+  const bool grouped = ncat > 0 && n_grp <= 8192 && n_grp <= N / 4 + 1 && gsum_bytes <= 24e9;
+  std::vector<int> dcol;
+  for (int k = 0; k < P; k++)
+    if (mc[k] == 1 || !grouped) dcol.push_back(k);
+  const int n_d = (int)dcol.size();
+  std::vector<double> Dh(ldN * n_d, 0.0);
+  for (int a = 0; a < n_d; a++) {
+    const int k = dcol[a], j = mk[k];
+    double* dst = &Dh[(size_t)a * ldN];
+    if (j == 0) {
+      for (int i = 0; i < N; i++) dst[i] = 1.0;
+    } else if (j == p - 1) {
+      // Knm: written by the kernel-matrix step
+    } else if (vc[j] == 1) {
+      memcpy(dst, bp + voff[j] + (int64_t)mv[k] * N * 8, sizeof(double) * N);
+    } else {
+      const int v = (int)(std::find(catv.begin(), catv.end(), j) - catv.begin());
+      for (int i = 0; i < N; i++) dst[i] = codes[v][i] == mv[k] ? 1.0 : 0.0;
+    }
+  }
   free_state(c);
   c->M = M;
   c->Q = Q;
@@ -370,38 +453,28 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   c->mc = mc;
   c->mv = mv;
   c->mk = mk;
-  c->ldN = (N + 31) / 32 * 32;
-  const int J = c->J;
-  const size_t ldN = c->ldN;
-  // model matrix on the host: intercept, file variables, GP block left for getKernelMats
-  std::vector<double> Zh(ldN * P, 0.0);
-  for (int i = 0; i < N; i++) Zh[i] = 1.0;
-  const char* bp = (const char*)body;
-  int64_t off = 0;
-  for (int j = 1; j < p - 1; j++) {
-    const int64_t bytes = (int64_t)N * vvv[j] * (vc[j] == 1 ? 8 : 4);
-    if (vc[j] == 1) {
-      for (int m = 0; m < vvv[j]; m++) {
-        double* dst = &Zh[(size_t)(nh[j] + m) * ldN];
-        memcpy(dst, bp + off + (int64_t)m * N * 8, sizeof(double) * N);
-      }
-    } else {
-      std::vector<int32_t> codes(N);
-      memcpy(codes.data(), bp + off, sizeof(int32_t) * N);
-      const int ncol = vc[j] * vvv[j];
-      for (int i = 0; i < N; i++) {
-        if (codes[i] < 0 || codes[i] >= ncol) {
-          c->err = "categorical level code out of range in variable " + std::to_string(j);
-          return GPL_ERR_FORMAT;
-        }
-        Zh[(size_t)(nh[j] + codes[i]) * ldN + i] = 1.0;
-      }
+  c->ldN = (int)ldN;
+  c->dcol = dcol;
+  c->n_d = n_d;
+  c->dg0 = n_d - M;
+  c->n_cv = grouped ? ncat : 0;
+  c->n_grp = grouped ? n_grp : 0;
+  c->cv_nh.clear();
+  c->cv_nlev.clear();
+  if (grouped)
+    for (int v = 0; v < ncat; v++) {
+      c->cv_nh.push_back(nh[catv[v]]);
+      c->cv_nlev.push_back(vc[catv[v]] * vvv[catv[v]]);
     }
-    off += bytes;
-  }
+  std::vector<int2> tiles;
+  if (grouped)
+    for (int g = 0; g < n_grp; g++)
+      for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 64) tiles.push_back(make_int2(g, r0));
+  c->n_hk_tiles = (int)tiles.size();
   c->tot_max = tot_len(c, 1);
   const size_t scratch_n = std::max({ldN * (size_t)J, (size_t)J * P * P, (size_t)c->tot_max, (size_t)M * M});
-  GPL_RUN(dalloc(c, &c->Z, ldN * P, "Z"));
+  GPL_RUN(dalloc(c, &c->Dm, ldN * n_d, "dense model columns"));
+  GPL_RUN(dalloc(c, &c->dcol_d, (size_t)n_d, "dense column map"));
   GPL_RUN(dalloc(c, &c->W, ldN * (J + 1), "W"));
   GPL_RUN(dalloc(c, &c->Nu, ldN * J, "Nu"));
   GPL_RUN(dalloc(c, &c->Psi, (size_t)J * P * P, "Psi"));
@@ -411,7 +484,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->bvec, (size_t)P * J, "bvec"));
   GPL_RUN(dalloc(c, &c->sol, (size_t)P * J, "sol"));
   GPL_RUN(dalloc(c, &c->scratch, scratch_n, "scratch"));
-  GPL_RUN(dalloc(c, &c->U, ldN * P, "U"));
+  GPL_RUN(dalloc(c, &c->U, ldN * n_d, "U"));
   GPL_RUN(dalloc(c, &c->Kmm, (size_t)M * M, "Kmm"));
   GPL_RUN(dalloc(c, &c->Kinv, (size_t)M * M, "Kinv"));
   GPL_RUN(dalloc(c, &c->KmmInv, (size_t)M * M, "KmmInv"));
@@ -442,7 +515,29 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->mv_d, (size_t)P, "mv"));
   GPL_RUN(dalloc(c, &c->mk_d, (size_t)P, "mk"));
   GPL_RUN(dalloc(c, &c->nh_d, (size_t)p + 1, "nh"));
-  GPL_TRY(c, cudaMemcpy(c->Z, Zh.data(), sizeof(double) * ldN * P, cudaMemcpyHostToDevice));
+  if (c->n_grp) {
+    std::vector<int32_t> codes_h((size_t)ncat * ldN, 0);
+    for (int v = 0; v < ncat; v++) memcpy(&codes_h[(size_t)v * ldN], codes[v].data(), sizeof(int32_t) * N);
+    GPL_RUN(dalloc(c, &c->codes_d, codes_h.size(), "level codes"));
+    GPL_RUN(dalloc(c, &c->cv_nh_d, (size_t)ncat, "grouped variable columns"));
+    GPL_RUN(dalloc(c, &c->cv_nlev_d, (size_t)ncat, "grouped variable levels"));
+    GPL_RUN(dalloc(c, &c->glev_d, glev.size(), "group levels"));
+    GPL_RUN(dalloc(c, &c->gcells_d, (size_t)N, "group cells"));
+    GPL_RUN(dalloc(c, &c->gstart_d, gstart.size(), "group offsets"));
+    GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
+    GPL_RUN(dalloc(c, &c->gsum, (size_t)J * n_grp * (n_d + 1), "group sums"));
+    GPL_RUN(dalloc(c, &c->gT, (size_t)J * n_grp, "group response sums"));
+    GPL_RUN(dalloc(c, &c->HK, ldN * (n_d + 1), "HK"));
+    GPL_TRY(c, cudaMemcpy(c->codes_d, codes_h.data(), sizeof(int32_t) * codes_h.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->cv_nh_d, c->cv_nh.data(), sizeof(int) * ncat, cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->cv_nlev_d, c->cv_nlev.data(), sizeof(int) * ncat, cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->glev_d, glev.data(), sizeof(int32_t) * glev.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->gcells_d, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->hk_tiles_d, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+  }
+  GPL_TRY(c, cudaMemcpy(c->Dm, Dh.data(), sizeof(double) * ldN * n_d, cudaMemcpyHostToDevice));
+  GPL_TRY(c, cudaMemcpy(c->dcol_d, dcol.data(), sizeof(int) * n_d, cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->mc_d, mc.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->mv_d, mv.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->mk_d, mk.data(), sizeof(int) * P, cudaMemcpyHostToDevice));
@@ -454,6 +549,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_TRY(c, cudaMemset(c->PsiInv, 0, sizeof(double) * (size_t)J * P * P));
   GPL_TRY(c, cudaMemset(c->Beta, 0, sizeof(double) * (size_t)P * J));
   GPL_TRY(c, cudaMemset(c->tBeta, 0, sizeof(double) * (size_t)P * J));
+  GPL_TRY(c, cudaMemset(c->bvec, 0, sizeof(double) * (size_t)P * J));
   GPL_TRY(c, cudaMemset(c->ss, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
   GPL_TRY(c, cudaMemset(c->grad, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
   GPL_TRY(c, cudaMemset(c->grad0, 0, sizeof(double) * ((size_t)c->tot_max + Q)));
@@ -772,11 +868,11 @@ int gpl_get(gpl_ctx* h, const char* name, double* out, int64_t cap, int64_t* len
     }
     return GPL_OK;
   }
-  if (s == "Knm") return cols(c->Z + (size_t)g0 * ldN, M);
+  if (s == "Knm") return cols(c->Dm + (size_t)c->dg0 * ldN, M);
   if (s == "W") return cols(c->W, J + 1);
   if (s == "Nu") return cols(c->Nu, J);
   if (s == "C1") return cols(c->C1, M);
-  if (s == "Z") return cols(c->Z, P);
+  if (s == "Dm") return cols(c->Dm, (size_t)c->n_d);
   if (s == "KinvKmn") {  // reference layout M x N (k + i*M)
     if (len) *len = (int64_t)(M * N);
     if (!out) return GPL_OK;

@@ -2,8 +2,15 @@
 //
 // Device data layout (HBM), all double precision unless noted; ldN = N rounded up to a
 // multiple of 32 so every column starts on a 256-byte boundary:
-//   Z        ldN x P   column-major model matrix [1 | covariates | Knm]; the last M columns
-//                      are Knm (getKernelMats writes them in place, as the reference does)
+//   Dm       ldN x n_d the dense model-matrix columns, in model order: intercept, numeric
+//                      covariates, any categorical one-hots kept dense, and last the M Knm
+//                      columns (getKernelMats writes them in place, as the reference does);
+//                      dcol[a] is the model column of dense column a
+//   groups   categorical variables handled by groups: every cell belongs to the group of
+//            its combination of levels; gid (cell -> group), glev (group -> levels), the
+//            cells of each group (gcells, gstart) and per-variable level codes
+//   gsum     J x n_grp x (n_d + 1): per (gene, group) weighted sums of the dense columns
+//            (Gram) or, in the gradient, the categorical blocks of Psi^{-1}
 //   W        ldN x (J+1) gene-major weights; column J holds Oinvt (ggplvm.cu:292)
 //   Nu       ldN x J   working responses
 //   Psi      J x (P x P) per-gene Gram, full symmetric, then Cholesky factor in the lower
@@ -54,6 +61,17 @@ struct Ctx {
 
   // host copies of the model-matrix metadata (DataFrame.cu:96-134)
   std::vector<int> vc, vv, nh, mc, mv, mk;
+
+  // dense columns and categorical groups
+  int n_d = 0, dg0 = 0;             // dense columns; dense index of the first Knm column
+  std::vector<int> dcol;            // model column of each dense column (ascending)
+  int n_cv = 0, n_grp = 0;          // grouped categorical variables; groups
+  std::vector<int> cv_nh, cv_nlev;  // first model column and level count of each grouped variable
+  int *dcol_d = nullptr, *cv_nh_d = nullptr, *cv_nlev_d = nullptr, *gid_d = nullptr, *glev_d = nullptr;
+  int *gcells_d = nullptr, *gstart_d = nullptr, *codes_d = nullptr;
+  int2* hk_tiles_d = nullptr;       // (group, first row) of every 64-cell tile of the group lists
+  int n_hk_tiles = 0;
+  double *Dm = nullptr, *gsum = nullptr, *gT = nullptr, *HK = nullptr;
 
   // device buffers
   double *Z = nullptr, *W = nullptr, *Nu = nullptr, *Psi = nullptr, *PsiInv = nullptr;
@@ -120,6 +138,12 @@ inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 int launch_kernel_mats(Ctx* c);          // Knm into Z, Kmm, Kinv copy, chol(Kinv), KinvKmn, titsias
 int launch_expand_delta(Ctx* c);         // DeltaInv (upper + diag)
 int launch_chol_single(Ctx* c, double* A, int n);  // choldc on one n x n matrix
+// k_groups.cu
+int launch_group_sums(Ctx* c, int mode);  // 0: S (W/Omega); 1: S unweighted (gene 0); 2: T of y0; 3: T of nu
+int launch_assemble_psi(Ctx* c, int J);   // categorical rows/columns of Psi from the group sums
+int launch_assemble_b(Ctx* c);            // categorical entries of bvec from the group sums
+int launch_group_tables(Ctx* c);          // per (gene, group) categorical blocks of Psi^{-1}
+int launch_hk(Ctx* c);                    // HK[i] = sum_j O_ij [h_{j,g(i)} | kappa_{j,g(i)}]
 // k_gemm.cu
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response

@@ -1,14 +1,18 @@
 // Double-precision (cell x gene) contractions of the IRLS and the gradient, all built on
 // one register-tiled FP64 GEMM (64x64 output tile, 16-deep K chunks in shared memory,
-// 4x4 accumulators per thread) with element-wise prologues and epilogues:
+// 4x4 accumulators per thread) with element-wise prologues and epilogues. The model
+// matrix enters as its dense columns D (ldN x n_d) plus per-cell level codes of the grouped
+// categorical variables, so every product z_i . beta is D_i . beta[dcol] + the coefficients
+// of the cell's levels.
 //
-//   W / Nu     eta = Z beta_j for every cell and gene, then the getWForBeta epilogue
+//   W / Nu     eta = z_i . beta_j for every cell and gene, then the getWForBeta epilogue
 //              (ggplvm.cu:468-514). The counts of the tile's genes are scattered into
 //              shared memory first: each gene's matched prefix is sorted by cell, so a
-//              binary search finds the tile's slice. Bound: FP64 FMA (N*J*P).
-//   bvec       Z^T diag(W_j/Omega) nu_j (getZtOinvjnj, util_cuda.cu:462-487) and the GLM
-//              initialisation right-hand sides Z^T y0_j (initBeta, init.cu:193-221).
-//   E          Z tBeta (cell x gene predictions used by the Omega/X gradient).
+//              binary search finds the tile's slice. Bound: FP64 FMA (N*J*n_d).
+//   bvec       dense rows of Z^T diag(W_j/Omega) nu_j (getZtOinvjnj, util_cuda.cu:462-487)
+//              and of the GLM initialisation right-hand sides Z^T y0_j (initBeta,
+//              init.cu:193-221); the categorical rows come from the group sums.
+//   E          z_i . tBeta_j (cell x gene predictions used by the Omega/X gradient).
 //   C1 (part)  sum_j (tn_ij / phi_j) tBeta_j[GP] (ggplvm.cu:344).
 #include "gpl_internal.cuh"
 
@@ -19,23 +23,24 @@ constexpr int TM = 64, TN = 64, TK = 16;
 }
 
 // A(r, k) and B(k, c) loaders. kFastK: the K index is contiguous in memory (load K-fastest).
-struct LoadZ {  // A(r = cell, k = column) = Z[k*ldN + r]
+struct LoadD {  // A(r = cell, k = dense column) = D[k*ldN + r]
   static constexpr bool kFastK = false;
-  const double* Z;
-  int ldN, N, P;
-  __device__ double operator()(int r, int k) const { return (r < N && k < P) ? Z[(size_t)k * ldN + r] : 0.0; }
+  const double* D;
+  int ldN, N, n_d;
+  __device__ double operator()(int r, int k) const { return (r < N && k < n_d) ? D[(size_t)k * ldN + r] : 0.0; }
 };
-struct LoadZt {  // A(r = column, k = cell) = Z[r*ldN + k]
+struct LoadDt {  // A(r = dense column, k = cell) = D[r*ldN + k]
   static constexpr bool kFastK = true;
-  const double* Z;
-  int ldN, N, P;
-  __device__ double operator()(int r, int k) const { return (r < P && k < N) ? Z[(size_t)r * ldN + k] : 0.0; }
+  const double* D;
+  int ldN, N, n_d;
+  __device__ double operator()(int r, int k) const { return (r < n_d && k < N) ? D[(size_t)r * ldN + k] : 0.0; }
 };
-struct LoadColMajor {  // B(k, c) = B[k + c*ld]
+struct LoadBetaDense {  // B(k = dense column, c = gene) = B[dcol[k] + c*P]
   static constexpr bool kFastK = true;
   const double* B;
-  int ld, K, C;
-  __device__ double operator()(int k, int c) const { return (k < K && c < C) ? B[k + (size_t)c * ld] : 0.0; }
+  const int* dcol;
+  int P, n_d, J;
+  __device__ double operator()(int k, int c) const { return (k < n_d && c < J) ? B[dcol[k] + (size_t)c * P] : 0.0; }
 };
 struct LoadOinvNu {  // B(k = cell, c = gene) = W/Omega * Nu
   static constexpr bool kFastK = true;
@@ -114,8 +119,19 @@ __device__ __forceinline__ void gemm_tile(int m0, int n0, int K, const LA& A, co
   }
 }
 
+// z_i . B_j for a tile: the dense GEMM result plus the coefficients of the cell's levels
+__device__ __forceinline__ double add_levels(double dense, int i, int j, int ldN, int P, int n_cv,
+                                             const int* __restrict__ cv_nh, const int* __restrict__ codes,
+                                             const double* __restrict__ B) {
+  double s = dense;
+  for (int v = 0; v < n_cv; v++) s += B[cv_nh[v] + codes[(size_t)v * ldN + i] + (size_t)j * P];
+  return s;
+}
+
 // ---- W / Nu -----------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int pvars, const double* __restrict__ Z,
+__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int pvars, int n_d, int n_cv,
+                                              const double* __restrict__ D, const int* __restrict__ dcol,
+                                              const int* __restrict__ cv_nh, const int* __restrict__ codes,
                                               const double* __restrict__ Beta, const double* __restrict__ ls,
                                               const double* __restrict__ delta, const double* __restrict__ titsias,
                                               const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
@@ -129,7 +145,7 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
   unsigned char(*yf)[TM] = reinterpret_cast<unsigned char(*)[TM]>(raw + TN * (TM + 1) * sizeof(double));
   const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
   double acc[4][4];
-  gemm_tile(m0, n0, P, LoadZ{Z, ldN, N, P}, LoadColMajor{Beta, P, P, J}, acc, As, Bs);
+  gemm_tile(m0, n0, n_d, LoadD{D, ldN, N, n_d}, LoadBetaDense{Beta, dcol, P, n_d, J}, acc, As, Bs);
   // counts of this tile
   for (int e = threadIdx.x; e < TN * TM; e += 256) yf[e / TM][e % TM] = 0;
   __syncthreads();
@@ -161,7 +177,7 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
     for (int y = 0; y < 4; y++) {
       const int cc = ty + 16 * y, j = n0 + cc;
       if (j >= J) continue;
-      const double eta = acc[x][y];
+      const double eta = add_levels(acc[x][y], i, j, ldN, P, n_cv, cv_nh, codes, Beta);
       const double logW = eta + lls + tt;
       const double w = exp(eta) * lsi * exp(tt);
       double nu;
@@ -176,16 +192,49 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
 int launch_w_nu(Ctx* c) {
   ProfScope ps(c, "w_nu");
   dim3 g(div_up(c->N, TM), div_up(c->J, TN));
-  k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->p, c->Z, c->Beta, c->ls, c->delta, c->titsias,
-                                   c->cell, c->gptr, c->gvalid, c->cnt, c->W, c->Nu);
+  k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->p, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                   c->codes_d, c->Beta, c->ls, c->delta, c->titsias, c->cell, c->gptr, c->gvalid,
+                                   c->cnt, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
   return GPL_OK;
 }
 
-// ---- generic GEMM with plain column-major store -----------------------------------------
+// ---- E = z_i . B_j ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n_d, int n_cv,
+                                             const double* __restrict__ D, const int* __restrict__ dcol,
+                                             const int* __restrict__ cv_nh, const int* __restrict__ codes,
+                                             const double* __restrict__ B, double* __restrict__ out) {
+  __shared__ double As[TK][TM + 1];
+  __shared__ double Bs[TK][TN + 1];
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  double acc[4][4];
+  gemm_tile(m0, n0, n_d, LoadD{D, ldN, N, n_d}, LoadBetaDense{B, dcol, P, n_d, J}, acc, As, Bs);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int i = m0 + tx + 16 * x;
+    if (i >= N) continue;
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const int j = n0 + ty + 16 * y;
+      if (j < J) out[i + (size_t)j * ldN] = add_levels(acc[x][y], i, j, ldN, P, n_cv, cv_nh, codes, B);
+    }
+  }
+}
+
+int launch_zbeta(Ctx* c, const double* B, double* out) {
+  ProfScope ps(c, "zbeta");
+  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                  c->codes_d, B, out);
+  GPL_LAUNCHED(c, "k_eta");
+  return GPL_OK;
+}
+
+// ---- generic GEMM with a column-major store; rows optionally mapped ------------------------
 template <class LA, class LB>
 __global__ void __launch_bounds__(256) k_gemm_store(int m, int n, int K, LA A, LB B, double* __restrict__ out,
-                                                    int64_t ldo) {
+                                                    int64_t ldo, const int* __restrict__ rowmap) {
   __shared__ double As[TK][TM + 1];
   __shared__ double Bs[TK][TN + 1];
   const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
@@ -196,10 +245,11 @@ __global__ void __launch_bounds__(256) k_gemm_store(int m, int n, int K, LA A, L
   for (int x = 0; x < 4; x++) {
     const int r = m0 + tx + 16 * x;
     if (r >= m) continue;
+    const int orow = rowmap ? rowmap[r] : r;
 #pragma unroll
     for (int y = 0; y < 4; y++) {
       const int cc = n0 + ty + 16 * y;
-      if (cc < n) out[r + (size_t)cc * ldo] = acc[x][y];
+      if (cc < n) out[orow + (size_t)cc * ldo] = acc[x][y];
     }
   }
 }
@@ -233,28 +283,25 @@ int launch_init_response(Ctx* c) {
   return GPL_OK;
 }
 
+// Z^T u: dense rows by GEMM (mode 0: u = W/Omega nu; 1: u = y0), categorical rows from groups
 int launch_zt_u(Ctx* c, int mode) {
-  ProfScope ps(c, "zt_u");
-  dim3 g(div_up(c->P, TM), div_up(c->J, TN));
-  LoadZt A{c->Z, c->ldN, c->N, c->P};
-  if (mode == 0) {
-    k_gemm_store<<<g, 256, 0, c->stream>>>(c->P, c->J, c->N, A, LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J},
-                                           c->bvec, (int64_t)c->P);
-  } else {
-    k_gemm_store<<<g, 256, 0, c->stream>>>(c->P, c->J, c->N, A, LoadCellGene{c->scratch, c->ldN, c->N, c->J},
-                                           c->bvec, (int64_t)c->P);
+  {
+    ProfScope ps(c, "zt_u");
+    dim3 g(div_up(c->n_d, TM), div_up(c->J, TN));
+    LoadDt A{c->Dm, c->ldN, c->N, c->n_d};
+    if (mode == 0) {
+      k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
+                                             LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J}, c->bvec,
+                                             (int64_t)c->P, c->dcol_d);
+    } else {
+      k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A, LoadCellGene{c->scratch, c->ldN, c->N, c->J},
+                                             c->bvec, (int64_t)c->P, c->dcol_d);
+    }
+    GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
   }
-  GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
-  return GPL_OK;
-}
-
-int launch_zbeta(Ctx* c, const double* B, double* out) {
-  ProfScope ps(c, "zbeta");
-  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
-  k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->J, c->P, LoadZ{c->Z, c->ldN, c->N, c->P},
-                                         LoadColMajor{B, c->P, c->P, c->J}, out, (int64_t)c->ldN);
-  GPL_LAUNCHED(c, "k_gemm_store(zbeta)");
-  return GPL_OK;
+  int rc = launch_group_sums(c, mode == 0 ? 3 : 2);
+  if (rc) return rc;
+  return launch_assemble_b(c);
 }
 
 // C1 <- sum_j (tn_ij/phi_j) tBeta_j[GP]   (stored cell-fastest, ld ldN)
@@ -264,7 +311,8 @@ int launch_c1_tn(Ctx* c) {
   dim3 g(div_up(c->N, TM), div_up(c->M, TN));
   k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->M, c->J,
                                          LoadTn{c->W, c->Nu, c->scratch, c->Omega, c->phi, c->ldN, c->N, c->J},
-                                         LoadTBetaGP{c->tBeta, c->P, g0, c->M, c->J}, c->C1, (int64_t)c->ldN);
+                                         LoadTBetaGP{c->tBeta, c->P, g0, c->M, c->J}, c->C1, (int64_t)c->ldN,
+                                         (const int*)nullptr);
   GPL_LAUNCHED(c, "k_gemm_store(c1_tn)");
   return GPL_OK;
 }

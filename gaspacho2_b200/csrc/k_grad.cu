@@ -4,11 +4,11 @@
 //
 // The reference solves Psi_j z_i for every (cell, gene) pair (N*J solves of size P). Here
 // the explicit inverses S_j = Psi_j^{-1} are formed once per gene and the per-cell sums
-// over genes become one contraction:
-//     U[i, a] = sum_j O_ij (S_j z_i)_a = sum_{j,b} (O_ij z_ib) S_j[b, a],   O = W / Omega
-// which gives both sum_j O_ij z_i^T S_j z_i = z_i . U[i, :] and the GP rows of the C1
-// adjoint. k_uq runs it as an FP64 GEMM over the flattened (gene, column) index with the
-// left operand O_ij z_ib formed while loading. Bound: FP64 FMA, N*J*P^2.
+// over genes become one contraction over the dense columns d_i of z_i,
+//     A[i, a] = sum_j O_ij (S_j[DD] d_i)_a = sum_{j,b} (O_ij d_ib) S_j[b, a],   O = W / Omega
+// plus per-group terms for the categorical levels (k_groups.cu). k_uq runs A as an FP64
+// GEMM over the flattened (gene, dense column) index with the left operand O_ij d_ib formed
+// while loading. Bound: FP64 FMA, N*J*n_d^2.
 #include "gpl_internal.cuh"
 
 namespace gpl {
@@ -93,8 +93,9 @@ int launch_grad_delta(Ctx* c) {
   return GPL_OK;
 }
 
-// ---- U = sum_j O_ij S_j z_i ----------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_uq(int N, int ldN, int P, int Pp, int J, const double* __restrict__ Z,
+// ---- A = sum_j O_ij S_j[DD] d_i --------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_uq(int N, int ldN, int n_d, int n_dp, int P, int J,
+                                            const double* __restrict__ D, const int* __restrict__ dcol,
                                             const double* __restrict__ W, const double* __restrict__ Omega,
                                             const double* __restrict__ S, double* __restrict__ U) {
   __shared__ double As[TK][TM + 1];
@@ -108,14 +109,14 @@ __global__ void __launch_bounds__(256) k_uq(int N, int ldN, int P, int Pp, int J
     for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
   for (int j = 0; j < J; j++) {
     const double* Sj = S + (size_t)j * P * P;
-    for (int b0 = 0; b0 < Pp; b0 += TK) {
+    for (int b0 = 0; b0 < n_dp; b0 += TK) {
 #pragma unroll
       for (int t = 0; t < (TM * TK) / 256; t++) {
         const int e = tid + t * 256;
         const int r = e % TM, k = e / TM;
         const int i = m0 + r, b = b0 + k;
         double v = 0.0;
-        if (i < N && b < P) v = W[(size_t)j * ldN + i] / Omega[i] * Z[(size_t)b * ldN + i];
+        if (i < N && b < n_d) v = W[(size_t)j * ldN + i] / Omega[i] * D[(size_t)b * ldN + i];
         As[k][r] = v;
       }
 #pragma unroll
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(256) k_uq(int N, int ldN, int P, int Pp, int J
         const int e = tid + t * 256;
         const int k = e % TK, cc = e / TK;
         const int b = b0 + k, a = n0 + cc;
-        Bs[k][cc] = (b < P && a < P) ? Sj[b + (size_t)a * P] : 0.0;
+        Bs[k][cc] = (b < n_d && a < n_d) ? Sj[dcol[b] + (size_t)dcol[a] * P] : 0.0;
       }
       __syncthreads();
 #pragma unroll
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(256) k_uq(int N, int ldN, int P, int Pp, int J
 #pragma unroll
     for (int y = 0; y < 4; y++) {
       const int a = n0 + ty + 16 * y;
-      if (a < P) U[i + (size_t)a * ldN] = acc[x][y];
+      if (a < n_d) U[i + (size_t)a * ldN] = acc[x][y];
     }
   }
 }
@@ -170,20 +171,29 @@ __global__ void k_tn_sum(int N, int ldN, int J, const double* __restrict__ W, co
   out[i] = s;
 }
 
-// per-cell epilogue of getGradLogOmega (ggplvm.cu:352-374)
-__global__ void k_grad_omega_cell(int N, int ldN, int P, int J, int M, int Q, int pvars, int g0,
-                                  const double* __restrict__ Z, const double* __restrict__ U,
-                                  const double* __restrict__ tnsum, const double* __restrict__ W,
-                                  const double* __restrict__ Omega, const double* __restrict__ delta,
-                                  const double* __restrict__ titsias, const double* __restrict__ KinvKmn,
-                                  const double* __restrict__ X, const double* __restrict__ T,
-                                  const double* __restrict__ rho, double* __restrict__ C1, double* __restrict__ grad) {
+// per-cell epilogue of getGradLogOmega (ggplvm.cu:352-374). With A = U (dense rows of
+// sum_j O_ij S_j z_i without the level terms) and HK = [sum_j O_ij h_{j,g(i)} | sum_j O_ij
+// kappa_{j,g(i)}] (absent when no variable is grouped):
+//   sum_j O_ij z_i^T S_j z_i = d_i . (A_i + 2 H_i) + K_i,   sum_j O_ij (S_j z_i)_GP = A_i[GP] + H_i[GP]
+__global__ void k_grad_omega_cell(int N, int ldN, int n_d, int dg0, int J, int M, int Q, int pvars,
+                                  const double* __restrict__ D, const double* __restrict__ U,
+                                  const double* __restrict__ HK, const double* __restrict__ tnsum,
+                                  const double* __restrict__ W, const double* __restrict__ Omega,
+                                  const double* __restrict__ delta, const double* __restrict__ titsias,
+                                  const double* __restrict__ KinvKmn, const double* __restrict__ X,
+                                  const double* __restrict__ T, const double* __restrict__ rho,
+                                  double* __restrict__ C1, double* __restrict__ grad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double om = Omega[i];
   const double Oii = W[(size_t)J * ldN + i];
   double q = 0.0;
-  for (int a = 0; a < P; a++) q += Z[(size_t)a * ldN + i] * U[i + (size_t)a * ldN];
+  for (int a = 0; a < n_d; a++) {
+    double u = U[i + (size_t)a * ldN];
+    if (HK) u += 2.0 * HK[i + (size_t)a * ldN];
+    q += D[(size_t)a * ldN + i] * u;
+  }
+  if (HK) q += HK[i + (size_t)n_d * ldN];
   const double dgp = delta[pvars - 1];
   double sum = -((double)J) / om / 2.0 + q / om / 2.0 + tnsum[i];
   sum += kWt * dgp * Oii / om * titsias[i];
@@ -191,9 +201,11 @@ __global__ void k_grad_omega_cell(int N, int ldN, int P, int J, int M, int Q, in
   double* gX = grad + N + pvars;
   double ci1 = 0.0, g0x = 0.0;
   for (int k = 0; k < M; k++) {
-    double cik = C1[i + (size_t)k * ldN] - U[i + (size_t)(g0 + k) * ldN];
+    double v = U[i + (size_t)(dg0 + k) * ldN];
+    if (HK) v += HK[i + (size_t)(dg0 + k) * ldN];
+    double cik = C1[i + (size_t)k * ldN] - v;
     cik += kWt * dgp * Oii * KinvKmn[i + (size_t)k * ldN];
-    cik *= Z[(size_t)(g0 + k) * ldN + i];
+    cik *= D[(size_t)(dg0 + k) * ldN + i];
     C1[i + (size_t)k * ldN] = cik;
     ci1 += cik;
     const double t = (X[i] - T[k]) / 2.0;
@@ -220,15 +232,20 @@ int launch_grad_omega(Ctx* c) {
   if (rc) return rc;
   {
     ProfScope ps(c, "uq");
-    const int Pp = div_up(c->P, TK) * TK;
-    dim3 g(div_up(c->N, TM), div_up(c->P, TN));
-    k_uq<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, Pp, c->J, c->Z, c->W, c->Omega, c->PsiInv, c->U);
+    const int n_dp = div_up(c->n_d, TK) * TK;
+    dim3 g(div_up(c->N, TM), div_up(c->n_d, TN));
+    k_uq<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, n_dp, c->P, c->J, c->Dm, c->dcol_d, c->W, c->Omega,
+                                   c->PsiInv, c->U);
     GPL_LAUNCHED(c, "k_uq");
   }
+  rc = launch_group_tables(c);
+  if (rc) return rc;
+  rc = launch_hk(c);
+  if (rc) return rc;
   ProfScope ps(c, "grad_omega_cell");
   k_grad_omega_cell<<<div_up(c->N, 128), 128, 0, c->stream>>>(
-      c->N, c->ldN, c->P, c->J, c->M, c->Q, c->p, c->nh[c->p - 1], c->Z, c->U, c->red, c->W, c->Omega, c->delta,
-      c->titsias, c->KinvKmn, c->X, c->T, c->rho, c->C1, c->grad);
+      c->N, c->ldN, c->n_d, c->dg0, c->J, c->M, c->Q, c->p, c->Dm, c->U, c->n_grp ? c->HK : nullptr, c->red, c->W,
+      c->Omega, c->delta, c->titsias, c->KinvKmn, c->X, c->T, c->rho, c->C1, c->grad);
   GPL_LAUNCHED(c, "k_grad_omega_cell");
   return GPL_OK;
 }

@@ -2,7 +2,9 @@
 // cholPsi :683-692, cholDeltaInv :695-700, cholKmm kernel_funcs.cu:139-143, solvePsi
 // ggplvm.cu:46-53, choldc/cholsl chol.cu:19-97, initPsi init.cu:125-181).
 //
-//   k_gram      Psi_j = Z^T diag(W_j / Omega) Z + DeltaInv, all genes. A CTA owns a 32x32
+//   k_gram      dense x dense block of Psi_j = Z^T diag(W_j / Omega) Z + DeltaInv over the
+//               dense model columns (the categorical rows come from the group sums), all
+//               genes, scattered to the model-column positions. A CTA owns a 32x32
 //               block pair (upper triangle of blocks) for 8 genes and streams every cell:
 //               Z column blocks and the weights for a 32-cell chunk go to shared memory,
 //               each thread accumulates a 4x8 tile for one gene in registers.
@@ -25,10 +27,10 @@ constexpr int GG = 8;    // genes per CTA
 constexpr int GC = 32;   // cells per chunk
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_gram(int N, int ldN, int P, int J, const double* __restrict__ Z,
-                                              const double* __restrict__ W, const double* __restrict__ Omega,
-                                              const double* __restrict__ Dinv, double* __restrict__ Psi,
-                                              int unweighted) {
+__global__ void __launch_bounds__(256) k_gram(int N, int ldN, int n_d, int P, int J, const double* __restrict__ Z,
+                                              const int* __restrict__ dcol, const double* __restrict__ W,
+                                              const double* __restrict__ Omega, const double* __restrict__ Dinv,
+                                              double* __restrict__ Psi, int unweighted) {
   __shared__ double sk[GC][GB + 1];
   __shared__ double sl[GC][GB + 1];
   __shared__ double sw[GC][GG];
@@ -53,8 +55,8 @@ __global__ void __launch_bounds__(256) k_gram(int N, int ldN, int P, int J, cons
       const int r = e & (GC - 1), col = e >> 5;
       const int i = i0 + r;
       const int ck = kb + col, cl = lb + col;
-      sk[r][col] = (i < N && ck < P) ? Z[(size_t)ck * ldN + i] : 0.0;
-      sl[r][col] = (i < N && cl < P) ? Z[(size_t)cl * ldN + i] : 0.0;
+      sk[r][col] = (i < N && ck < n_d) ? Z[(size_t)ck * ldN + i] : 0.0;
+      sl[r][col] = (i < N && cl < n_d) ? Z[(size_t)cl * ldN + i] : 0.0;
     }
     {
       const int r = tid & (GC - 1), gg = tid >> 5;
@@ -85,14 +87,15 @@ __global__ void __launch_bounds__(256) k_gram(int N, int ldN, int P, int J, cons
 #pragma unroll
   for (int x = 0; x < 4; x++) {
     const int k = kb + kq * 4 + x;
-    if (k >= P) continue;
+    if (k >= n_d) continue;
 #pragma unroll
     for (int y = 0; y < 8; y++) {
       const int l = lb + lq * 8 + y;
-      if (l >= P || k > l) continue;
-      const double v = acc[x][y] + Dinv[k + (size_t)l * P];
-      Pj[k + (size_t)l * P] = v;
-      Pj[l + (size_t)k * P] = v;
+      if (l >= n_d || k > l) continue;
+      const size_t mk = dcol[k], ml = dcol[l];  // model columns, mk <= ml
+      const double v = acc[x][y] + Dinv[mk + ml * P];
+      Pj[mk + ml * P] = v;
+      Pj[ml + mk * P] = v;
     }
   }
 }
@@ -251,15 +254,19 @@ __global__ void k_lauum(const double* __restrict__ Vrm, int n, int64_t stride, d
 }
 
 int launch_gram(Ctx* c, bool unweighted) {
-  const int nb = div_up(c->P, GB);
+  const int nb = div_up(c->n_d, GB);
   const int npairs = nb * (nb + 1) / 2;
   const int J = unweighted ? 1 : c->J;
-  ProfScope ps(c, "gram");
-  dim3 g(npairs, div_up(J, GG));
-  k_gram<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, J, c->Z, c->W, c->Omega, c->DeltaInv, c->Psi,
-                                   unweighted ? 1 : 0);
-  GPL_LAUNCHED(c, "k_gram");
-  return GPL_OK;
+  {
+    ProfScope ps(c, "gram");
+    dim3 g(npairs, div_up(J, GG));
+    k_gram<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, c->P, J, c->Dm, c->dcol_d, c->W, c->Omega, c->DeltaInv,
+                                     c->Psi, unweighted ? 1 : 0);
+    GPL_LAUNCHED(c, "k_gram");
+  }
+  int rc = launch_group_sums(c, unweighted ? 1 : 0);
+  if (rc) return rc;
+  return launch_assemble_psi(c, J);
 }
 
 int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride) {

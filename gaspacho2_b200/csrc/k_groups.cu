@@ -1,0 +1,346 @@
+// Categorical covariates through cell groups.
+//
+// A categorical variable contributes one-hot columns to the model matrix (getModelMatrix,
+// DataFrame.cu:72-82), and the reference's Gram treats them case by case
+// (ggplvm.cu:628-674): level x numeric sums, level x level co-occurrence sums. Here every
+// cell belongs to the group of its combination of levels (400 groups for batch x donor at
+// config 2), and everything categorical reduces to per-(gene, group) sums over the cells of
+// a group:
+//
+//   S[j][g][a] = sum_{i in g} w_ij D[i, a]       (dense column a; a = intercept gives sum w)
+//   T[j][g]    = sum_{i in g} w_ij u_ij          (u = nu for Z^T diag(w) nu, y0 for initBeta)
+//
+// from which the categorical rows of Psi_j and of Z^T diag(w) nu are assembled exactly as the
+// reference's case analysis defines them. In the gradient the same layout holds the
+// categorical blocks of Psi_j^{-1} seen by each group:
+//
+//   h[j][g][a] = sum_{c in cats(g)} S_j[dcol[a], c],  kappa[j][g] = sum_{c,c' in cats(g)} S_j[c, c']
+//
+// so that z_i^T S_j z_i = d_i^T S_DD d_i + 2 d_i . h + kappa for a cell of group g.
+// The group sums and HK are FP64 GEMMs over the gathered cells of one group (the shared
+// register-tiled tile of k_gemm.cu's scheme), N*J*n_d multiply-adds each.
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+namespace {
+constexpr int TM = 64, TN = 64, TK = 16;
+}
+
+// C[r, c] over K = gathered cells of group g: A(r = gene, k) = w(cell_k, gene), B(k, c = a) = D[a, cell_k]
+template <int MODE>
+__global__ void __launch_bounds__(256) k_group_sums(int N, int ldN, int J, int n_d, int n_grp,
+                                                    const int* __restrict__ gcells, const int* __restrict__ gstart,
+                                                    const double* __restrict__ W, const double* __restrict__ Omega,
+                                                    const double* __restrict__ D, double* __restrict__ S) {
+  __shared__ double As[TK][TM + 1];
+  __shared__ double Bs[TK][TN + 1];
+  const int g = blockIdx.z;
+  const int j0 = blockIdx.x * TM, a0 = blockIdx.y * TN;
+  const int c0 = gstart[g], nc = gstart[g + 1] - c0;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+  for (int k0 = 0; k0 < nc; k0 += TK) {
+#pragma unroll
+    for (int t = 0; t < (TM * TK) / 256; t++) {  // A: k fastest over cells
+      const int e = tid + t * 256;
+      const int k = e % TK, r = e / TK;
+      const int j = j0 + r;
+      double v = 0.0;
+      if (k0 + k < nc && j < J) {
+        const int i = gcells[c0 + k0 + k];
+        v = MODE == 0 ? W[(size_t)j * ldN + i] / Omega[i] : 1.0;
+      }
+      As[k][r] = v;
+    }
+#pragma unroll
+    for (int t = 0; t < (TN * TK) / 256; t++) {  // B: k fastest (cells of one dense column)
+      const int e = tid + t * 256;
+      const int k = e % TK, cc = e / TK;
+      const int a = a0 + cc;
+      double v = 0.0;
+      if (k0 + k < nc && a < n_d) v = D[(size_t)a * ldN + gcells[c0 + k0 + k]];
+      Bs[k][cc] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TK; k++) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int x = 0; x < 4; x++) av[x] = As[k][tx + 16 * x];
+#pragma unroll
+      for (int y = 0; y < 4; y++) bv[y] = Bs[k][ty + 16 * y];
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+    }
+    __syncthreads();
+  }
+  const int ld = n_d + 1;
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int j = j0 + tx + 16 * x;
+    if (j >= J) continue;
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const int a = a0 + ty + 16 * y;
+      if (a < n_d) S[((size_t)j * n_grp + g) * ld + a] = acc[x][y];
+    }
+  }
+}
+
+// T[j][g] = sum_{i in g} w_ij u_ij, one warp per (gene, group); mode 0: w = W/Omega, u = nu;
+// mode 2: w = 1, u = y0 (scratch).
+template <int MODE>
+__global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gcells, const int* __restrict__ gstart,
+                          const double* __restrict__ W, const double* __restrict__ Omega,
+                          const double* __restrict__ U, double* __restrict__ T) {
+  const int g = blockIdx.x;
+  const int j = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= J) return;
+  const int c0 = gstart[g], c1 = gstart[g + 1];
+  double s = 0.0;
+  for (int k = c0 + lane; k < c1; k += 32) {
+    const int i = gcells[k];
+    const size_t e = (size_t)j * ldN + i;
+    s += MODE == 0 ? W[e] / Omega[i] * U[e] : U[e];
+  }
+  s = warp_sum(s);
+  if (lane == 0) T[(size_t)j * n_grp + g] = s;
+}
+
+// mode 0: S with w = W/Omega (Gram of the objective and the IRLS); 1: S of gene 0 with w = 1
+// (GLM initialisation Gram); 2: T with w = 1, u = y0 (GLM initialisation right-hand side);
+// 3: T with w = W/Omega, u = nu (Z^T diag(W/Omega) nu).
+int launch_group_sums(Ctx* c, int mode) {
+  if (c->n_grp == 0) return GPL_OK;
+  ProfScope ps(c, "group_sums");
+  if (mode == 0 || mode == 1) {
+    const int J = mode == 1 ? 1 : c->J;
+    dim3 g(div_up(J, TM), div_up(c->n_d, TN), c->n_grp);
+    if (mode == 0)
+      k_group_sums<0><<<g, 256, 0, c->stream>>>(c->N, c->ldN, J, c->n_d, c->n_grp, c->gcells_d, c->gstart_d, c->W,
+                                                c->Omega, c->Dm, c->gsum);
+    else
+      k_group_sums<1><<<g, 256, 0, c->stream>>>(c->N, c->ldN, J, c->n_d, c->n_grp, c->gcells_d, c->gstart_d, c->W,
+                                                c->Omega, c->Dm, c->gsum);
+    GPL_LAUNCHED(c, "k_group_sums");
+  }
+  if (mode == 2 || mode == 3) {
+    dim3 g(c->n_grp, div_up(c->J, 8));
+    if (mode == 2)
+      k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+                                             c->scratch, c->gT);
+    else
+      k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega, c->Nu,
+                                             c->gT);
+    GPL_LAUNCHED(c, "k_group_t");
+  }
+  return GPL_OK;
+}
+
+// Categorical rows and columns of Psi_j (both triangles) from the group sums, plus the
+// prior's diagonal on them; the dense x dense entries are written by the Gram kernel.
+__global__ void __launch_bounds__(256) k_assemble_psi(int P, int n_d, int n_cv, int n_grp,
+                                                      const int* __restrict__ dcol, const int* __restrict__ cv_nh,
+                                                      const int* __restrict__ cv_nlev, const int* __restrict__ glev,
+                                                      const double* __restrict__ S, const double* __restrict__ Dinv,
+                                                      double* __restrict__ Psi) {
+  const int j = blockIdx.x;
+  double* Pj = Psi + (size_t)j * P * P;
+  const double* Sj = S + (size_t)j * n_grp * (n_d + 1);
+  // zero every row and column of a grouped categorical variable
+  for (int v = 0; v < n_cv; v++)
+    for (int e = threadIdx.x; e < cv_nlev[v] * P; e += blockDim.x) {
+      const int cidx = cv_nh[v] + e / P, r = e % P;
+      Pj[cidx + (size_t)r * P] = 0.0;
+      Pj[r + (size_t)cidx * P] = 0.0;
+    }
+  __syncthreads();
+  // level x dense column: thread owns dense column a
+  for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
+    const size_t col = (size_t)dcol[a] * P;
+    for (int g = 0; g < n_grp; g++) {
+      const double s = Sj[(size_t)g * (n_d + 1) + a];
+      for (int v = 0; v < n_cv; v++) Pj[cv_nh[v] + glev[g * n_cv + v] + col] += s;
+    }
+  }
+  // level x level (different variables) and the diagonal: one thread, groups in order
+  if (threadIdx.x == 0) {
+    for (int g = 0; g < n_grp; g++) {
+      const double s = Sj[(size_t)g * (n_d + 1) + 0];  // dense column 0 is the intercept: sum w
+      for (int v = 0; v < n_cv; v++) {
+        const int cv = cv_nh[v] + glev[g * n_cv + v];
+        Pj[cv + (size_t)cv * P] += s;
+        for (int v2 = v + 1; v2 < n_cv; v2++) Pj[cv + (size_t)(cv_nh[v2] + glev[g * n_cv + v2]) * P] += s;
+      }
+    }
+    for (int v = 0; v < n_cv; v++)
+      for (int L = 0; L < cv_nlev[v]; L++) {
+        const int cc = cv_nh[v] + L;
+        Pj[cc + (size_t)cc * P] += Dinv[cc + (size_t)cc * P];
+      }
+  }
+  __syncthreads();
+  // mirror: (dense column, level) and (level, later variable's level)
+  for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
+    const int dc = dcol[a];
+    for (int v = 0; v < n_cv; v++)
+      for (int L = 0; L < cv_nlev[v]; L++) {
+        const int cc = cv_nh[v] + L;
+        Pj[dc + (size_t)cc * P] = Pj[cc + (size_t)dc * P];
+      }
+  }
+  for (int v = 0; v < n_cv; v++)
+    for (int v2 = v + 1; v2 < n_cv; v2++)
+      for (int e = threadIdx.x; e < cv_nlev[v] * cv_nlev[v2]; e += blockDim.x) {
+        const int c1 = cv_nh[v] + e / cv_nlev[v2], c2 = cv_nh[v2] + e % cv_nlev[v2];
+        Pj[c2 + (size_t)c1 * P] = Pj[c1 + (size_t)c2 * P];
+      }
+}
+
+int launch_assemble_psi(Ctx* c, int J) {
+  if (c->n_grp == 0) return GPL_OK;
+  ProfScope ps(c, "assemble_psi");
+  k_assemble_psi<<<J, 256, 0, c->stream>>>(c->P, c->n_d, c->n_cv, c->n_grp, c->dcol_d, c->cv_nh_d, c->cv_nlev_d,
+                                           c->glev_d, c->gsum, c->DeltaInv, c->Psi);
+  GPL_LAUNCHED(c, "k_assemble_psi");
+  return GPL_OK;
+}
+
+// Categorical entries of bvec (P x J): sum over the groups at each level of T[j][g].
+__global__ void k_assemble_b(int P, int J, int n_cv, int n_grp, const int* __restrict__ cv_nh,
+                             const int* __restrict__ cv_nlev, const int* __restrict__ glev,
+                             const double* __restrict__ T, double* __restrict__ b) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= J) return;
+  double* bj = b + (size_t)j * P;
+  for (int v = 0; v < n_cv; v++)
+    for (int L = 0; L < cv_nlev[v]; L++) bj[cv_nh[v] + L] = 0.0;
+  for (int g = 0; g < n_grp; g++) {
+    const double t = T[(size_t)j * n_grp + g];
+    for (int v = 0; v < n_cv; v++) bj[cv_nh[v] + glev[g * n_cv + v]] += t;
+  }
+}
+
+int launch_assemble_b(Ctx* c) {
+  if (c->n_grp == 0) return GPL_OK;
+  ProfScope ps(c, "assemble_b");
+  k_assemble_b<<<div_up(c->J, 128), 128, 0, c->stream>>>(c->P, c->J, c->n_cv, c->n_grp, c->cv_nh_d, c->cv_nlev_d,
+                                                         c->glev_d, c->gT, c->bvec);
+  GPL_LAUNCHED(c, "k_assemble_b");
+  return GPL_OK;
+}
+
+// h and kappa per (gene, group) from Psi_j^{-1}
+__global__ void k_group_tables(int P, int n_d, int n_cv, int n_grp, const int* __restrict__ dcol,
+                               const int* __restrict__ cv_nh, const int* __restrict__ glev,
+                               const double* __restrict__ S, double* __restrict__ tab) {
+  const int j = blockIdx.x;
+  const double* Sj = S + (size_t)j * P * P;
+  const int ld = n_d + 1;
+  double* tj = tab + (size_t)j * n_grp * ld;
+  for (int e = threadIdx.x; e < n_grp * ld; e += blockDim.x) {
+    const int g = e / ld, a = e % ld;
+    const int* lv = glev + g * n_cv;
+    double s = 0.0;
+    if (a < n_d) {
+      const size_t r = dcol[a];
+      for (int v = 0; v < n_cv; v++) s += Sj[r + (size_t)(cv_nh[v] + lv[v]) * P];
+    } else {
+      for (int v = 0; v < n_cv; v++)
+        for (int v2 = 0; v2 < n_cv; v2++) s += Sj[(cv_nh[v] + lv[v]) + (size_t)(cv_nh[v2] + lv[v2]) * P];
+    }
+    tj[e] = s;
+  }
+}
+
+int launch_group_tables(Ctx* c) {
+  if (c->n_grp == 0) return GPL_OK;
+  ProfScope ps(c, "group_tables");
+  k_group_tables<<<c->J, 256, 0, c->stream>>>(c->P, c->n_d, c->n_cv, c->n_grp, c->dcol_d, c->cv_nh_d, c->glev_d,
+                                              c->PsiInv, c->gsum);
+  GPL_LAUNCHED(c, "k_group_tables");
+  return GPL_OK;
+}
+
+// HK[i, a] = sum_j O_ij tab[j][g(i)][a] over the gathered cells of each group (a <= n_d)
+__global__ void __launch_bounds__(256) k_hk(int ldN, int J, int n_d, int n_grp, const int2* __restrict__ tiles,
+                                            const int* __restrict__ gcells, const int* __restrict__ gstart,
+                                            const double* __restrict__ W, const double* __restrict__ Omega,
+                                            const double* __restrict__ tab, double* __restrict__ HK) {
+  __shared__ double As[TK][TM + 1];
+  __shared__ double Bs[TK][TN + 1];
+  __shared__ int cells[TM];
+  const int2 t2 = tiles[blockIdx.x];
+  const int g = t2.x, r0 = t2.y;
+  const int a0 = blockIdx.y * TN;
+  const int c0 = gstart[g], nc = gstart[g + 1] - c0;
+  const int ld = n_d + 1;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  if (tid < TM) cells[tid] = (r0 + tid < nc) ? gcells[c0 + r0 + tid] : -1;
+  __syncthreads();
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+  for (int k0 = 0; k0 < J; k0 += TK) {
+#pragma unroll
+    for (int t = 0; t < (TM * TK) / 256; t++) {
+      const int e = tid + t * 256;
+      const int r = e % TM, k = e / TM;
+      const int i = cells[r], j = k0 + k;
+      As[k][r] = (i >= 0 && j < J) ? W[(size_t)j * ldN + i] / Omega[i] : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < (TN * TK) / 256; t++) {
+      const int e = tid + t * 256;
+      const int cc = e % TN, k = e / TN;
+      const int a = a0 + cc, j = k0 + k;
+      Bs[k][cc] = (a < ld && j < J) ? tab[((size_t)j * n_grp + g) * ld + a] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TK; k++) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int x = 0; x < 4; x++) av[x] = As[k][tx + 16 * x];
+#pragma unroll
+      for (int y = 0; y < 4; y++) bv[y] = Bs[k][ty + 16 * y];
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int i = cells[tx + 16 * x];
+    if (i < 0) continue;
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+      const int a = a0 + ty + 16 * y;
+      if (a < ld) HK[i + (size_t)a * ldN] = acc[x][y];
+    }
+  }
+}
+
+int launch_hk(Ctx* c) {
+  if (c->n_grp == 0) return GPL_OK;
+  ProfScope ps(c, "hk");
+  dim3 g(c->n_hk_tiles, div_up(c->n_d + 1, TN));
+  k_hk<<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_d, c->n_grp, c->hk_tiles_d, c->gcells_d, c->gstart_d, c->W,
+                                 c->Omega, c->gsum, c->HK);
+  GPL_LAUNCHED(c, "k_hk");
+  return GPL_OK;
+}
+
+}  // namespace gpl

@@ -88,8 +88,7 @@ __global__ void k_expand(int P, int p, int g0, int M, const int* __restrict__ mk
 }
 
 int launch_kernel_mats(Ctx* c) {
-  const int g0 = c->nh[c->p - 1];
-  double* Knm = c->Z + (size_t)g0 * c->ldN;
+  double* Knm = c->Dm + (size_t)c->dg0 * c->ldN;
   {
     ProfScope ps(c, "kernel_mats");
     dim3 g(div_up(c->N, 128), c->M);

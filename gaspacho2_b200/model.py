@@ -172,6 +172,12 @@ class GPLVM:
         self._c(self._L.gpl_get(self.h, name.encode(), _d(out), n.value, ctypes.byref(n)), f"gpl_get({name})")
         return out
 
+    def n_dense(self) -> int:
+        """Number of dense model columns (intercept, numerics, one-hots kept dense, Knm)."""
+        n = ctypes.c_int64()
+        self._c(self._L.gpl_get(self.h, b"Dm", None, 0, ctypes.byref(n)), "gpl_get(Dm)")
+        return n.value // self.N
+
     def params_vector(self) -> np.ndarray:
         return np.concatenate([self.get(k) for k in ("Omega", "delta", "X", "T", "rho")])
 
