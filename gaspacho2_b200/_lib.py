@@ -37,6 +37,7 @@ SIGNATURES = {
     "gpl_kernel_mats": (ctypes.c_int, [_vp]),
     "gpl_glm_init": (ctypes.c_int, [_vp]),
     "gpl_expand_delta": (ctypes.c_int, [_vp]),
+    "gpl_gram": (ctypes.c_int, [_vp]),
     "gpl_irls_sweep": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "gpl_irls": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "gpl_objective_after_irls": (ctypes.c_int, [_vp, _dp]),

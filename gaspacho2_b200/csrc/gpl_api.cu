@@ -1,6 +1,7 @@
 // C ABI of libgpl_b200: context management, data loading and the phase drivers that follow
 // the reference driver's call order (ggplvm.cu:951-1354). See include/gpl.h.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -80,6 +81,7 @@ static int dalloc(Ctx* c, T** p, size_t n, const char* what) {
 }
 
 static void free_state(Ctx* c) {
+  tc_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
                    c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d};
   for (void* q : extra)
@@ -134,6 +136,7 @@ static int read_slot(Ctx* c, int slot, double* out) {
   double v = 0.0;
   GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + slot, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  GPL_RUN(tc_error_flag(c));
   c->lkhd[slot] = v;
   if (out) *out = v;
   return GPL_OK;
@@ -274,6 +277,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
     return GPL_ERR_ARG;
   }
   c->precision = precision;
+  c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
   return GPL_OK;
 }
 
@@ -654,6 +658,14 @@ int gpl_glm_init(gpl_ctx* h) {
   return GPL_OK;
 }
 
+int gpl_gram(gpl_ctx* h) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  GPL_RUN(launch_gram(c, false));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  return tc_error_flag(c);
+}
+
 int gpl_expand_delta(gpl_ctx* h) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));
@@ -697,7 +709,7 @@ int gpl_gradient(gpl_ctx* h, double* grad) {
     GPL_TRY(c, cudaMemcpyAsync(grad, c->grad, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
     GPL_TRY(c, cudaStreamSynchronize(c->stream));
   }
-  return GPL_OK;
+  return tc_error_flag(c);
 }
 
 int gpl_lbfgs_update(gpl_ctx* h, int jtr, int rhoflag) {
@@ -800,7 +812,7 @@ int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkh
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
   c->lkhd[1] = v;
   if (lkhd) *lkhd = v;
-  return GPL_OK;
+  return tc_error_flag(c);
 }
 
 int gpl_evaluate_device(gpl_ctx* h) {
@@ -923,7 +935,7 @@ int gpl_launch_count(const gpl_ctx* h, int64_t* launches) {
 int gpl_sync(gpl_ctx* h) {
   Ctx* c = C(h);
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
-  return GPL_OK;
+  return tc_error_flag(c);
 }
 
 }  // extern "C"

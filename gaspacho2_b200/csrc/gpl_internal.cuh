@@ -22,6 +22,8 @@
 //   counts   CSR (int32 cells, int64 offsets, double values) + per-gene valid prefix length
 #pragma once
 
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -44,6 +46,22 @@ struct Ctx;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+};
+
+// Operands, partial sums and TMA descriptors of the tensor-core contractions (k_tc.cu).
+struct TcState {
+  bool ready = false, check_each = false;
+  int n_dp = 0, cpad = 0, chunks_cells = 0, gram_tiles_n = 0;
+  int n_pairs = 0, pair_tiles = 0;
+  int n_b = 0, grad_chunks = 0, grad_chunks_per_split = 0, grad_splits = 0;
+  int64_t Kpad = 0;
+  int smem_gram = 0, smem_grad = 0;
+  __nv_bfloat16 *whi = nullptr, *wlo = nullptr, *bhi = nullptr, *blo = nullptr;
+  float* Dt = nullptr;
+  double* Up = nullptr;
+  int2* pairs = nullptr;
+  int* err = nullptr;
+  CUtensorMap map_whi, map_wlo, map_bhi, map_blo;
 };
 
 struct Ctx {
@@ -94,6 +112,8 @@ struct Ctx {
 
   // host mirror of the objective trace (lkhd_d in the reference, ggplvm.cu:1052)
   std::vector<double> lkhd;
+
+  TcState tc;
 
   // profiling
   bool prof = false;
@@ -161,6 +181,11 @@ int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // chols
 void launch_chol_exact_raw(cudaStream_t st, double* A, int n);
 int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
                            const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork);
+// k_tc.cu (precision form)
+int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
+int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
+int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting
+void tc_release(Ctx* c);
 // k_lkhd.cu
 int launch_oinvt(Ctx* c);
 int launch_beta_phi(Ctx* c, int jtr);

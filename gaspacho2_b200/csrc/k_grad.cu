@@ -230,7 +230,10 @@ int launch_grad_omega(Ctx* c) {
   }
   rc = launch_c1_tn(c);  // C1 = sum_j tn/phi tBeta_GP
   if (rc) return rc;
-  {
+  if (c->precision == GPL_PREC_BF16X3) {
+    rc = launch_tc_grad(c);
+    if (rc) return rc;
+  } else {
     ProfScope ps(c, "uq");
     const int n_dp = div_up(c->n_d, TK) * TK;
     dim3 g(div_up(c->N, TM), div_up(c->n_d, TN));

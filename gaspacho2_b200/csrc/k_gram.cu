@@ -257,7 +257,10 @@ int launch_gram(Ctx* c, bool unweighted) {
   const int nb = div_up(c->n_d, GB);
   const int npairs = nb * (nb + 1) / 2;
   const int J = unweighted ? 1 : c->J;
-  {
+  if (!unweighted && c->precision == GPL_PREC_BF16X3) {
+    int rc = launch_tc_gram(c);
+    if (rc) return rc;
+  } else {
     ProfScope ps(c, "gram");
     dim3 g(npairs, div_up(J, GG));
     k_gram<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, c->P, J, c->Dm, c->dcol_d, c->W, c->Omega, c->DeltaInv,

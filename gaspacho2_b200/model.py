@@ -102,6 +102,10 @@ class GPLVM:
     def glm_init(self):
         self._c(self._L.gpl_glm_init(self.h), "gpl_glm_init")
 
+    def gram(self):
+        """getPsi alone: every gene's Gram at the current W, Omega and DeltaInv (no factorization)."""
+        self._c(self._L.gpl_gram(self.h), "gpl_gram")
+
     def expand_delta(self):
         self._c(self._L.gpl_expand_delta(self.h), "gpl_expand_delta")
 

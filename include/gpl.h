@@ -103,6 +103,10 @@ GPL_API int gpl_kernel_mats(gpl_ctx* ctx);
 /* expandDelta_k + initPsi + initPsi2 + initBeta (ggplvm.cu:1134-1137, init.cu:125-221). */
 GPL_API int gpl_glm_init(gpl_ctx* ctx);
 
+/* getPsi alone (ggplvm.cu:621-680): every gene's Gram Z^T diag(W_j/Omega) Z + DeltaInv at the
+ * current W, Omega and DeltaInv, both triangles, before any factorization. */
+GPL_API int gpl_gram(gpl_ctx* ctx);
+
 /* expandDelta_k alone (util_cuda.cu:249-269). */
 GPL_API int gpl_expand_delta(gpl_ctx* ctx);
 
