@@ -210,6 +210,48 @@ static int gradient_launch(Ctx* c) {
   return GPL_OK;
 }
 
+// One outer iteration `itr` of the driver (ggplvm.cu:1146-1330): IRLS to convergence
+// (JTRMAX 200 on the first iteration, 100 after), the objective, then L-BFGS steps with the
+// backtracking line search (rhoflag once itr > 20; a 10000-step limit on itr 30), and the
+// beta revival. lbfgs_budget > 0 caps the L-BFGS steps of this call. st = IRLS sweeps,
+// L-BFGS steps, objective evaluations, trace entries written.
+static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* trace, int trace_cap) {
+  int JTRMAX = (itr == 0) ? 200 : 100;
+  int n = 0, ntrace = 0;
+  int rc = irls(c, JTRMAX, &n);
+  st[0] = n;
+  if (rc) return rc;
+  double l0 = 0.0;
+  GPL_RUN(objective_after_irls(c, &l0));
+  st[2]++;
+  if (trace && ntrace < trace_cap) trace[ntrace++] = l0;
+  const int rhoflag = itr > 20 ? 1 : 0;
+  if (itr == 30) JTRMAX = 10000;
+  for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
+    GPL_RUN(gradient_launch(c));
+    GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
+    double sr = 1.0;
+    std::vector<double>& l = c->lkhd;
+    for (int ktr = 1; ktr < 8; ktr++) {
+      GPL_RUN(objective_launch(c, jtr + 1));
+      GPL_RUN(read_slot(c, jtr + 1, nullptr));
+      st[2]++;
+      if (l[jtr + 1] > l[jtr] || ktr == 7) break;
+      else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
+      else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
+      GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
+    }
+    st[1]++;
+    if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
+    if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
+    if (lbfgs_budget > 0 && st[1] >= lbfgs_budget) break;
+  }
+  GPL_RUN(launch_expand_delta(c));
+  GPL_RUN(launch_beta_from_tilde(c));
+  st[3] = ntrace;
+  return GPL_OK;
+}
+
 static int glm_init(Ctx* c) {
   GPL_RUN(launch_expand_delta(c));
   GPL_RUN(launch_gram(c, true));
@@ -733,48 +775,24 @@ int gpl_beta_from_tilde(gpl_ctx* h) {
 int gpl_fit(gpl_ctx* h, int itr_max, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));
-  int itr, rhoflag = 0, total_lbfgs = 0, total_irls = 0, total_evals = 0, ntrace = 0, rc = GPL_OK;
-  bool budget_hit = false;
-  for (itr = 0; itr < itr_max && !budget_hit; itr++) {
-    int JTRMAX = (itr == 0) ? 200 : 100;
-    int n = 0;
-    rc = irls(c, JTRMAX, &n);
-    total_irls += n;
+  int itr, total_lbfgs = 0, total_irls = 0, total_evals = 0, ntrace = 0, rc = GPL_OK;
+  for (itr = 0; itr < itr_max; itr++) {
+    int32_t st[4] = {0, 0, 0, 0};
+    const int left = lbfgs_budget > 0 ? lbfgs_budget - total_lbfgs : 0;
+    rc = fit_outer(c, itr, left, st, trace ? trace + ntrace : nullptr, trace ? trace_cap - ntrace : 0);
+    total_irls += st[0];
+    total_lbfgs += st[1];
+    total_evals += st[2];
+    ntrace += st[3];
     if (rc == GPL_ERR_NAN) {
       itr++;
       break;
     }
     if (rc) return rc;
-    double l0 = 0.0;
-    GPL_RUN(objective_after_irls(c, &l0));
-    total_evals++;
-    if (trace && ntrace < trace_cap) trace[ntrace++] = l0;
-    if (itr > 20) rhoflag = 1;
-    if (itr == 30) JTRMAX = 10000;
-    for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
-      GPL_RUN(gradient_launch(c));
-      GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
-      double sr = 1.0;
-      std::vector<double>& l = c->lkhd;
-      for (int ktr = 1; ktr < 8; ktr++) {
-        GPL_RUN(objective_launch(c, jtr + 1));
-        GPL_RUN(read_slot(c, jtr + 1, nullptr));
-        total_evals++;
-        if (l[jtr + 1] > l[jtr] || ktr == 7) break;
-        else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
-        else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
-        GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
-      }
-      total_lbfgs++;
-      if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
-      if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
-      if (lbfgs_budget > 0 && total_lbfgs >= lbfgs_budget) {
-        budget_hit = true;
-        break;
-      }
+    if (lbfgs_budget > 0 && total_lbfgs >= lbfgs_budget) {
+      itr++;
+      break;
     }
-    GPL_RUN(launch_expand_delta(c));
-    GPL_RUN(launch_beta_from_tilde(c));
   }
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
   if (stats) {
@@ -784,6 +802,21 @@ int gpl_fit(gpl_ctx* h, int itr_max, int lbfgs_budget, int32_t* stats, double* t
     stats[3] = total_evals;
   }
   return rc == GPL_ERR_NAN ? GPL_ERR_NAN : GPL_OK;
+}
+
+int gpl_fit_outer(gpl_ctx* h, int itr, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (itr < 0) {
+    c->err = "itr must be >= 0";
+    return GPL_ERR_ARG;
+  }
+  int32_t st[4] = {0, 0, 0, 0};
+  const int rc = fit_outer(c, itr, lbfgs_budget, st, trace, trace ? trace_cap : 0);
+  if (stats)
+    for (int k = 0; k < 4; k++) stats[k] = st[k];
+  if (rc == GPL_OK) GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  return rc;
 }
 
 int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkhd, double* grad) {

@@ -141,6 +141,14 @@ GPL_API int gpl_beta_from_tilde(gpl_ctx* ctx);
  * objective evaluations; trace gets the accepted objective values (<= trace_cap). */
 GPL_API int gpl_fit(gpl_ctx* ctx, int itr_max, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap);
 
+/* One outer iteration of that loop, numbered itr (0-based; it selects JTRMAX 200 or 100,
+ * rhoflag for itr > 20 and the long L-BFGS run at itr 30), ending with the beta revival
+ * (ggplvm.cu:1317-1319). The CLI calls it to write X9.gz, phi.gz and Params9.bin after every
+ * outer iteration as the reference driver does (ggplvm.cu:1301-1315). lbfgs_budget > 0 caps
+ * this call's L-BFGS steps. stats[4] = IRLS sweeps, L-BFGS steps, objective evaluations,
+ * trace entries written. GPL_ERR_NAN when the IRLS likelihood is NaN (the reference exits 1). */
+GPL_API int gpl_fit_outer(gpl_ctx* ctx, int itr, int lbfgs_budget, int32_t* stats, double* trace, int trace_cap);
+
 /* One objective+gradient evaluation at host parameters (the unit of the throughput
  * metric): params = [Omega (N) | delta (p) | X (N*Q) | T (M*Q) | rho (Q)] in natural
  * scale (n_params = N + p + N*Q + M*Q + Q); the objective goes to *lkhd and the gradient
