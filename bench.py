@@ -135,8 +135,9 @@ def flops_table(N, J, M, P, n_dense):
     return {
         # Gram over the dense model columns: n_d*(n_d+1)/2 unique pairs, 2 flops per cell and gene
         "gram": float(N) * J * n_dense * (n_dense + 1),
-        # gradient contraction over genes of S_j[DD] d_i over the n_d dense columns: 2*N*J*n_d^2
-        "uq": 2.0 * N * J * n_dense * n_dense,
+        # gradient contraction sum_j O_ij S_j[DD] d_i over the unique pairs of the symmetric S_j
+        # (the pair form's V = O S_pairs; the epilogue to U is N*n_d^2, not counted)
+        "uq": float(N) * J * n_dense * (n_dense + 1),
         # batched SPD inverse (triangular inverse + its product, n^3/3 flops each) and Cholesky
         "inverse": 2.0 / 3.0 * J * float(P) ** 3,
         "chol": 1.0 / 3.0 * J * float(P) ** 3,
@@ -285,7 +286,7 @@ def run_ours(args):
     launches = m.launches() - l0
     ck = clocks.stop()
     prof = {}
-    for name in ("gram", "uq", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
+    for name in ("gram", "uq", "spair", "v_to_u", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
                  "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
                  "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk"):
         ms, n = m.profile_read(name)

@@ -82,6 +82,7 @@ static int dalloc(Ctx* c, T** p, size_t n, const char* what) {
 
 static void free_state(Ctx* c) {
   tc_release(c);
+  pair_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
                    c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d};
   for (void* q : extra)
@@ -320,6 +321,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
   }
   c->precision = precision;
   c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
+  c->simt_fp64 = getenv("GPL_FP64_SIMT") != nullptr;
   return GPL_OK;
 }
 

@@ -49,6 +49,16 @@ struct DevBuf {
 };
 
 // Operands, partial sums and TMA descriptors of the tensor-core contractions (k_tc.cu).
+// Column-pair FP64 GEMM state (k_dgemm.cu): the pair list (a <= b over the dense columns),
+// 1/Omega, the gathered Psi^{-1} pairs per gene and a range of V rows.
+struct PairState {
+  bool ready = false;
+  int n_pairs = 0, pairs_pad = 0, cpad = 0, v_cells = 0;
+  int smem_gram = 0, smem_v = 0, smem_vu = 0;
+  int2* pairs = nullptr;
+  double *rOm = nullptr, *Sp = nullptr, *V = nullptr;
+};
+
 struct TcState {
   bool ready = false, check_each = false;
   int n_dp = 0, cpad = 0, chunks_cells = 0, gram_tiles_n = 0;
@@ -69,6 +79,7 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int precision = GPL_PREC_FP64;
+  bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
   std::string err;
 
   // sizes
@@ -114,6 +125,7 @@ struct Ctx {
   std::vector<double> lkhd;
 
   TcState tc;
+  PairState pr;
 
   // profiling
   bool prof = false;
@@ -182,6 +194,9 @@ void launch_chol_exact_raw(cudaStream_t st, double* A, int n);
 int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
                            const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork);
 // k_tc.cu (precision form)
+int launch_pair_gram(Ctx* c);             // dense block of every Psi_j, FP64 DMMA over column pairs
+int launch_pair_uq(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i, FP64 DMMA over column pairs
+void pair_release(Ctx* c);
 int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
 int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting

@@ -1,0 +1,408 @@
+// FP64 tensor-core (DMMA, mma.sync m16n8k4 .f64) forms of the two dominant contractions of
+// the plain FP64 path. Both are written over the unique column pairs (a <= b) of the dense
+// model columns, which turns the per-gene P x P products into two plain GEMMs and uses the
+// symmetry of Psi_j and Psi_j^{-1} to halve the work.
+//
+//   k_pair_gram   G[p, j] = sum_i (D_ia D_ib / Omega_i) W_ij, written straight into Psi_j
+//                 (both triangles, plus DeltaInv) at model columns (dcol a, dcol b): the dense
+//                 block of getPsi (ggplvm.cu:621-680). M = pairs, N = genes, K = cells.
+//                 The weights, the dense columns and 1/Omega of every 16-cell slice arrive by
+//                 cp.async (three stages); the pair products are formed from them in shared
+//                 memory one slice ahead of the MMAs.
+//                 Work: N*J*n_d*(n_d+1) flops.
+//   k_pair_v      V[i, p] = (1/Omega_i) sum_j W_ij S_j[a, b] for a cell range, S_j = Psi_j^{-1}
+//                 gathered per pair (k_gather_spair). M = cells, N = pairs, K = genes; both
+//                 operands by cp.async. Work: N*J*n_d*(n_d+1) flops.
+//   k_v_to_u      U[i, a] = sum_b D_ib V[i, pair(a, b)]: the gradient contraction
+//                 sum_j O_ij S_j[DD] d_i of getGradLogOmega (ggplvm.cu:301-376) from V.
+//
+// CTA tile 128 x 128 x 16 (K), 8 warps as 2 (M) x 4 (N), warp tile 64 x 32 (4 x 4 DMMA tiles
+// of 16 x 8), double-buffered shared memory. m16n8k4 fragments (lane = 4*g + t):
+// A 16x4 row-major a0 = A[g][t], a1 = A[g+8][t]; B 4x8 b0 = B[t][g]; C 16x8
+// c0,c1 = C[g][2t, 2t+1], c2,c3 = C[g+8][2t, 2t+1]. Shared rows are padded so that the
+// 16 lanes of each half-warp hit 16 distinct 8-byte bank pairs.
+#include <algorithm>
+
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+namespace {
+constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int SA = BM + 4;   // As[k][m]
+constexpr int SBT = BK + 4;  // Bs[n][k] (weights, k contiguous)
+constexpr int SBN = BN + 4;  // Bs[k][n] (S pairs, n contiguous)
+constexpr int kThreads = 256;
+}  // namespace
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(n) : "memory");
+}
+
+// One 16-deep K slice of the warp tile. kNT: B stored [n][k] (true) or [k][n] (false).
+template <bool kNT>
+__device__ __forceinline__ void warp_slice(const double* __restrict__ As, const double* __restrict__ Bs, int wm,
+                                           int wn, int g, int t, double (&acc)[4][4][4]) {
+#pragma unroll
+  for (int kk = 0; kk < BK / 4; kk++) {
+    double a[4][2], b[4];
+    const double* ar = As + (kk * 4 + t) * SA + wm * 64 + g;
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++) {
+      a[mt][0] = ar[mt * 16];
+      a[mt][1] = ar[mt * 16 + 8];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) {
+      const int n = wn * 32 + nt * 8 + g;
+      b[nt] = kNT ? Bs[n * SBT + kk * 4 + t] : Bs[(kk * 4 + t) * SBN + n];
+    }
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) dmma_16x8x4(acc[mt][nt], a[mt][0], a[mt][1], b[nt]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gram over the dense column pairs
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 1)
+    k_pair_gram(int N, int ldN, int J, int P, int n_d, const double* __restrict__ D, const int2* __restrict__ pairs,
+                int n_pairs, const int* __restrict__ dcol, const double* __restrict__ rOm,
+                const double* __restrict__ W, const double* __restrict__ Dinv, double* __restrict__ Psi) {
+  extern __shared__ __align__(16) double smem_d[];
+  double* As = smem_d;                          // [2][BK][SA]   pair products
+  double* Bs = As + 2 * BK * SA;                // [3][BN][SBT]  weights
+  double* Rs = Bs + 3 * BN * SBT;               // [3][BK]       1/Omega
+  double* Ds = Rs + 3 * BK;                     // [3][BK][n_d]  dense columns
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
+  const int p0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+  const int nsl = (N + BK - 1) / BK;
+
+  // producer role for the A slice: pair m, cells [8h, 8h + 8) of the slice
+  const int pm = tid & (BM - 1), ph = tid >> 7;
+  const int2 ab = (p0 + pm < n_pairs) ? pairs[p0 + pm] : make_int2(-1, -1);
+
+  // slice s of the weights (cp.async 16 B), the dense columns and 1/Omega (8 B) into stage st
+  auto load = [&](int s, int st) {
+    const int i0 = s * BK;
+#pragma unroll
+    for (int r = 0; r < (BN * BK / 2) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int n = ch >> 3, part = ch & 7;
+      const int j = j0 + n, i = i0 + part * 2;
+      const int nb = (j < J) ? 8 * max(0, min(2, N - i)) : 0;
+      const double* src = W + (size_t)min(j, J - 1) * ldN + min(i, ldN - 2);
+      cp_async16(Bs + st * BN * SBT + n * SBT + part * 2, src, nb);
+    }
+    for (int e = tid; e < BK * n_d; e += kThreads) {
+      const int col = e / BK, k = e - col * BK;
+      const int i = i0 + k;
+      cp_async8(Ds + st * BK * n_d + k * n_d + col, D + (size_t)col * ldN + min(i, ldN - 1), i < N ? 8 : 0);
+    }
+    if (tid < BK) {
+      const int i = i0 + tid;
+      cp_async8(Rs + st * BK + tid, rOm + min(i, ldN - 1), i < N ? 8 : 0);
+    }
+  };
+  auto fill_a = [&](int st, int buf) {
+    const double* d = Ds + st * BK * n_d + (ph * 8) * n_d;
+    const double* r = Rs + st * BK + ph * 8;
+    double* dst = As + buf * BK * SA + (ph * 8) * SA + pm;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double v = 0.0;
+      if (ab.x >= 0) v = d[k * n_d + ab.x] * d[k * n_d + ab.y] * r[k];
+      dst[k * SA] = v;
+    }
+  };
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
+
+  load(0, 0);
+  cp_async_commit();
+  if (nsl > 1) load(1, 1);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncthreads();
+  fill_a(0, 0);
+  for (int s = 0; s < nsl; s++) {
+    if (s + 2 < nsl) load(s + 2, (s + 2) % 3);
+    cp_async_commit();
+    cp_async_wait<1>();  // slice s + 1 landed
+    __syncthreads();
+    warp_slice<true>(As + (s & 1) * BK * SA, Bs + (s % 3) * BN * SBT, wm, wn, g, t, acc);
+    if (s + 1 < nsl) fill_a((s + 1) % 3, (s + 1) & 1);
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+
+  // epilogue: both triangles of Psi_j plus DeltaInv
+#pragma unroll
+  for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int p = p0 + wm * 64 + mt * 16 + g + h * 8;
+      if (p >= n_pairs) continue;
+      const int2 q = pairs[p];
+      const size_t mk = dcol[q.x], ml = dcol[q.y];
+      const double dv = Dinv[mk + ml * P];
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int j = j0 + wn * 32 + nt * 8 + 2 * t + e;
+          if (j >= J) continue;
+          double* Pj = Psi + (size_t)j * P * P;
+          const double v = acc[mt][nt][h * 2 + e] + dv;
+          Pj[mk + ml * P] = v;
+          Pj[ml + mk * P] = v;
+        }
+    }
+}
+
+__global__ void k_recip_omega(int N, int cpad, const double* __restrict__ Omega, double* __restrict__ rOm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cpad) rOm[i] = i < N ? 1.0 / Omega[i] : 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gradient contraction over the pairs
+// ---------------------------------------------------------------------------------------------
+// Spair[j][p] = S_j[dcol a_p, dcol b_p] (0 for the padding pairs)
+__global__ void k_gather_spair(int J, int P, int n_pairs, int pairs_pad, const int2* __restrict__ pairs,
+                               const int* __restrict__ dcol, const double* __restrict__ S,
+                               double* __restrict__ Sp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pairs_pad) return;
+  int2 q = make_int2(0, 0);
+  const bool live = p < n_pairs;
+  if (live) q = pairs[p];
+  const size_t off = live ? (size_t)dcol[q.x] + (size_t)dcol[q.y] * P : 0;
+  for (int j = blockIdx.y; j < J; j += gridDim.y)
+    Sp[(size_t)j * pairs_pad + p] = live ? S[(size_t)j * P * P + off] : 0.0;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_pair_v(int N, int ldN, int J, int c0, int c1, int pairs_pad, const double* __restrict__ W,
+             const double* __restrict__ Sp, const double* __restrict__ rOm, double* __restrict__ V) {
+  extern __shared__ __align__(16) double smem_d[];
+  double* As = smem_d;                // [2][BK][SA]  W rows (cells contiguous)
+  double* Bs = smem_d + 2 * BK * SA;  // [2][BK][SBN] S pairs (pairs contiguous)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
+  const int i0 = c0 + blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nsl = (J + BK - 1) / BK;
+
+  auto load = [&](int s, int buf) {
+    const int jb = s * BK;
+#pragma unroll
+    for (int r = 0; r < (BM * BK / 2) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int k = ch >> 6, part = ch & 63;
+      const int j = jb + k, i = i0 + part * 2;
+      const int nb = (j < J) ? 8 * max(0, min(2, min(N, c1) - i)) : 0;
+      const double* src = W + (size_t)min(j, J - 1) * ldN + min(max(i, 0), ldN - 2);
+      cp_async16(As + buf * BK * SA + k * SA + part * 2, src, nb);
+    }
+#pragma unroll
+    for (int r = 0; r < (BN * BK / 2) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int k = ch >> 6, part = ch & 63;
+      const int j = jb + k;
+      const int nb = (j < J) ? 16 : 0;
+      const double* src = Sp + (size_t)min(j, J - 1) * pairs_pad + n0 + part * 2;
+      cp_async16(Bs + buf * BK * SBN + k * SBN + part * 2, src, nb);
+    }
+  };
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int x = 0; x < 4; x++)
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
+
+  load(0, 0);
+  cp_async_commit();
+  for (int s = 0; s < nsl; s++) {
+    const int buf = s & 1;
+    if (s + 1 < nsl) {
+      load(s + 1, buf ^ 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    warp_slice<false>(As + buf * BK * SA, Bs + buf * BK * SBN, wm, wn, g, t, acc);
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int i = i0 + wm * 64 + mt * 16 + g + h * 8;
+      if (i >= N || i >= c1) continue;
+      const double r = rOm[i];
+      double* vrow = V + (size_t)(i - c0) * pairs_pad + n0 + wn * 32 + 2 * t;
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        double2 v = make_double2(acc[mt][nt][h * 2] * r, acc[mt][nt][h * 2 + 1] * r);
+        *reinterpret_cast<double2*>(vrow + nt * 8) = v;
+      }
+    }
+}
+
+// U[i, a] = sum_b D_ib V[i, pair(min(a,b), max(a,b))], one CTA per cell, the V row staged in
+// shared memory; pair(a, b) = a*n_d - a*(a-1)/2 + (b - a) (row-major upper triangle).
+__global__ void __launch_bounds__(256) k_v_to_u(int N, int ldN, int n_d, int n_pairs, int pairs_pad, int c0,
+                                                int c1, const double* __restrict__ D,
+                                                const double* __restrict__ V, double* __restrict__ U) {
+  extern __shared__ __align__(16) double vs[];
+  double* ds = vs + pairs_pad;  // D row of the cell
+  for (int i = c0 + blockIdx.x; i < c1 && i < N; i += gridDim.x) {
+    const double* vr = V + (size_t)(i - c0) * pairs_pad;
+    for (int e = threadIdx.x; e < n_pairs; e += blockDim.x) vs[e] = vr[e];
+    for (int e = threadIdx.x; e < n_d; e += blockDim.x) ds[e] = D[(size_t)e * ldN + i];
+    __syncthreads();
+    for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
+      double s = 0.0;
+      // b < a: pair(b, a)
+      for (int b = 0; b < a; b++) s = fma(ds[b], vs[b * n_d - b * (b - 1) / 2 + (a - b)], s);
+      // b >= a: pair(a, b), contiguous
+      const double* row = vs + a * n_d - a * (a - 1) / 2 - a;
+      for (int b = a; b < n_d; b++) s = fma(ds[b], row[b], s);
+      U[i + (size_t)a * ldN] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+int pair_prepare(Ctx* c) {
+  PairState& s = c->pr;
+  if (s.ready) return GPL_OK;
+  const int n_d = c->n_d;
+  std::vector<int2> pairs;
+  for (int a = 0; a < n_d; a++)
+    for (int b = a; b < n_d; b++) pairs.push_back(make_int2(a, b));
+  s.n_pairs = (int)pairs.size();
+  s.pairs_pad = (s.n_pairs + BN - 1) / BN * BN;
+  s.cpad = (c->N + BM - 1) / BM * BM;
+  // V holds a range of cells at a time: at most 2 GiB or all cells
+  const size_t row = (size_t)s.pairs_pad * sizeof(double);
+  s.v_cells = (int)std::min<size_t>((size_t)s.cpad, std::max<size_t>(BM, ((size_t)2 << 30) / row / BM * BM));
+  if (cudaMalloc((void**)&s.pairs, sizeof(int2) * pairs.size()) != cudaSuccess ||
+      cudaMalloc((void**)&s.rOm, sizeof(double) * s.cpad) != cudaSuccess ||
+      cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess ||
+      cudaMalloc((void**)&s.V, sizeof(double) * (size_t)s.v_cells * s.pairs_pad) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "device allocation failed: pair GEMM buffers";
+    return GPL_ERR_ALLOC;
+  }
+  GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
+  s.smem_gram = (int)sizeof(double) * (2 * BK * SA + 3 * BN * SBT + 3 * BK + 3 * BK * n_d);
+  s.smem_v = (int)sizeof(double) * 2 * (BK * SA + BK * SBN);
+  s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
+  if (s.smem_vu > 200 * 1024) {
+    c->err = "too many dense model columns for the staged pair contraction";
+    return GPL_ERR_ARG;
+  }
+  GPL_TRY(c, cudaFuncSetAttribute(k_pair_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_gram));
+  GPL_TRY(c, cudaFuncSetAttribute(k_pair_v, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_v));
+  GPL_TRY(c, cudaFuncSetAttribute(k_v_to_u, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_vu));
+  s.ready = true;
+  return GPL_OK;
+}
+
+void pair_release(Ctx* c) {
+  PairState& s = c->pr;
+  void* bufs[] = {s.pairs, s.rOm, s.Sp, s.V};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  s = PairState();
+}
+
+static int launch_recip(Ctx* c) {
+  PairState& s = c->pr;
+  k_recip_omega<<<div_up(s.cpad, 256), 256, 0, c->stream>>>(c->N, s.cpad, c->Omega, s.rOm);
+  GPL_LAUNCHED(c, "k_recip_omega");
+  return GPL_OK;
+}
+
+int launch_pair_gram(Ctx* c) {
+  int rc = pair_prepare(c);
+  if (rc) return rc;
+  PairState& s = c->pr;
+  if ((rc = launch_recip(c))) return rc;
+  ProfScope ps(c, "gram");
+  dim3 g(div_up(s.n_pairs, BM), div_up(c->J, BN));
+  k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c->n_d, c->Dm, s.pairs, s.n_pairs,
+                                                      c->dcol_d, s.rOm, c->W, c->DeltaInv, c->Psi);
+  GPL_LAUNCHED(c, "k_pair_gram");
+  return GPL_OK;
+}
+
+int launch_pair_uq(Ctx* c) {
+  int rc = pair_prepare(c);
+  if (rc) return rc;
+  PairState& s = c->pr;
+  if ((rc = launch_recip(c))) return rc;
+  {
+    ProfScope ps(c, "spair");
+    dim3 g(div_up(s.pairs_pad, 256), std::min(c->J, 65535));
+    k_gather_spair<<<g, 256, 0, c->stream>>>(c->J, c->P, s.n_pairs, s.pairs_pad, s.pairs, c->dcol_d, c->PsiInv,
+                                             s.Sp);
+    GPL_LAUNCHED(c, "k_gather_spair");
+  }
+  for (int c0 = 0; c0 < c->N; c0 += s.v_cells) {
+    const int c1 = std::min(c->N, c0 + s.v_cells);
+    {
+      ProfScope ps(c, "uq");
+      dim3 g(div_up(c1 - c0, BM), s.pairs_pad / BN);
+      k_pair_v<<<g, kThreads, s.smem_v, c->stream>>>(c->N, c->ldN, c->J, c0, c1, s.pairs_pad, c->W, s.Sp, s.rOm,
+                                                     s.V);
+      GPL_LAUNCHED(c, "k_pair_v");
+    }
+    {
+      ProfScope ps(c, "v_to_u");
+      const int grid = std::min(c1 - c0, 148 * 8);
+      k_v_to_u<<<grid, 256, s.smem_vu, c->stream>>>(c->N, c->ldN, c->n_d, s.n_pairs, s.pairs_pad, c0, c1, c->Dm,
+                                                    s.V, c->U);
+      GPL_LAUNCHED(c, "k_v_to_u");
+    }
+  }
+  return GPL_OK;
+}
+
+}  // namespace gpl

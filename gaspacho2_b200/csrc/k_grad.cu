@@ -233,6 +233,9 @@ int launch_grad_omega(Ctx* c) {
   if (c->precision == GPL_PREC_BF16X3) {
     rc = launch_tc_grad(c);
     if (rc) return rc;
+  } else if (!c->simt_fp64) {
+    rc = launch_pair_uq(c);
+    if (rc) return rc;
   } else {
     ProfScope ps(c, "uq");
     const int n_dp = div_up(c->n_d, TK) * TK;

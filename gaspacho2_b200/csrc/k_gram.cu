@@ -260,6 +260,9 @@ int launch_gram(Ctx* c, bool unweighted) {
   if (!unweighted && c->precision == GPL_PREC_BF16X3) {
     int rc = launch_tc_gram(c);
     if (rc) return rc;
+  } else if (!unweighted && !c->simt_fp64) {
+    int rc = launch_pair_gram(c);
+    if (rc) return rc;
   } else {
     ProfScope ps(c, "gram");
     dim3 g(npairs, div_up(J, GG));

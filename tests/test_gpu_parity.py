@@ -5,8 +5,9 @@ Tolerances: the CUDA path computes in FP64 with different (deterministic) reduct
 orders and fused multiply-adds, so agreement is to rounding amplified by the phase chain:
 per-phase buffers within 1e-8 relative to the buffer's largest magnitude; over a budgeted
 fit (tens of IRLS sweeps and L-BFGS steps, whose two-loop recursion differences gradients)
-identical discrete decisions (IRLS sweep counts, accepted line-search steps) and the
-objective trace and parameters within 1e-6, the bar set for the FP64 path."""
+identical discrete decisions (IRLS sweep counts, accepted line-search steps), the objective
+trace within 1e-6 and the parameters within 1e-6, the bar set for the FP64 path, widened to
+20x the oracle's own sub-ulp sensitivity where that is larger."""
 import numpy as np
 import pytest
 
@@ -52,9 +53,43 @@ def test_phases_match_reference_golden(case):
         _compare(gu.run_phases(m, case), case.g, TOL_PHASE)
 
 
+def _fit_sensitivity(gd, seeds=(0, 1)):
+    """The oracle fit's own change when X and T move by a fraction of an ulp (per output)."""
+    import dataclasses
+
+    base = gu.run_fit(port.OracleModel.from_dataset(gd), gd)
+    sens = {}
+    for sd in seeds:
+        rng = np.random.default_rng(sd)
+        X2 = gd.init.X * (1 + 2e-16 * rng.standard_normal(gd.init.X.shape))
+        T2 = gd.init.T * (1 + 2e-16 * rng.standard_normal(gd.init.T.shape))
+        g2 = dataclasses.replace(gd, init=dataclasses.replace(gd.init, X=X2, T=T2))
+        pert = gu.run_fit(port.OracleModel.from_dataset(g2), g2)
+        for k in base:
+            if k not in ("fit_rc", "fit_stats"):
+                sens[k] = max(sens.get(k, 0.0), gu.rel_err(np.atleast_1d(pert[k]), np.atleast_1d(base[k])))
+    return sens
+
+
 def test_fit_matches_reference_golden(case):
+    """Identical discrete decisions; the objective trace within 1e-6; parameters within 1e-6
+    or, where the reference's fit itself moves by more under sub-ulp input changes (the
+    nearly singular Kmm of the edge-case fixture), within 20x that sensitivity."""
+    sens = _fit_sensitivity(case)
     with GPLVM.from_dataset(case) as m:
-        _compare(gu.run_fit(m, case), case.g, TOL_FIT)
+        out = gu.run_fit(m, case)
+    bad = []
+    for k, v in out.items():
+        if k in ("fit_rc", "fit_stats"):
+            if not np.array_equal(np.asarray(v), np.asarray(case.g[k])):
+                bad.append(f"{k}: {v} != {case.g[k]}")
+            continue
+        e = gu.rel_err(np.atleast_1d(v), np.atleast_1d(case.g[k]))
+        tol = TOL_FIT if k == "fit_trace" else max(TOL_FIT, 20.0 * sens[k])
+        print(f"{k:10s} err {e:.2e} sensitivity {sens[k]:.2e} tol {tol:.1e}")
+        if not e <= tol:
+            bad.append(f"{k}: {e:.2e} > {tol:.2e}")
+    assert not bad, "; ".join(bad)
 
 
 def test_count_walk_on_device():
