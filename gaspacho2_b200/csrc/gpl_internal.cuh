@@ -188,6 +188,7 @@ int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride);
 int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const double* B, int64_t bstride,
                          double* X, int64_t xstride, int batch);
 int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
+int launch_inverse_panels(Ctx* c);       // the same in 32-column panels with DMMA block products
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA
 void launch_chol_exact_raw(cudaStream_t st, double* A, int n);

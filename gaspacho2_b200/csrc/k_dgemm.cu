@@ -23,6 +23,7 @@
 // 16 lanes of each half-warp hit 16 distinct 8-byte bank pairs.
 #include <algorithm>
 
+#include "dmma_common.cuh"
 #include "gpl_internal.cuh"
 
 namespace gpl {
@@ -34,27 +35,6 @@ constexpr int SBT = BK + 4;  // Bs[n][k] (weights, k contiguous)
 constexpr int SBN = BN + 4;  // Bs[k][n] (S pairs, n contiguous)
 constexpr int kThreads = 256;
 }  // namespace
-
-__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
-      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b0));
-}
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
-  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
-  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int n>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(n) : "memory");
-}
 
 // One 16-deep K slice of the warp tile. kNT: B stored [n][k] (true) or [k][n] (false).
 template <bool kNT>

@@ -318,6 +318,10 @@ int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const 
 int launch_inverse_batched(Ctx* c) {
   const int64_t st = (int64_t)c->P * c->P;
   ProfScope ps(c, "inverse");
+  if (!c->simt_fp64) {
+    const int rc = launch_inverse_panels(c);
+    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: P beyond the panel kernels' shared memory
+  }
   k_trtri<<<c->J, 256, 0, c->stream>>>(c->Psi, c->P, st, c->scratch);
   GPL_LAUNCHED(c, "k_trtri");
   k_lauum<<<c->J, 256, 0, c->stream>>>(c->scratch, c->P, st, c->PsiInv);

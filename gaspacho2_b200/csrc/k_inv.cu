@@ -1,0 +1,187 @@
+// Batched inverse of the per-gene Psi_j from their Cholesky factors (solvePsi,
+// ggplvm.cu:46-53, which runs cholsl chol.cu:45-56 on every column of the identity):
+// Psi_j^{-1} = V^T V with V = L^{-1}, in 32-column panels with FP64 tensor-core (DMMA)
+// block products.
+//
+//   k_trtri_panel  one CTA per (panel jb, gene): the columns [32 jb, 32 jb + 32) of V by
+//                  forward substitution over 32-row blocks. Block i first takes the product of
+//                  the finished rows, R = E - L[i, jb..i) Y[jb..i) (DMMA), then solves
+//                  L[i,i] Y_i = R by column-oriented substitution: one warp per 4 right-hand
+//                  sides, lanes over rows, y_q = r_q / L[q,q] broadcast by shuffle, each row's
+//                  sum taken in increasing q as in cholsl. The panel stays in shared memory.
+//                  Work: P^3/6 multiply-adds per gene.
+//   k_lauum_panel  one CTA per (panel b, gene): S[a, b] = sum_{k >= a} V[k, a]^T V[k, b]
+//                  for the blocks a >= b, written to both triangles. Work: P^3/6 per gene.
+//
+// L is the lower triangle (with diagonal) of the factored Psi_j (column-major, ld P); V is
+// written column-major (ld P) below and on the diagonal of each panel, the strict upper part of
+// the diagonal blocks holding exact zeros. A factor zero-filled by a failed Cholesky gives
+// infinities and NaNs, as in the reference.
+#include "dmma_common.cuh"
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+namespace {
+constexpr int IB = 32;  // block size
+constexpr int IS = 36;  // shared row stride (doubles): conflict-free fragment loads
+constexpr int LS = 33;  // shared row stride of the 32 x 32 diagonal and right-hand-side blocks
+}  // namespace
+
+__global__ void __launch_bounds__(256, 1)
+    k_trtri_panel(const double* __restrict__ Psi, int P, int64_t stride, double* __restrict__ V) {
+  extern __shared__ __align__(16) double sm[];
+  const int nb = (P + IB - 1) / IB;
+  const int jb = blockIdx.x;
+  const double* L = Psi + (size_t)blockIdx.y * stride;
+  double* Vm = V + (size_t)blockIdx.y * stride;
+  const int r0 = jb * IB;
+  double* Yp = sm;                            // [nb*32][IS], local row r = global row r0 + r
+  double* As = Yp + (size_t)nb * IB * IS;     // [nb*32][IS], As[k][m] = L[rb + m][r0 + k]
+  double* Ld = As + (size_t)nb * IB * IS;     // [32][LS] diagonal block
+  double* Rs = Ld + IB * LS;                  // [32][LS] right-hand sides
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int m0 = (warp >> 2) * 16, n0 = (warp & 3) * 8;
+
+  for (int ib = jb; ib < nb; ib++) {
+    const int rb = ib * IB;
+    const int K = rb - r0;
+    for (int e = tid; e < K * IB; e += blockDim.x) {
+      const int k = e >> 5, m = e & 31;
+      const int row = rb + m;
+      cp_async8(As + k * IS + m, L + (size_t)min(row, P - 1) + (size_t)(r0 + k) * P, row < P ? 8 : 0);
+    }
+    cp_async_commit();
+    for (int e = tid; e < IB * IB; e += blockDim.x) {
+      const int m = e >> 5, q = e & 31;
+      const int row = rb + m, col = rb + q;
+      double v;
+      if (row < P && col < P) v = q <= m ? L[row + (size_t)col * P] : 0.0;
+      else v = (m == q) ? 1.0 : 0.0;
+      Ld[m * LS + q] = v;
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int kb = 0; kb < K; kb += 4) {
+      const double a0 = As[(kb + t) * IS + m0 + g];
+      const double a1 = As[(kb + t) * IS + m0 + g + 8];
+      const double b0 = Yp[(kb + t) * IS + n0 + g];
+      dmma_16x8x4(acc, a0, a1, b0);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int m = m0 + g + 8 * h, n = n0 + 2 * t + e;
+        const double ev = (ib == jb && m == n) ? 1.0 : 0.0;
+        Rs[m * LS + n] = ev - acc[2 * h + e];
+      }
+    __syncthreads();
+
+    // L[i,i] Y_i = R: warp owns columns 4*warp .. +3, lane = row
+    double rr[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) rr[c] = Rs[lane * LS + 4 * warp + c];
+    for (int q = 0; q < IB; q++) {
+      const double lqq = Ld[q * LS + q];
+      const double lrq = Ld[lane * LS + q];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const double yq = __shfl_sync(0xffffffffu, rr[c], q) / lqq;
+        if (lane == q) rr[c] = yq;
+        else if (lane > q) rr[c] = fma(-lrq, yq, rr[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) Yp[(K + lane) * IS + 4 * warp + c] = rr[c];
+    __syncthreads();
+  }
+  // the panel out: rows r0 .. P-1, columns r0 .. min(r0 + 32, P) - 1
+  const int ncol = min(IB, P - r0), nrow = P - r0;
+  for (int e = tid; e < nrow * ncol; e += blockDim.x) {
+    const int c = e / nrow, r = e - c * nrow;
+    Vm[(size_t)(r0 + r) + (size_t)(r0 + c) * P] = Yp[r * IS + c];
+  }
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_lauum_panel(const double* __restrict__ V, int P, int64_t stride, double* __restrict__ S) {
+  extern __shared__ __align__(16) double sm[];
+  const int nb = (P + IB - 1) / IB;
+  const int b = blockIdx.x;
+  const double* Vm = V + (size_t)blockIdx.y * stride;
+  double* Sm = S + (size_t)blockIdx.y * stride;
+  const int c0 = b * IB;
+  const int ncol = min(IB, P - c0);
+  double* Vb = sm;                          // [nb*32][IS]: Vb[k][n] = V[c0 + k][c0 + n]
+  double* Ak = Vb + (size_t)nb * IB * IS;   // [nb*32][IS]: Ak[k][m] = V[a0 + k][a0 + m]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int m0 = (warp >> 2) * 16, n0 = (warp & 3) * 8;
+  const int kb_rows = (P - c0 + 3) / 4 * 4;
+  for (int e = tid; e < kb_rows * IB; e += blockDim.x) {
+    const int k = e >> 5, n = e & 31;
+    const int row = c0 + k, col = c0 + n;
+    const bool ok = row < P && col < P;
+    cp_async8(Vb + k * IS + n, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
+  }
+  cp_async_commit();
+  for (int a = b; a < nb; a++) {
+    const int a0 = a * IB;
+    const int K = (P - a0 + 3) / 4 * 4;
+    for (int e = tid; e < K * IB; e += blockDim.x) {
+      const int k = e >> 5, m = e & 31;
+      const int row = a0 + k, col = a0 + m;
+      const bool ok = row < P && col < P;
+      cp_async8(Ak + k * IS + m, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int off = a0 - c0;
+    for (int kb = 0; kb < K; kb += 4) {
+      const double a0v = Ak[(kb + t) * IS + m0 + g];
+      const double a1v = Ak[(kb + t) * IS + m0 + g + 8];
+      const double b0v = Vb[(off + kb + t) * IS + n0 + g];
+      dmma_16x8x4(acc, a0v, a1v, b0v);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int m = m0 + g + 8 * h, n = n0 + 2 * t + e;
+        const int row = a0 + m, col = c0 + n;
+        if (row < P && n < ncol) {
+          Sm[(size_t)row + (size_t)col * P] = acc[2 * h + e];
+          Sm[(size_t)col + (size_t)row * P] = acc[2 * h + e];
+        }
+      }
+    __syncthreads();
+  }
+}
+
+int inverse_panel_smem(int P) {
+  const int nb = (P + IB - 1) / IB;
+  return (int)sizeof(double) * (2 * nb * IB * IS + 2 * IB * LS);
+}
+
+// Returns GPL_ERR_ARG when P is beyond the shared-memory budget of the panel kernels.
+int launch_inverse_panels(Ctx* c) {
+  const int P = c->P;
+  const int smem = inverse_panel_smem(P);
+  if (smem > 220 * 1024) return GPL_ERR_ARG;
+  GPL_TRY(c, cudaFuncSetAttribute(k_trtri_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  GPL_TRY(c, cudaFuncSetAttribute(k_lauum_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int64_t st = (int64_t)P * P;
+  const int nb = (P + IB - 1) / IB;
+  dim3 g(nb, c->J);
+  k_trtri_panel<<<g, 256, smem, c->stream>>>(c->Psi, P, st, c->scratch);
+  GPL_LAUNCHED(c, "k_trtri_panel");
+  k_lauum_panel<<<g, 256, smem, c->stream>>>(c->scratch, P, st, c->PsiInv);
+  GPL_LAUNCHED(c, "k_lauum_panel");
+  return GPL_OK;
+}
+
+}  // namespace gpl
