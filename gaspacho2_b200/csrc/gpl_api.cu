@@ -84,9 +84,13 @@ static void free_state(Ctx* c) {
   tc_release(c);
   pair_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
-                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d};
+                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part};
   for (void* q : extra)
     if (q) cudaFree(q);
+  c->hk_tiles128_d = nullptr;
+  c->n_hk_tiles128 = 0;
+  c->part = nullptr;
+  c->part_n = 0;
   c->Dm = c->gsum = c->gT = c->HK = nullptr;
   c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
   c->hk_tiles_d = nullptr;
@@ -519,6 +523,11 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     for (int g = 0; g < n_grp; g++)
       for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 64) tiles.push_back(make_int2(g, r0));
   c->n_hk_tiles = (int)tiles.size();
+  std::vector<int2> tiles128;
+  if (grouped)
+    for (int g = 0; g < n_grp; g++)
+      for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 128) tiles128.push_back(make_int2(g, r0));
+  c->n_hk_tiles128 = (int)tiles128.size();
   c->tot_max = tot_len(c, 1);
   const size_t scratch_n = std::max({ldN * (size_t)J, (size_t)J * P * P, (size_t)c->tot_max, (size_t)M * M});
   GPL_RUN(dalloc(c, &c->Dm, ldN * n_d, "dense model columns"));
@@ -573,6 +582,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_RUN(dalloc(c, &c->gcells_d, (size_t)N, "group cells"));
     GPL_RUN(dalloc(c, &c->gstart_d, gstart.size(), "group offsets"));
     GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
+    GPL_RUN(dalloc(c, &c->hk_tiles128_d, tiles128.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->gsum, (size_t)J * n_grp * (n_d + 1), "group sums"));
     GPL_RUN(dalloc(c, &c->gT, (size_t)J * n_grp, "group response sums"));
     GPL_RUN(dalloc(c, &c->HK, ldN * (n_d + 1), "HK"));
@@ -583,6 +593,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_TRY(c, cudaMemcpy(c->gcells_d, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles_d, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->hk_tiles128_d, tiles128.data(), sizeof(int2) * tiles128.size(), cudaMemcpyHostToDevice));
   }
   GPL_TRY(c, cudaMemcpy(c->Dm, Dh.data(), sizeof(double) * ldN * n_d, cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->dcol_d, dcol.data(), sizeof(int) * n_d, cudaMemcpyHostToDevice));

@@ -100,6 +100,10 @@ struct Ctx {
   int *gcells_d = nullptr, *gstart_d = nullptr, *codes_d = nullptr;
   int2* hk_tiles_d = nullptr;       // (group, first row) of every 64-cell tile of the group lists
   int n_hk_tiles = 0;
+  int2* hk_tiles128_d = nullptr;    // the same for 128-cell tiles
+  int n_hk_tiles128 = 0;
+  double* part = nullptr;           // split-K partial sums
+  size_t part_n = 0;
   double *Dm = nullptr, *gsum = nullptr, *gT = nullptr, *HK = nullptr;
 
   // device buffers
@@ -198,6 +202,12 @@ int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X
 int launch_pair_gram(Ctx* c);             // dense block of every Psi_j, FP64 DMMA over column pairs
 int launch_pair_uq(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i, FP64 DMMA over column pairs
 void pair_release(Ctx* c);
+int recip_omega(Ctx* c, const double** rOm);  // 1/Omega (0 past N), refreshed on every call
+int dgen_zt_u(Ctx* c, int mode);          // DMMA forms of the cell x gene GEMMs (k_dgen.cu);
+int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns exceed one tile
+int dgen_eta(Ctx* c, const double* B, double* out);
+int dgen_group_sums(Ctx* c, int mode);
+int dgen_hk(Ctx* c);
 int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
 int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting

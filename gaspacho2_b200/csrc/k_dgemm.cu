@@ -333,6 +333,16 @@ void pair_release(Ctx* c) {
   s = PairState();
 }
 
+int recip_omega(Ctx* c, const double** rOm) {
+  int rc = pair_prepare(c);
+  if (rc) return rc;
+  PairState& s = c->pr;
+  k_recip_omega<<<div_up(s.cpad, 256), 256, 0, c->stream>>>(c->N, s.cpad, c->Omega, s.rOm);
+  GPL_LAUNCHED(c, "k_recip_omega");
+  *rOm = s.rOm;
+  return GPL_OK;
+}
+
 static int launch_recip(Ctx* c) {
   PairState& s = c->pr;
   k_recip_omega<<<div_up(s.cpad, 256), 256, 0, c->stream>>>(c->N, s.cpad, c->Omega, s.rOm);

@@ -1,0 +1,390 @@
+// FP64 tensor-core (DMMA) forms of the cell x gene contractions around the Gram: one
+// register-staged GEMM template whose operand loaders apply the element-wise prologues
+// (W/Omega, products with nu, the gathers of a cell group) and whose epilogues scatter the
+// results.
+//
+//   zt_u      bvec[dcol a, j] = sum_i D_ia u_ij (getZtOinvjnj util_cuda.cu:462-487 with
+//             u = W nu / Omega; initBeta init.cu:193-221 with u = y0), split over the cells
+//             into 8 ranges whose partial sums are added in order.  2*N*J*n_d flops.
+//   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
+//   eta       E[i, j] = d_i . B_j[dcol] + the cell's level coefficients.  2*N*J*n_d flops.
+//   group     S[j][g][a] = sum_{i in g} w_ij D_ia over the gathered cells of each group.
+//   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for the cells of each group.
+//
+// Tile: 8 warps as WARPS_M x WARPS_N, each warp WM x WN DMMA tiles of 16 x 8, K slices of 16
+// staged through registers (the next slice's global loads are in flight during the current
+// slice's MMAs) into double-buffered shared memory laid out [k][m] and [k][n] with rows padded
+// to 4 mod 16 doubles (conflict-free fragment loads).
+#include <algorithm>
+
+#include "dmma_common.cuh"
+#include "gpl_internal.cuh"
+
+namespace gpl {
+
+namespace {
+
+template <int WARPS_M_, int WM_, int WN_>
+struct DTile {
+  static constexpr int WARPS_M = WARPS_M_, WARPS_N = 8 / WARPS_M_, WM = WM_, WN = WN_;
+  static constexpr int BM = WARPS_M * WM * 16, BN = WARPS_N * WN * 8, BK = 16;
+  static constexpr int SA = BM + 4, SB = BN + 4;
+  static constexpr int NA = BM * BK / 256, NB = BN * BK / 256;
+  static constexpr int smem() { return (int)sizeof(double) * 2 * BK * (SA + SB); }
+};
+using TileSq = DTile<2, 4, 4>;    // 128 x 128
+using TileTall = DTile<1, 9, 2>;  // 144 x 128: the dense columns (n_d <= 144) in one tile
+
+constexpr int kSplitK = 8;
+
+}  // namespace
+
+// KR(z) -> [kbeg, kend); A(r, k, z); B(k, c, z); E(r, c, z, v). kFastK: the loader's K index
+// is the contiguous one in memory (threads sweep k first).
+template <class T, class LA, class LB, class KR, class Epi>
+__global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr, Epi epi) {
+  extern __shared__ __align__(16) double sm[];
+  double* As = sm;
+  double* Bs = sm + 2 * T::BK * T::SA;
+  constexpr int BK = T::BK;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int wm = warp / T::WARPS_N, wn = warp % T::WARPS_N;
+  const int m0 = blockIdx.x * T::BM, n0 = blockIdx.y * T::BN, z = blockIdx.z;
+  const int2 kk = kr(z);
+  const int nsl = kk.y > kk.x ? (kk.y - kk.x + BK - 1) / BK : 0;
+  double ra[T::NA], rb[T::NB];
+
+  auto fetch = [&](int s) {
+    const int k0 = kk.x + s * BK;
+#pragma unroll
+    for (int q = 0; q < T::NA; q++) {
+      const int e = tid + q * 256;
+      int r, k;
+      if (LA::kFastK) { k = e % BK; r = e / BK; } else { r = e % T::BM; k = e / T::BM; }
+      ra[q] = (m0 + r < m && k0 + k < kk.y) ? A(m0 + r, k0 + k, z) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < T::NB; q++) {
+      const int e = tid + q * 256;
+      int c, k;
+      if (LB::kFastK) { k = e % BK; c = e / BK; } else { c = e % T::BN; k = e / T::BN; }
+      rb[q] = (n0 + c < n && k0 + k < kk.y) ? B(k0 + k, n0 + c, z) : 0.0;
+    }
+  };
+  auto stash = [&](int buf) {
+    double* as = As + buf * BK * T::SA;
+    double* bs = Bs + buf * BK * T::SB;
+#pragma unroll
+    for (int q = 0; q < T::NA; q++) {
+      const int e = tid + q * 256;
+      int r, k;
+      if (LA::kFastK) { k = e % BK; r = e / BK; } else { r = e % T::BM; k = e / T::BM; }
+      as[k * T::SA + r] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < T::NB; q++) {
+      const int e = tid + q * 256;
+      int c, k;
+      if (LB::kFastK) { k = e % BK; c = e / BK; } else { c = e % T::BN; k = e / T::BN; }
+      bs[k * T::SB + c] = rb[q];
+    }
+  };
+
+  double acc[T::WM][T::WN][4];
+#pragma unroll
+  for (int x = 0; x < T::WM; x++)
+#pragma unroll
+    for (int y = 0; y < T::WN; y++)
+#pragma unroll
+      for (int w = 0; w < 4; w++) acc[x][y][w] = 0.0;
+
+  // The stash into buffer s & 1 happens after the barrier of slice s - 1, which every thread
+  // passes only once it finished the MMAs of slice s - 2 that read that buffer.
+  if (nsl > 0) fetch(0);
+  for (int s = 0; s < nsl; s++) {
+    const int buf = s & 1;
+    stash(buf);
+    __syncthreads();
+    if (s + 1 < nsl) fetch(s + 1);
+    const double* as = As + buf * BK * T::SA + wm * T::WM * 16 + g;
+    const double* bs = Bs + buf * BK * T::SB + wn * T::WN * 8 + g;
+#pragma unroll
+    for (int k4 = 0; k4 < BK / 4; k4++) {
+      double a[T::WM][2], b[T::WN];
+#pragma unroll
+      for (int x = 0; x < T::WM; x++) {
+        a[x][0] = as[(k4 * 4 + t) * T::SA + x * 16];
+        a[x][1] = as[(k4 * 4 + t) * T::SA + x * 16 + 8];
+      }
+#pragma unroll
+      for (int y = 0; y < T::WN; y++) b[y] = bs[(k4 * 4 + t) * T::SB + y * 8];
+#pragma unroll
+      for (int x = 0; x < T::WM; x++)
+#pragma unroll
+        for (int y = 0; y < T::WN; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < T::WM; x++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = m0 + wm * T::WM * 16 + x * 16 + g + 8 * h;
+      if (r >= m) continue;
+#pragma unroll
+      for (int y = 0; y < T::WN; y++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int c = n0 + wn * T::WN * 8 + y * 8 + 2 * t + e;
+          if (c < n) epi(r, c, z, acc[x][y][2 * h + e]);
+        }
+    }
+}
+
+// ---- operand loaders ------------------------------------------------------------------------
+namespace {
+
+struct KSplit {  // z-th of the equal ranges of [0, K)
+  int K, per;
+  __device__ int2 operator()(int z) const { return make_int2(min(K, z * per), min(K, (z + 1) * per)); }
+};
+struct KAll {
+  int K;
+  __device__ int2 operator()(int) const { return make_int2(0, K); }
+};
+struct KGroup {  // the cells of group z
+  const int* gstart;
+  __device__ int2 operator()(int z) const { return make_int2(0, gstart[z + 1] - gstart[z]); }
+};
+
+struct LdDt {  // A(r = dense column, k = cell) = D[r*ldN + k]
+  static constexpr bool kFastK = true;
+  const double* D;
+  int ldN;
+  __device__ double operator()(int r, int k, int) const { return D[(size_t)r * ldN + k]; }
+};
+struct LdD {  // A(r = cell, k = dense column) = D[k*ldN + r]
+  static constexpr bool kFastK = false;
+  const double* D;
+  int ldN;
+  __device__ double operator()(int r, int k, int) const { return D[(size_t)k * ldN + r]; }
+};
+struct LdU {  // B(k = cell, c = gene): mode 0 W nu / Omega, mode 1 y0
+  static constexpr bool kFastK = true;
+  const double *W, *Nu, *rOm;
+  int ldN, mode;
+  __device__ double operator()(int k, int c, int) const {
+    const size_t e = (size_t)c * ldN + k;
+    return mode == 0 ? W[e] * rOm[k] * Nu[e] : Nu[e];
+  }
+};
+struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega
+  static constexpr bool kFastK = false;
+  const double *W, *Nu, *E, *rOm, *phi;
+  int ldN;
+  __device__ double operator()(int r, int k, int) const {
+    const size_t e = (size_t)k * ldN + r;
+    const double o = W[e] * rOm[r];
+    return (o * Nu[e] - o * E[e]) / phi[k];
+  }
+};
+struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
+  static constexpr bool kFastK = false;
+  const double* tB;
+  int P, g0;
+  __device__ double operator()(int k, int c, int) const { return tB[g0 + c + (size_t)k * P]; }
+};
+struct LdBetaDense {  // B(k = dense column, c = gene) = B[dcol[k] + c*P]
+  static constexpr bool kFastK = true;
+  const double* B;
+  const int* dcol;
+  int P;
+  __device__ double operator()(int k, int c, int) const { return B[dcol[k] + (size_t)c * P]; }
+};
+struct LdGroupD {  // A(r = dense column, k = k-th cell of group z) = D[r*ldN + cell]
+  static constexpr bool kFastK = true;
+  const double* D;
+  const int *gcells, *gstart;
+  int ldN;
+  __device__ double operator()(int r, int k, int z) const { return D[(size_t)r * ldN + gcells[gstart[z] + k]]; }
+};
+struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) or 1 (mode 1)
+  static constexpr bool kFastK = true;
+  const double *W, *rOm;
+  const int *gcells, *gstart;
+  int ldN, mode;
+  __device__ double operator()(int k, int c, int z) const {
+    if (mode == 1) return 1.0;
+    const int i = gcells[gstart[z] + k];
+    return W[(size_t)c * ldN + i] * rOm[i];
+  }
+};
+struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the tile list
+  static constexpr bool kFastK = false;
+  const double* tab;
+  const int2* tiles;
+  int n_grp, ld;
+  __device__ double operator()(int r, int k, int z) const {
+    return tab[((size_t)k * n_grp + tiles[z].x) * ld + r];
+  }
+};
+struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell
+  static constexpr bool kFastK = false;
+  const double *W, *rOm;
+  const int *gcells, *gstart;
+  const int2* tiles;
+  int ldN;
+  __device__ double operator()(int k, int c, int z) const {
+    const int2 tl = tiles[z];
+    const int g = tl.x, q = tl.y + c;
+    if (q >= gstart[g + 1] - gstart[g]) return 0.0;
+    const int i = gcells[gstart[g] + q];
+    return W[(size_t)k * ldN + i] * rOm[i];
+  }
+};
+
+// ---- epilogues -------------------------------------------------------------------------------
+struct EpPart {  // split-K partials part[z][r][c]
+  double* part;
+  int m, n;
+  __device__ void operator()(int r, int c, int z, double v) const { part[((size_t)z * m + r) * n + c] = v; }
+};
+struct EpColMajor {  // out[r + c*ld]
+  double* out;
+  int64_t ld;
+  __device__ void operator()(int r, int c, int, double v) const { out[r + (size_t)c * ld] = v; }
+};
+struct EpEta {  // E[i + j*ldN] = v + level coefficients of cell i in B_j
+  double* out;
+  const double* B;
+  const int *cv_nh, *codes;
+  int ldN, P, n_cv;
+  __device__ void operator()(int i, int j, int, double v) const {
+    double s = v;
+    for (int q = 0; q < n_cv; q++) s += B[cv_nh[q] + codes[(size_t)q * ldN + i] + (size_t)j * P];
+    out[i + (size_t)j * ldN] = s;
+  }
+};
+struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
+  double* S;
+  int n_grp, ld;
+  __device__ void operator()(int a, int j, int g, double v) const { S[((size_t)j * n_grp + g) * ld + a] = v; }
+};
+struct EpHK {  // HK[cell + a*ldN] with r = a, c = cell slot of tile z
+  double* HK;
+  const int *gcells, *gstart;
+  const int2* tiles;
+  int ldN;
+  __device__ void operator()(int a, int c, int z, double v) const {
+    const int2 tl = tiles[z];
+    const int q = tl.y + c;
+    if (q >= gstart[tl.x + 1] - gstart[tl.x]) return;
+    HK[gcells[gstart[tl.x] + q] + (size_t)a * ldN] = v;
+  }
+};
+
+}  // namespace
+
+// bvec[dcol[a] + j*P] = sum_z part[z][a][j]
+__global__ void k_reduce_bvec(int n_d, int J, int P, int nz, const int* __restrict__ dcol,
+                              const double* __restrict__ part, double* __restrict__ bvec) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = blockIdx.y;
+  if (j >= J) return;
+  double s = 0.0;
+  for (int z = 0; z < nz; z++) s += part[((size_t)z * n_d + a) * J + j];
+  bvec[dcol[a] + (size_t)j * P] = s;
+}
+
+template <class T, class LA, class LB, class KR, class Epi>
+static int launch_dgen(Ctx* c, dim3 grid, int m, int n, LA A, LB B, KR kr, Epi epi, const char* name) {
+  auto* fn = k_dgen<T, LA, LB, KR, Epi>;
+  GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, T::smem()));
+  fn<<<grid, 256, T::smem(), c->stream>>>(m, n, A, B, kr, epi);
+  GPL_LAUNCHED(c, name);
+  return GPL_OK;
+}
+
+static int ensure_part(Ctx* c, size_t n) {
+  if (c->part_n >= n) return GPL_OK;
+  if (c->part) cudaFree(c->part);
+  c->part = nullptr;
+  c->part_n = 0;
+  if (cudaMalloc((void**)&c->part, sizeof(double) * n) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "device allocation failed: split-K partials";
+    return GPL_ERR_ALLOC;
+  }
+  c->part_n = n;
+  return GPL_OK;
+}
+
+int dgen_zt_u(Ctx* c, int mode) {
+  using T = TileTall;
+  if (c->n_d > T::BM) return GPL_ERR_ARG;
+  const double* rOm = nullptr;
+  if (mode == 0) {
+    int rc = recip_omega(c, &rOm);
+    if (rc) return rc;
+  }
+  int rc = ensure_part(c, (size_t)kSplitK * c->n_d * c->J);
+  if (rc) return rc;
+  const int per = (c->N + kSplitK - 1) / kSplitK;
+  dim3 g(1, div_up(c->J, T::BN), kSplitK);
+  const double* u = mode == 0 ? c->Nu : c->scratch;
+  rc = launch_dgen<T>(c, g, c->n_d, c->J, LdDt{c->Dm, c->ldN}, LdU{c->W, u, rOm, c->ldN, mode},
+                      KSplit{c->N, per}, EpPart{c->part, c->n_d, c->J}, "k_dgen(zt_u)");
+  if (rc) return rc;
+  dim3 g2(div_up(c->J, 256), c->n_d);
+  k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, kSplitK, c->dcol_d, c->part, c->bvec);
+  GPL_LAUNCHED(c, "k_reduce_bvec");
+  return GPL_OK;
+}
+
+int dgen_c1_tn(Ctx* c) {
+  using T = TileSq;
+  const double* rOm = nullptr;
+  int rc = recip_omega(c, &rOm);
+  if (rc) return rc;
+  const int g0 = c->nh[c->p - 1];
+  dim3 g(div_up(c->N, T::BM), div_up(c->M, T::BN), 1);
+  return launch_dgen<T>(c, g, c->N, c->M, LdTn{c->W, c->Nu, c->scratch, rOm, c->phi, c->ldN},
+                        LdTBetaGP{c->tBeta, c->P, g0}, KAll{c->J}, EpColMajor{c->C1, (int64_t)c->ldN},
+                        "k_dgen(c1_tn)");
+}
+
+int dgen_eta(Ctx* c, const double* B, double* out) {
+  using T = TileSq;
+  dim3 g(div_up(c->N, T::BM), div_up(c->J, T::BN), 1);
+  return launch_dgen<T>(c, g, c->N, c->J, LdD{c->Dm, c->ldN}, LdBetaDense{B, c->dcol_d, c->P}, KAll{c->n_d},
+                        EpEta{out, B, c->cv_nh_d, c->codes_d, c->ldN, c->P, c->n_cv}, "k_dgen(eta)");
+}
+
+int dgen_group_sums(Ctx* c, int mode) {
+  using T = TileTall;
+  if (c->n_d > T::BM) return GPL_ERR_ARG;
+  const double* rOm = nullptr;
+  if (mode == 0) {
+    int rc = recip_omega(c, &rOm);
+    if (rc) return rc;
+  }
+  const int J = mode == 1 ? 1 : c->J;
+  dim3 g(1, div_up(J, T::BN), c->n_grp);
+  return launch_dgen<T>(c, g, c->n_d, J, LdGroupD{c->Dm, c->gcells_d, c->gstart_d, c->ldN},
+                        LdGroupW{c->W, rOm, c->gcells_d, c->gstart_d, c->ldN, mode}, KGroup{c->gstart_d},
+                        EpGroup{c->gsum, c->n_grp, c->n_d + 1}, "k_dgen(group_sums)");
+}
+
+int dgen_hk(Ctx* c) {
+  using T = TileTall;
+  const int ld = c->n_d + 1;
+  if (ld > T::BM) return GPL_ERR_ARG;
+  const double* rOm = nullptr;
+  int rc = recip_omega(c, &rOm);
+  if (rc) return rc;
+  dim3 g(1, 1, c->n_hk_tiles128);
+  return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
+                        LdTileO{c->W, rOm, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, KAll{c->J},
+                        EpHK{c->HK, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, "k_dgen(hk)");
+}
+
+}  // namespace gpl

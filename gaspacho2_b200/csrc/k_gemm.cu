@@ -289,15 +289,19 @@ int launch_zt_u(Ctx* c, int mode) {
     ProfScope ps(c, "zt_u");
     dim3 g(div_up(c->n_d, TM), div_up(c->J, TN));
     LoadDt A{c->Dm, c->ldN, c->N, c->n_d};
-    if (mode == 0) {
-      k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
-                                             LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J}, c->bvec,
-                                             (int64_t)c->P, c->dcol_d);
-    } else {
-      k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A, LoadCellGene{c->scratch, c->ldN, c->N, c->J},
-                                             c->bvec, (int64_t)c->P, c->dcol_d);
+    const int rc = c->simt_fp64 ? GPL_ERR_ARG : dgen_zt_u(c, mode);
+    if (rc != GPL_OK && rc != GPL_ERR_ARG) return rc;
+    if (rc == GPL_ERR_ARG) {  // the FFMA form: forced, or more dense columns than one DMMA tile
+      if (mode == 0)
+        k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
+                                               LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J}, c->bvec,
+                                               (int64_t)c->P, c->dcol_d);
+      else
+        k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
+                                               LoadCellGene{c->scratch, c->ldN, c->N, c->J}, c->bvec,
+                                               (int64_t)c->P, c->dcol_d);
+      GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
     }
-    GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
   }
   int rc = launch_group_sums(c, mode == 0 ? 3 : 2);
   if (rc) return rc;
@@ -307,6 +311,7 @@ int launch_zt_u(Ctx* c, int mode) {
 // C1 <- sum_j (tn_ij/phi_j) tBeta_j[GP]   (stored cell-fastest, ld ldN)
 int launch_c1_tn(Ctx* c) {
   ProfScope ps(c, "c1_tn");
+  if (!c->simt_fp64) return dgen_c1_tn(c);
   const int g0 = c->nh[c->p - 1];
   dim3 g(div_up(c->N, TM), div_up(c->M, TN));
   k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->M, c->J,

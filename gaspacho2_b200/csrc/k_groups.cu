@@ -121,6 +121,10 @@ __global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gce
 int launch_group_sums(Ctx* c, int mode) {
   if (c->n_grp == 0) return GPL_OK;
   ProfScope ps(c, "group_sums");
+  if ((mode == 0 || mode == 1) && !c->simt_fp64) {
+    const int rc = dgen_group_sums(c, mode);
+    if (rc != GPL_ERR_ARG) return rc;
+  }
   if (mode == 0 || mode == 1) {
     const int J = mode == 1 ? 1 : c->J;
     dim3 g(div_up(J, TM), div_up(c->n_d, TN), c->n_grp);
@@ -336,6 +340,10 @@ __global__ void __launch_bounds__(256) k_hk(int ldN, int J, int n_d, int n_grp, 
 int launch_hk(Ctx* c) {
   if (c->n_grp == 0) return GPL_OK;
   ProfScope ps(c, "hk");
+  if (!c->simt_fp64) {
+    const int rc = dgen_hk(c);
+    if (rc != GPL_ERR_ARG) return rc;
+  }
   dim3 g(c->n_hk_tiles, div_up(c->n_d + 1, TN));
   k_hk<<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_d, c->n_grp, c->hk_tiles_d, c->gcells_d, c->gstart_d, c->W,
                                  c->Omega, c->gsum, c->HK);
