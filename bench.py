@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--irls-sweeps", type=int, default=2)
     ap.add_argument("--cpu-genes", type=int, default=6, help="genes in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fit-config", type=int, default=1, help="configuration of the time-to-fit leg")
+    ap.add_argument("--fit-lbfgs", type=int, default=200, help="L-BFGS step budget of the time-to-fit leg")
+    ap.add_argument("--no-fit", action="store_true", help="skip the time-to-fit leg")
     return ap.parse_args()
 
 
@@ -231,6 +234,41 @@ def workload_config(ds, args, precision):
             "global_batch": ds.N, "seq_len": None}
 
 
+def time_to_fit(args, stream, device):
+    """The driver's whole fit (kernel matrices, GLM initialisation, then outer iterations of
+    IRLS to convergence and L-BFGS with the backtracking line search) from the seeded
+    PCA / k-means initialisation, up to the L-BFGS step budget, timed with CUDA events on the
+    library's stream (the line-search decisions read the objective on the host, as in the
+    reference driver, so this is also the wall time)."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+
+    ds = synth.make(args.fit_config, 0, init=True)
+    m = GPLVM.from_dataset(ds, device=device, stream=stream.cuda_stream, precision=args.precision)
+    m.set_params(ds.init)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    s.record(stream)
+    m.kernel_mats()
+    m.glm_init()
+    rc, st, trace = m.fit(100000, args.fit_lbfgs)
+    e.record(stream)
+    torch.cuda.synchronize()
+    wall = time.time() - t0
+    secs = s.elapsed_time(e) / 1e3
+    m.close()
+    cfg = synth.CONFIGS[args.fit_config]
+    return {"seconds": secs, "wall_seconds": wall, "lbfgs_budget": args.fit_lbfgs,
+            "workload": f"config {args.fit_config}: N={ds.N} cells, G={ds.J} genes, M={ds.M}, Q={ds.Q}, "
+                        f"seeded PCA/k-means initialisation",
+            "precision": args.precision, "outer_iterations": st["outer"], "irls_sweeps": st["irls"],
+            "lbfgs_steps": st["lbfgs"], "objective_evaluations": st["evals"],
+            "final_objective": float(trace[-1]) if len(trace) else None, "nan_exit": bool(rc),
+            "batch_levels": cfg.get("batch"), "donors": cfg.get("donors")}
+
+
 def run_ours(args):
     import torch
 
@@ -365,6 +403,8 @@ def run_ours(args):
             "hbm_gbs_measured": peaks.get("hbm_gbs"), "bf16_tflops_measured": peaks.get("bf16_tflops"),
         }
     m.close()
+    if rank == 0 and not args.no_fit:
+        line["time_to_fit"] = time_to_fit(args, stream, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cs = CpuSample(ds, args.cpu_genes)
         t = cs.step()
