@@ -324,7 +324,7 @@ def run_ours(args):
     launches = m.launches() - l0
     ck = clocks.stop()
     prof = {}
-    for name in ("gram", "uq", "spair", "v_to_u", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
+    for name in ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
                  "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
                  "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk"):
         ms, n = m.profile_read(name)
@@ -367,7 +367,8 @@ def run_ours(args):
         P = m.P
         ft = flops_table(m.N, m.J, m.M, P, m.n_dense())
         peaks = measured_peaks()
-        if dom in ft and args.precision == "bf16x3" and dom in ("gram", "uq"):
+        tc_kernels = ("gram", "uq") if os.environ.get("GPL_TC_GRAD") else ("gram",)
+        if dom in ft and args.precision == "bf16x3" and dom in tc_kernels:
             # useful flops of the contraction; the hi/lo split issues 3 BF16 products per useful MAC
             tflops = ft[dom]
             pk = peaks.get("bf16_tflops_sustained") or FALLBACK_BF16_SUSTAINED

@@ -326,6 +326,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
   c->precision = precision;
   c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
   c->simt_fp64 = getenv("GPL_FP64_SIMT") != nullptr;
+  c->tc_grad = getenv("GPL_TC_GRAD") != nullptr;
   return GPL_OK;
 }
 

@@ -69,6 +69,11 @@ struct TcState {
   __nv_bfloat16 *whi = nullptr, *wlo = nullptr, *bhi = nullptr, *blo = nullptr;
   float* Dt = nullptr;
   double* Up = nullptr;
+  double *Lw = nullptr, *Gt = nullptr, *Tt = nullptr;  // prior factor, whitened Gram, product
+  float* DtC = nullptr;                                 // whitened dense columns (cell fastest)
+  __nv_bfloat16 *ahi = nullptr, *alo = nullptr;         // pair products, pair rows x cells
+  CUtensorMap map_ahi, map_alo;
+  int smem_whiten = 0;
   int2* pairs = nullptr;
   int* err = nullptr;
   CUtensorMap map_whi, map_wlo, map_bhi, map_blo;
@@ -79,6 +84,7 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int precision = GPL_PREC_FP64;
+  bool tc_grad = false;    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
   bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
   std::string err;
 
@@ -208,6 +214,7 @@ int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns 
 int dgen_eta(Ctx* c, const double* B, double* out);
 int dgen_group_sums(Ctx* c, int mode);
 int dgen_hk(Ctx* c);
+int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw);  // Psi_DD = L G L^T + DeltaInv
 int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
 int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting

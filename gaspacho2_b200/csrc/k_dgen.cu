@@ -282,6 +282,52 @@ struct EpHK {  // HK[cell + a*ldN] with r = a, c = cell slot of tile z
   }
 };
 
+// Un-whitening of the precision form's Gram, one gene per z: T = G L^T, then L T.
+struct LdGene {  // A(r, k, z) = G_z[r + k*n] (r contiguous)
+  static constexpr bool kFastK = false;
+  const double* G;
+  int n;
+  __device__ double operator()(int r, int k, int z) const { return G[(size_t)z * n * n + r + (size_t)k * n]; }
+};
+struct LdGeneT {  // B(k, c, z) = T_z[k + c*n] (k contiguous)
+  static constexpr bool kFastK = true;
+  const double* T;
+  int n;
+  __device__ double operator()(int k, int c, int z) const { return T[(size_t)z * n * n + k + (size_t)c * n]; }
+};
+// L is the lower triangle of a factor whose strict upper triangle still holds the input
+struct LdLT {  // B(k, c) = L[c][k] = L[c + k*n] (c contiguous), 0 above the diagonal
+  static constexpr bool kFastK = false;
+  const double* L;
+  int n;
+  __device__ double operator()(int k, int c, int) const { return c >= k ? L[c + (size_t)k * n] : 0.0; }
+};
+struct LdL {  // A(r, k) = L[r][k] = L[r + k*n] (r contiguous), 0 above the diagonal
+  static constexpr bool kFastK = false;
+  const double* L;
+  int n;
+  __device__ double operator()(int r, int k, int) const { return r >= k ? L[r + (size_t)k * n] : 0.0; }
+};
+struct EpGene {  // T_z[r + c*n]
+  double* T;
+  int n;
+  __device__ void operator()(int r, int c, int z, double v) const { T[(size_t)z * n * n + r + (size_t)c * n] = v; }
+};
+struct EpPsiDD {  // Psi_z at (dcol r, dcol c) and its mirror, plus DeltaInv; r <= c only
+  double* Psi;
+  const double* Dinv;
+  const int* dcol;
+  int P;
+  __device__ void operator()(int r, int c, int z, double v) const {
+    if (r > c) return;
+    const size_t mk = dcol[r], ml = dcol[c];
+    const double x = v + Dinv[mk + ml * P];
+    double* Pz = Psi + (size_t)z * P * P;
+    Pz[mk + ml * P] = x;
+    Pz[ml + mk * P] = x;
+  }
+};
+
 }  // namespace
 
 // bvec[dcol[a] + j*P] = sum_z part[z][a][j]
@@ -385,6 +431,17 @@ int dgen_hk(Ctx* c) {
   return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
                         LdTileO{c->W, rOm, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, KAll{c->J},
                         EpHK{c->HK, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, "k_dgen(hk)");
+}
+
+int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw) {
+  using T = TileTall;
+  const int n = c->n_d;
+  if (n > T::BM || c->J > 65535) return GPL_ERR_ARG;
+  dim3 g(1, div_up(n, T::BN), c->J);
+  int rc = launch_dgen<T>(c, g, n, n, LdGene{Gt, n}, LdLT{Lw, n}, KAll{n}, EpGene{Tt, n}, "k_dgen(unwhiten GL^T)");
+  if (rc) return rc;
+  return launch_dgen<T>(c, g, n, n, LdL{Lw, n}, LdGeneT{Tt, n}, KAll{n}, EpPsiDD{c->Psi, c->DeltaInv, c->dcol_d, c->P},
+                        "k_dgen(unwhiten L(GL^T))");
 }
 
 }  // namespace gpl

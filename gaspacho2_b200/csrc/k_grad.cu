@@ -230,7 +230,7 @@ int launch_grad_omega(Ctx* c) {
   }
   rc = launch_c1_tn(c);  // C1 = sum_j tn/phi tBeta_GP
   if (rc) return rc;
-  if (c->precision == GPL_PREC_BF16X3) {
+  if (c->precision == GPL_PREC_BF16X3 && c->tc_grad) {
     rc = launch_tc_grad(c);
     if (rc) return rc;
   } else if (!c->simt_fp64) {

@@ -42,7 +42,8 @@ namespace gpl {
 using namespace tc;
 
 namespace {
-constexpr int kThreads = 320;
+constexpr int kThreads = 320;           // gradient: TMA, MMA, 4 producer and 4 drain warps
+constexpr int kThreadsGram = 192;       // Gram: TMA, MMA and 4 drain warps
 constexpr int kStagesGram = 3;          // pipeline depth, Gram (192 KB of operand tiles)
 constexpr int kStagesGrad = 2;          // pipeline depth, gradient (B tiles up to 20 KB, plus D rows)
 constexpr int kMaxStages = 3;
@@ -52,6 +53,7 @@ constexpr int kSBGrad = 8;              // chunks per FP32 run (gradient)
 constexpr int kTileA = 128 * 128;       // 128 rows x 64 BF16
 constexpr int kTileBG = kGramN * 128;   // 128 gene rows x 64 BF16
 constexpr int kGradSplits = 4;
+constexpr int kMaxWhiten = 160;         // dense columns the whitened rows kernel holds per cell
 constexpr uint32_t kIdescGram = idesc_bf16_f32(128, kGramN);
 }  // namespace
 
@@ -70,9 +72,9 @@ __device__ __forceinline__ void tc_fail(int* err, TcShared* sh, int code) {
   atomicCAS(err, 0, code);
 }
 
-__device__ __forceinline__ void tc_init(TcShared* sh, const int* err) {
+__device__ __forceinline__ void tc_init(TcShared* sh, const int* err, int full_count) {
   for (int s = 0; s < kMaxStages; s++) {
-    mbar_init(&sh->full[s], 1 + 128);
+    mbar_init(&sh->full[s], full_count);
     mbar_init(&sh->empty[s], 1);
   }
   for (int b = 0; b < 2; b++) {
@@ -125,11 +127,12 @@ __device__ __forceinline__ void drain_f32_to_f64(uint32_t lane_addr, uint32_t sr
 // ---------------------------------------------------------------------------------------------
 // Gram
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 1)
-    k_tc_gram(const __grid_constant__ CUtensorMap map_whi, const __grid_constant__ CUtensorMap map_wlo,
-              const float* __restrict__ Dt, int n_dp, const int2* __restrict__ pairs, int n_pairs,
+__global__ void __launch_bounds__(kThreadsGram, 1)
+    k_tc_gram(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
+              const __grid_constant__ CUtensorMap map_whi, const __grid_constant__ CUtensorMap map_wlo,
+              const int2* __restrict__ pairs, int n_pairs,
               int chunks_total, const int* __restrict__ dcol, int P, int J, const double* __restrict__ Dinv,
-              double* __restrict__ Psi, int* __restrict__ err) {
+              double* __restrict__ Psi, double* __restrict__ Gt, int n_d, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* A_hi = base;
@@ -144,10 +147,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nch = chunks_total;
   const int nsb = (nch + kSBGram - 1) / kSBGram;
 
-  if (threadIdx.x == 0) tc_init(sh, err);
+  if (threadIdx.x == 0) tc_init(sh, err, 1);
   __syncthreads();
   if (sh->abort) return;
-  for (int r = threadIdx.x; r < 128; r += kThreads) {
+  for (int r = threadIdx.x; r < 128; r += kThreadsGram) {
     const int p = ptile * 128 + r;
     spairs[r] = p < n_pairs ? pairs[p] : make_int2(-1, -1);
   }
@@ -161,14 +164,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = sh->tmem;
 
   if (warp == 0) {
-    if (lane == 0) {  // TMA: the weights of 128 genes x 64 cells per stage
+    if (lane == 0) {  // TMA: pair products (128 pairs) and weights (128 genes) of 64 cells per stage
       int issued = 0;
       for (int it = 0; it < nch; it++) {
         const int s = it % kStagesGram;
         if (it >= kStagesGram && !mbar_wait(&sh->empty[s], ((it / kStagesGram) - 1) & 1, err)) { tc_fail(err, sh, 11); break; }
         if (sh->abort) break;
-        mbar_arrive_expect_tx(&sh->full[s], 2u * kTileBG);
+        mbar_arrive_expect_tx(&sh->full[s], 2u * kTileA + 2u * kTileBG);
         const int x = it * 64;
+        tma_load_2d(A_hi + s * kTileA, &map_ahi, &sh->full[s], x, ptile * 128);
+        tma_load_2d(A_lo + s * kTileA, &map_alo, &sh->full[s], x, ptile * 128);
         tma_load_2d(B_hi + s * kTileBG, &map_whi, &sh->full[s], x, n0);
         tma_load_2d(B_lo + s * kTileBG, &map_wlo, &sh->full[s], x, n0);
         issued = it + 1;
@@ -202,36 +207,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       mma_finish(sh, err, 17);
     }
-  } else if (warp < 6) {
-    // A producers: thread r owns A row r (pair r of the tile)
-    const int r = threadIdx.x - 64;
-    const int2 ab = spairs[r];
-    for (int it = 0; it < nch; it++) {
-      const int s = it % kStagesGram;
-      if (it >= kStagesGram && !mbar_wait(&sh->empty[s], ((it / kStagesGram) - 1) & 1, err)) { tc_fail(err, sh, 14); break; }
-      if (sh->abort) break;
-      const int cell0 = it * 64;
-      const uint32_t ah = smem_u32(A_hi + s * kTileA), al = smem_u32(A_lo + s * kTileA);
-#pragma unroll 2
-      for (int c16 = 0; c16 < 8; c16++) {
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          float x0 = 0.f, x1 = 0.f;
-          if (ab.x >= 0) {
-            const float* d0 = Dt + (size_t)(cell0 + c16 * 8 + 2 * q) * n_dp;
-            x0 = d0[ab.x] * d0[ab.y];
-            x1 = d0[n_dp + ab.x] * d0[n_dp + ab.y];
-          }
-          split_bf16x2(x0, x1, h[q], l[q]);
-        }
-        const uint32_t o = sw128_offset(r, c16);
-        st_shared_v4(ah + o, h[0], h[1], h[2], h[3]);
-        st_shared_v4(al + o, l[0], l[1], l[2], l[3]);
-      }
-      fence_proxy_async();
-      mbar_arrive(&sh->full[s]);
-    }
   } else {
     // drain warps: FP32 runs -> FP64 sum, then the results into Psi
     const int q = warp & 3;
@@ -264,9 +239,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int k = 0; k < 16; k++) {
           const int j = n0 + cb + k;
           if (live && j < J) {
-            double* Pj = Psi + (size_t)j * P * P;
-            Pj[ml + mk * P] = v[k] + dv;
-            Pj[mk + ml * P] = v[k] + dv;
+            if (Gt) {  // whitened Gram of the dense columns, both triangles, un-whitened later
+              double* Gj = Gt + (size_t)j * n_d * n_d;
+              Gj[ab.x + (size_t)ab.y * n_d] = v[k];
+              Gj[ab.y + (size_t)ab.x * n_d] = v[k];
+            } else {
+              double* Pj = Psi + (size_t)j * P * P;
+              Pj[ml + mk * P] = v[k] + dv;
+              Pj[mk + ml * P] = v[k] + dv;
+            }
           }
         }
       }
@@ -302,6 +283,67 @@ __global__ void k_dense_rows(int N, int ldN, int n_d, int n_dp, int rows, const 
   Dt[e] = (i < N && a < n_d) ? (float)D[(size_t)a * ldN + i] : 0.f;
 }
 
+// The prior block of the dense columns, DeltaInv[dcol a, dcol b] (upper triangle, a <= b), for
+// its Cholesky factor L (DeltaInv_DD = L L^T).
+__global__ void k_gather_dinv(int n_d, int P, const int* __restrict__ dcol, const double* __restrict__ Dinv,
+                              double* __restrict__ Lw) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+  if (a >= n_d) return;
+  Lw[a + (size_t)b * n_d] = a <= b ? Dinv[dcol[a] + (size_t)dcol[b] * P] : 0.0;
+}
+
+// Whitened dense rows L^{-1} d_i in FP64 by forward substitution, stored as FP32 rows of n_dp
+// (zero padding). The factor's lower triangle is staged in shared memory.
+__global__ void __launch_bounds__(128) k_whiten_rows(int N, int ldN, int n_d, int n_dp, int rows,
+                                                     const double* __restrict__ D, const double* __restrict__ Lw,
+                                                     float* __restrict__ Dt, float* __restrict__ DtC) {
+  extern __shared__ double ls[];  // lower triangle, row a at a*(a+1)/2
+  for (int e = threadIdx.x; e < n_d * n_d; e += blockDim.x) {
+    const int a = e % n_d, b = e / n_d;
+    if (b <= a) ls[a * (a + 1) / 2 + b] = Lw[a + (size_t)b * n_d];
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows) return;
+  float* out = Dt + (size_t)i * n_dp;
+  if (i >= N) {
+    for (int a = 0; a < n_dp; a++) out[a] = 0.f;
+    for (int a = 0; a < n_d; a++) DtC[(size_t)a * rows + i] = 0.f;
+    return;
+  }
+  double y[kMaxWhiten];
+  for (int a = 0; a < n_d; a++) {
+    const double* la = ls + a * (a + 1) / 2;
+    double s = D[(size_t)a * ldN + i];
+    for (int b = 0; b < a; b++) s = fma(-la[b], y[b], s);
+    y[a] = s / la[a];
+    out[a] = (float)y[a];
+    DtC[(size_t)a * rows + i] = (float)y[a];
+  }
+  for (int a = n_d; a < n_dp; a++) out[a] = 0.f;
+}
+
+// Pair products of the whitened columns as BF16 hi/lo, one row of cells per column pair
+// (rows past the pairs are zero): the A operand of the tensor-core Gram, read by TMA.
+__global__ void k_pair_split(int cpad, int n_pairs, const int2* __restrict__ pairs, const float* __restrict__ DtC,
+                             __nv_bfloat16* __restrict__ ahi, __nv_bfloat16* __restrict__ alo) {
+  const int p = blockIdx.y;
+  const int2 ab = p < n_pairs ? pairs[p] : make_int2(-1, -1);
+  for (int i2 = (blockIdx.x * blockDim.x + threadIdx.x) * 2; i2 < cpad; i2 += gridDim.x * blockDim.x * 2) {
+    float x0 = 0.f, x1 = 0.f;
+    if (ab.x >= 0) {
+      const float2 da = *reinterpret_cast<const float2*>(DtC + (size_t)ab.x * cpad + i2);
+      const float2 db = *reinterpret_cast<const float2*>(DtC + (size_t)ab.y * cpad + i2);
+      x0 = da.x * db.x;
+      x1 = da.y * db.y;
+    }
+    uint32_t h, l;
+    split_bf16x2(x0, x1, h, l);
+    *reinterpret_cast<uint32_t*>(ahi + (size_t)p * cpad + i2) = h;
+    *reinterpret_cast<uint32_t*>(alo + (size_t)p * cpad + i2) = l;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Gradient contraction
 // ---------------------------------------------------------------------------------------------
@@ -334,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nsb = (nch + kSBGrad - 1) / kSBGrad;
   const uint32_t idesc = idesc_bf16_f32(128, n_b);
 
-  if (threadIdx.x == 0) tc_init(sh, err);
+  if (threadIdx.x == 0) tc_init(sh, err, 1 + 128);
   __syncthreads();
   if (sh->abort) return;
   for (int e = threadIdx.x; e < 128 * n_d; e += kThreads) {
@@ -572,14 +614,28 @@ int tc_prepare(Ctx* c) {
   if ((rc = tc_alloc(c, &t.whi, (size_t)J * t.cpad, "w hi"))) return rc;
   if ((rc = tc_alloc(c, &t.wlo, (size_t)J * t.cpad, "w lo"))) return rc;
   if ((rc = tc_alloc(c, &t.Dt, (size_t)t.cpad * t.n_dp, "dense rows"))) return rc;
+  if ((rc = tc_alloc(c, &t.DtC, (size_t)t.cpad * n_d, "whitened dense columns"))) return rc;
+  if ((rc = tc_alloc(c, &t.ahi, (size_t)t.pair_tiles * 128 * t.cpad, "pair products hi"))) return rc;
+  if ((rc = tc_alloc(c, &t.alo, (size_t)t.pair_tiles * 128 * t.cpad, "pair products lo"))) return rc;
   if ((rc = tc_alloc(c, &t.pairs, (size_t)t.n_pairs, "pairs"))) return rc;
   if ((rc = tc_alloc(c, &t.bhi, (size_t)t.n_b * t.Kpad, "S hi"))) return rc;
   if ((rc = tc_alloc(c, &t.blo, (size_t)t.n_b * t.Kpad, "S lo"))) return rc;
   if ((rc = tc_alloc(c, &t.Up, (size_t)t.grad_splits * t.n_b * t.cpad, "grad partials"))) return rc;
   if ((rc = tc_alloc(c, &t.err, 1, "tc error flag"))) return rc;
+  if ((rc = tc_alloc(c, &t.Lw, (size_t)n_d * n_d, "prior factor"))) return rc;
+  if ((rc = tc_alloc(c, &t.Gt, (size_t)J * n_d * n_d, "whitened Gram"))) return rc;
+  if ((rc = tc_alloc(c, &t.Tt, (size_t)J * n_d * n_d, "un-whitening product"))) return rc;
+  if (n_d > kMaxWhiten || J > 65535) {
+    c->err = "the tensor-core form supports at most 160 dense model columns and 65535 genes";
+    return GPL_ERR_ARG;
+  }
+  t.smem_whiten = (int)sizeof(double) * n_d * (n_d + 1) / 2;
+  GPL_TRY(c, cudaFuncSetAttribute(k_whiten_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_whiten));
   GPL_TRY(c, cudaMemset(t.err, 0, sizeof(int)));
   GPL_TRY(c, cudaMemcpy(t.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  if (!make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN) ||
+  if (!make_map(&t.map_ahi, t.ahi, t.cpad, (uint64_t)t.pair_tiles * 128, 128) ||
+      !make_map(&t.map_alo, t.alo, t.cpad, (uint64_t)t.pair_tiles * 128, 128) ||
+      !make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN) ||
       !make_map(&t.map_bhi, t.bhi, t.Kpad, t.n_b, t.n_b) || !make_map(&t.map_blo, t.blo, t.Kpad, t.n_b, t.n_b)) {
     c->err = "cuTensorMapEncodeTiled failed";
     return GPL_ERR_CUDA;
@@ -599,7 +655,7 @@ int tc_prepare(Ctx* c) {
 
 void tc_release(Ctx* c) {
   TcState& t = c->tc;
-  void* bufs[] = {t.whi, t.wlo, t.Dt, t.pairs, t.bhi, t.blo, t.Up, t.err};
+  void* bufs[] = {t.whi, t.wlo, t.Dt, t.pairs, t.bhi, t.blo, t.Up, t.err, t.Lw, t.Gt, t.Tt, t.DtC, t.ahi, t.alo};
   for (void* p : bufs)
     if (p) cudaFree(p);
   const bool keep = t.check_each;
@@ -630,7 +686,24 @@ int launch_tc_gram(Ctx* c) {
   int rc = tc_prepare(c);
   if (rc) return rc;
   TcState& t = c->tc;
-  if ((rc = launch_dense_rows(c))) return rc;
+  {
+    // Whitening by the prior's factor: the tensor-core Gram of L^{-1} d_i, whose errors are then
+    // relative to a matrix bounded below by the identity, is mapped back as L G L^T + DeltaInv in
+    // FP64. Without it, cond(Psi_j) ~ 1e14 (no jitter on Kmm) turns 1e-6 Gram errors into failed
+    // Cholesky factorizations.
+    ProfScope ps(c, "whiten");
+    dim3 g(div_up(c->n_d, 128), c->n_d);
+    k_gather_dinv<<<g, 128, 0, c->stream>>>(c->n_d, c->P, c->dcol_d, c->DeltaInv, t.Lw);
+    GPL_LAUNCHED(c, "k_gather_dinv");
+    launch_chol_exact_raw(c->stream, t.Lw, c->n_d);
+    GPL_LAUNCHED(c, "k_chol_exact");
+    k_whiten_rows<<<t.cpad / 128, 128, t.smem_whiten, c->stream>>>(c->N, c->ldN, c->n_d, t.n_dp, t.cpad, c->Dm,
+                                                                    t.Lw, t.Dt, t.DtC);
+    GPL_LAUNCHED(c, "k_whiten_rows");
+    dim3 gp(std::min(16, div_up(t.cpad, 512)), t.pair_tiles * 128);
+    k_pair_split<<<gp, 256, 0, c->stream>>>(t.cpad, t.n_pairs, t.pairs, t.DtC, t.ahi, t.alo);
+    GPL_LAUNCHED(c, "k_pair_split");
+  }
   {
     ProfScope ps(c, "split_weights");
     dim3 g(std::min(64, div_up(t.cpad, 512)), std::min(c->J, 65535));
@@ -640,10 +713,15 @@ int launch_tc_gram(Ctx* c) {
   {
     ProfScope ps(c, "gram");
     dim3 g(t.pair_tiles, t.gram_tiles_n);
-    k_tc_gram<<<g, kThreads, t.smem_gram, c->stream>>>(t.map_whi, t.map_wlo, t.Dt, t.n_dp, t.pairs, t.n_pairs,
+    k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
+                                                           t.n_pairs,
                                                        t.chunks_cells, c->dcol_d, c->P, c->J, c->DeltaInv, c->Psi,
-                                                       t.err);
+                                                       t.Gt, c->n_d, t.err);
     GPL_LAUNCHED(c, "k_tc_gram");
+  }
+  {
+    ProfScope ps(c, "unwhiten");
+    if ((rc = dgen_unwhiten(c, t.Gt, t.Tt, t.Lw))) return rc;
   }
   return c->tc.check_each ? tc_check_flag(c) : GPL_OK;
 }
