@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--fit-config", type=int, default=1, help="configuration of the time-to-fit leg")
     ap.add_argument("--fit-lbfgs", type=int, default=200, help="L-BFGS step budget of the time-to-fit leg")
     ap.add_argument("--no-fit", action="store_true", help="skip the time-to-fit leg")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="instead of the benchmark: the precision form against FP64 along a fit, every 10 steps")
     return ap.parse_args()
 
 
@@ -419,8 +421,60 @@ def run_ours(args):
     return 0
 
 
+def precision_report(args):
+    """The precision form against the plain FP64 path along a fit of --fit-config, every 10th
+    L-BFGS step up to --fit-lbfgs: the two fits are run to each budget from the same seeded
+    initialisation (the runs are deterministic, so the first k steps of a longer run are the
+    k-step run), and compared on the objective, X and the GLM coefficients; at the precision
+    fit's state both forms then evaluate the objective and gradient, which gives the
+    per-evaluation errors along the trajectory. One JSON line per checkpoint."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ds = synth.make(args.fit_config, 0, init=True)
+
+    def fit(prec, budget):
+        m = GPLVM.from_dataset(ds, stream=stream.cuda_stream, precision=prec)
+        m.set_params(ds.init)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        m.kernel_mats()
+        m.glm_init()
+        rc, st, tr = m.fit(100000, budget)
+        m.sync()
+        return m, time.time() - t0, st, tr
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+    for k in range(10, args.fit_lbfgs + 1, 10):
+        mf, tf, sf, trf = fit("fp64", k)
+        mb, tb, sb, trb = fit("bf16x3", k)
+        row = {"config": args.fit_config, "lbfgs_steps": k, "seconds_fp64": tf, "seconds_bf16x3": tb,
+               "objective_fp64": float(trf[-1]), "objective_bf16x3": float(trb[-1]),
+               "objective_rel_diff": abs(trb[-1] - trf[-1]) / abs(trf[-1]),
+               "X_rel_l2": rel(mb.get("X"), mf.get("X")), "beta_rel_l2": rel(mb.get("Beta"), mf.get("Beta")),
+               "evals_fp64": sf["evals"], "evals_bf16x3": sb["evals"]}
+        x = mb.params_vector()
+        vb, gb = mb.evaluate(x)
+        gb = gb.copy()
+        mb.set_precision("fp64")
+        vf, gf = mb.evaluate(x)
+        row["at_bf16x3_state"] = {"objective_rel_err": abs(vb - vf) / abs(vf), "gradient_rel_l2": rel(gb, gf)}
+        mf.close()
+        mb.close()
+        print(json.dumps(row), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.precision_report:
+        return precision_report(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -100,7 +100,7 @@ static void free_state(Ctx* c) {
                   c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
                   c->grad0,  c->ss,     c->SS,      c->XX,      c->gdtmp,  c->C1,     c->C2,     c->grtmp,
                   c->KmmInv, c->bvec,   c->sol,     c->red,     c->lb_work, c->mc_d,  c->mv_d,   c->mk_d,
-                  c->nh_d};
+                  c->nh_d,   c->rres,   c->bx};
   for (void* p : bufs)
     if (p) cudaFree(p);
   c->Z = c->W = c->Nu = c->Psi = c->PsiInv = c->Beta = c->tBeta = c->scratch = c->U = nullptr;
@@ -108,6 +108,7 @@ static void free_state(Ctx* c) {
   c->rho = c->phi = c->ls = c->lkhds = c->lkhd_dev = c->grad = c->grad0 = c->ss = c->SS = c->XX = nullptr;
   c->gdtmp = c->C1 = c->C2 = c->grtmp = c->KmmInv = c->bvec = c->sol = c->red = c->lb_work = nullptr;
   c->mc_d = c->mv_d = c->mk_d = c->nh_d = nullptr;
+  c->rres = c->bx = nullptr;
   c->have_design = false;
 }
 
@@ -206,7 +207,7 @@ static int gradient_launch(Ctx* c) {
   GPL_RUN(launch_expand_delta(c));
   GPL_RUN(launch_oinvt(c));
   GPL_RUN(launch_zt_u(c, 0));
-  GPL_RUN(launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->tBeta, c->P, c->J));
+  GPL_RUN(solve_refined(c, c->bvec, c->tBeta));
   GPL_RUN(launch_inverse_batched(c));
   GPL_RUN(launch_grad_delta(c));
   GPL_RUN(launch_grad_omega(c));
@@ -327,6 +328,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
   c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
   c->simt_fp64 = getenv("GPL_FP64_SIMT") != nullptr;
   c->tc_grad = getenv("GPL_TC_GRAD") != nullptr;
+  if (const char* rs = getenv("GPL_REFINE")) c->refine_steps = atoi(rs);
   return GPL_OK;
 }
 
@@ -541,6 +543,8 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->tBeta, (size_t)P * J, "tBeta"));
   GPL_RUN(dalloc(c, &c->bvec, (size_t)P * J, "bvec"));
   GPL_RUN(dalloc(c, &c->sol, (size_t)P * J, "sol"));
+  GPL_RUN(dalloc(c, &c->rres, (size_t)P * J, "refinement residual"));
+  GPL_RUN(dalloc(c, &c->bx, (size_t)P * J, "refinement product"));
   GPL_RUN(dalloc(c, &c->scratch, scratch_n, "scratch"));
   GPL_RUN(dalloc(c, &c->U, ldN * n_d, "U"));
   GPL_RUN(dalloc(c, &c->Kmm, (size_t)M * M, "Kmm"));

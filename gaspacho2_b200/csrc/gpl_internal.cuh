@@ -84,7 +84,10 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int precision = GPL_PREC_FP64;
-  bool tc_grad = false;    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
+  bool tc_grad = false;
+  int refine_steps = 1;              // precision form: FP64-residual refinement steps per solve
+  const double* zt_u_src = nullptr;  // u of Z^T diag(W/Omega) u when not nu (set during a refinement)
+  double *rres = nullptr, *bx = nullptr;  // refinement residual and product, P x J    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
   bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
   std::string err;
 
@@ -183,12 +186,14 @@ int launch_chol_single(Ctx* c, double* A, int n);  // choldc on one n x n matrix
 // k_groups.cu
 int launch_group_sums(Ctx* c, int mode);  // 0: S (W/Omega); 1: S unweighted (gene 0); 2: T of y0; 3: T of nu
 int launch_assemble_psi(Ctx* c, int J);   // categorical rows/columns of Psi from the group sums
-int launch_assemble_b(Ctx* c);            // categorical entries of bvec from the group sums
+int launch_assemble_b(Ctx* c, double* out);  // categorical entries of Z^T u (P x J) from the group sums
 int launch_group_tables(Ctx* c);          // per (gene, group) categorical blocks of Psi^{-1}
 int launch_hk(Ctx* c);                    // HK[i] = sum_j O_ij [h_{j,g(i)} | kappa_{j,g(i)}]
 // k_gemm.cu
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
+int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output
+int solve_refined(Ctx* c, const double* b, double* x);  // Psi_j x = b; FP64-residual refinement (precision form)
 int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
 int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
 int launch_c1_tn(Ctx* c);                // C1 partial from tn/phi and tBeta GP block
@@ -209,7 +214,7 @@ int launch_pair_gram(Ctx* c);             // dense block of every Psi_j, FP64 DM
 int launch_pair_uq(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i, FP64 DMMA over column pairs
 void pair_release(Ctx* c);
 int recip_omega(Ctx* c, const double** rOm);  // 1/Omega (0 past N), refreshed on every call
-int dgen_zt_u(Ctx* c, int mode);          // DMMA forms of the cell x gene GEMMs (k_dgen.cu);
+int dgen_zt_u(Ctx* c, int mode, const double* u, double* out);          // DMMA forms of the cell x gene GEMMs (k_dgen.cu);
 int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns exceed one tile
 int dgen_eta(Ctx* c, const double* B, double* out);
 int dgen_group_sums(Ctx* c, int mode);

@@ -364,7 +364,7 @@ static int ensure_part(Ctx* c, size_t n) {
   return GPL_OK;
 }
 
-int dgen_zt_u(Ctx* c, int mode) {
+int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
   using T = TileTall;
   if (c->n_d > T::BM) return GPL_ERR_ARG;
   const double* rOm = nullptr;
@@ -376,12 +376,11 @@ int dgen_zt_u(Ctx* c, int mode) {
   if (rc) return rc;
   const int per = (c->N + kSplitK - 1) / kSplitK;
   dim3 g(1, div_up(c->J, T::BN), kSplitK);
-  const double* u = mode == 0 ? c->Nu : c->scratch;
   rc = launch_dgen<T>(c, g, c->n_d, c->J, LdDt{c->Dm, c->ldN}, LdU{c->W, u, rOm, c->ldN, mode},
                       KSplit{c->N, per}, EpPart{c->part, c->n_d, c->J}, "k_dgen(zt_u)");
   if (rc) return rc;
   dim3 g2(div_up(c->J, 256), c->n_d);
-  k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, kSplitK, c->dcol_d, c->part, c->bvec);
+  k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, kSplitK, c->dcol_d, c->part, out);
   GPL_LAUNCHED(c, "k_reduce_bvec");
   return GPL_OK;
 }

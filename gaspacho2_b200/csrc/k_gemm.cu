@@ -284,28 +284,31 @@ int launch_init_response(Ctx* c) {
 }
 
 // Z^T u: dense rows by GEMM (mode 0: u = W/Omega nu; 1: u = y0), categorical rows from groups
-int launch_zt_u(Ctx* c, int mode) {
+int launch_zt_u(Ctx* c, int mode) { return launch_zt_u_ex(c, mode, mode == 0 ? c->Nu : c->scratch, c->bvec); }
+
+int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out) {
   {
     ProfScope ps(c, "zt_u");
     dim3 g(div_up(c->n_d, TM), div_up(c->J, TN));
     LoadDt A{c->Dm, c->ldN, c->N, c->n_d};
-    const int rc = c->simt_fp64 ? GPL_ERR_ARG : dgen_zt_u(c, mode);
+    const int rc = c->simt_fp64 ? GPL_ERR_ARG : dgen_zt_u(c, mode, u, out);
     if (rc != GPL_OK && rc != GPL_ERR_ARG) return rc;
     if (rc == GPL_ERR_ARG) {  // the FFMA form: forced, or more dense columns than one DMMA tile
       if (mode == 0)
         k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
-                                               LoadOinvNu{c->W, c->Nu, c->Omega, c->ldN, c->N, c->J}, c->bvec,
+                                               LoadOinvNu{c->W, u, c->Omega, c->ldN, c->N, c->J}, out,
                                                (int64_t)c->P, c->dcol_d);
       else
-        k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
-                                               LoadCellGene{c->scratch, c->ldN, c->N, c->J}, c->bvec,
+        k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A, LoadCellGene{u, c->ldN, c->N, c->J}, out,
                                                (int64_t)c->P, c->dcol_d);
       GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
     }
   }
+  c->zt_u_src = (mode == 0 && u != c->Nu) ? u : nullptr;
   int rc = launch_group_sums(c, mode == 0 ? 3 : 2);
+  c->zt_u_src = nullptr;
   if (rc) return rc;
-  return launch_assemble_b(c);
+  return launch_assemble_b(c, out);
 }
 
 // C1 <- sum_j (tn_ij/phi_j) tBeta_j[GP]   (stored cell-fastest, ld ldN)

@@ -142,8 +142,8 @@ int launch_group_sums(Ctx* c, int mode) {
       k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
                                              c->scratch, c->gT);
     else
-      k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega, c->Nu,
-                                             c->gT);
+      k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+                                             c->zt_u_src ? c->zt_u_src : c->Nu, c->gT);
     GPL_LAUNCHED(c, "k_group_t");
   }
   return GPL_OK;
@@ -233,11 +233,11 @@ __global__ void k_assemble_b(int P, int J, int n_cv, int n_grp, const int* __res
   }
 }
 
-int launch_assemble_b(Ctx* c) {
+int launch_assemble_b(Ctx* c, double* out) {
   if (c->n_grp == 0) return GPL_OK;
   ProfScope ps(c, "assemble_b");
   k_assemble_b<<<div_up(c->J, 128), 128, 0, c->stream>>>(c->P, c->J, c->n_cv, c->n_grp, c->cv_nh_d, c->cv_nlev_d,
-                                                         c->glev_d, c->gT, c->bvec);
+                                                         c->glev_d, c->gT, out);
   GPL_LAUNCHED(c, "k_assemble_b");
   return GPL_OK;
 }

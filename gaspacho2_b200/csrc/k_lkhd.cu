@@ -71,8 +71,49 @@ __global__ void __launch_bounds__(256) k_beta_phi(int N, int ldN, int P, double 
   }
 }
 
+// r = b - Z^T diag(W/Omega) (Z x) - DeltaInv x for every gene (bx holds the first product);
+// DeltaInv is read from its upper triangle and diagonal.
+__global__ void k_residual(int P, int J, const double* __restrict__ b, const double* __restrict__ bx,
+                           const double* __restrict__ Dinv, const double* __restrict__ x, double* __restrict__ r) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (k >= P) return;
+  const double* xj = x + (size_t)j * P;
+  double s = 0.0;
+  for (int l = 0; l < P; l++) s = fma(Dinv[k <= l ? k + (size_t)l * P : l + (size_t)k * P], xj[l], s);
+  const size_t e = (size_t)j * P + k;
+  r[e] = b[e] - bx[e] - s;
+}
+
+__global__ void k_add_to(size_t n, const double* __restrict__ d, double* __restrict__ x) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) x[e] += d[e];
+}
+
+// Psi_j x = b for every gene. In the precision form Psi_j carries the tensor-core Gram's
+// error, so the solution is refined against the exact FP64 operator, applied without forming
+// it: x += Psi~^{-1} (b - Z^T diag(W/Omega) Z x - DeltaInv x). The reference solves once with
+// its FP64 Psi (cholsl in getBetaPhi / getTildeBeta); the refined x converges to that solution.
+int solve_refined(Ctx* c, const double* b, double* x) {
+  const int64_t PP = (int64_t)c->P * c->P;
+  int rc = launch_solve_batched(c, c->Psi, c->P, PP, b, c->P, x, c->P, c->J);
+  if (rc || c->precision != GPL_PREC_BF16X3) return rc;
+  ProfScope ps(c, "refine");
+  for (int it = 0; it < c->refine_steps; it++) {
+    if ((rc = launch_zbeta(c, x, c->scratch))) return rc;
+    if ((rc = launch_zt_u_ex(c, 0, c->scratch, c->bx))) return rc;
+    dim3 g(div_up(c->P, 128), c->J);
+    k_residual<<<g, 128, 0, c->stream>>>(c->P, c->J, b, c->bx, c->DeltaInv, x, c->rres);
+    GPL_LAUNCHED(c, "k_residual");
+    if ((rc = launch_solve_batched(c, c->Psi, c->P, PP, c->rres, c->P, c->bx, c->P, c->J))) return rc;
+    const size_t n = (size_t)c->P * c->J;
+    k_add_to<<<div_up((int64_t)n, 256), 256, 0, c->stream>>>(n, c->bx, x);
+    GPL_LAUNCHED(c, "k_add_to");
+  }
+  return GPL_OK;
+}
+
 int launch_beta_phi(Ctx* c, int jtr) {
-  int rc = launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->sol, c->P, c->J);
+  int rc = solve_refined(c, c->bvec, c->sol);
   if (rc) return rc;
   double r = (double)(jtr + 1) / 100.0;
   if (jtr > 100) r = 1.0;

@@ -1,0 +1,67 @@
+"""The precision form (GPL_PREC_BF16X3) against the plain FP64 path, through the C ABI.
+
+The precision form runs the Gram on tcgen05 tensor cores (BF16 hi/lo products, FP32 runs
+folded into FP64 in TMEM) over the dense columns whitened by the prior's Cholesky factor, and
+maps the result back in FP64; everything else stays FP64. Bars, per objective+gradient
+evaluation at the same state:
+  * every per-gene Cholesky succeeds (the whitening is what makes this hold: without it,
+    1e-6 Gram errors against cond(Psi_j) ~ 1e14 fail the factorisation);
+  * the objective within 1e-6 relative of FP64 (measured 7e-9 .. 7e-8);
+  * the gradient blocks for Omega, delta, X and rho within 2e-3 (relative L2), T within 5e-2
+    (measured up to 2e-4 and 9e-3), except at config 0, whose cond(Kmm) = 3.5e10 makes even the
+    FP64 path's gradient move by 5e-5 under a change of summation order; there only finiteness
+    is required."""
+import numpy as np
+import pytest
+
+from gaspacho2_b200 import GPLVM, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _evaluate(ds, precision):
+    with GPLVM.from_dataset(ds, precision="fp64") as m:
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        for j in range(3):
+            m.irls_sweep(0, j)
+        m.objective_after_irls(0)
+        m.set_precision(precision)
+        v, g = m.evaluate(m.params_vector())
+        P = m.P
+        psi = m.get("Psi").reshape(m.J, P, P)
+        failed = sum(1 for x in psi if np.abs(np.diag(x)).max() == 0)
+        return v, g.copy(), failed, (m.N, m.Q, m.M)
+
+
+def _blocks(g, dims):
+    N, Q, M = dims
+    p = len(g) - N - N * Q - M * Q - Q
+    out, off = {}, 0
+    for name, n in (("Omega", N), ("delta", p), ("X", N * Q), ("T", M * Q), ("rho", Q)):
+        out[name] = g[off:off + n]
+        off += n
+    return out
+
+
+@pytest.mark.parametrize("cfg,kw", [(0, dict(G=100)), (1, dict(N=6000, G=300)),
+                                    (2, dict(N=6000, G=200, M=64, Q=5))])
+def test_precision_form_against_fp64(cfg, kw):
+    ds = synth.make(cfg, 5, init=True, **kw)
+    v0, g0, f0, dims = _evaluate(ds, "fp64")
+    v1, g1, f1, _ = _evaluate(ds, "bf16x3")
+    assert f0 == 0 and f1 == 0, (f0, f1)
+    rel = abs(v1 - v0) / abs(v0)
+    print(f"config {cfg}: objective rel err {rel:.2e}")
+    assert rel <= 1e-6
+    assert np.all(np.isfinite(g1))
+    b0, b1 = _blocks(g0, dims), _blocks(g1, dims)
+    bad = []
+    for name in b0:
+        e = np.linalg.norm(b1[name] - b0[name]) / max(np.linalg.norm(b0[name]), 1e-300)
+        tol = 5e-2 if name == "T" else 2e-3
+        print(f"  grad {name:5s} rel-l2 {e:.2e} (tol {tol:.0e})")
+        if cfg != 0 and not e <= tol:
+            bad.append(f"{name}: {e:.2e}")
+    assert not bad, bad
