@@ -143,6 +143,11 @@ def flops_table(N, J, M, P, n_dense):
         # gradient contraction sum_j O_ij S_j[DD] d_i over the unique pairs of the symmetric S_j
         # (the pair form's V = O S_pairs; the epilogue to U is N*n_d^2, not counted)
         "uq": float(N) * J * n_dense * (n_dense + 1),
+        # the cell x gene FP64 GEMMs around them (per launch)
+        "zt_u": 2.0 * N * J * n_dense,
+        "group_sums": 2.0 * N * J * n_dense,
+        "hk": 2.0 * N * J * (n_dense + 1),
+        "c1_tn": 2.0 * N * J * M,
         # batched SPD inverse (triangular inverse + its product, n^3/3 flops each) and Cholesky
         "inverse": 2.0 / 3.0 * J * float(P) ** 3,
         "chol": 1.0 / 3.0 * J * float(P) ** 3,
@@ -328,7 +333,7 @@ def run_ours(args):
     prof = {}
     for name in ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
                  "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
-                 "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk"):
+                 "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk", "group_t", "refine", "unwhiten_u"):
         ms, n = m.profile_read(name)
         if n:
             prof[name] = (ms, n)
@@ -369,7 +374,7 @@ def run_ours(args):
         P = m.P
         ft = flops_table(m.N, m.J, m.M, P, m.n_dense())
         peaks = measured_peaks()
-        tc_kernels = ("gram", "uq") if os.environ.get("GPL_TC_GRAD") else ("gram",)
+        tc_kernels = ("gram",) if os.environ.get("GPL_TC_GRAD", "1") == "0" else ("gram", "uq")
         if dom in ft and args.precision == "bf16x3" and dom in tc_kernels:
             # useful flops of the contraction; the hi/lo split issues 3 BF16 products per useful MAC
             tflops = ft[dom]

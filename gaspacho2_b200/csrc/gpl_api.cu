@@ -327,7 +327,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
   c->precision = precision;
   c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
   c->simt_fp64 = getenv("GPL_FP64_SIMT") != nullptr;
-  c->tc_grad = getenv("GPL_TC_GRAD") != nullptr;
+  if (const char* tg = getenv("GPL_TC_GRAD")) c->tc_grad = atoi(tg) != 0;
   if (const char* rs = getenv("GPL_REFINE")) c->refine_steps = atoi(rs);
   return GPL_OK;
 }

@@ -61,22 +61,19 @@ struct PairState {
 
 struct TcState {
   bool ready = false, check_each = false;
-  int n_dp = 0, cpad = 0, chunks_cells = 0, gram_tiles_n = 0;
+  int cpad = 0, chunks_cells = 0, gram_tiles_n = 0, Jpad = 0;
   int n_pairs = 0, pair_tiles = 0;
-  int n_b = 0, grad_chunks = 0, grad_chunks_per_split = 0, grad_splits = 0;
-  int64_t Kpad = 0;
-  int smem_gram = 0, smem_grad = 0;
-  __nv_bfloat16 *whi = nullptr, *wlo = nullptr, *bhi = nullptr, *blo = nullptr;
-  float* Dt = nullptr;
-  double* Up = nullptr;
-  double *Lw = nullptr, *Gt = nullptr, *Tt = nullptr;  // prior factor, whitened Gram, product
-  float* DtC = nullptr;                                 // whitened dense columns (cell fastest)
-  __nv_bfloat16 *ahi = nullptr, *alo = nullptr;         // pair products, pair rows x cells
-  CUtensorMap map_ahi, map_alo;
-  int smem_whiten = 0;
+  int smem_gram = 0, smem_whiten = 0;
+  __nv_bfloat16 *whi = nullptr, *wlo = nullptr;   // w = W/Omega, gene rows x cpad
+  __nv_bfloat16 *ahi = nullptr, *alo = nullptr;   // whitened pair products, pair rows x cpad
+  __nv_bfloat16 *shi = nullptr, *slo = nullptr;   // whitened inverse pairs, pair rows x Jpad
+  __nv_bfloat16 *ohi = nullptr, *olo = nullptr;   // (W/Omega)^T, cpad x Jpad
+  float* DtC = nullptr;                           // whitened dense columns (cell fastest), FP32
+  double* DwC = nullptr;                          // the same in FP64, ld ldN
+  double *Lw = nullptr, *Gt = nullptr, *Tt = nullptr;  // prior factor, whitened Gram / inverse, product
   int2* pairs = nullptr;
   int* err = nullptr;
-  CUtensorMap map_whi, map_wlo, map_bhi, map_blo;
+  CUtensorMap map_whi, map_wlo, map_ahi, map_alo, map_shi, map_slo, map_ohi, map_olo;
 };
 
 struct Ctx {
@@ -84,7 +81,7 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int precision = GPL_PREC_FP64;
-  bool tc_grad = false;
+  bool tc_grad = true;     // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
   int refine_steps = 1;              // precision form: FP64-residual refinement steps per solve
   const double* zt_u_src = nullptr;  // u of Z^T diag(W/Omega) u when not nu (set during a refinement)
   double *rres = nullptr, *bx = nullptr;  // refinement residual and product, P x J    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
@@ -213,6 +210,7 @@ int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X
 int launch_pair_gram(Ctx* c);             // dense block of every Psi_j, FP64 DMMA over column pairs
 int launch_pair_uq(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i, FP64 DMMA over column pairs
 void pair_release(Ctx* c);
+int pair_prepare(Ctx* c);                 // column-pair list, 1/Omega, gathered S pairs, V rows
 int recip_omega(Ctx* c, const double** rOm);  // 1/Omega (0 past N), refreshed on every call
 int dgen_zt_u(Ctx* c, int mode, const double* u, double* out);          // DMMA forms of the cell x gene GEMMs (k_dgen.cu);
 int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns exceed one tile
@@ -220,6 +218,8 @@ int dgen_eta(Ctx* c, const double* B, double* out);
 int dgen_group_sums(Ctx* c, int mode);
 int dgen_hk(Ctx* c);
 int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw);  // Psi_DD = L G L^T + DeltaInv
+int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St);  // S~ = L^T S_DD L per gene
+int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D);  // U from the V rows of cells [c0, c1)
 int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
 int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting

@@ -384,14 +384,17 @@ int launch_pair_uq(Ctx* c) {
                                                      s.V);
       GPL_LAUNCHED(c, "k_pair_v");
     }
-    {
-      ProfScope ps(c, "v_to_u");
-      const int grid = std::min(c1 - c0, 148 * 8);
-      k_v_to_u<<<grid, 256, s.smem_vu, c->stream>>>(c->N, c->ldN, c->n_d, s.n_pairs, s.pairs_pad, c0, c1, c->Dm,
-                                                    s.V, c->U);
-      GPL_LAUNCHED(c, "k_v_to_u");
-    }
+    if ((rc = launch_v_to_u_cells(c, c0, c1, c->Dm))) return rc;
   }
+  return GPL_OK;
+}
+
+int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D) {
+  PairState& s = c->pr;
+  ProfScope ps(c, "v_to_u");
+  const int grid = std::min(c1 - c0, 148 * 8);
+  k_v_to_u<<<grid, 256, s.smem_vu, c->stream>>>(c->N, c->ldN, c->n_d, s.n_pairs, s.pairs_pad, c0, c1, D, s.V, c->U);
+  GPL_LAUNCHED(c, "k_v_to_u");
   return GPL_OK;
 }
 

@@ -308,6 +308,27 @@ struct LdL {  // A(r, k) = L[r][k] = L[r + k*n] (r contiguous), 0 above the diag
   int n;
   __device__ double operator()(int r, int k, int) const { return r >= k ? L[r + (size_t)k * n] : 0.0; }
 };
+struct LdGeneS {  // A(r = a, k = b, z) = S_z[dcol a, dcol b] (the dense block of Psi_z^{-1})
+  static constexpr bool kFastK = false;
+  const double* S;
+  const int* dcol;
+  int P;
+  __device__ double operator()(int r, int k, int z) const {
+    return S[(size_t)z * P * P + dcol[r] + (size_t)dcol[k] * P];
+  }
+};
+struct LdLk {  // B(k, c) = L[k][c] = L[k + c*n] (k contiguous), 0 above the diagonal
+  static constexpr bool kFastK = true;
+  const double* L;
+  int n;
+  __device__ double operator()(int k, int c, int) const { return k >= c ? L[k + (size_t)c * n] : 0.0; }
+};
+struct LdLTk {  // A(r, k) = L[k][r] = L[k + r*n] (k contiguous), 0 above the diagonal
+  static constexpr bool kFastK = true;
+  const double* L;
+  int n;
+  __device__ double operator()(int r, int k, int) const { return k >= r ? L[k + (size_t)r * n] : 0.0; }
+};
 struct EpGene {  // T_z[r + c*n]
   double* T;
   int n;
@@ -441,6 +462,17 @@ int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw) {
   if (rc) return rc;
   return launch_dgen<T>(c, g, n, n, LdL{Lw, n}, LdGeneT{Tt, n}, KAll{n}, EpPsiDD{c->Psi, c->DeltaInv, c->dcol_d, c->P},
                         "k_dgen(unwhiten L(GL^T))");
+}
+
+int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St) {
+  using T = TileTall;
+  const int n = c->n_d;
+  if (n > T::BM || c->J > 65535) return GPL_ERR_ARG;
+  dim3 g(1, div_up(n, T::BN), c->J);
+  int rc = launch_dgen<T>(c, g, n, n, LdGeneS{c->PsiInv, c->dcol_d, c->P}, LdLk{Lw, n}, KAll{n}, EpGene{Tt, n},
+                          "k_dgen(S L)");
+  if (rc) return rc;
+  return launch_dgen<T>(c, g, n, n, LdLTk{Lw, n}, LdGeneT{Tt, n}, KAll{n}, EpGene{St, n}, "k_dgen(L^T S L)");
 }
 
 }  // namespace gpl

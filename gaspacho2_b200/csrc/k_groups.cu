@@ -120,12 +120,12 @@ __global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gce
 // 3: T with w = W/Omega, u = nu (Z^T diag(W/Omega) nu).
 int launch_group_sums(Ctx* c, int mode) {
   if (c->n_grp == 0) return GPL_OK;
-  ProfScope ps(c, "group_sums");
-  if ((mode == 0 || mode == 1) && !c->simt_fp64) {
-    const int rc = dgen_group_sums(c, mode);
-    if (rc != GPL_ERR_ARG) return rc;
-  }
   if (mode == 0 || mode == 1) {
+    ProfScope ps(c, "group_sums");
+    if (!c->simt_fp64) {
+      const int rc = dgen_group_sums(c, mode);
+      if (rc != GPL_ERR_ARG) return rc;
+    }
     const int J = mode == 1 ? 1 : c->J;
     dim3 g(div_up(J, TM), div_up(c->n_d, TN), c->n_grp);
     if (mode == 0)
@@ -135,17 +135,17 @@ int launch_group_sums(Ctx* c, int mode) {
       k_group_sums<1><<<g, 256, 0, c->stream>>>(c->N, c->ldN, J, c->n_d, c->n_grp, c->gcells_d, c->gstart_d, c->W,
                                                 c->Omega, c->Dm, c->gsum);
     GPL_LAUNCHED(c, "k_group_sums");
+    return GPL_OK;
   }
-  if (mode == 2 || mode == 3) {
-    dim3 g(c->n_grp, div_up(c->J, 8));
-    if (mode == 2)
-      k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
-                                             c->scratch, c->gT);
-    else
-      k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
-                                             c->zt_u_src ? c->zt_u_src : c->Nu, c->gT);
-    GPL_LAUNCHED(c, "k_group_t");
-  }
+  ProfScope pt(c, "group_t");
+  dim3 g(c->n_grp, div_up(c->J, 8));
+  if (mode == 2)
+    k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+                                           c->scratch, c->gT);
+  else
+    k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+                                           c->zt_u_src ? c->zt_u_src : c->Nu, c->gT);
+  GPL_LAUNCHED(c, "k_group_t");
   return GPL_OK;
 }
 

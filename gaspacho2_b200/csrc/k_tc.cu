@@ -11,24 +11,30 @@
 // columns per value) and the MMAs continue in the other FP32 buffer. The bias is then that of
 // a few chunks (~1e-6) and the long reduction is FP64.
 //
-// k_tc_gram   G[p, j] = sum_i (D_ia D_ib) w_ij for the dense column pairs p = (a <= b) and
-//             128 genes per CTA over every cell, written straight into Psi_j (both triangles,
-//             plus DeltaInv). M = 128 pairs, N = 128 genes, K = 64 cells per stage. The pair
-//             products are generated by four producer warps straight into the 128-byte-swizzled
-//             A tiles; w = W/Omega (BF16 hi/lo, gene x cell) arrives by TMA. TMEM: two FP32
-//             128 x 128 accumulators (columns 0-255) and the FP64 sum (columns 256-511).
-//             Algorithmic work: N*J*n_d*(n_d+1) flops.
-// k_tc_grad   U[i, a] = sum_{j,b} (O_ij D_ib) S_j[b, a] over dense columns a, b: M = 128 cells,
-//             N = n_d rounded to 16 (<= 160), K = (gene, b) flattened, 64 per stage, split over
-//             4 K ranges whose FP64 partials are summed in order. One FP32 accumulator drained
-//             every 8 chunks into the FP64 sum. Algorithmic work: 2*N*J*n_d^2 flops.
+// k_tc_gram   C[p, n] = sum_k A[p, k] B[n, k] for 128 column pairs p and 128 columns n per CTA,
+//             A and B both BF16 hi/lo, K-major, 128-byte swizzled, by TMA (64-wide K chunks,
+//             three stages). TMEM: two FP32 128 x 128 accumulators (columns 0-255) and the FP64
+//             sum (columns 256-511). Two uses:
+//             * the Gram: A = products of the whitened dense columns per pair, B = w = W/Omega
+//               per gene, K = cells; the FP64 tile goes to the whitened Gram of every gene
+//               (un-whitened in FP64 afterwards) or straight into Psi_j;
+//             * the gradient pairs: A = S~_j[pair] (the whitened inverse, per gene), B = O^T
+//               (W/Omega per cell), K = genes; the FP64 tile goes to V[cell][pair].
+//             Work per use: N*J*n_d*(n_d+1) useful flops (3x on the tensor pipe).
 //
-// Warp roles (320 threads): warp 0 allocates TMEM and issues the TMA loads, warp 1 issues the
-// MMAs (one thread), warps 2-5 produce the A tiles, warps 6-9 drain the accumulators and write
-// the results (warp w reads TMEM lanes 32*(w % 4) .. +31). Full barriers count the TMA bytes
-// plus 128 producer arrivals; empty barriers and the accumulator barriers are armed by
-// tcgen05.commit; drained barriers count the 128 drain threads. Every wait is bounded: one that
-// runs out records an error code, and every role drains what it started before TMEM is freed.
+// Whitening. The reference adds no jitter to Kmm, so cond(Psi_j) reaches ~1e14 and a 1e-6
+// relative Gram error fails the Cholesky. The dense columns are therefore first mapped to
+// L^{-1} d_i with DeltaInv_DD = L L^T (k_whiten_rows): the Gram of those, G~, enters Psi as
+// L G~ L^T + DeltaInv, so its errors are relative to a matrix bounded below by the identity.
+// The gradient contraction runs on the same coordinates: U_i = S_DD d_i = L^{-T} S~ d~_i with
+// S~ = L^T S_DD L (k_unwhiten_u maps U~ back).
+//
+// Warp roles (192 threads): warp 0 allocates TMEM and issues the TMA loads, warp 1 issues the
+// MMAs (one thread), warps 2-5 drain the accumulators and write the results (warp w reads TMEM
+// lanes 32*(w % 4) .. +31). Full barriers count the TMA bytes; empty barriers and the
+// accumulator barriers are armed by tcgen05.commit; drained barriers count the 128 drain
+// threads. Every wait is bounded: one that runs out records an error code, and every role
+// drains what it started before TMEM is freed.
 #include <cuda.h>
 #include <stdlib.h>
 
@@ -42,17 +48,13 @@ namespace gpl {
 using namespace tc;
 
 namespace {
-constexpr int kThreads = 320;           // gradient: TMA, MMA, 4 producer and 4 drain warps
-constexpr int kThreadsGram = 192;       // Gram: TMA, MMA and 4 drain warps
-constexpr int kStagesGram = 3;          // pipeline depth, Gram (192 KB of operand tiles)
-constexpr int kStagesGrad = 2;          // pipeline depth, gradient (B tiles up to 20 KB, plus D rows)
+constexpr int kThreadsGram = 192;       // TMA, MMA and 4 drain warps
+constexpr int kStagesGram = 3;          // pipeline depth (192 KB of operand tiles)
 constexpr int kMaxStages = 3;
 constexpr int kGramN = 128;             // genes per Gram tile
-constexpr int kSBGram = 4;              // chunks per FP32 run (Gram)
-constexpr int kSBGrad = 8;              // chunks per FP32 run (gradient)
+constexpr int kSBGram = 4;              // chunks per FP32 run
 constexpr int kTileA = 128 * 128;       // 128 rows x 64 BF16
 constexpr int kTileBG = kGramN * 128;   // 128 gene rows x 64 BF16
-constexpr int kGradSplits = 4;
 constexpr int kMaxWhiten = 160;         // dense columns the whitened rows kernel holds per cell
 constexpr uint32_t kIdescGram = idesc_bf16_f32(128, kGramN);
 }  // namespace
@@ -132,7 +134,8 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
               const __grid_constant__ CUtensorMap map_whi, const __grid_constant__ CUtensorMap map_wlo,
               const int2* __restrict__ pairs, int n_pairs,
               int chunks_total, const int* __restrict__ dcol, int P, int J, const double* __restrict__ Dinv,
-              double* __restrict__ Psi, double* __restrict__ Gt, int n_d, int* __restrict__ err) {
+              double* __restrict__ Psi, double* __restrict__ Gt, int n_d, int n_base, double* __restrict__ V,
+              int v_ld, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* A_hi = base;
@@ -174,8 +177,8 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
         const int x = it * 64;
         tma_load_2d(A_hi + s * kTileA, &map_ahi, &sh->full[s], x, ptile * 128);
         tma_load_2d(A_lo + s * kTileA, &map_alo, &sh->full[s], x, ptile * 128);
-        tma_load_2d(B_hi + s * kTileBG, &map_whi, &sh->full[s], x, n0);
-        tma_load_2d(B_lo + s * kTileBG, &map_wlo, &sh->full[s], x, n0);
+        tma_load_2d(B_hi + s * kTileBG, &map_whi, &sh->full[s], x, n_base + n0);
+        tma_load_2d(B_lo + s * kTileBG, &map_wlo, &sh->full[s], x, n_base + n0);
         issued = it + 1;
       }
       for (int it = max(0, issued - kStagesGram); it < issued; it++)
@@ -238,8 +241,10 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
 #pragma unroll
         for (int k = 0; k < 16; k++) {
           const int j = n0 + cb + k;
-          if (live && j < J) {
-            if (Gt) {  // whitened Gram of the dense columns, both triangles, un-whitened later
+          if (live && n_base + j < J) {
+            if (V) {  // gradient pairs: V[cell][pair] for the cells of this launch
+              V[(size_t)j * v_ld + ptile * 128 + row] = v[k];
+            } else if (Gt) {  // whitened Gram of the dense columns, both triangles, un-whitened later
               double* Gj = Gt + (size_t)j * n_d * n_d;
               Gj[ab.x + (size_t)ab.y * n_d] = v[k];
               Gj[ab.y + (size_t)ab.x * n_d] = v[k];
@@ -274,15 +279,6 @@ __global__ void k_split_weights(int N, int ldN, int J, int cpad, const double* _
     }
 }
 
-// Dense model columns as FP32, cell-major rows of n_dp (zero padding)
-__global__ void k_dense_rows(int N, int ldN, int n_d, int n_dp, int rows, const double* __restrict__ D,
-                             float* __restrict__ Dt) {
-  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)rows * n_dp) return;
-  const int i = (int)(e / n_dp), a = (int)(e % n_dp);
-  Dt[e] = (i < N && a < n_d) ? (float)D[(size_t)a * ldN + i] : 0.f;
-}
-
 // The prior block of the dense columns, DeltaInv[dcol a, dcol b] (upper triangle, a <= b), for
 // its Cholesky factor L (DeltaInv_DD = L L^T).
 __global__ void k_gather_dinv(int n_d, int P, const int* __restrict__ dcol, const double* __restrict__ Dinv,
@@ -292,11 +288,12 @@ __global__ void k_gather_dinv(int n_d, int P, const int* __restrict__ dcol, cons
   Lw[a + (size_t)b * n_d] = a <= b ? Dinv[dcol[a] + (size_t)dcol[b] * P] : 0.0;
 }
 
-// Whitened dense rows L^{-1} d_i in FP64 by forward substitution, stored as FP32 rows of n_dp
-// (zero padding). The factor's lower triangle is staged in shared memory.
-__global__ void __launch_bounds__(128) k_whiten_rows(int N, int ldN, int n_d, int n_dp, int rows,
+// Whitened dense rows L^{-1} d_i in FP64 by forward substitution, stored column by column in
+// FP32 (cpad per column, zero padding) and FP64 (ld ldN). The factor's lower triangle is staged
+// in shared memory.
+__global__ void __launch_bounds__(128) k_whiten_rows(int N, int ldN, int n_d, int rows,
                                                      const double* __restrict__ D, const double* __restrict__ Lw,
-                                                     float* __restrict__ Dt, float* __restrict__ DtC) {
+                                                     float* __restrict__ DtC, double* __restrict__ DwC) {
   extern __shared__ double ls[];  // lower triangle, row a at a*(a+1)/2
   for (int e = threadIdx.x; e < n_d * n_d; e += blockDim.x) {
     const int a = e % n_d, b = e / n_d;
@@ -305,9 +302,7 @@ __global__ void __launch_bounds__(128) k_whiten_rows(int N, int ldN, int n_d, in
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= rows) return;
-  float* out = Dt + (size_t)i * n_dp;
   if (i >= N) {
-    for (int a = 0; a < n_dp; a++) out[a] = 0.f;
     for (int a = 0; a < n_d; a++) DtC[(size_t)a * rows + i] = 0.f;
     return;
   }
@@ -317,10 +312,9 @@ __global__ void __launch_bounds__(128) k_whiten_rows(int N, int ldN, int n_d, in
     double s = D[(size_t)a * ldN + i];
     for (int b = 0; b < a; b++) s = fma(-la[b], y[b], s);
     y[a] = s / la[a];
-    out[a] = (float)y[a];
     DtC[(size_t)a * rows + i] = (float)y[a];
+    DwC[(size_t)a * ldN + i] = y[a];
   }
-  for (int a = n_d; a < n_dp; a++) out[a] = 0.f;
 }
 
 // Pair products of the whitened columns as BF16 hi/lo, one row of cells per column pair
@@ -344,205 +338,61 @@ __global__ void k_pair_split(int cpad, int n_pairs, const int2* __restrict__ pai
   }
 }
 
-// ---------------------------------------------------------------------------------------------
-// Gradient contraction
-// ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 1)
-    k_tc_grad(const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo, int N,
-              int ldN, int n_d, int n_b, const float* __restrict__ Dt, int n_dp, const double* __restrict__ W,
-              const double* __restrict__ Omega, int64_t K_total, int chunks_total, int chunks_per_split,
-              int cpad, double* __restrict__ Up, int* __restrict__ err) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int tileB = n_b * 128;  // n_b rows x 128 bytes
-  const int tileBa = (tileB + 1023) & ~1023;
-  unsigned char* A_hi = base;
-  unsigned char* A_lo = A_hi + kStagesGrad * kTileA;
-  unsigned char* B_hi = A_lo + kStagesGrad * kTileA;
-  unsigned char* B_lo = B_hi + kStagesGrad * tileBa;
-  float* Ds = (float*)(B_lo + kStagesGrad * tileBa);  // 128 x (n_d + 1)
-  TcShared* sh = (TcShared*)(Ds + 128 * (n_d + 1));
-  const int ldD = n_d + 1;
-  const int nb32 = (n_b + 31) / 32 * 32;          // FP32 columns drained (multiple of 32)
-  const uint32_t f64col = (uint32_t)nb32;         // FP64 sum at columns [nb32, 3*nb32)
-  uint32_t tcols = 32;                            // TMEM columns allocated: a power of two >= 3*nb32
-  while (tcols < 3u * nb32) tcols <<= 1;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i0 = blockIdx.x * 128, split = blockIdx.y;
-  const int kc0 = split * chunks_per_split;
-  const int kc1 = min(chunks_total, kc0 + chunks_per_split);
-  const int nch = kc1 - kc0;
-  const int nsb = (nch + kSBGrad - 1) / kSBGrad;
-  const uint32_t idesc = idesc_bf16_f32(128, n_b);
-
-  if (threadIdx.x == 0) tc_init(sh, err, 1 + 128);
-  __syncthreads();
-  if (sh->abort) return;
-  for (int e = threadIdx.x; e < 128 * n_d; e += kThreads) {
-    const int r = e / n_d, a = e % n_d;
-    Ds[r * ldD + a] = Dt[(size_t)(i0 + r) * n_dp + a];
-  }
-  if (warp == 0) {
-    tmem_alloc(&sh->tmem, tcols);
-    tmem_relinquish();
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = sh->tmem;
-
-  if (warp == 0) {
-    if (lane == 0) {
-      int issued = 0;
-      for (int it = 0; it < nch; it++) {
-        const int s = it % kStagesGrad;
-        if (it >= kStagesGrad && !mbar_wait(&sh->empty[s], ((it / kStagesGrad) - 1) & 1, err)) { tc_fail(err, sh, 21); break; }
-        if (sh->abort) break;
-        mbar_arrive_expect_tx(&sh->full[s], 2u * (uint32_t)tileB);
-        const int x = (kc0 + it) * 64;
-        tma_load_2d(B_hi + s * tileBa, &map_bhi, &sh->full[s], x, 0);
-        tma_load_2d(B_lo + s * tileBa, &map_blo, &sh->full[s], x, 0);
-        issued = it + 1;
-      }
-      for (int it = max(0, issued - kStagesGrad); it < issued; it++)
-        if (!mbar_wait(&sh->full[it % kStagesGrad], (it / kStagesGrad) & 1, nullptr)) atomicCAS(err, 0, 22);
-    }
-  } else if (warp == 1) {
-    if (lane == 0) {
-      for (int it = 0; it < nch; it++) {
-        const int s = it % kStagesGrad, sb = it / kSBGrad, pos = it % kSBGrad;
-        if (pos == 0 && sb >= 1 && !mbar_wait(&sh->drained[0], (sb - 1) & 1, err)) { tc_fail(err, sh, 26); break; }
-        if (!mbar_wait(&sh->full[s], (it / kStagesGrad) & 1, err)) { tc_fail(err, sh, 23); break; }
-        if (sh->abort) break;
-        tc_fence_after();
-        const uint32_t ah = smem_u32(A_hi + s * kTileA), al = smem_u32(A_lo + s * kTileA);
-        const uint32_t bh = smem_u32(B_hi + s * tileBa), bl = smem_u32(B_lo + s * tileBa);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const uint32_t off = k * 32;
-          mma_bf16(tmem, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc, (pos | k) ? 1u : 0u);
-          mma_bf16(tmem, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
-          mma_bf16(tmem, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
-        }
-        mma_commit(&sh->empty[s]);
-        if (pos == kSBGrad - 1 || it == nch - 1) mma_commit(&sh->accb[0]);
-      }
-      mma_finish(sh, err, 27);
-    }
-  } else if (warp < 6) {
-    const int r = threadIdx.x - 64;
-    const int i = i0 + r;
-    const bool live = i < N;
-    const double om = live ? Omega[i] : 1.0;
-    const float* drow = Ds + r * ldD;
-    int jcur = -1;
-    float ocur = 0.f;
-    for (int it = 0; it < nch; it++) {
-      const int s = it % kStagesGrad;
-      if (it >= kStagesGrad && !mbar_wait(&sh->empty[s], ((it / kStagesGrad) - 1) & 1, err)) { tc_fail(err, sh, 24); break; }
-      if (sh->abort) break;
-      const int64_t k0 = (int64_t)(kc0 + it) * 64;
-      int j = (int)(k0 / n_d), b = (int)(k0 - (int64_t)j * n_d);
-      const uint32_t ah = smem_u32(A_hi + s * kTileA), al = smem_u32(A_lo + s * kTileA);
-#pragma unroll 1
-      for (int c16 = 0; c16 < 8; c16++) {
-        float x[8];
-#pragma unroll
-        for (int e = 0; e < 8; e++) {
-          const int64_t kk = k0 + c16 * 8 + e;
-          float v = 0.f;
-          if (live && kk < K_total) {
-            if (j != jcur) {
-              jcur = j;
-              ocur = (float)(W[(size_t)j * ldN + i] / om);
-            }
-            v = ocur * drow[b];
-          }
-          x[e] = v;
-          if (++b == n_d) { b = 0; j++; }
-        }
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) split_bf16x2(x[2 * q], x[2 * q + 1], h[q], l[q]);
-        const uint32_t o = sw128_offset(r, c16);
-        st_shared_v4(ah + o, h[0], h[1], h[2], h[3]);
-        st_shared_v4(al + o, l[0], l[1], l[2], l[3]);
-      }
-      fence_proxy_async();
-      mbar_arrive(&sh->full[s]);
-    }
-  } else {
-    const int q = warp & 3;
-    const int row = q * 32 + lane;
-    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
-    bool ok = true;
-    for (int sb = 0; sb < nsb; sb++) {
-      const bool w = mbar_wait(&sh->accb[0], sb & 1, err);
-      if (!warp_all(w)) {
-        if (!w) tc_fail(err, sh, 25);
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      drain_f32_to_f64(lane_addr, 0, f64col, nb32, sb == 0);
-      tc_fence_before();
-      mbar_arrive(&sh->drained[0]);
-    }
-    if (warp_all(ok && !aborted(sh)) && nsb > 0) {
-      tc_fence_after();
-      const int i = i0 + row;
-      for (int cb = 0; cb < nb32; cb += 16) {
-        double v[16];
-        tmem_ld_f64x16(lane_addr + f64col + 2 * cb, v);
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-          const int a = cb + k;
-          if (a < n_d) Up[((size_t)split * n_b + a) * cpad + i] = v[k];
-        }
-      }
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (warp == 0) tmem_dealloc(tmem, tcols);
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
-// S_j[DD] as the B operand: Bt[a][j*n_d + b] = S_j[dcol[b], dcol[a]] in BF16 hi/lo (rows n_b)
-__global__ void k_split_sdd(int J, int P, int n_d, int64_t Kpad, const int* __restrict__ dcol,
-                            const double* __restrict__ S, __nv_bfloat16* __restrict__ bhi,
-                            __nv_bfloat16* __restrict__ blo) {
-  const int a = blockIdx.y;
-  const int64_t K = (int64_t)J * n_d;
-  for (int64_t k2 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 2; k2 < Kpad;
-       k2 += (int64_t)gridDim.x * blockDim.x * 2) {
-    float v[2];
-#pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int64_t kk = k2 + e;
-      float x = 0.f;
-      if (a < n_d && kk < K) {
-        const int j = (int)(kk / n_d), b = (int)(kk - (int64_t)j * n_d);
-        x = (float)S[(size_t)j * P * P + dcol[b] + (size_t)dcol[a] * P];
-      }
-      v[e] = x;
-    }
-    uint32_t h, l;
-    split_bf16x2(v[0], v[1], h, l);
-    *reinterpret_cast<uint32_t*>(bhi + (size_t)a * Kpad + k2) = h;
-    *reinterpret_cast<uint32_t*>(blo + (size_t)a * Kpad + k2) = l;
+// The whitened inverse's pairs S~_j[a, b] (a <= b) as BF16 hi/lo, pair rows x gene columns
+// (Jpad, zero padding): the A operand of the tensor-core gradient contraction.
+__global__ void k_split_spairs(int J, int Jpad, int n_d, int n_pairs, const int2* __restrict__ pairs,
+                               const double* __restrict__ St, __nv_bfloat16* __restrict__ shi,
+                               __nv_bfloat16* __restrict__ slo) {
+  const int p = blockIdx.y;
+  const int2 ab = p < n_pairs ? pairs[p] : make_int2(-1, -1);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < Jpad; j += gridDim.x * blockDim.x) {
+    float x = 0.f;
+    if (ab.x >= 0 && j < J) x = (float)St[(size_t)j * n_d * n_d + ab.x + (size_t)ab.y * n_d];
+    split_bf16(x, shi[(size_t)p * Jpad + j], slo[(size_t)p * Jpad + j]);
   }
 }
 
-__global__ void k_tc_grad_reduce(int N, int ldN, int n_d, int n_b, int cpad, int nsplit,
-                                 const double* __restrict__ Up, double* __restrict__ U) {
+// O^T = (W/Omega)^T as BF16 hi/lo, cell rows x gene columns (cpad x Jpad, zero padding), by
+// 32 x 32 tiles through shared memory (reads along cells, writes along genes).
+__global__ void k_split_ot(int N, int ldN, int J, int Jpad, const double* __restrict__ W,
+                           const double* __restrict__ Omega, __nv_bfloat16* __restrict__ ohi,
+                           __nv_bfloat16* __restrict__ olo) {
+  __shared__ float tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, i = i0 + threadIdx.x;
+    tile[r][threadIdx.x] = (j < J && i < N) ? (float)(W[(size_t)j * ldN + i] / Omega[i]) : 0.f;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, j = j0 + threadIdx.x;
+    if (j < Jpad) split_bf16(tile[threadIdx.x][r], ohi[(size_t)i * Jpad + j], olo[(size_t)i * Jpad + j]);
+  }
+}
+
+// U_i = L^{-T} U~_i per cell (in place), by back substitution with the prior factor.
+__global__ void __launch_bounds__(128) k_unwhiten_u(int N, int ldN, int n_d, const double* __restrict__ Lw,
+                                                    double* __restrict__ U) {
+  extern __shared__ double ls[];  // lower triangle, row a at a*(a+1)/2
+  for (int e = threadIdx.x; e < n_d * n_d; e += blockDim.x) {
+    const int a = e % n_d, b = e / n_d;
+    if (b <= a) ls[a * (a + 1) / 2 + b] = Lw[a + (size_t)b * n_d];
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int a = blockIdx.y;
-  if (i >= N || a >= n_d) return;
-  double s = 0.0;
-  for (int k = 0; k < nsplit; k++) s += Up[((size_t)k * n_b + a) * cpad + i];
-  U[i + (size_t)a * ldN] = s;
+  if (i >= N) return;
+  double u[kMaxWhiten];
+  for (int a = n_d - 1; a >= 0; a--) {
+    double s = U[i + (size_t)a * ldN];
+    for (int b = a + 1; b < n_d; b++) s = fma(-ls[b * (b + 1) / 2 + a], u[b], s);
+    u[a] = s / ls[a * (a + 1) / 2 + a];
+    U[i + (size_t)a * ldN] = u[a];
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -591,71 +441,58 @@ int tc_prepare(Ctx* c) {
   if (c->tc.ready) return GPL_OK;
   TcState& t = c->tc;
   const int J = c->J, n_d = c->n_d;
-  t.n_dp = (n_d + 3) / 4 * 4;
-  t.cpad = (c->N + 127) / 128 * 128;  // cells: a multiple of 64 for K and of 128 for the gradient tiles
+  if (n_d > kMaxWhiten || J > 65535) {
+    c->err = "the tensor-core form supports at most 160 dense model columns and 65535 genes";
+    return GPL_ERR_ARG;
+  }
+  t.cpad = (c->N + 127) / 128 * 128;  // cells: a multiple of 64 for K and of 128 for the V tiles
   t.chunks_cells = t.cpad / 64;
   t.gram_tiles_n = (J + kGramN - 1) / kGramN;
+  t.Jpad = (J + 63) / 64 * 64;
   std::vector<int2> pairs;
   for (int a = 0; a < n_d; a++)
     for (int b = a; b < n_d; b++) pairs.push_back(make_int2(a, b));
   t.n_pairs = (int)pairs.size();
   t.pair_tiles = (t.n_pairs + 127) / 128;
-  t.n_b = (n_d + 15) / 16 * 16;
-  const int64_t K = (int64_t)J * n_d;
-  t.Kpad = (K + 63) / 64 * 64;
-  t.grad_chunks = (int)(t.Kpad / 64);
-  t.grad_chunks_per_split = (t.grad_chunks + kGradSplits - 1) / kGradSplits;
-  t.grad_splits = (t.grad_chunks + t.grad_chunks_per_split - 1) / t.grad_chunks_per_split;  // none empty
-  if (3 * ((t.n_b + 31) / 32 * 32) > 512) {
-    c->err = "the tensor-core form supports at most 160 dense model columns";
-    return GPL_ERR_ARG;
-  }
+  const size_t prow = (size_t)t.pair_tiles * 128;
   int rc;
   if ((rc = tc_alloc(c, &t.whi, (size_t)J * t.cpad, "w hi"))) return rc;
   if ((rc = tc_alloc(c, &t.wlo, (size_t)J * t.cpad, "w lo"))) return rc;
-  if ((rc = tc_alloc(c, &t.Dt, (size_t)t.cpad * t.n_dp, "dense rows"))) return rc;
   if ((rc = tc_alloc(c, &t.DtC, (size_t)t.cpad * n_d, "whitened dense columns"))) return rc;
-  if ((rc = tc_alloc(c, &t.ahi, (size_t)t.pair_tiles * 128 * t.cpad, "pair products hi"))) return rc;
-  if ((rc = tc_alloc(c, &t.alo, (size_t)t.pair_tiles * 128 * t.cpad, "pair products lo"))) return rc;
+  if ((rc = tc_alloc(c, &t.DwC, (size_t)c->ldN * n_d, "whitened dense columns (FP64)"))) return rc;
+  if ((rc = tc_alloc(c, &t.ahi, prow * t.cpad, "pair products hi"))) return rc;
+  if ((rc = tc_alloc(c, &t.alo, prow * t.cpad, "pair products lo"))) return rc;
+  if ((rc = tc_alloc(c, &t.shi, prow * t.Jpad, "inverse pairs hi"))) return rc;
+  if ((rc = tc_alloc(c, &t.slo, prow * t.Jpad, "inverse pairs lo"))) return rc;
+  if ((rc = tc_alloc(c, &t.ohi, (size_t)t.cpad * t.Jpad, "O^T hi"))) return rc;
+  if ((rc = tc_alloc(c, &t.olo, (size_t)t.cpad * t.Jpad, "O^T lo"))) return rc;
   if ((rc = tc_alloc(c, &t.pairs, (size_t)t.n_pairs, "pairs"))) return rc;
-  if ((rc = tc_alloc(c, &t.bhi, (size_t)t.n_b * t.Kpad, "S hi"))) return rc;
-  if ((rc = tc_alloc(c, &t.blo, (size_t)t.n_b * t.Kpad, "S lo"))) return rc;
-  if ((rc = tc_alloc(c, &t.Up, (size_t)t.grad_splits * t.n_b * t.cpad, "grad partials"))) return rc;
   if ((rc = tc_alloc(c, &t.err, 1, "tc error flag"))) return rc;
   if ((rc = tc_alloc(c, &t.Lw, (size_t)n_d * n_d, "prior factor"))) return rc;
   if ((rc = tc_alloc(c, &t.Gt, (size_t)J * n_d * n_d, "whitened Gram"))) return rc;
   if ((rc = tc_alloc(c, &t.Tt, (size_t)J * n_d * n_d, "un-whitening product"))) return rc;
-  if (n_d > kMaxWhiten || J > 65535) {
-    c->err = "the tensor-core form supports at most 160 dense model columns and 65535 genes";
-    return GPL_ERR_ARG;
-  }
   t.smem_whiten = (int)sizeof(double) * n_d * (n_d + 1) / 2;
   GPL_TRY(c, cudaFuncSetAttribute(k_whiten_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_whiten));
+  GPL_TRY(c, cudaFuncSetAttribute(k_unwhiten_u, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_whiten));
   GPL_TRY(c, cudaMemset(t.err, 0, sizeof(int)));
   GPL_TRY(c, cudaMemcpy(t.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  if (!make_map(&t.map_ahi, t.ahi, t.cpad, (uint64_t)t.pair_tiles * 128, 128) ||
-      !make_map(&t.map_alo, t.alo, t.cpad, (uint64_t)t.pair_tiles * 128, 128) ||
-      !make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN) ||
-      !make_map(&t.map_bhi, t.bhi, t.Kpad, t.n_b, t.n_b) || !make_map(&t.map_blo, t.blo, t.Kpad, t.n_b, t.n_b)) {
+  if (!make_map(&t.map_shi, t.shi, t.Jpad, prow, 128) || !make_map(&t.map_slo, t.slo, t.Jpad, prow, 128) ||
+      !make_map(&t.map_ohi, t.ohi, t.Jpad, t.cpad, 128) || !make_map(&t.map_olo, t.olo, t.Jpad, t.cpad, 128) ||
+      !make_map(&t.map_ahi, t.ahi, t.cpad, prow, 128) || !make_map(&t.map_alo, t.alo, t.cpad, prow, 128) ||
+      !make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN)) {
     c->err = "cuTensorMapEncodeTiled failed";
     return GPL_ERR_CUDA;
   }
   t.smem_gram = 1024 + kStagesGram * (2 * kTileA + 2 * kTileBG) + (int)sizeof(TcShared) + 128 * (int)sizeof(int2);
-  const int tileBa = (t.n_b * 128 + 1023) & ~1023;
-  t.smem_grad = 1024 + kStagesGrad * (2 * kTileA + 2 * tileBa) + 128 * (n_d + 1) * 4 + (int)sizeof(TcShared);
-  if (t.smem_grad > 227 * 1024) {
-    c->err = "the tensor-core gradient needs more shared memory than a CTA has";
-    return GPL_ERR_ARG;
-  }
   GPL_TRY(c, cudaFuncSetAttribute(k_tc_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_gram));
-  GPL_TRY(c, cudaFuncSetAttribute(k_tc_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_grad));
   t.ready = true;
   return GPL_OK;
 }
 
 void tc_release(Ctx* c) {
   TcState& t = c->tc;
-  void* bufs[] = {t.whi, t.wlo, t.Dt, t.pairs, t.bhi, t.blo, t.Up, t.err, t.Lw, t.Gt, t.Tt, t.DtC, t.ahi, t.alo};
+  void* bufs[] = {t.whi, t.wlo, t.pairs, t.err, t.Lw, t.Gt, t.Tt, t.DtC, t.DwC, t.ahi, t.alo, t.shi, t.slo,
+                  t.ohi, t.olo};
   for (void* p : bufs)
     if (p) cudaFree(p);
   const bool keep = t.check_each;
@@ -674,14 +511,6 @@ static int tc_check_flag(Ctx* c) {
   return GPL_OK;
 }
 
-int launch_dense_rows(Ctx* c) {
-  TcState& t = c->tc;
-  const size_t n = (size_t)t.cpad * t.n_dp;
-  k_dense_rows<<<div_up((int64_t)n, 256), 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, t.n_dp, t.cpad, c->Dm, t.Dt);
-  GPL_LAUNCHED(c, "k_dense_rows");
-  return GPL_OK;
-}
-
 int launch_tc_gram(Ctx* c) {
   int rc = tc_prepare(c);
   if (rc) return rc;
@@ -697,8 +526,8 @@ int launch_tc_gram(Ctx* c) {
     GPL_LAUNCHED(c, "k_gather_dinv");
     launch_chol_exact_raw(c->stream, t.Lw, c->n_d);
     GPL_LAUNCHED(c, "k_chol_exact");
-    k_whiten_rows<<<t.cpad / 128, 128, t.smem_whiten, c->stream>>>(c->N, c->ldN, c->n_d, t.n_dp, t.cpad, c->Dm,
-                                                                    t.Lw, t.Dt, t.DtC);
+    k_whiten_rows<<<t.cpad / 128, 128, t.smem_whiten, c->stream>>>(c->N, c->ldN, c->n_d, t.cpad, c->Dm, t.Lw,
+                                                                    t.DtC, t.DwC);
     GPL_LAUNCHED(c, "k_whiten_rows");
     dim3 gp(std::min(16, div_up(t.cpad, 512)), t.pair_tiles * 128);
     k_pair_split<<<gp, 256, 0, c->stream>>>(t.cpad, t.n_pairs, t.pairs, t.DtC, t.ahi, t.alo);
@@ -714,9 +543,8 @@ int launch_tc_gram(Ctx* c) {
     ProfScope ps(c, "gram");
     dim3 g(t.pair_tiles, t.gram_tiles_n);
     k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
-                                                           t.n_pairs,
-                                                       t.chunks_cells, c->dcol_d, c->P, c->J, c->DeltaInv, c->Psi,
-                                                       t.Gt, c->n_d, t.err);
+                                                           t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
+                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.err);
     GPL_LAUNCHED(c, "k_tc_gram");
   }
   {
@@ -726,30 +554,43 @@ int launch_tc_gram(Ctx* c) {
   return c->tc.check_each ? tc_check_flag(c) : GPL_OK;
 }
 
+// The gradient contraction on tensor cores, over the column pairs of the whitened columns:
+// S~_j = L^T S_DD,j L (FP64), V[i, pair] = sum_j O_ij S~_j[pair] (tcgen05, FP64-accumulated),
+// U~_i = sum_b D~_ib V[i, pair(a, b)], and U_i = L^{-T} U~_i (FP64). Needs the factor and the
+// whitened columns of the preceding tensor-core Gram.
 int launch_tc_grad(Ctx* c) {
   int rc = tc_prepare(c);
   if (rc) return rc;
+  if ((rc = pair_prepare(c))) return rc;
   TcState& t = c->tc;
-  if ((rc = launch_dense_rows(c))) return rc;
+  PairState& s = c->pr;
   {
-    ProfScope ps(c, "split_sdd");
-    dim3 g(std::min<int64_t>(1024, div_up(t.Kpad, 512)), t.n_b);
-    k_split_sdd<<<g, 256, 0, c->stream>>>(c->J, c->P, c->n_d, t.Kpad, c->dcol_d, c->PsiInv, t.bhi, t.blo);
-    GPL_LAUNCHED(c, "k_split_sdd");
+    ProfScope ps(c, "spair");
+    if ((rc = dgen_whiten_inverse(c, t.Lw, t.Tt, t.Gt))) return rc;
+    dim3 g(std::min(64, div_up(t.Jpad, 256)), t.pair_tiles * 128);
+    k_split_spairs<<<g, 256, 0, c->stream>>>(c->J, t.Jpad, c->n_d, t.n_pairs, t.pairs, t.Gt, t.shi, t.slo);
+    GPL_LAUNCHED(c, "k_split_spairs");
+    dim3 g2(t.cpad / 32, t.Jpad / 32);
+    k_split_ot<<<g2, dim3(32, 8), 0, c->stream>>>(c->N, c->ldN, c->J, t.Jpad, c->W, c->Omega, t.ohi, t.olo);
+    GPL_LAUNCHED(c, "k_split_ot");
+  }
+  for (int c0 = 0; c0 < c->N; c0 += s.v_cells) {
+    const int c1 = std::min(c->N, c0 + s.v_cells);
+    {
+      ProfScope ps(c, "uq");
+      dim3 g(t.pair_tiles, div_up(c1 - c0, kGramN));
+      k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
+                                                             t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
+                                                             c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
+                                                             s.pairs_pad, t.err);
+      GPL_LAUNCHED(c, "k_tc_gram(gradient pairs)");
+    }
+    if ((rc = launch_v_to_u_cells(c, c0, c1, t.DwC))) return rc;
   }
   {
-    ProfScope ps(c, "uq");
-    dim3 g(t.cpad / 128, t.grad_splits);
-    k_tc_grad<<<g, kThreads, t.smem_grad, c->stream>>>(t.map_bhi, t.map_blo, c->N, c->ldN, c->n_d, t.n_b, t.Dt,
-                                                       t.n_dp, c->W, c->Omega, (int64_t)c->J * c->n_d,
-                                                       t.grad_chunks, t.grad_chunks_per_split, t.cpad, t.Up, t.err);
-    GPL_LAUNCHED(c, "k_tc_grad");
-  }
-  {
-    ProfScope ps(c, "grad_reduce");
-    dim3 g(div_up(c->N, 256), c->n_d);
-    k_tc_grad_reduce<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, t.n_b, t.cpad, t.grad_splits, t.Up, c->U);
-    GPL_LAUNCHED(c, "k_tc_grad_reduce");
+    ProfScope ps(c, "unwhiten_u");
+    k_unwhiten_u<<<div_up(c->N, 128), 128, t.smem_whiten, c->stream>>>(c->N, c->ldN, c->n_d, t.Lw, c->U);
+    GPL_LAUNCHED(c, "k_unwhiten_u");
   }
   return c->tc.check_each ? tc_check_flag(c) : GPL_OK;
 }
