@@ -279,18 +279,12 @@ def time_to_fit(args, stream, device):
 def run_ours(args):
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from gaspacho2_b200 import GPLVM
+    from gaspacho2_b200.replicas import Replicas
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rep = Replicas("nccl")  # one independent replica per GPU; barrier and max-over-ranks time only
+    world, rank, local = rep.world, rep.rank, rep.local
 
     ds = dataset(args)
     # a dedicated stream: the library runs every kernel on it and the CUDA events below are
@@ -308,9 +302,7 @@ def run_ours(args):
         m.evaluate_device()
     torch.cuda.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = rep.barrier
 
     # device-resident throughput
     m.profile(True)
@@ -338,11 +330,7 @@ def run_ours(args):
         if n:
             prof[name] = (ms, n)
     m.profile(False)
-    t_max = dt
-    if dist is not None:
-        tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max = rep.max_time(dt)
     value = world * args.steps / t_max
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
@@ -359,11 +347,7 @@ def run_ours(args):
     e2.record(stream)
     torch.cuda.synchronize()
     barrier()
-    dt2 = s2.elapsed_time(e2) / 1e3
-    if dist is not None:
-        tt = torch.tensor([dt2], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dt2 = float(tt.item())
+    dt2 = rep.max_time(s2.elapsed_time(e2) / 1e3)
     e2e = {"value": world * args.steps / dt2, "unit": "evals/s", "h2d_bytes_per_step": int(params.nbytes),
            "d2h_bytes_per_step": int(grad.nbytes + 8)}
 
@@ -420,9 +404,7 @@ def run_ours(args):
                                 "sample": cs.desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 

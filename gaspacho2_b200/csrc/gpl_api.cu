@@ -100,7 +100,7 @@ static void free_state(Ctx* c) {
                   c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
                   c->grad0,  c->ss,     c->SS,      c->XX,      c->gdtmp,  c->C1,     c->C2,     c->grtmp,
                   c->KmmInv, c->bvec,   c->sol,     c->red,     c->lb_work, c->mc_d,  c->mv_d,   c->mk_d,
-                  c->nh_d,   c->rres,   c->bx};
+                  c->nh_d,   c->rres,   c->bx,      c->rphi};
   for (void* p : bufs)
     if (p) cudaFree(p);
   c->Z = c->W = c->Nu = c->Psi = c->PsiInv = c->Beta = c->tBeta = c->scratch = c->U = nullptr;
@@ -108,7 +108,7 @@ static void free_state(Ctx* c) {
   c->rho = c->phi = c->ls = c->lkhds = c->lkhd_dev = c->grad = c->grad0 = c->ss = c->SS = c->XX = nullptr;
   c->gdtmp = c->C1 = c->C2 = c->grtmp = c->KmmInv = c->bvec = c->sol = c->red = c->lb_work = nullptr;
   c->mc_d = c->mv_d = c->mk_d = c->nh_d = nullptr;
-  c->rres = c->bx = nullptr;
+  c->rres = c->bx = c->rphi = nullptr;
   c->have_design = false;
 }
 
@@ -545,6 +545,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->sol, (size_t)P * J, "sol"));
   GPL_RUN(dalloc(c, &c->rres, (size_t)P * J, "refinement residual"));
   GPL_RUN(dalloc(c, &c->bx, (size_t)P * J, "refinement product"));
+  GPL_RUN(dalloc(c, &c->rphi, (size_t)J, "1/phi"));
   GPL_RUN(dalloc(c, &c->scratch, scratch_n, "scratch"));
   GPL_RUN(dalloc(c, &c->U, ldN * n_d, "U"));
   GPL_RUN(dalloc(c, &c->Kmm, (size_t)M * M, "Kmm"));

@@ -84,7 +84,8 @@ struct Ctx {
   bool tc_grad = true;     // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
   int refine_steps = 1;              // precision form: FP64-residual refinement steps per solve
   const double* zt_u_src = nullptr;  // u of Z^T diag(W/Omega) u when not nu (set during a refinement)
-  double *rres = nullptr, *bx = nullptr;  // refinement residual and product, P x J    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
+  double *rres = nullptr, *bx = nullptr;  // refinement residual and product, P x J
+  double* rphi = nullptr;                 // 1/phi, refreshed before each gradient    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
   bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
   std::string err;
 
@@ -200,6 +201,7 @@ int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride);
 int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const double* B, int64_t bstride,
                          double* X, int64_t xstride, int batch);
 int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
+int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride);  // 32-column panels, DMMA
 int launch_inverse_panels(Ctx* c);       // the same in 32-column panels with DMMA block products
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA

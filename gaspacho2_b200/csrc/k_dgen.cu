@@ -177,14 +177,14 @@ struct LdU {  // B(k = cell, c = gene): mode 0 W nu / Omega, mode 1 y0
     return mode == 0 ? W[e] * rOm[k] * Nu[e] : Nu[e];
   }
 };
-struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega
+struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega (1/phi given)
   static constexpr bool kFastK = false;
-  const double *W, *Nu, *E, *rOm, *phi;
+  const double *W, *Nu, *E, *rOm, *rphi;
   int ldN;
   __device__ double operator()(int r, int k, int) const {
     const size_t e = (size_t)k * ldN + r;
     const double o = W[e] * rOm[r];
-    return (o * Nu[e] - o * E[e]) / phi[k];
+    return (o * Nu[e] - o * E[e]) * rphi[k];
   }
 };
 struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
@@ -413,7 +413,7 @@ int dgen_c1_tn(Ctx* c) {
   if (rc) return rc;
   const int g0 = c->nh[c->p - 1];
   dim3 g(div_up(c->N, T::BM), div_up(c->M, T::BN), 1);
-  return launch_dgen<T>(c, g, c->N, c->M, LdTn{c->W, c->Nu, c->scratch, rOm, c->phi, c->ldN},
+  return launch_dgen<T>(c, g, c->N, c->M, LdTn{c->W, c->Nu, c->scratch, rOm, c->rphi, c->ldN},
                         LdTBetaGP{c->tBeta, c->P, g0}, KAll{c->J}, EpColMajor{c->C1, (int64_t)c->ldN},
                         "k_dgen(c1_tn)");
 }

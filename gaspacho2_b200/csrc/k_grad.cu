@@ -155,20 +155,35 @@ __global__ void __launch_bounds__(256) k_uq(int N, int ldN, int n_d, int n_dp, i
 }
 
 // per cell: sum_j tn_ij^2 / W_ij / phi_j with tn = O (nu - E), E = z_i . tBeta_j (in scratch)
+__global__ void k_recip(int n, const double* __restrict__ x, double* __restrict__ r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = 1.0 / x[i];
+}
+
 __global__ void k_tn_sum(int N, int ldN, int J, const double* __restrict__ W, const double* __restrict__ Nu,
                          const double* __restrict__ E, const double* __restrict__ Omega,
-                         const double* __restrict__ phi, double* __restrict__ out) {
+                         const double* __restrict__ rphi, double* __restrict__ out) {
+  // tn^2 / W / phi / 2 with tn = (W/Omega)(nu - E) is W (nu - E)^2 / (2 phi Omega^2): no division
+  // per entry; four independent partial sums (genes 4q + r) keep loads in flight.
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const double om = Omega[i];
-  double s = 0.0;
-  for (int j = 0; j < J; j++) {
-    const size_t e = (size_t)j * ldN + i;
-    const double w = W[e], o = w / om;
-    const double tn = o * Nu[e] - o * E[e];
-    s += tn * tn / w / phi[j] / 2.0;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  int j = 0;
+  for (; j + 4 <= J; j += 4) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const size_t e = (size_t)(j + r) * ldN + i;
+      const double d = Nu[e] - E[e];
+      s[r] += W[e] * d * d * rphi[j + r];
+    }
   }
-  out[i] = s;
+  for (; j < J; j++) {
+    const size_t e = (size_t)j * ldN + i;
+    const double d = Nu[e] - E[e];
+    s[0] += W[e] * d * d * rphi[j];
+  }
+  const double om = Omega[i];
+  out[i] = ((s[0] + s[1]) + (s[2] + s[3])) / (2.0 * om * om);
 }
 
 // per-cell epilogue of getGradLogOmega (ggplvm.cu:352-374). With A = U (dense rows of
@@ -224,8 +239,10 @@ int launch_grad_omega(Ctx* c) {
   if (rc) return rc;
   {
     ProfScope ps(c, "tn_sum");
-    k_tn_sum<<<div_up(c->N, 128), 128, 0, c->stream>>>(c->N, c->ldN, c->J, c->W, c->Nu, c->scratch, c->Omega, c->phi,
-                                                       c->red);
+    k_recip<<<div_up(c->J, 256), 256, 0, c->stream>>>(c->J, c->phi, c->rphi);
+    GPL_LAUNCHED(c, "k_recip");
+    k_tn_sum<<<div_up(c->N, 128), 128, 0, c->stream>>>(c->N, c->ldN, c->J, c->W, c->Nu, c->scratch, c->Omega,
+                                                       c->rphi, c->red);
     GPL_LAUNCHED(c, "k_tn_sum");
   }
   rc = launch_c1_tn(c);  // C1 = sum_j tn/phi tBeta_GP

@@ -277,6 +277,10 @@ int launch_gram(Ctx* c, bool unweighted) {
 
 int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride) {
   ProfScope ps(c, "chol");
+  if (!c->simt_fp64) {
+    const int rc = launch_potrf_panels(c, A, n, batch, stride);
+    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: n beyond the panel kernel's shared memory
+  }
   k_chol<<<batch, 256, 0, c->stream>>>(A, n, stride, 0);
   GPL_LAUNCHED(c, "k_chol");
   return GPL_OK;

@@ -7,8 +7,8 @@
 //                  forward substitution over 32-row blocks. Block i first takes the product of
 //                  the finished rows, R = E - L[i, jb..i) Y[jb..i) (DMMA), then solves
 //                  L[i,i] Y_i = R by column-oriented substitution: one warp per 4 right-hand
-//                  sides, lanes over rows, y_q = r_q / L[q,q] broadcast by shuffle, each row's
-//                  sum taken in increasing q as in cholsl. The panel stays in shared memory.
+//                  sides, lanes over rows, y_q = r_q * (1/L[q,q]) broadcast by shuffle, each
+//                  row's sum taken in increasing q as in cholsl. The panel stays in shared memory.
 //                  Work: P^3/6 multiply-adds per gene.
 //   k_lauum_panel  one CTA per (panel b, gene): S[a, b] = sum_{k >= a} V[k, a]^T V[k, b]
 //                  for the blocks a >= b, written to both triangles. Work: P^3/6 per gene.
@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(256, 1)
   double* As = Yp + (size_t)nb * IB * IS;     // [nb*32][IS], As[k][m] = L[rb + m][r0 + k]
   double* Ld = As + (size_t)nb * IB * IS;     // [32][LS] diagonal block
   double* Rs = Ld + IB * LS;                  // [32][LS] right-hand sides
+  double* Rd = Rs + IB * LS;                  // [32] reciprocals of the diagonal
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int m0 = (warp >> 2) * 16, n0 = (warp & 3) * 8;
 
@@ -63,12 +64,12 @@ __global__ void __launch_bounds__(256, 1)
     cp_async_wait<0>();
     __syncthreads();
 
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int kb = 0; kb < K; kb += 4) {
-      const double a0 = As[(kb + t) * IS + m0 + g];
-      const double a1 = As[(kb + t) * IS + m0 + g + 8];
-      const double b0 = Yp[(kb + t) * IS + n0 + g];
-      dmma_16x8x4(acc, a0, a1, b0);
+    // two accumulators over alternating K steps (K is a multiple of 32) break the DMMA chain
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, acc2[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int kb = 0; kb < K; kb += 8) {
+      dmma_16x8x4(acc, As[(kb + t) * IS + m0 + g], As[(kb + t) * IS + m0 + g + 8], Yp[(kb + t) * IS + n0 + g]);
+      dmma_16x8x4(acc2, As[(kb + 4 + t) * IS + m0 + g], As[(kb + 4 + t) * IS + m0 + g + 8],
+                  Yp[(kb + 4 + t) * IS + n0 + g]);
     }
 #pragma unroll
     for (int h = 0; h < 2; h++)
@@ -76,8 +77,9 @@ __global__ void __launch_bounds__(256, 1)
       for (int e = 0; e < 2; e++) {
         const int m = m0 + g + 8 * h, n = n0 + 2 * t + e;
         const double ev = (ib == jb && m == n) ? 1.0 : 0.0;
-        Rs[m * LS + n] = ev - acc[2 * h + e];
+        Rs[m * LS + n] = ev - (acc[2 * h + e] + acc2[2 * h + e]);
       }
+    if (tid < IB) Rd[tid] = 1.0 / Ld[tid * LS + tid];
     __syncthreads();
 
     // L[i,i] Y_i = R: warp owns columns 4*warp .. +3, lane = row
@@ -85,11 +87,11 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
     for (int c = 0; c < 4; c++) rr[c] = Rs[lane * LS + 4 * warp + c];
     for (int q = 0; q < IB; q++) {
-      const double lqq = Ld[q * LS + q];
+      const double rq = Rd[q];
       const double lrq = Ld[lane * LS + q];
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        const double yq = __shfl_sync(0xffffffffu, rr[c], q) / lqq;
+        const double yq = __shfl_sync(0xffffffffu, rr[c], q) * rq;
         if (lane == q) rr[c] = yq;
         else if (lane > q) rr[c] = fma(-lrq, yq, rr[c]);
       }
@@ -162,9 +164,150 @@ __global__ void __launch_bounds__(256, 1)
   }
 }
 
+// Batched Cholesky (cholPsi, ggplvm.cu:683-692), one CTA per gene, 32-column panels left to
+// right (left-looking): the panel is loaded into shared memory, takes the product of the
+// finished columns (DMMA, the finished part streamed through shared memory 32 columns at a
+// time), then its 32 x 32 diagonal block is factored by one warp (lane = row; each entry's sum
+// in increasing column order as in choldc) and the rows below solve against it (thread per
+// row). A non-positive pivot zero-fills the matrix, as choldc does. Reads the lower triangle,
+// writes the factor over it; the strict upper triangle is left as it was.
+__global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi, int P, int64_t stride) {
+  extern __shared__ __align__(16) double sm[];
+  const int rows_pad = (P + 15) / 16 * 16;
+  const int SA = rows_pad + 4;                 // La[q][r]: rows contiguous, 4 mod 16
+  double* Ap = sm;                             // [rows_pad][IS]: the panel, Ap[r][c]
+  double* La = Ap + (size_t)rows_pad * IS;     // [2][32][SA]: finished columns, one 32-chunk
+  double* Rd = La + 2 * (size_t)IB * SA;       // [32] reciprocals of the diagonal
+  __shared__ int fail;
+  double* A = Psi + (size_t)blockIdx.x * stride;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int nb = (P + IB - 1) / IB;
+  if (tid == 0) fail = 0;
+  for (int kp = 0; kp < nb; kp++) {
+    const int c0 = kp * IB, rows = P - c0, ncol = min(IB, rows);
+    const int rpad = (rows + 15) / 16 * 16;
+    // the panel's lower part: rows c0.., columns c0..c0+ncol
+    for (int e = tid; e < rpad * IB; e += blockDim.x) {
+      const int r = e >> 5, cc = e & 31;
+      Ap[r * IS + cc] = (r < rows && cc < ncol) ? A[(size_t)(c0 + r) + (size_t)(c0 + cc) * P] : 0.0;
+    }
+    if (kp > 0) {
+      // Ap -= L[c0.., 0..c0) L[c0..c0+32, 0..c0)^T, 32 finished columns per chunk
+      double acc[2][4][4];
+#pragma unroll
+      for (int x = 0; x < 2; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++)
+#pragma unroll
+          for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
+      auto stage = [&](int ch, int buf) {
+        double* dst = La + (size_t)buf * IB * SA;
+        for (int e = tid; e < IB * rpad; e += blockDim.x) {
+          const int q = e / rpad, r = e - q * rpad;
+          const bool ok = r < rows;
+          cp_async8(dst + q * SA + r, A + (ok ? (size_t)(c0 + r) + (size_t)(ch * IB + q) * P : 0), ok ? 8 : 0);
+        }
+        cp_async_commit();
+      };
+      stage(0, 0);
+      for (int ch = 0; ch < kp; ch++) {
+        if (ch + 1 < kp) {
+          stage(ch + 1, (ch + 1) & 1);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* la = La + (size_t)(ch & 1) * IB * SA;
+#pragma unroll
+        for (int k4 = 0; k4 < IB / 4; k4++) {
+          const double* lr = la + (k4 * 4 + t) * SA;
+          double b[4];
+#pragma unroll
+          for (int y = 0; y < 4; y++) b[y] = lr[y * 8 + g];  // B[k][n] = L[c0 + n][q]
+#pragma unroll
+          for (int x = 0; x < 2; x++) {
+            const int mt = warp + 8 * x;
+            if (mt * 16 < rpad) {
+              const double a0 = lr[mt * 16 + g], a1 = lr[mt * 16 + g + 8];
+#pragma unroll
+              for (int y = 0; y < 4; y++) dmma_16x8x4(acc[x][y], a0, a1, b[y]);
+            }
+          }
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int x = 0; x < 2; x++) {
+        const int mt = warp + 8 * x;
+        if (mt * 16 >= rpad) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++)
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) Ap[(mt * 16 + g + 8 * h) * IS + y * 8 + 2 * t + e] -= acc[x][y][2 * h + e];
+      }
+    }
+    __syncthreads();
+    // the diagonal block, one warp: lane = row
+    if (warp == 0) {
+      for (int cc = 0; cc < ncol; cc++) {
+        if (lane == cc) {
+          double piv = Ap[cc * IS + cc];
+          for (int q = 0; q < cc; q++) piv -= Ap[cc * IS + q] * Ap[cc * IS + q];
+          if (piv <= 0.0) fail = 1;  // a NaN pivot passes, as in choldc
+          const double l = sqrt(piv);
+          Ap[cc * IS + cc] = l;
+          Rd[cc] = 1.0 / l;
+        }
+        __syncwarp();
+        if (lane > cc && lane < ncol) {
+          double sacc = Ap[lane * IS + cc];
+          for (int q = 0; q < cc; q++) sacc -= Ap[lane * IS + q] * Ap[cc * IS + q];
+          Ap[lane * IS + cc] = sacc * Rd[cc];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // rows below the block: L[r][0..32) against the factored block, thread per row
+    for (int r = IB + tid; r < rows; r += blockDim.x) {
+      for (int cc = 0; cc < ncol; cc++) {
+        double sacc = Ap[r * IS + cc];
+        for (int q = 0; q < cc; q++) sacc -= Ap[r * IS + q] * Ap[cc * IS + q];
+        Ap[r * IS + cc] = sacc * Rd[cc];
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < rows * IB; e += blockDim.x) {
+      const int r = e >> 5, cc = e & 31;
+      if (cc < ncol && r >= cc) A[(size_t)(c0 + r) + (size_t)(c0 + cc) * P] = Ap[r * IS + cc];
+    }
+    __threadfence_block();
+    __syncthreads();
+  }
+  if (fail)
+    for (int e = tid; e < P * P; e += blockDim.x) A[e] = 0.0;
+}
+
+int potrf_panel_smem(int P) {
+  const int rows_pad = (P + 15) / 16 * 16;
+  return (int)sizeof(double) * (rows_pad * IS + 2 * IB * (rows_pad + 4) + IB);
+}
+
+int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride) {
+  const int smem = potrf_panel_smem(n);
+  if (smem > 220 * 1024) return GPL_ERR_ARG;
+  GPL_TRY(c, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_potrf_panel<<<batch, 256, smem, c->stream>>>(A, n, stride);
+  GPL_LAUNCHED(c, "k_potrf_panel");
+  return GPL_OK;
+}
+
 int inverse_panel_smem(int P) {
   const int nb = (P + IB - 1) / IB;
-  return (int)sizeof(double) * (2 * nb * IB * IS + 2 * IB * LS);
+  return (int)sizeof(double) * (2 * nb * IB * IS + 2 * IB * LS + IB);
 }
 
 // Returns GPL_ERR_ARG when P is beyond the shared-memory budget of the panel kernels.

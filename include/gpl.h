@@ -46,7 +46,12 @@ extern "C" {
 #define GPL_ERR_LIMIT (-8)    /* size beyond a fixed limit of the allocation-free entry point */
 
 #define GPL_PREC_FP64 0       /* plain double precision: the drop-in path */
-#define GPL_PREC_BF16X3 1     /* Gram-family contractions on tensor cores, BF16 hi/lo split, FP32 accumulation */
+/* The precision form (no reference counterpart): the Gram and the gradient contraction on
+ * tensor cores (BF16 hi/lo products, FP32 runs folded into FP64) over the dense columns
+ * whitened by the prior's Cholesky factor, everything else FP64, and one FP64-residual
+ * refinement step on every per-gene solve. Objective within ~1e-7 of GPL_PREC_FP64 per
+ * evaluation. */
+#define GPL_PREC_BF16X3 1
 
 typedef struct gpl_ctx gpl_ctx;
 
@@ -56,6 +61,7 @@ typedef struct gpl_ctx gpl_ctx;
 GPL_API int gpl_create(gpl_ctx** out, int device, void* stream);
 GPL_API int gpl_destroy(gpl_ctx* ctx);
 GPL_API const char* gpl_last_error(const gpl_ctx* ctx);
+/* Selects GPL_PREC_FP64 (default) or GPL_PREC_BF16X3 for the following calls. */
 GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
 
 /* Gene-major CSR counts: replaces loadSparseMat + newSparseMatOnDevice
