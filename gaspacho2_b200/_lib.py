@@ -48,6 +48,7 @@ SIGNATURES = {
     "gpl_beta_from_tilde": (ctypes.c_int, [_vp]),
     "gpl_fit": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]),
     "gpl_fit_outer": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]),
+    "gpl_score_stats": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
     "gpl_evaluate": (ctypes.c_int, [_vp, _dp, ctypes.c_int64, _dp, _dp]),
     "gpl_evaluate_device": (ctypes.c_int, [_vp]),
     "gpl_get": (ctypes.c_int, [_vp, ctypes.c_char_p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),

@@ -838,6 +838,49 @@ int gpl_fit_outer(gpl_ctx* h, int itr, int lbfgs_budget, int32_t* stats, double*
   return rc;
 }
 
+int gpl_score_stats(gpl_ctx* h, int L, const double* G, double* S) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (L <= 0 || !G || !S) {
+    c->err = "score statistics need L >= 1 genotype columns and non-NULL G and S";
+    return GPL_ERR_ARG;
+  }
+  const size_t N = c->N, J = c->J;
+  const int LB = 64;  // genotype columns per pass (two per column in the GEMM tile of 128)
+  double *dG = nullptr, *dW = nullptr, *dS = nullptr;
+  const size_t work = (size_t)2 * LB * N + (size_t)4 * LB * J;
+  if (cudaMalloc((void**)&dG, sizeof(double) * N * LB) != cudaSuccess ||
+      cudaMalloc((void**)&dW, sizeof(double) * work) != cudaSuccess ||
+      cudaMalloc((void**)&dS, sizeof(double) * J * LB) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dG);
+    cudaFree(dW);
+    cudaFree(dS);
+    c->err = "device allocation failed: score statistics";
+    return GPL_ERR_ALLOC;
+  }
+  int rc = GPL_OK;
+  for (int l0 = 0; l0 < L && rc == GPL_OK; l0 += LB) {
+    const int nl = std::min(LB, L - l0);
+    if (cudaMemcpyAsync(dG, G + (size_t)l0 * N, sizeof(double) * N * nl, cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess) {
+      rc = GPL_ERR_CUDA;
+      break;
+    }
+    rc = launch_score_stats(c, nl, dG, dS, dW);
+    if (rc == GPL_OK &&
+        cudaMemcpyAsync(S + (size_t)l0 * J, dS, sizeof(double) * J * nl, cudaMemcpyDeviceToHost, c->stream) !=
+            cudaSuccess)
+      rc = GPL_ERR_CUDA;
+    if (rc == GPL_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GPL_ERR_CUDA;
+  }
+  if (rc == GPL_ERR_CUDA && c->err.empty()) c->err = cudaGetErrorString(cudaGetLastError());
+  cudaFree(dG);
+  cudaFree(dW);
+  cudaFree(dS);
+  return rc;
+}
+
 int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkhd, double* grad) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));

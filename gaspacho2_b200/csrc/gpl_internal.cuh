@@ -182,7 +182,8 @@ int launch_kernel_mats(Ctx* c);          // Knm into Z, Kmm, Kinv copy, chol(Kin
 int launch_expand_delta(Ctx* c);         // DeltaInv (upper + diag)
 int launch_chol_single(Ctx* c, double* A, int n);  // choldc on one n x n matrix
 // k_groups.cu
-int launch_group_sums(Ctx* c, int mode);  // 0: S (W/Omega); 1: S unweighted (gene 0); 2: T of y0; 3: T of nu
+int launch_group_sums(Ctx* c, int mode);  // 0: S (W/Omega); 1: S unweighted (gene 0); 2: T of y0; 3: T of nu;
+                                          // 4: T of a per-cell u (zt_u_src)
 int launch_assemble_psi(Ctx* c, int J);   // categorical rows/columns of Psi from the group sums
 int launch_assemble_b(Ctx* c, double* out);  // categorical entries of Z^T u (P x J) from the group sums
 int launch_group_tables(Ctx* c);          // per (gene, group) categorical blocks of Psi^{-1}
@@ -190,7 +191,8 @@ int launch_hk(Ctx* c);                    // HK[i] = sum_j O_ij [h_{j,g(i)} | ka
 // k_gemm.cu
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
-int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output
+int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output;
+                                                                      // mode 2: u is one value per cell
 int solve_refined(Ctx* c, const double* b, double* x);  // Psi_j x = b; FP64-residual refinement (precision form)
 int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
 int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
@@ -219,6 +221,8 @@ int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns 
 int dgen_eta(Ctx* c, const double* B, double* out);
 int dgen_group_sums(Ctx* c, int mode);
 int dgen_hk(Ctx* c);
+int dgen_weighted_colsums(Ctx* c, const double* G2, int n2, double* out);  // out[j + c*J] = sum_i W_ij G2[c][i]
+int launch_score_stats(Ctx* c, int L, const double* G, double* S, double* scratch);  // device G (N x L) -> S (J x L)
 int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw);  // Psi_DD = L G L^T + DeltaInv
 int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St);  // S~ = L^T S_DD L per gene
 int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D);  // U from the V rows of cells [c0, c1)

@@ -168,13 +168,13 @@ struct LdD {  // A(r = cell, k = dense column) = D[k*ldN + r]
   int ldN;
   __device__ double operator()(int r, int k, int) const { return D[(size_t)k * ldN + r]; }
 };
-struct LdU {  // B(k = cell, c = gene): mode 0 W nu / Omega, mode 1 y0
+struct LdU {  // B(k = cell, c = gene): mode 0 W u / Omega, 1 u (y0), 2 W g / Omega with g per cell
   static constexpr bool kFastK = true;
   const double *W, *Nu, *rOm;
   int ldN, mode;
   __device__ double operator()(int k, int c, int) const {
     const size_t e = (size_t)c * ldN + k;
-    return mode == 0 ? W[e] * rOm[k] * Nu[e] : Nu[e];
+    return mode == 0 ? W[e] * rOm[k] * Nu[e] : mode == 1 ? Nu[e] : W[e] * rOm[k] * Nu[k];
   }
 };
 struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega (1/phi given)
@@ -389,7 +389,7 @@ int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
   using T = TileTall;
   if (c->n_d > T::BM) return GPL_ERR_ARG;
   const double* rOm = nullptr;
-  if (mode == 0) {
+  if (mode != 1) {
     int rc = recip_omega(c, &rOm);
     if (rc) return rc;
   }
@@ -473,6 +473,47 @@ int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St) {
                           "k_dgen(S L)");
   if (rc) return rc;
   return launch_dgen<T>(c, g, n, n, LdLTk{Lw, n}, LdGeneT{Tt, n}, KAll{n}, EpGene{St, n}, "k_dgen(L^T S L)");
+}
+
+// Score statistics: C[j][c] = sum_i W_ij G2[c][i] over all cells, split over the cells into
+// kSplitK ranges whose partials are added in order.
+namespace {
+struct LdWrow {  // A(r = gene, k = cell) = W[r*ldN + k]
+  static constexpr bool kFastK = true;
+  const double* W;
+  int ldN;
+  __device__ double operator()(int r, int k, int) const { return W[(size_t)r * ldN + k]; }
+};
+struct LdCols {  // B(k = cell, c) = G2[c*N + k]
+  static constexpr bool kFastK = true;
+  const double* G2;
+  int N;
+  __device__ double operator()(int k, int c, int) const { return G2[(size_t)c * N + k]; }
+};
+}  // namespace
+
+__global__ void k_reduce_parts(int m, int n, int nz, const double* __restrict__ part, double* __restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, cc = blockIdx.y;
+  if (r >= m) return;
+  double s = 0.0;
+  for (int z = 0; z < nz; z++) s += part[((size_t)z * m + r) * n + cc];
+  out[r + (size_t)cc * m] = s;
+}
+
+int dgen_weighted_colsums(Ctx* c, const double* G2, int n2, double* out) {
+  using T = TileSq;
+  if (n2 > T::BN) return GPL_ERR_ARG;
+  int rc = ensure_part(c, (size_t)kSplitK * c->J * n2);
+  if (rc) return rc;
+  const int per = (c->N + kSplitK - 1) / kSplitK;
+  dim3 g(div_up(c->J, T::BM), 1, kSplitK);
+  rc = launch_dgen<T>(c, g, c->J, n2, LdWrow{c->W, c->ldN}, LdCols{G2, c->N}, KSplit{c->N, per},
+                      EpPart{c->part, c->J, n2}, "k_dgen(score sums)");
+  if (rc) return rc;
+  dim3 g2(div_up(c->J, 256), n2);
+  k_reduce_parts<<<g2, 256, 0, c->stream>>>(c->J, n2, kSplitK, c->part, out);
+  GPL_LAUNCHED(c, "k_reduce_parts");
+  return GPL_OK;
 }
 
 }  // namespace gpl

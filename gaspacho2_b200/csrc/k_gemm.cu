@@ -293,6 +293,10 @@ int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out) {
     LoadDt A{c->Dm, c->ldN, c->N, c->n_d};
     const int rc = c->simt_fp64 ? GPL_ERR_ARG : dgen_zt_u(c, mode, u, out);
     if (rc != GPL_OK && rc != GPL_ERR_ARG) return rc;
+    if (rc == GPL_ERR_ARG && mode == 2) {
+      c->err = "per-cell Z^T u needs the DMMA form (at most 144 dense columns)";
+      return GPL_ERR_ARG;
+    }
     if (rc == GPL_ERR_ARG) {  // the FFMA form: forced, or more dense columns than one DMMA tile
       if (mode == 0)
         k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
@@ -304,8 +308,8 @@ int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out) {
       GPL_LAUNCHED(c, "k_gemm_store(zt_u)");
     }
   }
-  c->zt_u_src = (mode == 0 && u != c->Nu) ? u : nullptr;
-  int rc = launch_group_sums(c, mode == 0 ? 3 : 2);
+  c->zt_u_src = (mode == 2 || (mode == 0 && u != c->Nu)) ? u : nullptr;
+  int rc = launch_group_sums(c, mode == 0 ? 3 : mode == 2 ? 4 : 2);
   c->zt_u_src = nullptr;
   if (rc) return rc;
   return launch_assemble_b(c, out);

@@ -109,7 +109,7 @@ __global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gce
   for (int k = c0 + lane; k < c1; k += 32) {
     const int i = gcells[k];
     const size_t e = (size_t)j * ldN + i;
-    s += MODE == 0 ? W[e] / Omega[i] * U[e] : U[e];
+    s += MODE == 0 ? W[e] / Omega[i] * U[e] : MODE == 4 ? W[e] / Omega[i] * U[i] : U[e];
   }
   s = warp_sum(s);
   if (lane == 0) T[(size_t)j * n_grp + g] = s;
@@ -142,6 +142,9 @@ int launch_group_sums(Ctx* c, int mode) {
   if (mode == 2)
     k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
                                            c->scratch, c->gT);
+  else if (mode == 4)  // u per cell, the same for every gene
+    k_group_t<4><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+                                           c->zt_u_src, c->gT);
   else
     k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
                                            c->zt_u_src ? c->zt_u_src : c->Nu, c->gT);

@@ -164,6 +164,16 @@ class GPLVM:
                 "gpl_evaluate")
         return v.value, g
 
+    def score_stats(self, G: np.ndarray) -> np.ndarray:
+        """Genotype score statistics (getScoreStats, ggplvm_de.cu:489-535): G is N x L, the
+        result J x L, at the current fitted state."""
+        G = np.asfortranarray(G, dtype=np.float64)
+        L = G.shape[1]
+        S = np.zeros(self.J * L)
+        self._c(self._L.gpl_score_stats(self.h, int(L), _d(np.ascontiguousarray(G.ravel(order="F"))), _d(S)),
+                "gpl_score_stats")
+        return S.reshape(L, self.J).T
+
     def evaluate_device(self):
         """Enqueues one objective+gradient evaluation at the device-resident parameters."""
         self._c(self._L.gpl_evaluate_device(self.h), "gpl_evaluate_device")

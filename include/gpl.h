@@ -163,6 +163,14 @@ GPL_API int gpl_fit_outer(gpl_ctx* ctx, int itr, int lbfgs_budget, int32_t* stat
  * line-search evaluation followed by the gradient (ggplvm.cu:1258-1277 then 1215-1240). */
 GPL_API int gpl_evaluate(gpl_ctx* ctx, const double* params, int64_t n_params, double* lkhd, double* grad);
 
+/* Genotype score statistics against the fitted model: getScoreStats of the reference's
+ * differential-expression driver (ggplvm_de.cu:489-535, run after its fit at :1205-1209).
+ * G[N*L] holds L genotype columns (column-major, e.g. dosages 0/1/2); S[J*L] receives
+ * S[j + l*J] = s / sqrt(phi_j v) with s = sum_i g_il/Omega_i (y_ij - W_ij) and
+ * v = g^T diag(W_j/Omega) g - t^T Psi_j^{-1} t, t = Z^T diag(W_j/Omega) g, at the current W,
+ * phi and factored Psi_j (call after gpl_fit, an IRLS phase or an objective). */
+GPL_API int gpl_score_stats(gpl_ctx* ctx, int L, const double* G, double* S);
+
 /* The same evaluation at the parameters already on the device, enqueued on the context's
  * stream without host copies or synchronisation (device-resident throughput). The objective
  * lands in slot 1 of the trace; read it with gpl_get("lkhd_dev") or the next evaluate. */

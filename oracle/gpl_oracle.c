@@ -1029,6 +1029,47 @@ int orc_fit(orc_ctx* o, int itr_max, int lbfgs_budget, int* stats, double* trace
   return rc;
 }
 
+/* getScoreStats (ggplvm_de.cu:489-535): for gene j and genotype column l of G (N x L,
+ * column-major), t = Z^T diag(W_j / Omega) g (getZtOinvjnj), v = g^T diag(W_j/Omega) g -
+ * t^T Psi_j^{-1} t (cholsl with the factored Psi_j), and the score
+ * sum_i g_i / Omega_i (y_ij - W_ij) over the merge walk of gene j's counts (unmatched cells
+ * contribute -g_i W_ij / Omega_i), divided by sqrt(phi_j v). S is J x L (S[j + l*J]). */
+void orc_score_stats(orc_ctx* o, int L, const double* G, double* S) {
+  const int N = o->N, J = o->J, P = o->P;
+#pragma omp parallel
+  {
+    double* tmp = (double*)xcalloc(P, sizeof(double));
+    double* tmp2 = (double*)xcalloc(P, sizeof(double));
+#pragma omp for collapse(2) schedule(dynamic, 4)
+    for (int lg = 0; lg < L; lg++)
+      for (int j = 0; j < J; j++) {
+        const double* Wj = o->W + (size_t)j * N;
+        const double* gl = G + (size_t)lg * N;
+        const double* Psij = o->Psi + (size_t)j * P * P;
+        memset(tmp2, 0, sizeof(double) * P);
+        zt_oinv_nu(o, Wj, gl, tmp);
+        cholsl(Psij, P, tmp, tmp2);
+        double v = 0.0;
+        for (int i = 0; i < N; i++) v += gl[i] * gl[i] * Wj[i] / o->Omega[i];
+        for (int i = 0; i < P; i++) v -= tmp[i] * tmp2[i];
+        int l = o->gp[j];
+        const int lmax = o->gp[j + 1];
+        double ss = 0.0;
+        for (int i = 0; i < N; i++) {
+          if (l < lmax && i == o->ci[l]) {
+            ss += gl[i] / o->Omega[i] * (o->cx[l] - Wj[i]);
+            l++;
+          } else {
+            ss += gl[i] * Wj[i] / o->Omega[i] * (-1.0);
+          }
+        }
+        S[j + (size_t)lg * J] = ss / sqrt(o->phi[j] * v);
+      }
+    free(tmp);
+    free(tmp2);
+  }
+}
+
 long orc_get(orc_ctx* o, const char* name, double* out) {
   const size_t N = o->N, J = o->J, M = o->M, Q = o->Q, P = o->P, p = o->p;
   struct { const char* n; const double* ptr; size_t len; } items[] = {

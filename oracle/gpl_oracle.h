@@ -45,6 +45,7 @@ void orc_downdate(orc_ctx* o, int jtr, double sr, int rhoflag);
 void orc_beta_from_tilde(orc_ctx* o);
 int orc_fit(orc_ctx* o, int itr_max, int lbfgs_budget, int* stats, double* trace, int trace_cap);
 long orc_get(orc_ctx* o, const char* name, double* out);
+void orc_score_stats(orc_ctx* o, int L, const double* G, double* S); /* getScoreStats */
 void orc_set_threads(int n);
 
 #ifdef __cplusplus

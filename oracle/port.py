@@ -55,6 +55,7 @@ def lib():
         L.orc_fit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]
         L.orc_get.restype = ctypes.c_long
         L.orc_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
+        L.orc_score_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
@@ -155,6 +156,14 @@ class OracleModel:
         rc = lib().orc_fit(self.h, itr_max, lbfgs_budget, st, _dptr(tr), trace_cap)
         stats = dict(outer=st[0], irls=st[1], lbfgs=st[2], evals=st[3])
         return rc, stats, tr[:stats["outer"] + stats["lbfgs"]].copy()
+
+    def score_stats(self, G: np.ndarray) -> np.ndarray:
+        """getScoreStats (ggplvm_de.cu:489-535): G is N x L, the result J x L."""
+        G = np.asfortranarray(G, dtype=np.float64)
+        L = G.shape[1]
+        S = np.zeros(self.J * L)
+        lib().orc_score_stats(self.h, L, _dptr(np.ascontiguousarray(G.ravel(order="F"))), _dptr(S))
+        return S.reshape(L, self.J).T
 
     def get(self, name: str) -> np.ndarray:
         n = lib().orc_get(self.h, name.encode(), None)

@@ -67,6 +67,9 @@ void Downdate(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double
 void LBFGS(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K, double* Xi, double* Ta, double* rho,
            double* grad, double* grad0, double* SS, double* XX, double* ss, double* Work, int rhoflag);
 
+void getScoreStats(int L, SparseMat* Y, DataFrame* Z, double* G, double* Psi, double* W, double* Omega,
+                   double* phi, double* Work, double* S);
+
 namespace {
 
 struct RefCtx {
@@ -444,5 +447,17 @@ void ref_model_meta(void* h, int* nh_out, int* mc_out, int* mv_out, int* mk_out)
 }
 
 void ref_set_verbose(int v) { ref_verbose = v; }
+
+/* The genotype score statistics of ggplvm_de.cu (getScoreStats :489-535, launched over a
+ * J x L grid at :1205-1209) at the current W, Psi factor, Omega and phi. G is N x L
+ * (column-major), S is J x L. */
+void ref_score_stats(void* h, int L, const double* G, double* S) {
+  RefCtx* c = (RefCtx*)h;
+  std::vector<double> g(G, G + (size_t)c->N * L), work((size_t)2 * c->J * L * c->P), s((size_t)c->J * L);
+  ref_launch(dim3(c->J, L), dim3(1), [&] {
+    getScoreStats(L, c->Y, c->Z, g.data(), c->Psi, c->W, c->Omega, c->phi, work.data(), s.data());
+  });
+  std::memcpy(S, s.data(), sizeof(double) * s.size());
+}
 
 }  // extern "C"

@@ -60,6 +60,7 @@ def lib():
         L.ref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
         L.ref_model_meta.argtypes = [ctypes.c_void_p, _ip, _ip, _ip, _ip]
         L.ref_set_verbose.argtypes = [ctypes.c_int]
+        L.ref_score_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         _lib = L
     return _lib
 
@@ -159,6 +160,14 @@ class RefModel:
         out = np.zeros(n)
         lib().ref_get(self.h, name.encode(), _ptr(out))
         return out
+
+    def score_stats(self, G: np.ndarray) -> np.ndarray:
+        """getScoreStats (ggplvm_de.cu:489-535): G is N x L, the result J x L."""
+        G = np.asfortranarray(G, dtype=np.float64)
+        L = G.shape[1]
+        S = np.zeros(self.J * L)
+        lib().ref_score_stats(self.h, L, _ptr(G.ravel(order="F")), _ptr(S))
+        return S.reshape(L, self.J).T
 
     def model_meta(self):
         nh = (ctypes.c_int * (self.p + 1))()

@@ -99,6 +99,12 @@ def make_case(name: str, spec: dict) -> dict:
     out["irls_lkhd"] = m.get("lkhd")[:n]
     for k in ("Beta", "phi"):
         out["irls_" + k] = m.get(k)
+    # genotype score statistics at the IRLS state (getScoreStats, ggplvm_de.cu:489-535):
+    # seeded dosages 0/1/2 with allele frequencies in U(0.05, 0.5)
+    rs = np.random.default_rng(1000 + spec["seed"])
+    freq = rs.uniform(0.05, 0.5, size=5)
+    out["score_G"] = rs.binomial(2, freq, size=(ds.y.N, 5)).astype(np.float64)
+    out["score_S"] = m.score_stats(out["score_G"])
     out["obj0"] = np.array(m.objective_after_irls(0))
     out["obj0_lkhds"] = m.get("lkhds")
     out["grad0"] = m.gradient()

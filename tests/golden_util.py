@@ -89,6 +89,9 @@ def run_phases(model, gd: GoldenData) -> dict:
     out["irls_lkhd"] = model.get("lkhd")[:n]
     for k in ("Beta", "phi"):
         out["irls_" + k] = model.get(k)
+    g = getattr(gd, "g", None)
+    if g is not None and "score_G" in g:
+        out["score_S"] = model.score_stats(g["score_G"])
     out["obj0"] = model.objective_after_irls(0)
     out["obj0_lkhds"] = model.get("lkhds")
     out["grad0"] = model.gradient()
