@@ -3,7 +3,7 @@
 //
 //   ggplvm Y.bin Z.bin ls.bin Xi.bin [-M m] [-Q q] [--init-params params.bin]
 //          [--max-outer n] [--max-lbfgs-iters n] [--precision fp64|bf16x3] [--device d]
-//          [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--quiet]
+//          [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--genotypes G.bin -L l] [--quiet]
 //
 // Inputs (same formats as the reference): Y.bin gene-major compressed counts
 // (int N, J, L; int i[L]; int p[J+1]; double x[L], SparseMat.cu:37-52), Z.bin covariate
@@ -26,6 +26,10 @@
 //   params.bin   at the end: the headerless parameter blocks (ggplvm.cu:1333-1346)
 //   beta.bin     at the end: double[P*J], gene j's coefficients at j*P (the reference
 //                never writes beta)
+//   ScoreStats.gz with --genotypes: after the fit, J rows of the L genotype columns' score
+//                statistics, "%lf," each (the output of the reference's differential-expression
+//                driver, ggplvm_de.cu:1205-1214; G.bin holds double[N*L], column-major, already
+//                transformed as that driver does with its dox and scaling)
 // Exit status 0 on success, 1 on an input, allocation or CUDA error or a NaN IRLS
 // likelihood (the reference returns 1 there, ggplvm.cu:1182), 2 on bad usage.
 //
@@ -46,8 +50,8 @@
 namespace {
 
 struct Options {
-  std::string y, z, ls, xi, init_params, out_dir = ".", precision = "fp64", phi_gz = "omega";
-  int M = 100, Q = 51, max_outer = 5000, max_lbfgs = 0, device = 0;
+  std::string y, z, ls, xi, init_params, out_dir = ".", precision = "fp64", phi_gz = "omega", genotypes;
+  int M = 100, Q = 51, max_outer = 5000, max_lbfgs = 0, device = 0, L = 0;
   uint64_t seed = 0;
   bool quiet = false;
 };
@@ -56,7 +60,7 @@ void usage() {
   fprintf(stderr,
           "usage: ggplvm Y.bin Z.bin ls.bin Xi.bin [-M m] [-Q q] [--init-params params.bin]\n"
           "              [--max-outer n] [--max-lbfgs-iters n] [--precision fp64|bf16x3] [--device d]\n"
-          "              [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--quiet]\n");
+          "              [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--genotypes G.bin -L l] [--quiet]\n");
 }
 
 bool parse_int(const char* s, long lo, long hi, long* out) {
@@ -80,7 +84,7 @@ int parse(int argc, char** argv, Options* o) {
       return argv[++i];
     };
     long v;
-    if (a == "-M" || a == "-Q" || a == "--max-outer" || a == "--max-lbfgs-iters" || a == "--device") {
+    if (a == "-M" || a == "-Q" || a == "-L" || a == "--max-outer" || a == "--max-lbfgs-iters" || a == "--device") {
       const char* s = need(a.c_str());
       if (!s) return 2;
       const long lo = (a == "--max-lbfgs-iters" || a == "--device") ? 0 : 1;
@@ -90,6 +94,7 @@ int parse(int argc, char** argv, Options* o) {
       }
       if (a == "-M") o->M = (int)v;
       else if (a == "-Q") o->Q = (int)v;
+      else if (a == "-L") o->L = (int)v;
       else if (a == "--max-outer") o->max_outer = (int)v;
       else if (a == "--max-lbfgs-iters") o->max_lbfgs = (int)v;
       else o->device = (int)v;
@@ -97,10 +102,12 @@ int parse(int argc, char** argv, Options* o) {
       const char* s = need("--seed");
       if (!s || !parse_int(s, 0, 1L << 62, &v)) return 2;
       o->seed = (uint64_t)v;
-    } else if (a == "--init-params" || a == "--precision" || a == "--out-dir" || a == "--phi-gz") {
+    } else if (a == "--init-params" || a == "--precision" || a == "--out-dir" || a == "--phi-gz" ||
+               a == "--genotypes") {
       const char* s = need(a.c_str());
       if (!s) return 2;
-      if (a == "--init-params") o->init_params = s;
+      if (a == "--genotypes") o->genotypes = s;
+      else if (a == "--init-params") o->init_params = s;
       else if (a == "--precision") o->precision = s;
       else if (a == "--out-dir") o->out_dir = s;
       else o->phi_gz = s;
@@ -118,6 +125,10 @@ int parse(int argc, char** argv, Options* o) {
   }
   if (pos.size() != 4) {
     usage();
+    return 2;
+  }
+  if (!o->genotypes.empty() && o->L < 1) {
+    fprintf(stderr, "ggplvm: --genotypes needs -L with the number of genotype columns\n");
     return 2;
   }
   if (o->precision != "fp64" && o->precision != "bf16x3") {
@@ -392,6 +403,22 @@ int main(int argc, char** argv) {
   if (!o.quiet) printf("Iteration end...\n");
   std::vector<double> beta((size_t)P * J);
   if ((rc = gpl_get_beta(ctx, beta.data()))) return fail(ctx, "gpl_get_beta", rc);
+  if (!o.genotypes.empty()) {
+    std::vector<double> G((size_t)N * o.L), S((size_t)J * o.L);
+    if (!load_doubles(o.genotypes, G.data(), G.size())) return 1;
+    if ((rc = gpl_score_stats(ctx, o.L, G.data(), S.data()))) return fail(ctx, "gpl_score_stats", rc);
+    const std::string path = join(o.out_dir, "ScoreStats.gz");
+    gzFile f = gzopen(path.c_str(), "w6h");
+    if (!f) {
+      fprintf(stderr, "ggplvm: cannot write %s\n", path.c_str());
+      return 1;
+    }
+    for (int j = 0; j < J; j++) {
+      for (int l = 0; l < o.L; l++) gzprintf(f, "%lf,", S[j + (size_t)l * J]);
+      gzprintf(f, "\n");
+    }
+    if (gzclose(f) != Z_OK) return 1;
+  }
   if (!write_file(join(o.out_dir, "params.bin"), q.blocks()) ||
       !write_file(join(o.out_dir, "beta.bin"), {{beta.data(), beta.size() * 8}}))
     return 1;

@@ -3,7 +3,8 @@
 CPU tests cover argument and input-file errors (answered before any device work); the GPU
 test runs a budgeted fit of the c0_small fixture through the CLI and compares params.bin,
 Params9.bin, beta.bin, X9.gz and phi.gz with the reference's own fit of the same inputs
-(ggplvm.cu:1301-1346 for the file layouts)."""
+(ggplvm.cu:1301-1346 for the file layouts), plus the genotype score statistics of the
+differential-expression driver (ScoreStats.gz, ggplvm_de.cu:1205-1214)."""
 import gzip
 import os
 import subprocess
@@ -72,8 +73,11 @@ def test_cli_fit_matches_reference_fit(cli, tmp_path):
     out = tmp_path / "out"
     out.mkdir()
     budget = 12
+    G = gd.g["score_G"]
+    G.T.tofile(tmp_path / "G.bin")  # column-major N x L
     r = _run(cli, [p["Y"], p["Z"], p["ls"], p["Xi"], "-M", gd.M, "-Q", gd.Q, "--init-params", p["params"],
-                   "--max-outer", 1, "--max-lbfgs-iters", budget, "--out-dir", out, "--quiet"], tmp_path)
+                   "--max-outer", 1, "--max-lbfgs-iters", budget, "--out-dir", out, "--quiet",
+                   "--genotypes", tmp_path / "G.bin", "-L", G.shape[1]], tmp_path)
     assert r.returncode == 0, r.stderr
     N, J, M, Q = gd.N, gd.J, gd.M, gd.Q
     p_ = gd.init.delta.shape[0]
@@ -102,6 +106,19 @@ def test_cli_fit_matches_reference_fit(cli, tmp_path):
     phi_rows = _read_gz_rows(out / "phi.gz")
     assert len(phi_rows) == J
     assert phi_rows[:3] == ["%f" % v for v in prm.Omega[:3]]
+    # ScoreStats.gz: J rows of L "%lf," values, the same statistics as the C ABI at the fitted state
+    srows = _read_gz_rows(out / "ScoreStats.gz")
+    assert len(srows) == J
+    S_cli = np.array([[float(v) for v in row.split(",") if v] for row in srows])
+    assert S_cli.shape == (J, G.shape[1]) and np.all(np.isfinite(S_cli))
+    from gaspacho2_b200 import GPLVM
+    with GPLVM.from_dataset(gd) as m:
+        m.set_params(gd.init)
+        m.kernel_mats()
+        m.glm_init()
+        m.fit(1, budget)
+        S_api = m.score_stats(G)
+    assert np.allclose(S_cli, S_api, rtol=0, atol=1e-6)
     tau = np.fromfile(out / "Tau.bin", np.float64)
     assert tau.shape[0] == M * Q
     assert np.allclose(tau[:M], (np.arange(1, M + 1) / (M + 1)) * 2.0 * 3.14159265358979, rtol=0, atol=1e-15)
