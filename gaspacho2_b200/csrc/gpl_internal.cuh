@@ -63,7 +63,7 @@ struct TcState {
   bool ready = false, check_each = false;
   int cpad = 0, chunks_cells = 0, gram_tiles_n = 0, Jpad = 0;
   int n_pairs = 0, pair_tiles = 0;
-  int smem_gram = 0, smem_whiten = 0;
+  int smem_gram = 0, smem_whiten = 0, run = 4;  // run: K chunks per FP32 accumulator run
   __nv_bfloat16 *whi = nullptr, *wlo = nullptr;   // w = W/Omega, gene rows x cpad
   __nv_bfloat16 *ahi = nullptr, *alo = nullptr;   // whitened pair products, pair rows x cpad
   __nv_bfloat16 *shi = nullptr, *slo = nullptr;   // whitened inverse pairs, pair rows x Jpad
@@ -193,7 +193,8 @@ int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
 int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output;
                                                                       // mode 2: u is one value per cell
-int solve_refined(Ctx* c, const double* b, double* x);  // Psi_j x = b; FP64-residual refinement (precision form)
+int solve_refined(Ctx* c, const double* b, double* x, bool dinv_factored = false);  // Psi_j x = b; FP64-residual
+                                                        // refinement in the precision form
 int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
 int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
 int launch_c1_tn(Ctx* c);                // C1 partial from tn/phi and tBeta GP block

@@ -79,17 +79,36 @@ __global__ void __launch_bounds__(256) k_beta_phi(int N, int ldN, int P, double 
   }
 }
 
-// r = b - Z^T diag(W/Omega) (Z x) - DeltaInv x for every gene (bx holds the first product);
-// DeltaInv is read from its upper triangle and diagonal.
-__global__ void k_residual(int P, int J, const double* __restrict__ b, const double* __restrict__ bx,
-                           const double* __restrict__ Dinv, const double* __restrict__ x, double* __restrict__ r) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
-  if (k >= P) return;
+// r = b - Z^T diag(W/Omega) (Z x) - DeltaInv x for every gene (bx holds the first product), one
+// CTA per gene. DeltaInv is read from its upper triangle and diagonal, or, once cholDeltaInv has
+// overwritten its lower triangle and diagonal with the factor L (factored), as L (L^T x).
+__global__ void __launch_bounds__(256) k_residual(int P, int J, const double* __restrict__ b,
+                                                  const double* __restrict__ bx, const double* __restrict__ Dinv,
+                                                  int factored, const double* __restrict__ x,
+                                                  double* __restrict__ r) {
+  extern __shared__ double xs[];  // x_j, then L^T x_j
+  const int j = blockIdx.x;
   const double* xj = x + (size_t)j * P;
-  double s = 0.0;
-  for (int l = 0; l < P; l++) s = fma(Dinv[k <= l ? k + (size_t)l * P : l + (size_t)k * P], xj[l], s);
-  const size_t e = (size_t)j * P + k;
-  r[e] = b[e] - bx[e] - s;
+  double* ts = xs + P;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) xs[k] = xj[k];
+  __syncthreads();
+  if (factored) {
+    for (int k = threadIdx.x; k < P; k += blockDim.x) {
+      double t = 0.0;
+      for (int l = k; l < P; l++) t = fma(Dinv[l + (size_t)k * P], xs[l], t);
+      ts[k] = t;
+    }
+    __syncthreads();
+  }
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    double s = 0.0;
+    if (factored)
+      for (int l = 0; l <= k; l++) s = fma(Dinv[k + (size_t)l * P], ts[l], s);
+    else
+      for (int l = 0; l < P; l++) s = fma(Dinv[k <= l ? k + (size_t)l * P : l + (size_t)k * P], xs[l], s);
+    const size_t e = (size_t)j * P + k;
+    r[e] = b[e] - bx[e] - s;
+  }
 }
 
 __global__ void k_add_to(size_t n, const double* __restrict__ d, double* __restrict__ x) {
@@ -101,7 +120,7 @@ __global__ void k_add_to(size_t n, const double* __restrict__ d, double* __restr
 // error, so the solution is refined against the exact FP64 operator, applied without forming
 // it: x += Psi~^{-1} (b - Z^T diag(W/Omega) Z x - DeltaInv x). The reference solves once with
 // its FP64 Psi (cholsl in getBetaPhi / getTildeBeta); the refined x converges to that solution.
-int solve_refined(Ctx* c, const double* b, double* x) {
+int solve_refined(Ctx* c, const double* b, double* x, bool dinv_factored) {
   const int64_t PP = (int64_t)c->P * c->P;
   int rc = launch_solve_batched(c, c->Psi, c->P, PP, b, c->P, x, c->P, c->J);
   if (rc || c->precision != GPL_PREC_BF16X3) return rc;
@@ -109,8 +128,8 @@ int solve_refined(Ctx* c, const double* b, double* x) {
   for (int it = 0; it < c->refine_steps; it++) {
     if ((rc = launch_zbeta(c, x, c->scratch))) return rc;
     if ((rc = launch_zt_u_ex(c, 0, c->scratch, c->bx))) return rc;
-    dim3 g(div_up(c->P, 128), c->J);
-    k_residual<<<g, 128, 0, c->stream>>>(c->P, c->J, b, c->bx, c->DeltaInv, x, c->rres);
+    k_residual<<<c->J, 256, 2 * sizeof(double) * c->P, c->stream>>>(c->P, c->J, b, c->bx, c->DeltaInv,
+                                                                     dinv_factored ? 1 : 0, x, c->rres);
     GPL_LAUNCHED(c, "k_residual");
     if ((rc = launch_solve_batched(c, c->Psi, c->P, PP, c->rres, c->P, c->bx, c->P, c->J))) return rc;
     const size_t n = (size_t)c->P * c->J;
@@ -118,6 +137,44 @@ int solve_refined(Ctx* c, const double* b, double* x) {
     GPL_LAUNCHED(c, "k_add_to");
   }
   return GPL_OK;
+}
+
+// phi from the exact quadratic form (precision form): beta^T Psi beta =
+// sum_i (W_ij/Omega_i) (z_i . beta_j)^2 + beta^T DeltaInv beta with E = Z beta given, instead of
+// |L^T beta|^2 with the factor of the tensor-core Gram; the same clamps as k_beta_phi.
+__global__ void __launch_bounds__(256) k_phi_exact(int N, int ldN, int P, const double* __restrict__ W,
+                                                   const double* __restrict__ Nu, const double* __restrict__ E,
+                                                   const double* __restrict__ Omega, const double* __restrict__ Dinv,
+                                                   const double* __restrict__ Beta, double* __restrict__ phi) {
+  __shared__ double sh[32];
+  const int j = blockIdx.x;
+  const double* Wj = W + (size_t)j * ldN;
+  const double* nj = Nu + (size_t)j * ldN;
+  const double* ej = E + (size_t)j * ldN;
+  double q = 0.0, s = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double w = Wj[i] / Omega[i];
+    q += nj[i] * nj[i] * w;
+    s += ej[i] * ej[i] * w;
+  }
+  const double* bj = Beta + (size_t)j * P;
+  double d = 0.0;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    double t = 0.0;
+    for (int l = 0; l < P; l++) t += Dinv[k <= l ? k + (size_t)l * P : l + (size_t)k * P] * bj[l];
+    d += bj[k] * t;
+  }
+  const double sq = block_sum(q, sh);
+  const double ss = block_sum(s, sh);
+  const double sd = block_sum(d, sh);
+  if (threadIdx.x == 0) {
+    double ph = (sq - (ss + sd)) / (double)N;
+    if (isnan(ph)) ph = 1.0;
+    if (ph < 0.0) ph = 1.0;
+    if (ph < 0.01) ph = 0.01;
+    if (ph > 1000.0) ph = 1000.0;
+    phi[j] = ph;
+  }
 }
 
 int launch_beta_phi(Ctx* c, int jtr) {
@@ -129,6 +186,12 @@ int launch_beta_phi(Ctx* c, int jtr) {
   k_beta_phi<<<c->J, 256, sizeof(double) * c->P, c->stream>>>(c->N, c->ldN, c->P, r, c->W, c->Nu, c->Omega, c->Psi,
                                                               c->sol, c->Beta, c->phi);
   GPL_LAUNCHED(c, "k_beta_phi");
+  if (c->precision == GPL_PREC_BF16X3) {
+    if ((rc = launch_zbeta(c, c->Beta, c->scratch))) return rc;
+    k_phi_exact<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->W, c->Nu, c->scratch, c->Omega, c->DeltaInv,
+                                              c->Beta, c->phi);
+    GPL_LAUNCHED(c, "k_phi_exact");
+  }
   return GPL_OK;
 }
 
@@ -193,7 +256,9 @@ __global__ void __launch_bounds__(256) k_lkhd_genes(int N, int ldN, int P, const
 }
 
 int launch_lkhd_genes(Ctx* c) {
-  int rc = launch_solve_batched(c, c->Psi, c->P, (int64_t)c->P * c->P, c->bvec, c->P, c->sol, c->P, c->J);
+  // b^T Psi^{-1} b enters as the difference q - b^T x of two large sums: in the precision form
+  // x is refined against the FP64 operator (a 1e-6 error in x would survive the cancellation)
+  int rc = solve_refined(c, c->bvec, c->sol, true);  // cholDeltaInv has run (ggplvm.cu:1206,1266)
   if (rc) return rc;
   ProfScope ps(c, "lkhd_genes");
   k_lkhd_genes<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->W, c->Nu, c->Omega, c->Psi, c->DeltaInv, c->bvec,

@@ -52,7 +52,7 @@ constexpr int kThreadsGram = 192;       // TMA, MMA and 4 drain warps
 constexpr int kStagesGram = 3;          // pipeline depth (192 KB of operand tiles)
 constexpr int kMaxStages = 3;
 constexpr int kGramN = 128;             // genes per Gram tile
-constexpr int kSBGram = 4;              // chunks per FP32 run
+constexpr int kSBGram = 4;              // chunks per FP32 run (default; GPL_TC_RUN overrides)
 constexpr int kTileA = 128 * 128;       // 128 rows x 64 BF16
 constexpr int kTileBG = kGramN * 128;   // 128 gene rows x 64 BF16
 constexpr int kMaxWhiten = 160;         // dense columns the whitened rows kernel holds per cell
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
               const int2* __restrict__ pairs, int n_pairs,
               int chunks_total, const int* __restrict__ dcol, int P, int J, const double* __restrict__ Dinv,
               double* __restrict__ Psi, double* __restrict__ Gt, int n_d, int n_base, double* __restrict__ V,
-              int v_ld, int* __restrict__ err) {
+              int v_ld, int run, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* A_hi = base;
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ptile = blockIdx.x, n0 = blockIdx.y * kGramN;
   const int nch = chunks_total;
-  const int nsb = (nch + kSBGram - 1) / kSBGram;
+  const int nsb = (nch + run - 1) / run;
 
   if (threadIdx.x == 0) tc_init(sh, err, 1);
   __syncthreads();
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
       for (int it = 0; it < nch; it++) {
-        const int s = it % kStagesGram, sb = it / kSBGram, pos = it % kSBGram, buf = sb & 1;
+        const int s = it % kStagesGram, sb = it / run, pos = it % run, buf = sb & 1;
         if (pos == 0 && sb >= 2 && !mbar_wait(&sh->drained[buf], ((sb >> 1) - 1) & 1, err)) {
           tc_fail(err, sh, 16);
           break;
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
           mma_bf16(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), kIdescGram, 1u);
         }
         mma_commit(&sh->empty[s]);
-        if (pos == kSBGram - 1 || it == nch - 1) mma_commit(&sh->accb[buf]);
+        if (pos == run - 1 || it == nch - 1) mma_commit(&sh->accb[buf]);
       }
       mma_finish(sh, err, 17);
     }
@@ -483,6 +483,8 @@ int tc_prepare(Ctx* c) {
     c->err = "cuTensorMapEncodeTiled failed";
     return GPL_ERR_CUDA;
   }
+  t.run = kSBGram;
+  if (const char* r = getenv("GPL_TC_RUN")) t.run = std::max(1, atoi(r));
   t.smem_gram = 1024 + kStagesGram * (2 * kTileA + 2 * kTileBG) + (int)sizeof(TcShared) + 128 * (int)sizeof(int2);
   GPL_TRY(c, cudaFuncSetAttribute(k_tc_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_gram));
   t.ready = true;
@@ -544,7 +546,7 @@ int launch_tc_gram(Ctx* c) {
     dim3 g(t.pair_tiles, t.gram_tiles_n);
     k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
                                                            t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
-                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.err);
+                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.run, t.err);
     GPL_LAUNCHED(c, "k_tc_gram");
   }
   {
@@ -582,7 +584,7 @@ int launch_tc_grad(Ctx* c) {
       k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
                                                              t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
                                                              c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
-                                                             s.pairs_pad, t.err);
+                                                             s.pairs_pad, t.run, t.err);
       GPL_LAUNCHED(c, "k_tc_gram(gradient pairs)");
     }
     if ((rc = launch_v_to_u_cells(c, c0, c1, t.DwC))) return rc;
