@@ -1,14 +1,16 @@
 """The precision form (GPL_PREC_BF16X3) against the plain FP64 path, through the C ABI.
 
-The precision form runs the Gram on tcgen05 tensor cores (BF16 hi/lo products, FP32 runs
-folded into FP64 in TMEM) over the dense columns whitened by the prior's Cholesky factor, and
-maps the result back in FP64; everything else stays FP64. Bars, per objective+gradient
+The precision form runs the Gram and the gradient contraction on tcgen05 tensor cores (BF16
+hi/lo products, FP32 runs folded into FP64 in TMEM) over the dense columns whitened by the
+prior's Cholesky factor, maps the results back in FP64 and refines every per-gene solve against
+the FP64 operator; everything else stays FP64. Bars, per objective+gradient
 evaluation at the same state:
   * every per-gene Cholesky succeeds (the whitening is what makes this hold: without it,
     1e-6 Gram errors against cond(Psi_j) ~ 1e14 fail the factorisation);
-  * the objective within 1e-6 relative of FP64 (measured 7e-9 .. 7e-8);
+  * the objective within 1e-6 relative of FP64 (measured ~1e-9 after the refinement of the
+    solve that enters it);
   * the gradient blocks for Omega, delta, X and rho within 2e-3 (relative L2), T within 5e-2
-    (measured up to 2e-4 and 9e-3), except at config 0, whose cond(Kmm) = 3.5e10 makes even the
+    (measured up to 1.2e-5 and 4.4e-4), except at config 0, whose cond(Kmm) = 3.5e10 makes even the
     FP64 path's gradient move by 5e-5 under a change of summation order; there only finiteness
     is required."""
 import numpy as np
