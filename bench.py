@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--fit-config", type=int, default=1, help="configuration of the time-to-fit leg")
     ap.add_argument("--fit-lbfgs", type=int, default=200, help="L-BFGS step budget of the time-to-fit leg")
     ap.add_argument("--no-fit", action="store_true", help="skip the time-to-fit leg")
+    ap.add_argument("--no-precision-leg", action="store_true",
+                    help="skip the precision form's throughput beside the FP64 line")
     ap.add_argument("--precision-report", action="store_true",
                     help="instead of the benchmark: the precision form against FP64 along a fit, every 10 steps")
     return ap.parse_args()
@@ -241,6 +243,54 @@ def workload_config(ds, args, precision):
             "global_batch": ds.N, "seq_len": None}
 
 
+def precision_leg(args, ds, stream, device):
+    """The precision form (tensor-core Gram and gradient contraction over whitened columns,
+    FP64 elsewhere, refined solves) on the same workload and state as the FP64 line: its
+    device-resident evaluation rate, and its objective and gradient against FP64 at the
+    same parameters."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM
+
+    m = GPLVM.from_dataset(ds, device=device, stream=stream.cuda_stream, precision="fp64")
+    m.set_params(ds.init)
+    m.kernel_mats()
+    m.glm_init()
+    for j in range(args.irls_sweeps):
+        m.irls_sweep(0, j)
+    m.objective_after_irls(0)
+    x = m.params_vector()
+    v64, g64 = m.evaluate(x)
+    g64 = g64.copy()
+    m.set_precision("bf16x3")
+    vbf, gbf = m.evaluate(x)
+    for _ in range(args.warmup):
+        m.evaluate_device()
+    m.profile(True)
+    m.profile_reset()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        m.evaluate_device()
+    e.record(stream)
+    torch.cuda.synchronize()
+    dt = s.elapsed_time(e) / 1e3
+    phases = {}
+    for name in ("gram", "uq"):
+        ms, n = m.profile_read(name)
+        if n:
+            phases[name] = ms / args.steps
+    m.profile(False)
+    m.close()
+    return {"value": args.steps / dt, "unit": "evals/s", "ms_per_step": dt / args.steps * 1e3,
+            "dtype": "bf16x3+f64", "objective_rel_err_vs_fp64": abs(vbf - v64) / abs(v64),
+            "gradient_rel_l2_vs_fp64": float(np.linalg.norm(gbf - g64) / np.linalg.norm(g64)),
+            "tensor_phase_ms_per_step": phases,
+            "note": "Gram and gradient contraction on tcgen05 (BF16 hi/lo, FP64-folded TMEM runs) over "
+                    "whitened dense columns; FP64 elsewhere; one FP64-residual refinement per solve"}
+
+
 def time_to_fit(args, stream, device):
     """The driver's whole fit (kernel matrices, GLM initialisation, then outer iterations of
     IRLS to convergence and L-BFGS with the backtracking line search) from the seeded
@@ -395,6 +445,8 @@ def run_ours(args):
             "hbm_gbs_measured": peaks.get("hbm_gbs"), "bf16_tflops_measured": peaks.get("bf16_tflops"),
         }
     m.close()
+    if rank == 0 and args.precision == "fp64" and not args.no_precision_leg:
+        line["precision_form"] = precision_leg(args, ds, stream, local)
     if rank == 0 and not args.no_fit:
         line["time_to_fit"] = time_to_fit(args, stream, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -84,10 +84,11 @@ static void free_state(Ctx* c) {
   tc_release(c);
   pair_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
-                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part};
+                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d};
   for (void* q : extra)
     if (q) cudaFree(q);
   c->hk_tiles128_d = nullptr;
+  c->hk_cells_d = nullptr;
   c->n_hk_tiles128 = 0;
   c->part = nullptr;
   c->part_n = 0;
@@ -527,9 +528,14 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
       for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 64) tiles.push_back(make_int2(g, r0));
   c->n_hk_tiles = (int)tiles.size();
   std::vector<int2> tiles128;
+  std::vector<int32_t> tile_cells;  // the cell of each of the 128 slots of every tile, -1 past the group
   if (grouped)
     for (int g = 0; g < n_grp; g++)
-      for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 128) tiles128.push_back(make_int2(g, r0));
+      for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 128) {
+        tiles128.push_back(make_int2(g, r0));
+        for (int q = 0; q < 128; q++)
+          tile_cells.push_back(r0 + q < gstart[g + 1] - gstart[g] ? order[gstart[g] + r0 + q] : -1);
+      }
   c->n_hk_tiles128 = (int)tiles128.size();
   c->tot_max = tot_len(c, 1);
   const size_t scratch_n = std::max({ldN * (size_t)J, (size_t)J * P * P, (size_t)c->tot_max, (size_t)M * M});
@@ -589,6 +595,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_RUN(dalloc(c, &c->gstart_d, gstart.size(), "group offsets"));
     GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->hk_tiles128_d, tiles128.size(), "group tiles"));
+    GPL_RUN(dalloc(c, &c->hk_cells_d, tile_cells.size(), "group tile cells"));
     GPL_RUN(dalloc(c, &c->gsum, (size_t)J * n_grp * (n_d + 1), "group sums"));
     GPL_RUN(dalloc(c, &c->gT, (size_t)J * n_grp, "group response sums"));
     GPL_RUN(dalloc(c, &c->HK, ldN * (n_d + 1), "HK"));
@@ -600,6 +607,8 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles_d, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles128_d, tiles128.data(), sizeof(int2) * tiles128.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->hk_cells_d, tile_cells.data(), sizeof(int32_t) * tile_cells.size(),
+                          cudaMemcpyHostToDevice));
   }
   GPL_TRY(c, cudaMemcpy(c->Dm, Dh.data(), sizeof(double) * ldN * n_d, cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->dcol_d, dcol.data(), sizeof(int) * n_d, cudaMemcpyHostToDevice));

@@ -108,6 +108,7 @@ struct Ctx {
   int2* hk_tiles_d = nullptr;       // (group, first row) of every 64-cell tile of the group lists
   int n_hk_tiles = 0;
   int2* hk_tiles128_d = nullptr;    // the same for 128-cell tiles
+  int* hk_cells_d = nullptr;        // the cell of each slot of those tiles (-1 past the group)
   int n_hk_tiles128 = 0;
   double* part = nullptr;           // split-K partial sums
   size_t part_n = 0;

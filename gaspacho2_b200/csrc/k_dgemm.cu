@@ -33,6 +33,7 @@ constexpr int BM = 128, BN = 128, BK = 16;
 constexpr int SA = BM + 4;   // As[k][m]
 constexpr int SBT = BK + 4;  // Bs[n][k] (weights, k contiguous)
 constexpr int SBN = BN + 4;  // Bs[k][n] (S pairs, n contiguous)
+constexpr int SD = BK + 2;   // Ds[col][k] (dense columns of a slice, k contiguous, 16-byte rows)
 constexpr int kThreads = 256;
 }  // namespace
 
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   double* As = smem_d;                          // [2][BK][SA]   pair products
   double* Bs = As + 2 * BK * SA;                // [3][BN][SBT]  weights
   double* Rs = Bs + 3 * BN * SBT;               // [3][BK]       1/Omega
-  double* Ds = Rs + 3 * BK;                     // [3][BK][n_d]  dense columns
+  double* Ds = Rs + 3 * BK;                     // [3][n_d][SD]  dense columns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
   const int p0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
@@ -94,10 +95,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double* src = W + (size_t)min(j, J - 1) * ldN + min(i, ldN - 2);
       cp_async16(Bs + st * BN * SBT + n * SBT + part * 2, src, nb);
     }
-    for (int e = tid; e < BK * n_d; e += kThreads) {
-      const int col = e / BK, k = e - col * BK;
-      const int i = i0 + k;
-      cp_async8(Ds + st * BK * n_d + k * n_d + col, D + (size_t)col * ldN + min(i, ldN - 1), i < N ? 8 : 0);
+    for (int e = tid; e < (BK / 2) * n_d; e += kThreads) {  // 16-byte chunks: 2 cells of a column
+      const int col = e / (BK / 2), part = e - col * (BK / 2);
+      const int i = i0 + part * 2;
+      const int nb = 8 * max(0, min(2, N - i));
+      cp_async16(Ds + (size_t)st * n_d * SD + col * SD + part * 2, D + (size_t)col * ldN + min(i, ldN - 2), nb);
     }
     if (tid < BK) {
       const int i = i0 + tid;
@@ -105,14 +107,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   };
   auto fill_a = [&](int st, int buf) {
-    const double* d = Ds + st * BK * n_d + (ph * 8) * n_d;
     const double* r = Rs + st * BK + ph * 8;
     double* dst = As + buf * BK * SA + (ph * 8) * SA + pm;
+    if (ab.x < 0) {
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      double v = 0.0;
-      if (ab.x >= 0) v = d[k * n_d + ab.x] * d[k * n_d + ab.y] * r[k];
-      dst[k * SA] = v;
+      for (int k = 0; k < 8; k++) dst[k * SA] = 0.0;
+      return;
+    }
+    const double2* da = reinterpret_cast<const double2*>(Ds + (size_t)st * n_d * SD + ab.x * SD + ph * 8);
+    const double2* db = reinterpret_cast<const double2*>(Ds + (size_t)st * n_d * SD + ab.y * SD + ph * 8);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) {
+      const double2 x = da[k2], y = db[k2];
+      dst[(2 * k2) * SA] = x.x * y.x * r[2 * k2];
+      dst[(2 * k2 + 1) * SA] = x.y * y.y * r[2 * k2 + 1];
     }
   };
 
@@ -311,7 +319,7 @@ int pair_prepare(Ctx* c) {
     return GPL_ERR_ALLOC;
   }
   GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  s.smem_gram = (int)sizeof(double) * (2 * BK * SA + 3 * BN * SBT + 3 * BK + 3 * BK * n_d);
+  s.smem_gram = (int)sizeof(double) * (2 * BK * SA + 3 * BN * SBT + 3 * BK + 3 * n_d * SD);
   s.smem_v = (int)sizeof(double) * 2 * (BK * SA + BK * SBN);
   s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
   if (s.smem_vu > 200 * 1024) {

@@ -37,6 +37,16 @@ using TileTall = DTile<1, 9, 2>;  // 144 x 128: the dense columns (n_d <= 144) i
 
 constexpr int kSplitK = 8;
 
+// Epilogues that take the whole C tile from shared memory (coalesced stores) declare kTile.
+template <class E, class = void>
+struct TileEpi {
+  static constexpr bool value = false;
+};
+template <class E>
+struct TileEpi<E, decltype((void)E::kTile)> {
+  static constexpr bool value = E::kTile;
+};
+
 }  // namespace
 
 // KR(z) -> [kbeg, kend); A(r, k, z); B(k, c, z); E(r, c, z, v). kFastK: the loader's K index
@@ -124,20 +134,37 @@ __global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr
         for (int y = 0; y < T::WN; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
     }
   }
+  if constexpr (TileEpi<Epi>::value) {
+    // the C tile through shared memory (the pipeline buffers are free after the last slice)
+    constexpr int LC = T::BN + 1;
+    __syncthreads();
 #pragma unroll
-  for (int x = 0; x < T::WM; x++)
+    for (int x = 0; x < T::WM; x++)
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int r = m0 + wm * T::WM * 16 + x * 16 + g + 8 * h;
-      if (r >= m) continue;
+      for (int h = 0; h < 2; h++)
 #pragma unroll
-      for (int y = 0; y < T::WN; y++)
+        for (int y = 0; y < T::WN; y++)
 #pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int c = n0 + wn * T::WN * 8 + y * 8 + 2 * t + e;
-          if (c < n) epi(r, c, z, acc[x][y][2 * h + e]);
-        }
-    }
+          for (int e = 0; e < 2; e++)
+            sm[(wm * T::WM * 16 + x * 16 + g + 8 * h) * LC + wn * T::WN * 8 + y * 8 + 2 * t + e] = acc[x][y][2 * h + e];
+    __syncthreads();
+    epi.tile(sm, LC, T::BM, T::BN, m0, n0, m, n, z);
+  } else {
+#pragma unroll
+    for (int x = 0; x < T::WM; x++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int r = m0 + wm * T::WM * 16 + x * 16 + g + 8 * h;
+        if (r >= m) continue;
+#pragma unroll
+        for (int y = 0; y < T::WN; y++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int c = n0 + wn * T::WN * 8 + y * 8 + 2 * t + e;
+            if (c < n) epi(r, c, z, acc[x][y][2 * h + e]);
+          }
+      }
+  }
 }
 
 // ---- operand loaders ------------------------------------------------------------------------
@@ -230,15 +257,11 @@ struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the ti
 struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell
   static constexpr bool kFastK = false;
   const double *W, *rOm;
-  const int *gcells, *gstart;
-  const int2* tiles;
+  const int* cells;  // 128 slots per tile
   int ldN;
   __device__ double operator()(int k, int c, int z) const {
-    const int2 tl = tiles[z];
-    const int g = tl.x, q = tl.y + c;
-    if (q >= gstart[g + 1] - gstart[g]) return 0.0;
-    const int i = gcells[gstart[g] + q];
-    return W[(size_t)k * ldN + i] * rOm[i];
+    const int i = cells[(size_t)z * 128 + c];
+    return i < 0 ? 0.0 : W[(size_t)k * ldN + i] * rOm[i];
   }
 };
 
@@ -264,6 +287,28 @@ struct EpEta {  // E[i + j*ldN] = v + level coefficients of cell i in B_j
     out[i + (size_t)j * ldN] = s;
   }
 };
+struct EpEtaTile {  // E[i + j*ldN] = C + level coefficients, stored along cells (coalesced)
+  static constexpr bool kTile = true;
+  double* out;
+  const double* B;
+  const int *cv_nh, *codes;
+  int ldN, P, n_cv;
+  __device__ void operator()(int, int, int, double) const {}
+  __device__ void tile(const double* Cs, int ld, int BM, int BN, int m0, int n0, int m, int n, int) const {
+    for (int r = threadIdx.x % BM; m0 + r < m && r < BM; r += BM) {
+      const int i = m0 + r;
+      int lv[4] = {0, 0, 0, 0};
+      for (int q = 0; q < n_cv && q < 4; q++) lv[q] = cv_nh[q] + codes[(size_t)q * ldN + i];
+      for (int cc = threadIdx.x / BM; cc < BN && n0 + cc < n; cc += blockDim.x / BM) {
+        const int j = n0 + cc;
+        double s = Cs[r * ld + cc];
+        for (int q = 0; q < n_cv && q < 4; q++) s += B[lv[q] + (size_t)j * P];
+        for (int q = 4; q < n_cv; q++) s += B[cv_nh[q] + codes[(size_t)q * ldN + i] + (size_t)j * P];
+        out[i + (size_t)j * ldN] = s;
+      }
+    }
+  }
+};
 struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
   double* S;
   int n_grp, ld;
@@ -271,14 +316,11 @@ struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
 };
 struct EpHK {  // HK[cell + a*ldN] with r = a, c = cell slot of tile z
   double* HK;
-  const int *gcells, *gstart;
-  const int2* tiles;
+  const int* cells;
   int ldN;
   __device__ void operator()(int a, int c, int z, double v) const {
-    const int2 tl = tiles[z];
-    const int q = tl.y + c;
-    if (q >= gstart[tl.x + 1] - gstart[tl.x]) return;
-    HK[gcells[gstart[tl.x] + q] + (size_t)a * ldN] = v;
+    const int i = cells[(size_t)z * 128 + c];
+    if (i >= 0) HK[i + (size_t)a * ldN] = v;
   }
 };
 
@@ -365,8 +407,9 @@ __global__ void k_reduce_bvec(int n_d, int J, int P, int nz, const int* __restri
 template <class T, class LA, class LB, class KR, class Epi>
 static int launch_dgen(Ctx* c, dim3 grid, int m, int n, LA A, LB B, KR kr, Epi epi, const char* name) {
   auto* fn = k_dgen<T, LA, LB, KR, Epi>;
-  GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, T::smem()));
-  fn<<<grid, 256, T::smem(), c->stream>>>(m, n, A, B, kr, epi);
+  const int smem = TileEpi<Epi>::value ? std::max(T::smem(), (int)sizeof(double) * T::BM * (T::BN + 1)) : T::smem();
+  GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  fn<<<grid, 256, smem, c->stream>>>(m, n, A, B, kr, epi);
   GPL_LAUNCHED(c, name);
   return GPL_OK;
 }
@@ -422,7 +465,7 @@ int dgen_eta(Ctx* c, const double* B, double* out) {
   using T = TileSq;
   dim3 g(div_up(c->N, T::BM), div_up(c->J, T::BN), 1);
   return launch_dgen<T>(c, g, c->N, c->J, LdD{c->Dm, c->ldN}, LdBetaDense{B, c->dcol_d, c->P}, KAll{c->n_d},
-                        EpEta{out, B, c->cv_nh_d, c->codes_d, c->ldN, c->P, c->n_cv}, "k_dgen(eta)");
+                        EpEtaTile{out, B, c->cv_nh_d, c->codes_d, c->ldN, c->P, c->n_cv}, "k_dgen(eta)");
 }
 
 int dgen_group_sums(Ctx* c, int mode) {
@@ -449,8 +492,8 @@ int dgen_hk(Ctx* c) {
   if (rc) return rc;
   dim3 g(1, 1, c->n_hk_tiles128);
   return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
-                        LdTileO{c->W, rOm, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, KAll{c->J},
-                        EpHK{c->HK, c->gcells_d, c->gstart_d, c->hk_tiles128_d, c->ldN}, "k_dgen(hk)");
+                        LdTileO{c->W, rOm, c->hk_cells_d, c->ldN}, KAll{c->J}, EpHK{c->HK, c->hk_cells_d, c->ldN},
+                        "k_dgen(hk)");
 }
 
 int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw) {
