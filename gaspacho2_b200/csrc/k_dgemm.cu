@@ -17,7 +17,7 @@
 //                 sum_j O_ij S_j[DD] d_i of getGradLogOmega (ggplvm.cu:301-376) from V.
 //
 // CTA tile 128 x 128 x 16 (K), 8 warps as 2 (M) x 4 (N), warp tile 64 x 32 (4 x 4 DMMA tiles
-// of 16 x 8), double-buffered shared memory. m16n8k4 fragments (lane = 4*g + t):
+// of 16 x 8), three-stage cp.async pipelines with one barrier per slice. m16n8k4 fragments (lane = 4*g + t):
 // A 16x4 row-major a0 = A[g][t], a1 = A[g+8][t]; B 4x8 b0 = B[t][g]; C 16x8
 // c0,c1 = C[g][2t, 2t+1], c2,c3 = C[g+8][2t, 2t+1]. Shared rows are padded so that the
 // 16 lanes of each half-warp hit 16 distinct 8-byte bank pairs.
@@ -132,6 +132,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
 
+  // One barrier per slice. At the top of iteration s: slice s + 1 has landed (its copies were
+  // issued one iteration earlier) and, after the barrier, every warp is done with iteration
+  // s - 1, so stage (s + 2) % 3 and pair-product buffer (s + 1) & 1 are free. The products of
+  // slice s + 1 are formed after this warp's MMAs of slice s are issued, overlapping them.
   load(0, 0);
   cp_async_commit();
   if (nsl > 1) load(1, 1);
@@ -140,13 +144,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   fill_a(0, 0);
   for (int s = 0; s < nsl; s++) {
+    cp_async_wait<0>();  // slice s + 1 landed
+    __syncthreads();
     if (s + 2 < nsl) load(s + 2, (s + 2) % 3);
     cp_async_commit();
-    cp_async_wait<1>();  // slice s + 1 landed
-    __syncthreads();
     warp_slice<true>(As + (s & 1) * BK * SA, Bs + (s % 3) * BN * SBT, wm, wn, g, t, acc);
     if (s + 1 < nsl) fill_a((s + 1) % 3, (s + 1) & 1);
-    __syncthreads();
   }
   cp_async_wait<0>();
 
@@ -200,8 +203,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_pair_v(int N, int ldN, int J, int c0, int c1, int pairs_pad, const double* __restrict__ W,
              const double* __restrict__ Sp, const double* __restrict__ rOm, double* __restrict__ V) {
   extern __shared__ __align__(16) double smem_d[];
-  double* As = smem_d;                // [2][BK][SA]  W rows (cells contiguous)
-  double* Bs = smem_d + 2 * BK * SA;  // [2][BK][SBN] S pairs (pairs contiguous)
+  double* As = smem_d;                // [3][BK][SA]  W rows (cells contiguous)
+  double* Bs = smem_d + 3 * BK * SA;  // [3][BK][SBN] S pairs (pairs contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
   const int i0 = c0 + blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -237,21 +240,20 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
 
+  // three stages, one barrier per slice: after the barrier of iteration s every warp is done
+  // with slice s - 1, whose stage (s + 2) % 3 is refilled while slice s is multiplied
   load(0, 0);
   cp_async_commit();
+  if (nsl > 1) load(1, 1);
+  cp_async_commit();
   for (int s = 0; s < nsl; s++) {
-    const int buf = s & 1;
-    if (s + 1 < nsl) {
-      load(s + 1, buf ^ 1);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    cp_async_wait<1>();  // slice s landed
     __syncthreads();
-    warp_slice<false>(As + buf * BK * SA, Bs + buf * BK * SBN, wm, wn, g, t, acc);
-    __syncthreads();
+    if (s + 2 < nsl) load(s + 2, (s + 2) % 3);
+    cp_async_commit();
+    warp_slice<false>(As + (s % 3) * BK * SA, Bs + (s % 3) * BK * SBN, wm, wn, g, t, acc);
   }
+  cp_async_wait<0>();
 
 #pragma unroll
   for (int mt = 0; mt < 4; mt++)
@@ -320,7 +322,7 @@ int pair_prepare(Ctx* c) {
   }
   GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
   s.smem_gram = (int)sizeof(double) * (2 * BK * SA + 3 * BN * SBT + 3 * BK + 3 * n_d * SD);
-  s.smem_v = (int)sizeof(double) * 2 * (BK * SA + BK * SBN);
+  s.smem_v = (int)sizeof(double) * 3 * (BK * SA + BK * SBN);
   s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
   if (s.smem_vu > 200 * 1024) {
     c->err = "too many dense model columns for the staged pair contraction";
