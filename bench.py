@@ -57,6 +57,12 @@ def parse():
                     help="skip the precision form's throughput beside the FP64 line")
     ap.add_argument("--precision-report", action="store_true",
                     help="instead of the benchmark: the precision form against FP64 along a fit, every 10 steps")
+    ap.add_argument("--no-de-leg", action="store_true",
+                    help="skip the DE driver's model-comparison pass beside the FP64 line")
+    ap.add_argument("--de-mredc", type=int, default=5, help="inducing points of the DE per-dimension models")
+    ap.add_argument("--fit-spread", action="store_true",
+                    help="instead of the benchmark: the --fit-config fit's end point from starts perturbed by "
+                         "1e-12 and 1e-9 (relative, X), FP64 and the precision form")
     return ap.parse_args()
 
 
@@ -243,6 +249,71 @@ def workload_config(ds, args, precision):
             "global_batch": ds.N, "seq_len": None}
 
 
+def de_leg(args, ds, stream, device):
+    """The DE driver's model comparison (ggplvm_de.cu:1067-1207) on the bench workload: one pass
+    of its table, i.e. the GLM initialisation and one IRLS sweep of each of the Q + 2 models
+    (null, the GP over each latent dimension with --de-mredc equispaced points, the full GP),
+    at the workload's starting parameters. Timed with CUDA events on the library's stream
+    around `de.de_bfs(jtr_max=1)` on contexts opened beforehand (one warm-up pass). The CPU
+    baseline runs the same pass through the oracle on 8 and 16 genes with all cells and
+    extrapolates linearly in the gene count (the kernel matrices and the single initial
+    factorisation do not grow with genes)."""
+    import torch
+
+    from gaspacho2_b200 import de
+
+    Mr = args.de_mredc
+    ctxs = de.open_contexts(ds.y, ds.z, ds.ls, ds.init.X, ds.Q, Mr, ds.M, device, stream.cuda_stream)
+    try:
+        de.de_bfs(ds.y, ds.z, ds.ls, ds.init, ds.Q, Mr, ds.M, 1, contexts=ctxs)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        out = de.de_bfs(ds.y, ds.z, ds.ls, ds.init, ds.Q, Mr, ds.M, 1, contexts=ctxs)
+        e.record(stream)
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3
+    finally:
+        for m in ctxs:
+            m.close()
+    res = {"metric": "DE model-table passes/s (GLM init + 1 IRLS sweep of each of the Q+2 models)",
+           "value": 1.0 / t, "unit": "passes/s", "seconds_per_pass": t, "models": ds.Q + 2, "Mredc": Mr,
+           "Mfull": ds.M, "dtype": "f64", "finite": bool(np.all(np.isfinite(out["BFs"])))}
+    if not args.no_cpu_baseline:
+        from gaspacho2_b200 import synth
+        from oracle import port
+
+        # the oracle's restatement (bit-exact with the reference's DE kernels on the golden
+        # cases): the reference's own null model reads level codes out of range when the last
+        # design variable is categorical, as it is here (the donor), so it cannot run this design
+        threads = os.cpu_count() or 1
+        port.set_threads(threads)
+        ts = {}
+        for g in (8, 16):
+            sub = synth.gene_subset(ds, g)
+            t0 = time.perf_counter()
+            port.de_bfs(sub, sub.init, Mr, ds.M, 1)
+            ts[g] = time.perf_counter() - t0
+        slope = (ts[16] - ts[8]) / 8.0
+        t_cpu = max(ts[16] + slope * (ds.J - 16), ts[16])
+        res["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "passes/s", "cores": threads, "kind": "port",
+                               "sample": f"8 and 16 of {ds.J} genes with all {ds.N} cells ({ts[8]:.1f} s, "
+                                         f"{ts[16]:.1f} s), linear in genes to all {ds.J}"}
+    return res
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the dominant FP64
+# kernel, from a single-pass ncu capture of this bench's own command at the full workload (the
+# metric is not available inside the timed run): k_pair_gram at config 2 read 18.16 GB and wrote
+# 1.51 GB per launch, against 9.5 GB of algorithmic operand bytes (W 8.0 GB, the dense columns
+# 0.1 GB, both triangles of the Psi dense blocks 1.4 GB): W is read about 2.2 times.
+TRAFFIC_BYTES = {("gram", 2, 100000, 10000, 128, 10): 18.16e9 + 1.51e9}
+
+
+def measured_traffic(kernel, ds, args):
+    return TRAFFIC_BYTES.get((kernel, args.config, ds.N, ds.J, ds.M, ds.Q))
+
+
 def precision_leg(args, ds, stream, device):
     """The precision form (tensor-core Gram and gradient contraction over whitened columns,
     FP64 elsewhere, refined solves) on the same workload and state as the FP64 line: its
@@ -427,7 +498,7 @@ def run_ours(args):
             avg_s = prof[dom][0] / prof[dom][1] / 1e3
             achieved = ft[dom] / avg_s / 1e12
             roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": f64, "unit": "TFLOP/s",
-                    "frac": achieved / f64, "traffic": None,
+                    "frac": achieved / f64, "traffic": measured_traffic(dom, ds, args),
                     "peak_source": "measured in this run: torch.matmul float64 8192^3 best of 5 "
                                    "(MEASURED_PEAKS.json has no FP64 entry)",
                     "flops_per_launch": ft[dom], "avg_launch_ms": avg_s * 1e3,
@@ -447,6 +518,8 @@ def run_ours(args):
     m.close()
     if rank == 0 and args.precision == "fp64" and not args.no_precision_leg:
         line["precision_form"] = precision_leg(args, ds, stream, local)
+    if rank == 0 and args.precision == "fp64" and not args.no_de_leg:
+        line["de_model_comparison"] = de_leg(args, ds, stream, local)
     if rank == 0 and not args.no_fit:
         line["time_to_fit"] = time_to_fit(args, stream, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -457,6 +530,37 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     rep.close()
+    return 0
+
+
+def fit_spread(args):
+    """How far the fit's own discrete decisions carry rounding: the --fit-config fit to
+    --fit-lbfgs steps from the seeded start and from starts whose X is scaled by (1 + eps z),
+    z standard normal, in FP64 and in the precision form. One JSON line per fit."""
+    import dataclasses
+
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ds = synth.make(args.fit_config, 0, init=True)
+    for prec, eps, seed in (("fp64", 0.0, 0), ("fp64", 1e-12, 1), ("fp64", 1e-12, 2), ("fp64", 1e-9, 3),
+                            ("bf16x3", 0.0, 0), ("bf16x3", 1e-12, 1)):
+        init = ds.init
+        if eps:
+            z = np.random.default_rng(seed).standard_normal(init.X.shape)
+            init = dataclasses.replace(init, X=init.X * (1.0 + eps * z))
+        with GPLVM.from_dataset(ds, stream=stream.cuda_stream, precision=prec) as m:
+            m.set_params(init)
+            m.kernel_mats()
+            m.glm_init()
+            rc, st, tr = m.fit(100000, args.fit_lbfgs)
+        print(json.dumps({"config": args.fit_config, "lbfgs_budget": args.fit_lbfgs, "precision": prec, "eps": eps,
+                          "seed": seed, "final_objective": float(tr[-1]), "outer_iterations": st["outer"],
+                          "objective_evaluations": st["evals"], "nan_exit": bool(rc)}), flush=True)
     return 0
 
 
@@ -514,6 +618,8 @@ def main():
     args = parse()
     if args.precision_report:
         return precision_report(args)
+    if args.fit_spread:
+        return fit_spread(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -13,12 +13,14 @@ ERRORS = {-1: "GPL_ERR_ARG", -2: "GPL_ERR_CUDA", -3: "GPL_ERR_ALLOC", -4: "GPL_E
           -6: "GPL_ERR_FORMAT", -7: "GPL_ERR_IO",
           -8: "GPL_ERR_LIMIT"}
 PREC = {"fp64": 0, "bf16x3": 1}
+DE_NULL, DE_FULL = -2, -1  # gpl_de_model's model codes besides a latent dimension
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
 _vp = ctypes.c_void_p
 
-# name -> (restype, argtypes); every entry point returns int except gpl_last_error
+# name -> (restype, argtypes); every entry point returns int except gpl_last_error and
+# gpl_ta_equispaced
 SIGNATURES = {
     "gpl_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _vp]),
     "gpl_destroy": (ctypes.c_int, [_vp]),
@@ -49,6 +51,9 @@ SIGNATURES = {
     "gpl_fit": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]),
     "gpl_fit_outer": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]),
     "gpl_score_stats": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
+    "gpl_de_model": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gpl_de_irls": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _dp, _ip, _dp, ctypes.c_int]),
+    "gpl_ta_equispaced": (None, [ctypes.c_int, ctypes.c_int, _dp]),
     "gpl_evaluate": (ctypes.c_int, [_vp, _dp, ctypes.c_int64, _dp, _dp]),
     "gpl_evaluate_device": (ctypes.c_int, [_vp]),
     "gpl_get": (ctypes.c_int, [_vp, ctypes.c_char_p, _dp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),

@@ -67,14 +67,16 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    cli_src = os.path.join(CSRC, "cli_ggplvm.cpp")
-    if os.path.exists(cli_src) and _newer(CLI, [cli_src, LIB] + headers):
-        os.makedirs(os.path.dirname(CLI), exist_ok=True)
-        cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), cli_src, "-o", CLI,
-               "-L", PKG, "-lgpl_b200", "-Wl,-rpath,$ORIGIN/..", "-lz"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
+    # the command-line drop-ins: csrc/cli_<name>.cpp -> bin/<name> (host C++ over the C ABI)
+    for cli_src in sorted(glob.glob(os.path.join(CSRC, "cli_*.cpp"))):
+        exe = os.path.join(PKG, "bin", os.path.basename(cli_src)[4:-4])
+        if _newer(exe, [cli_src, LIB] + headers):
+            os.makedirs(os.path.dirname(exe), exist_ok=True)
+            cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC, cli_src,
+                   "-o", exe, "-L", PKG, "-lgpl_b200", "-Wl,-rpath,$ORIGIN/..", "-lz"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

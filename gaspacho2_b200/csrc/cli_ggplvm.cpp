@@ -45,9 +45,12 @@
 #include <string>
 #include <vector>
 
+#include "cli_io.h"
 #include "gpl.h"
 
 namespace {
+
+using namespace cli;
 
 struct Options {
   std::string y, z, ls, xi, init_params, out_dir = ".", precision = "fp64", phi_gz = "omega", genotypes;
@@ -146,91 +149,6 @@ int parse(int argc, char** argv, Options* o) {
   return 0;
 }
 
-// Whole-file reader with exact-size checks (the reference's freads are unchecked).
-struct Reader {
-  FILE* f = nullptr;
-  std::string path;
-  bool ok = true;
-  explicit Reader(const std::string& p) : path(p) {
-    f = fopen(p.c_str(), "rb");
-    if (!f) {
-      fprintf(stderr, "ggplvm: cannot open %s\n", p.c_str());
-      ok = false;
-    }
-  }
-  ~Reader() {
-    if (f) fclose(f);
-  }
-  bool read(void* dst, size_t size, size_t n) {
-    if (!ok) return false;
-    if (n && fread(dst, size, n, f) != n) {
-      fprintf(stderr, "ggplvm: %s is truncated\n", path.c_str());
-      ok = false;
-    }
-    return ok;
-  }
-};
-
-struct Counts {
-  int N = 0, J = 0, L = 0;
-  std::vector<int32_t> i, p;
-  std::vector<double> x;
-};
-
-bool load_counts(const std::string& path, Counts* y) {
-  Reader r(path);
-  int32_t hdr[3];
-  if (!r.read(hdr, sizeof(int32_t), 3)) return false;
-  y->N = hdr[0];
-  y->J = hdr[1];
-  y->L = hdr[2];
-  if (y->N <= 0 || y->J <= 0 || y->L < 0) {
-    fprintf(stderr, "ggplvm: %s: bad header N=%d J=%d L=%d\n", path.c_str(), y->N, y->J, y->L);
-    return false;
-  }
-  y->i.resize(y->L);
-  y->p.resize((size_t)y->J + 1);
-  y->x.resize(y->L);
-  return r.read(y->i.data(), sizeof(int32_t), y->L) && r.read(y->p.data(), sizeof(int32_t), (size_t)y->J + 1) &&
-         r.read(y->x.data(), sizeof(double), y->L);
-}
-
-struct Design {
-  int N = 0, n_var = 0;
-  std::vector<int32_t> c, v;
-  std::vector<unsigned char> body;
-};
-
-bool load_design(const std::string& path, Design* z) {
-  Reader r(path);
-  int32_t hdr[2];
-  if (!r.read(hdr, sizeof(int32_t), 2)) return false;
-  z->N = hdr[0];
-  z->n_var = hdr[1];
-  if (z->N <= 0 || z->n_var < 0) {
-    fprintf(stderr, "ggplvm: %s: bad header N=%d p=%d\n", path.c_str(), z->N, z->n_var);
-    return false;
-  }
-  z->c.resize(z->n_var);
-  z->v.resize(z->n_var);
-  if (!r.read(z->c.data(), sizeof(int32_t), z->n_var) || !r.read(z->v.data(), sizeof(int32_t), z->n_var)) return false;
-  size_t bytes = 0;
-  for (int k = 0; k < z->n_var; k++) {
-    if (z->c[k] < 1 || z->v[k] < 1) {
-      fprintf(stderr, "ggplvm: %s: variable %d has c=%d v=%d\n", path.c_str(), k, z->c[k], z->v[k]);
-      return false;
-    }
-    bytes += (size_t)z->N * z->v[k] * (z->c[k] == 1 ? sizeof(double) : sizeof(int32_t));
-  }
-  z->body.resize(bytes);
-  return r.read(z->body.data(), 1, bytes);
-}
-
-bool load_doubles(const std::string& path, double* dst, size_t n) {
-  Reader r(path);
-  return r.read(dst, sizeof(double), n);
-}
-
 // Seeded standard normals for T's dimensions 1..Q-1 (splitmix64 + Box-Muller). The
 // reference draws them from GSL's MT19937 (util.c:73-87), which is not reproduced: pass T
 // through --init-params for runs that must match the reference.
@@ -247,30 +165,6 @@ struct Normal {
   double operator()() {
     const double u1 = uniform(), u2 = uniform();
     return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
-  }
-};
-
-std::string join(const std::string& dir, const char* name) { return dir.empty() ? name : dir + "/" + name; }
-
-bool write_file(const std::string& path, const std::vector<std::pair<const void*, size_t>>& parts) {
-  FILE* f = fopen(path.c_str(), "wb");
-  if (!f) {
-    fprintf(stderr, "ggplvm: cannot write %s\n", path.c_str());
-    return false;
-  }
-  bool ok = true;
-  for (auto& pr : parts) ok = ok && (pr.second == 0 || fwrite(pr.first, 1, pr.second, f) == pr.second);
-  ok = (fclose(f) == 0) && ok;
-  if (!ok) fprintf(stderr, "ggplvm: short write to %s\n", path.c_str());
-  return ok;
-}
-
-struct Params {
-  std::vector<double> Omega, delta, X, T, rho, phi;
-  Params(int N, int J, int M, int p, int Q) : Omega(N), delta(p), X((size_t)N * Q), T((size_t)M * Q), rho(Q), phi(J) {}
-  std::vector<std::pair<const void*, size_t>> blocks() const {
-    return {{Omega.data(), Omega.size() * 8}, {delta.data(), delta.size() * 8}, {X.data(), X.size() * 8},
-            {T.data(), T.size() * 8},         {rho.data(), rho.size() * 8},     {phi.data(), phi.size() * 8}};
   }
 };
 

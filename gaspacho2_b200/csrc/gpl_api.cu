@@ -101,7 +101,7 @@ static void free_state(Ctx* c) {
                   c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
                   c->grad0,  c->ss,     c->SS,      c->XX,      c->gdtmp,  c->C1,     c->C2,     c->grtmp,
                   c->KmmInv, c->bvec,   c->sol,     c->red,     c->lb_work, c->mc_d,  c->mv_d,   c->mk_d,
-                  c->nh_d,   c->rres,   c->bx,      c->rphi};
+                  c->nh_d,   c->rres,   c->bx,      c->rphi,    c->e0,      c->zeta};
   for (void* p : bufs)
     if (p) cudaFree(p);
   c->Z = c->W = c->Nu = c->Psi = c->PsiInv = c->Beta = c->tBeta = c->scratch = c->U = nullptr;
@@ -109,7 +109,7 @@ static void free_state(Ctx* c) {
   c->rho = c->phi = c->ls = c->lkhds = c->lkhd_dev = c->grad = c->grad0 = c->ss = c->SS = c->XX = nullptr;
   c->gdtmp = c->C1 = c->C2 = c->grtmp = c->KmmInv = c->bvec = c->sol = c->red = c->lb_work = nullptr;
   c->mc_d = c->mv_d = c->mk_d = c->nh_d = nullptr;
-  c->rres = c->bx = c->rphi = nullptr;
+  c->rres = c->bx = c->rphi = c->e0 = c->zeta = nullptr;
   c->have_design = false;
 }
 
@@ -266,6 +266,65 @@ static int glm_init(Ctx* c) {
   GPL_RUN(launch_init_response(c));
   GPL_RUN(launch_zt_u(c, 1));
   GPL_RUN(launch_init_beta_solve(c));
+  return GPL_OK;
+}
+
+// One model of the DE driver (ggplvm_de.cu:1071-1104 for the null model, 1135-1177 for the
+// others): GLM initialisation, zeta, then IRLS sweeps in the DE forms with its stopping rule.
+// The summed likelihood is read back after every sweep, as the reference does.
+static int de_irls(Ctx* c, int jtr_max, double tol, int* n_sweeps, double* trace, int trace_cap) {
+  GPL_RUN(glm_init(c));
+  GPL_RUN(launch_de_zeta(c));
+  const int64_t PP = (int64_t)c->P * c->P;
+  double prev = 0.0;
+  int jtr;
+  for (jtr = 0; jtr < jtr_max; jtr++) {
+    GPL_RUN(launch_w_nu(c));
+    GPL_RUN(launch_gram(c, false));
+    GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, PP));
+    GPL_RUN(launch_zt_u(c, 0));
+    GPL_RUN(launch_de_beta_phi(c));
+    GPL_RUN(launch_de_zeta(c));
+    GPL_RUN(launch_de_lkhd(c, 0));
+    double cur = 0.0;
+    GPL_RUN(read_slot(c, 0, &cur));
+    if (trace && jtr < trace_cap) trace[jtr] = cur;
+    if (jtr > 0) {
+      if (isinf(cur) || isnan(cur) || jtr == jtr_max - 1 || fabs(prev - cur) / fabs(cur) < tol) {
+        jtr++;
+        break;
+      }
+    }
+    prev = cur;
+  }
+  *n_sweeps = jtr;
+  return GPL_OK;
+}
+
+// The reference's loader leaves 199.0 in the first cell of the last design variable of a
+// design without GP (DataFrame.cu:112-113, 131): the null model sees it, the GP models do not.
+static int de_loader_value(Ctx* c, bool on) {
+  if (on && c->de_quirk_col < 0) {
+    const int v = c->p - 2;  // last design variable (the intercept when there is none)
+    if (c->vc[v] != 1) return GPL_OK;  // categorical: the reference reads out of range
+    const int col = c->nh[v];
+    int d = -1;
+    for (int a = 0; a < c->n_d; a++)
+      if (c->dcol[a] == col) d = a;
+    if (d < 0) return GPL_OK;
+    double* cell0 = c->Dm + (size_t)d * c->ldN;
+    GPL_TRY(c, cudaMemcpyAsync(&c->de_quirk_orig, cell0, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GPL_TRY(c, cudaStreamSynchronize(c->stream));
+    const double v199 = 199.0;
+    GPL_TRY(c, cudaMemcpyAsync(cell0, &v199, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GPL_TRY(c, cudaStreamSynchronize(c->stream));
+    c->de_quirk_col = d;
+  } else if (!on && c->de_quirk_col >= 0) {
+    double* cell0 = c->Dm + (size_t)c->de_quirk_col * c->ldN;
+    GPL_TRY(c, cudaMemcpyAsync(cell0, &c->de_quirk_orig, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GPL_TRY(c, cudaStreamSynchronize(c->stream));
+    c->de_quirk_col = -1;
+  }
   return GPL_OK;
 }
 
@@ -552,6 +611,8 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->rres, (size_t)P * J, "refinement residual"));
   GPL_RUN(dalloc(c, &c->bx, (size_t)P * J, "refinement product"));
   GPL_RUN(dalloc(c, &c->rphi, (size_t)J, "1/phi"));
+  GPL_RUN(dalloc(c, &c->e0, ldN, "z.zeta"));
+  GPL_RUN(dalloc(c, &c->zeta, (size_t)P, "zeta"));
   GPL_RUN(dalloc(c, &c->scratch, scratch_n, "scratch"));
   GPL_RUN(dalloc(c, &c->U, ldN * n_d, "U"));
   GPL_RUN(dalloc(c, &c->Kmm, (size_t)M * M, "Kmm"));
@@ -888,6 +949,50 @@ int gpl_score_stats(gpl_ctx* h, int L, const double* G, double* S) {
   cudaFree(dW);
   cudaFree(dS);
   return rc;
+}
+
+int gpl_de_model(gpl_ctx* h, int model) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (model < GPL_DE_NULL || model >= c->Q) {
+    c->err = "model must be GPL_DE_NULL, GPL_DE_FULL or a latent dimension in [0, Q)";
+    return GPL_ERR_ARG;
+  }
+  GPL_RUN(de_loader_value(c, model == GPL_DE_NULL));
+  c->de = true;
+  c->kernel_lv = model == GPL_DE_NULL ? kLvNone : (model == GPL_DE_FULL ? kLvAll : model);
+  GPL_RUN(launch_kernel_mats(c));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  return GPL_OK;
+}
+
+int gpl_de_irls(gpl_ctx* h, int jtr_max, double tol, double* lkhds, int32_t* sweeps, double* trace, int trace_cap) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (!c->de) {
+    c->err = "select a model with gpl_de_model first";
+    return GPL_ERR_STATE;
+  }
+  if (jtr_max < 1 || !(tol >= 0.0) || (trace && trace_cap < 0)) {
+    c->err = "jtr_max must be >= 1 and tol >= 0";
+    return GPL_ERR_ARG;
+  }
+  const int prec = c->precision;
+  c->precision = GPL_PREC_FP64;
+  int n = 0;
+  const int rc = de_irls(c, jtr_max, tol, &n, trace, trace ? trace_cap : 0);
+  c->precision = prec;
+  if (rc) return rc;
+  if (lkhds) GPL_TRY(c, cudaMemcpy(lkhds, c->lkhds, sizeof(double) * c->J, cudaMemcpyDeviceToHost));
+  if (sweeps) *sweeps = n;
+  return GPL_OK;
+}
+
+void gpl_ta_equispaced(int M, int Q, double* T) {
+  if (!T || M <= 0 || Q <= 0) return;
+  for (int i = 0; i < M; i++) T[i] = ((double)(i + 1) / (double)(M + 1)) * 2.0 * 3.14159265358979;
+  for (int k = 1; k < Q; k++)
+    for (int i = 0; i < M; i++) T[i + (size_t)k * M] = ((double)(i + 1) / (double)(M + 1) - 0.5) * 6.0;
 }
 
 int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkhd, double* grad) {

@@ -76,6 +76,9 @@ struct TcState {
   CUtensorMap map_whi, map_wlo, map_ahi, map_alo, map_shi, map_slo, map_ohi, map_olo;
 };
 
+constexpr int kLvAll = -1;   // kernel over every latent dimension
+constexpr int kLvNone = -2;  // no GP (inert GP block): the DE driver's null model
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -85,7 +88,14 @@ struct Ctx {
   int refine_steps = 1;              // precision form: FP64-residual refinement steps per solve
   const double* zt_u_src = nullptr;  // u of Z^T diag(W/Omega) u when not nu (set during a refinement)
   double *rres = nullptr, *bx = nullptr;  // refinement residual and product, P x J
-  double* rphi = nullptr;                 // 1/phi, refreshed before each gradient    // precision form: the gradient contraction on tcgen05 too (else FP64 DMMA)
+  double* rphi = nullptr;                 // 1/phi, refreshed before each gradient
+  // the differential-expression driver's model comparison (ggplvm_de.cu)
+  int kernel_lv = kLvAll;  // GP over all latent dimensions, one dimension (>= 0), or none (kLvNone)
+  bool de = false;         // IRLS in the DE driver's forms (W/nu, beta/phi, zeta, per-gene likelihood)
+  double* e0 = nullptr;    // z_i . zeta per cell (DE working response)
+  double* zeta = nullptr;  // the DE driver's zeta (P)
+  int de_quirk_col = -1;   // dense column whose first cell holds the null model's loader value
+  double de_quirk_orig = 0.0;
   bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
   std::string err;
 
@@ -180,6 +190,7 @@ inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 // ---- launchers (one per kernel family; each returns GPL_OK or an error code) ----------
 // k_kmats.cu
 int launch_kernel_mats(Ctx* c);          // Knm into Z, Kmm, Kinv copy, chol(Kinv), KinvKmn, titsias
+int launch_kernel_mats_lv(Ctx* c, int lv);  // the same over latent dimension lv alone, all (kLvAll), none (kLvNone)
 int launch_expand_delta(Ctx* c);         // DeltaInv (upper + diag)
 int launch_chol_single(Ctx* c, double* A, int n);  // choldc on one n x n matrix
 // k_groups.cu
@@ -198,6 +209,7 @@ int solve_refined(Ctx* c, const double* b, double* x, bool dinv_factored = false
                                                         // refinement in the precision form
 int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
 int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
+int launch_eta_one(Ctx* c, const double* b, double* out);  // out[N] = Z * b for one coefficient vector
 int launch_c1_tn(Ctx* c);                // C1 partial from tn/phi and tBeta GP block
 // k_gram.cu
 int launch_gram(Ctx* c, bool unweighted);  // Psi (full symmetric) = Z^T diag(W/Omega) Z + DeltaInv
@@ -220,7 +232,6 @@ int pair_prepare(Ctx* c);                 // column-pair list, 1/Omega, gathered
 int recip_omega(Ctx* c, const double** rOm);  // 1/Omega (0 past N), refreshed on every call
 int dgen_zt_u(Ctx* c, int mode, const double* u, double* out);          // DMMA forms of the cell x gene GEMMs (k_dgen.cu);
 int dgen_c1_tn(Ctx* c);                   // GPL_ERR_ARG when the dense columns exceed one tile
-int dgen_eta(Ctx* c, const double* B, double* out);
 int dgen_group_sums(Ctx* c, int mode);
 int dgen_hk(Ctx* c);
 int dgen_weighted_colsums(Ctx* c, const double* G2, int n2, double* out);  // out[j + c*J] = sum_i W_ij G2[c][i]
@@ -239,6 +250,10 @@ int launch_lkhd_pois(Ctx* c);
 int launch_lkhd_genes(Ctx* c);
 int launch_collect_lkhd(Ctx* c, int n_cells, int slot);
 int launch_init_beta_solve(Ctx* c);
+// k_de.cu (the DE driver's IRLS forms)
+int launch_de_zeta(Ctx* c);               // zeta from Beta and phi (getZeta), then e0 = Z zeta
+int launch_de_beta_phi(Ctx* c);           // beta = Psi^{-1} b + zeta, phi with the DE clamps
+int launch_de_lkhd(Ctx* c, int slot);     // per-gene DE log-likelihood, their sum into lkhd slot
 // k_grad.cu
 int launch_grad_delta(Ctx* c);
 int launch_grad_omega(Ctx* c);

@@ -7,7 +7,6 @@
 //             u = W nu / Omega; initBeta init.cu:193-221 with u = y0), split over the cells
 //             into 8 ranges whose partial sums are added in order.  2*N*J*n_d flops.
 //   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
-//   eta       E[i, j] = d_i . B_j[dcol] + the cell's level coefficients.  2*N*J*n_d flops.
 //   group     S[j][g][a] = sum_{i in g} w_ij D_ia over the gathered cells of each group.
 //   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for the cells of each group.
 //
@@ -36,16 +35,6 @@ using TileSq = DTile<2, 4, 4>;    // 128 x 128
 using TileTall = DTile<1, 9, 2>;  // 144 x 128: the dense columns (n_d <= 144) in one tile
 
 constexpr int kSplitK = 8;
-
-// Epilogues that take the whole C tile from shared memory (coalesced stores) declare kTile.
-template <class E, class = void>
-struct TileEpi {
-  static constexpr bool value = false;
-};
-template <class E>
-struct TileEpi<E, decltype((void)E::kTile)> {
-  static constexpr bool value = E::kTile;
-};
 
 }  // namespace
 
@@ -134,37 +123,20 @@ __global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr
         for (int y = 0; y < T::WN; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
     }
   }
-  if constexpr (TileEpi<Epi>::value) {
-    // the C tile through shared memory (the pipeline buffers are free after the last slice)
-    constexpr int LC = T::BN + 1;
-    __syncthreads();
 #pragma unroll
-    for (int x = 0; x < T::WM; x++)
+  for (int x = 0; x < T::WM; x++)
 #pragma unroll
-      for (int h = 0; h < 2; h++)
+    for (int h = 0; h < 2; h++) {
+      const int r = m0 + wm * T::WM * 16 + x * 16 + g + 8 * h;
+      if (r >= m) continue;
 #pragma unroll
-        for (int y = 0; y < T::WN; y++)
+      for (int y = 0; y < T::WN; y++)
 #pragma unroll
-          for (int e = 0; e < 2; e++)
-            sm[(wm * T::WM * 16 + x * 16 + g + 8 * h) * LC + wn * T::WN * 8 + y * 8 + 2 * t + e] = acc[x][y][2 * h + e];
-    __syncthreads();
-    epi.tile(sm, LC, T::BM, T::BN, m0, n0, m, n, z);
-  } else {
-#pragma unroll
-    for (int x = 0; x < T::WM; x++)
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int r = m0 + wm * T::WM * 16 + x * 16 + g + 8 * h;
-        if (r >= m) continue;
-#pragma unroll
-        for (int y = 0; y < T::WN; y++)
-#pragma unroll
-          for (int e = 0; e < 2; e++) {
-            const int c = n0 + wn * T::WN * 8 + y * 8 + 2 * t + e;
-            if (c < n) epi(r, c, z, acc[x][y][2 * h + e]);
-          }
-      }
-  }
+        for (int e = 0; e < 2; e++) {
+          const int c = n0 + wn * T::WN * 8 + y * 8 + 2 * t + e;
+          if (c < n) epi(r, c, z, acc[x][y][2 * h + e]);
+        }
+    }
 }
 
 // ---- operand loaders ------------------------------------------------------------------------
@@ -188,12 +160,6 @@ struct LdDt {  // A(r = dense column, k = cell) = D[r*ldN + k]
   const double* D;
   int ldN;
   __device__ double operator()(int r, int k, int) const { return D[(size_t)r * ldN + k]; }
-};
-struct LdD {  // A(r = cell, k = dense column) = D[k*ldN + r]
-  static constexpr bool kFastK = false;
-  const double* D;
-  int ldN;
-  __device__ double operator()(int r, int k, int) const { return D[(size_t)k * ldN + r]; }
 };
 struct LdU {  // B(k = cell, c = gene): mode 0 W u / Omega, 1 u (y0), 2 W g / Omega with g per cell
   static constexpr bool kFastK = true;
@@ -219,13 +185,6 @@ struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
   const double* tB;
   int P, g0;
   __device__ double operator()(int k, int c, int) const { return tB[g0 + c + (size_t)k * P]; }
-};
-struct LdBetaDense {  // B(k = dense column, c = gene) = B[dcol[k] + c*P]
-  static constexpr bool kFastK = true;
-  const double* B;
-  const int* dcol;
-  int P;
-  __device__ double operator()(int k, int c, int) const { return B[dcol[k] + (size_t)c * P]; }
 };
 struct LdGroupD {  // A(r = dense column, k = k-th cell of group z) = D[r*ldN + cell]
   static constexpr bool kFastK = true;
@@ -275,39 +234,6 @@ struct EpColMajor {  // out[r + c*ld]
   double* out;
   int64_t ld;
   __device__ void operator()(int r, int c, int, double v) const { out[r + (size_t)c * ld] = v; }
-};
-struct EpEta {  // E[i + j*ldN] = v + level coefficients of cell i in B_j
-  double* out;
-  const double* B;
-  const int *cv_nh, *codes;
-  int ldN, P, n_cv;
-  __device__ void operator()(int i, int j, int, double v) const {
-    double s = v;
-    for (int q = 0; q < n_cv; q++) s += B[cv_nh[q] + codes[(size_t)q * ldN + i] + (size_t)j * P];
-    out[i + (size_t)j * ldN] = s;
-  }
-};
-struct EpEtaTile {  // E[i + j*ldN] = C + level coefficients, stored along cells (coalesced)
-  static constexpr bool kTile = true;
-  double* out;
-  const double* B;
-  const int *cv_nh, *codes;
-  int ldN, P, n_cv;
-  __device__ void operator()(int, int, int, double) const {}
-  __device__ void tile(const double* Cs, int ld, int BM, int BN, int m0, int n0, int m, int n, int) const {
-    for (int r = threadIdx.x % BM; m0 + r < m && r < BM; r += BM) {
-      const int i = m0 + r;
-      int lv[4] = {0, 0, 0, 0};
-      for (int q = 0; q < n_cv && q < 4; q++) lv[q] = cv_nh[q] + codes[(size_t)q * ldN + i];
-      for (int cc = threadIdx.x / BM; cc < BN && n0 + cc < n; cc += blockDim.x / BM) {
-        const int j = n0 + cc;
-        double s = Cs[r * ld + cc];
-        for (int q = 0; q < n_cv && q < 4; q++) s += B[lv[q] + (size_t)j * P];
-        for (int q = 4; q < n_cv; q++) s += B[cv_nh[q] + codes[(size_t)q * ldN + i] + (size_t)j * P];
-        out[i + (size_t)j * ldN] = s;
-      }
-    }
-  }
 };
 struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
   double* S;
@@ -407,7 +333,7 @@ __global__ void k_reduce_bvec(int n_d, int J, int P, int nz, const int* __restri
 template <class T, class LA, class LB, class KR, class Epi>
 static int launch_dgen(Ctx* c, dim3 grid, int m, int n, LA A, LB B, KR kr, Epi epi, const char* name) {
   auto* fn = k_dgen<T, LA, LB, KR, Epi>;
-  const int smem = TileEpi<Epi>::value ? std::max(T::smem(), (int)sizeof(double) * T::BM * (T::BN + 1)) : T::smem();
+  const int smem = T::smem();
   GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   fn<<<grid, 256, smem, c->stream>>>(m, n, A, B, kr, epi);
   GPL_LAUNCHED(c, name);
@@ -459,13 +385,6 @@ int dgen_c1_tn(Ctx* c) {
   return launch_dgen<T>(c, g, c->N, c->M, LdTn{c->W, c->Nu, c->scratch, rOm, c->rphi, c->ldN},
                         LdTBetaGP{c->tBeta, c->P, g0}, KAll{c->J}, EpColMajor{c->C1, (int64_t)c->ldN},
                         "k_dgen(c1_tn)");
-}
-
-int dgen_eta(Ctx* c, const double* B, double* out) {
-  using T = TileSq;
-  dim3 g(div_up(c->N, T::BM), div_up(c->J, T::BN), 1);
-  return launch_dgen<T>(c, g, c->N, c->J, LdD{c->Dm, c->ldN}, LdBetaDense{B, c->dcol_d, c->P}, KAll{c->n_d},
-                        EpEtaTile{out, B, c->cv_nh_d, c->codes_d, c->ldN, c->P, c->n_cv}, "k_dgen(eta)");
 }
 
 int dgen_group_sums(Ctx* c, int mode) {

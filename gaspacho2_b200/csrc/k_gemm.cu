@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
                                               const double* __restrict__ delta, const double* __restrict__ titsias,
                                               const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
                                               const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
-                                              double* __restrict__ W, double* __restrict__ Nu) {
+                                              int de, const double* __restrict__ e0, double* __restrict__ W,
+                                              double* __restrict__ Nu) {
   // the GEMM tiles and the count tile are live at different times: overlay them
   __shared__ __align__(16) unsigned char raw[TN * (TM + 1) * sizeof(double) + TN * TM];
   double(*As)[TM + 1] = reinterpret_cast<double(*)[TM + 1]>(raw);
@@ -171,8 +172,10 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
   for (int x = 0; x < 4; x++) {
     const int r = tx + 16 * x, i = m0 + r;
     if (i >= N) continue;
-    const double lsi = ls[i], tt = dgp * titsias[i] * kWt;
-    const double lls = log(lsi);
+    // the DE driver takes the Titsias factor at weight 1 and nu = z.(beta - zeta) + (y - W)/W
+    // (ggplvm_de.cu:442-486); the fit driver weights it by wt and has zeta = 0
+    const double lsi = ls[i], tt = de ? dgp * titsias[i] : dgp * titsias[i] * kWt;
+    const double lls = log(lsi), ez = de ? e0[i] : 0.0;
 #pragma unroll
     for (int y = 0; y < 4; y++) {
       const int cc = ty + 16 * y, j = n0 + cc;
@@ -181,7 +184,8 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int 
       const double logW = eta + lls + tt;
       const double w = exp(eta) * lsi * exp(tt);
       double nu;
-      if (yf[cc][r]) nu = eta + exp(log(ys[cc][r]) - logW) - 1.0;
+      if (de) nu = yf[cc][r] ? (eta - ez) + (ys[cc][r] - w) / w : (eta - ez) - 1.0;
+      else if (yf[cc][r]) nu = eta + exp(log(ys[cc][r]) - logW) - 1.0;
       else nu = eta - 1.0;
       W[(size_t)j * ldN + i] = w;
       Nu[(size_t)j * ldN + i] = nu;
@@ -194,7 +198,7 @@ int launch_w_nu(Ctx* c) {
   dim3 g(div_up(c->N, TM), div_up(c->J, TN));
   k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->p, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
                                    c->codes_d, c->Beta, c->ls, c->delta, c->titsias, c->cell, c->gptr, c->gvalid,
-                                   c->cnt, c->W, c->Nu);
+                                   c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
   return GPL_OK;
 }
@@ -227,6 +231,14 @@ int launch_zbeta(Ctx* c, const double* B, double* out) {
   dim3 g(div_up(c->N, TM), div_up(c->J, TN));
   k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
                                   c->codes_d, B, out);
+  GPL_LAUNCHED(c, "k_eta");
+  return GPL_OK;
+}
+
+int launch_eta_one(Ctx* c, const double* b, double* out) {
+  dim3 g(div_up(c->N, TM), 1);
+  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, 1, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d, c->codes_d,
+                                  b, out);
   GPL_LAUNCHED(c, "k_eta");
   return GPL_OK;
 }

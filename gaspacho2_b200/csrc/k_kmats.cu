@@ -1,7 +1,8 @@
 // Kernel matrices of the sparse GP (replaces kernel_funcs.cu:61-162 and util_cuda.cu:249-269).
 //
 //   k_knm        Knm[i, m] = exp(-(sin^2((x_i0 - t_m0)/2)/rho_0 + sum_q>=1 (x_iq - t_mq)^2/(2 rho_q)))
-//                written into the model matrix's GP block (column-major, cell fastest).
+//                written into the model matrix's GP block (column-major, cell fastest); with
+//                lv >= 0 only latent dimension lv enters (the DE driver's per-dimension models).
 //                Bound: N*M*Q transcendental work, ~2% of one objective evaluation.
 //   k_kmm        Kmm (upper, unit diagonal, zero lower) and its copy Kinv.
 //   k_kinvkmn    per cell: x = Kmm^{-1} k_n by two triangular solves against the factor in
@@ -10,45 +11,66 @@
 //                address (broadcast), the solution lives in a cell-fastest scratch so the
 //                per-step loads coalesce.
 //   k_expand     DeltaInv = blockdiag(1/delta_k I, Kmm/delta_GP), upper + diagonal.
+#include <algorithm>
+
 #include "gpl_internal.cuh"
 
 namespace gpl {
 
-__global__ void k_knm(int N, int ldN, int M, int Q, const double* __restrict__ X, const double* __restrict__ T,
-                      const double* __restrict__ rho, double* __restrict__ Knm) {
+// Squared-distance sum of one point pair: all latent dimensions (periodic dim 0, ARD dims
+// >= 1; getKernelMatsWithPer) when lv < 0, dimension lv alone otherwise
+// (getKernelMatsWithPerSpecificLV, kernel_funcs.cu:101-135), in the reference's order.
+__device__ __forceinline__ double kern_sum(const double* __restrict__ A, size_t lda, int a,
+                                           const double* __restrict__ B, int ldb, int b,
+                                           const double* __restrict__ rho, int Q, int lv) {
+  double sum = 0.0, t;
+  if (lv <= 0) {
+    t = sin((A[a] - B[b]) / 2.0);
+    sum += t * t / rho[0];
+  }
+  const int k0 = lv < 0 ? 1 : lv, k1 = lv < 0 ? Q : (lv == 0 ? 0 : lv + 1);
+  for (int k = k0; k < k1; k++) {
+    t = A[a + k * lda] - B[b + k * ldb];
+    sum += t * t / 2.0 / rho[k];
+  }
+  return sum;
+}
+
+__global__ void k_knm(int N, int ldN, int M, int Q, int lv, const double* __restrict__ X,
+                      const double* __restrict__ T, const double* __restrict__ rho, double* __restrict__ Knm) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= N) return;
-  double sum = 0.0, t = sin((X[i] - T[j]) / 2.0);
-  sum += t * t / rho[0];
-  for (int k = 1; k < Q; k++) {
-    t = X[i + (size_t)k * N] - T[j + k * M];
-    sum += t * t / 2.0 / rho[k];
-  }
-  Knm[i + (size_t)j * ldN] = exp(-sum);
+  Knm[i + (size_t)j * ldN] = exp(-kern_sum(X, (size_t)N, i, T, M, j, rho, Q, lv));
 }
 
-__global__ void k_kmm(int M, int Q, const double* __restrict__ T, const double* __restrict__ rho,
+__global__ void k_kmm(int M, int Q, int lv, const double* __restrict__ T, const double* __restrict__ rho,
                       double* __restrict__ K, double* __restrict__ Kinv) {
   const int ii = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (ii >= M) return;
   double val;
-  if (ii == j) {
-    val = 1.0;
-  } else if (ii > j) {
-    val = 0.0;
-  } else {
-    double sum = 0.0, t = sin((T[ii] - T[j]) / 2.0);
-    sum += t * t / rho[0];
-    for (int k = 1; k < Q; k++) {
-      t = T[ii + k * M] - T[j + k * M];
-      sum += t * t / 2.0 / rho[k];
-    }
-    val = exp(-sum);
-  }
+  if (ii == j) val = 1.0;
+  else if (ii > j) val = 0.0;
+  else val = exp(-kern_sum(T, (size_t)M, ii, T, M, j, rho, Q, lv));
   K[ii + j * M] = val;
   Kinv[ii + j * M] = val;
+}
+
+// The DE driver's null model as a design whose GP block is inert: Knm = 0, Kmm = Kinv = I,
+// Kmm^{-1} k_n = 0, titsias = 0 (initTitsias). The GP columns then decouple from the rest of
+// every Psi_j (their Gram entries vanish, DeltaInv holds 1/delta_GP on their diagonal), and
+// their coefficients stay 0.
+__global__ void k_gp_null(int N, int ldN, int M, double* __restrict__ Knm, double* __restrict__ KinvKmn,
+                          double* __restrict__ titsias, double* __restrict__ K, double* __restrict__ Kinv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ldN)
+    for (int m = 0; m < M; m++) {
+      Knm[i + (size_t)m * ldN] = 0.0;
+      KinvKmn[i + (size_t)m * ldN] = 0.0;
+    }
+  if (i < N) titsias[i] = 0.0;
+  if (i < M * M) K[i] = Kinv[i] = (i % M == i / M) ? 1.0 : 0.0;
 }
 
 // Two triangular solves per cell with the lower factor L (n x n, col-major) held in the
@@ -87,15 +109,25 @@ __global__ void k_expand(int P, int p, int g0, int M, const int* __restrict__ mk
   D[r + (size_t)col * P] = v;
 }
 
-int launch_kernel_mats(Ctx* c) {
+int launch_kernel_mats(Ctx* c) { return launch_kernel_mats_lv(c, c->kernel_lv); }
+
+int launch_kernel_mats_lv(Ctx* c, int lv) {
   double* Knm = c->Dm + (size_t)c->dg0 * c->ldN;
+  if (lv == kLvNone) {
+    ProfScope ps(c, "kernel_mats");
+    const int n = std::max(c->ldN, c->M * c->M);
+    k_gp_null<<<div_up(n, 256), 256, 0, c->stream>>>(c->N, c->ldN, c->M, Knm, c->KinvKmn, c->titsias, c->Kmm,
+                                                     c->Kinv);
+    GPL_LAUNCHED(c, "k_gp_null");
+    return GPL_OK;
+  }
   {
     ProfScope ps(c, "kernel_mats");
     dim3 g(div_up(c->N, 128), c->M);
-    k_knm<<<g, 128, 0, c->stream>>>(c->N, c->ldN, c->M, c->Q, c->X, c->T, c->rho, Knm);
+    k_knm<<<g, 128, 0, c->stream>>>(c->N, c->ldN, c->M, c->Q, lv, c->X, c->T, c->rho, Knm);
     GPL_LAUNCHED(c, "k_knm");
     dim3 g2(div_up(c->M, 64), c->M);
-    k_kmm<<<g2, 64, 0, c->stream>>>(c->M, c->Q, c->T, c->rho, c->Kmm, c->Kinv);
+    k_kmm<<<g2, 64, 0, c->stream>>>(c->M, c->Q, lv, c->T, c->rho, c->Kmm, c->Kinv);
     GPL_LAUNCHED(c, "k_kmm");
   }
   int rc = launch_chol_single(c, c->Kinv, c->M);
@@ -120,9 +152,9 @@ int launch_expand_delta(Ctx* c) {
 int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
                            const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork) {
   dim3 g(div_up(N, 128), M);
-  k_knm<<<g, 128, 0, st>>>(N, N, M, Q, X, T, rho, Knm);
+  k_knm<<<g, 128, 0, st>>>(N, N, M, Q, -1, X, T, rho, Knm);
   dim3 g2(div_up(M, 64), M);
-  k_kmm<<<g2, 64, 0, st>>>(M, Q, T, rho, Lwork, Lwork);
+  k_kmm<<<g2, 64, 0, st>>>(M, Q, -1, T, rho, Lwork, Lwork);
   launch_chol_exact_raw(st, Lwork, M);
   k_kinvkmn<<<div_up(N, 128), 128, 0, st>>>(N, N, M, Lwork, Knm, KinvKmn, titsias);
   return (int)cudaGetLastError();

@@ -155,6 +155,23 @@ class GPLVM:
         stats = dict(outer=st[0], irls=st[1], lbfgs=st[2], evals=st[3])
         return (1 if rc == -5 else 0), stats, tr[:stats["outer"] + stats["lbfgs"]].copy()
 
+    # -- the differential-expression driver's model comparison (ggplvm_de.cu) ------------------
+    def de_model(self, model) -> None:
+        """Select the DE driver's model: "null" (no GP), "full" (the GP over every latent
+        dimension) or a latent dimension q (the GP over dimension q alone)."""
+        code = {"null": _lib.DE_NULL, "full": _lib.DE_FULL}.get(model, model)
+        self._c(self._L.gpl_de_model(self.h, int(code)), "gpl_de_model")
+
+    def de_irls(self, jtr_max: int = 1000, tol: float = 1e-8, trace_cap: int = 0):
+        """The selected model's GLM initialisation and IRLS in the DE driver's forms; returns
+        (per-gene log-likelihoods, sweeps, summed likelihood per sweep)."""
+        lk = np.zeros(self.J)
+        n = ctypes.c_int32()
+        tr = np.zeros(max(1, trace_cap))
+        self._c(self._L.gpl_de_irls(self.h, int(jtr_max), float(tol), _d(lk), ctypes.byref(n),
+                                    _d(tr) if trace_cap else None, int(trace_cap)), "gpl_de_irls")
+        return lk, n.value, tr[:min(n.value, trace_cap)].copy()
+
     def evaluate(self, params: np.ndarray, grad_out: Optional[np.ndarray] = None):
         """Objective and gradient at natural-scale params [Omega | delta | X | T | rho]."""
         params = np.ascontiguousarray(params, np.float64)

@@ -171,6 +171,43 @@ GPL_API int gpl_evaluate(gpl_ctx* ctx, const double* params, int64_t n_params, d
  * phi and factored Psi_j (call after gpl_fit, an IRLS phase or an objective). */
 GPL_API int gpl_score_stats(gpl_ctx* ctx, int L, const double* G, double* S);
 
+/* The model comparison of the differential-expression driver (ggplvm_de.cu:1067-1207), which
+ * refits the GLM part by IRLS at the fitted Omega, delta, X, T and rho for several GPs and
+ * keeps each model's per-gene log-likelihood ("BFs", J x (Q+2), written to BFs_de.gz). One
+ * context holds one model family: load the design with the model's M (Mfull, Mredc, or any M
+ * >= 1 for the null model), set the parameters, then select the model and run its IRLS.
+ *
+ * gpl_de_model selects the GP (getKernelMats at ggplvm_de.cu:1118-1128 and the kernel
+ * matrices after it) and switches the context's IRLS to the DE driver's kernels (getWForBeta,
+ * getBetaPhi, getZeta, getLkhdPois of ggplvm_de.cu):
+ *   GPL_DE_NULL  no GP, the null model Z0 (the GP block is held inert: Knm = 0, Kmm = I,
+ *                titsias = 0, its coefficients stay 0 and it is left out of the likelihood).
+ *                As the reference's loader (DataFrame.cu:112-113, 131), the first cell of the
+ *                last design variable reads 199.0 while this model is selected, when that
+ *                variable is numeric (for a categorical one the reference reads level codes
+ *                out of range; the loaded codes are kept).
+ *   GPL_DE_FULL  the GP over all latent dimensions (T as set: the fitted Mfull points)
+ *   q in [0, Q)  the GP over latent dimension q alone (getKernelMatsWithPerSpecificLV,
+ *                kernel_funcs.cu:101-135; T as set: the equispaced Mredc points, see
+ *                gpl_ta_equispaced)
+ *
+ * gpl_de_irls runs that model's GLM initialisation (initPsi, initPsi2, initBeta, getZeta)
+ * and IRLS sweeps until the relative change of the summed likelihood is below tol (the
+ * reference: 1e-5 for the null model, 1e-8 for the others), a NaN/inf sum, or jtr_max sweeps
+ * (the reference: 1000). phi carries in from the context (the reference starts at 1 and
+ * keeps each model's final phi for the next model's zeta). lkhds[J] receives the per-gene
+ * log-likelihoods, *sweeps the number of sweeps, trace the summed likelihood of every sweep
+ * (up to trace_cap). Always FP64. */
+#define GPL_DE_NULL (-2)
+#define GPL_DE_FULL (-1)
+GPL_API int gpl_de_model(gpl_ctx* ctx, int model);
+GPL_API int gpl_de_irls(gpl_ctx* ctx, int jtr_max, double tol, double* lkhds, int32_t* sweeps, double* trace,
+                        int trace_cap);
+
+/* initTaEquispaced (util.c:57-71): M x Q inducing points (column-major), dim 0 equispaced on
+ * (0, 2 pi), dims >= 1 on (-3, 3): the DE driver's points for the per-dimension models. */
+GPL_API void gpl_ta_equispaced(int M, int Q, double* T);
+
 /* The same evaluation at the parameters already on the device, enqueued on the context's
  * stream without host copies or synchronisation (device-resident throughput). The objective
  * lands in slot 1 of the trace; read it with gpl_get("lkhd_dev") or the next evaluate. */

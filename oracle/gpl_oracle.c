@@ -23,6 +23,7 @@ static const double WT = 0.1, IGAP1 = 100.0, IGB = 100.0;
 
 struct orc_ctx {
   int N, J, M, Q, P, p;
+  int gpv; /* 1 when the design carries the GP variable (M > 0); 0 for the DE null model */
   long L;
   int *ci, *gp;
   double *cx;
@@ -128,7 +129,7 @@ static inline double zval(const orc_ctx* o, int i, int k) {
 orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene_ptr, const double* counts,
                     int n_var, const int* c, const int* v, const void* body, long body_bytes, int M, int Q,
                     const double* ls, const double* X0) {
-  if (N <= 0 || J <= 0 || M <= 0 || Q <= 0 || n_var < 0 || nnz < 0) return NULL;
+  if (N <= 0 || J <= 0 || M < 0 || Q <= 0 || n_var < 0 || nnz < 0) return NULL;
   orc_ctx* o = (orc_ctx*)xcalloc(1, sizeof(orc_ctx));
   o->N = N; o->J = J; o->M = M; o->Q = Q; o->L = nnz;
   o->ci = (int*)xcalloc(nnz, sizeof(int));
@@ -138,14 +139,16 @@ orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene
   memcpy(o->gp, gene_ptr, sizeof(int) * (J + 1));
   memcpy(o->cx, counts, sizeof(double) * nnz);
 
-  const int p = n_var + 2;
+  /* loadDataFrame (DataFrame.cu:56-75): intercept, the file's variables, then Knm when M > 0 */
+  o->gpv = M > 0 ? 1 : 0;
+  const int p = n_var + 1 + o->gpv;
   o->p = p;
   o->vc = (int*)xcalloc(p, sizeof(int));
   o->vv = (int*)xcalloc(p, sizeof(int));
   o->nh = (int*)xcalloc(p + 1, sizeof(int));
   o->vc[0] = 1; o->vv[0] = 1;
   for (int k = 0; k < n_var; k++) { o->vc[k + 1] = c[k]; o->vv[k + 1] = v[k]; }
-  o->vc[p - 1] = 1; o->vv[p - 1] = M;
+  if (o->gpv) { o->vc[p - 1] = 1; o->vv[p - 1] = M; }
   long need = 0;
   for (int j = 0; j < p; j++) o->nh[j + 1] = o->nh[j] + o->vv[j] * o->vc[j];
   for (int k = 0; k < n_var; k++) need += (long)N * v[k] * (c[k] == 1 ? 8 : 4);
@@ -166,7 +169,7 @@ orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene
   const char* bp = (const char*)body;
   long off = 0;
   o->varbase[0] = o->ones;
-  for (int j = 1; j < p - 1; j++) {
+  for (int j = 1; j <= n_var; j++) {
     long bytes = (long)N * o->vv[j] * (o->vc[j] == 1 ? 8 : 4);
     if (o->vc[j] == 1) {
       double* d = (double*)xcalloc((size_t)N * o->vv[j], sizeof(double));
@@ -179,7 +182,7 @@ orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene
     }
     off += bytes;
   }
-  o->varbase[p - 1] = o->Knm;
+  if (o->gpv) o->varbase[p - 1] = o->Knm;
   for (int j = 0; j < p; j++) {
     for (int k = o->nh[j]; k < o->nh[j + 1]; k++) {
       o->mc[k] = o->vc[j];
@@ -189,8 +192,15 @@ orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene
       else o->catcol[k] = o->varcat[j];
     }
   }
+  /* loadDataFrame stores 99.0, and newDataFrameOnDevice 199.0, at the start of the last
+   * variable's block (DataFrame.cu:112-113, 131): that is Knm's first entry when M > 0
+   * (rewritten by getKernelMats) and the first cell of the last design variable when M = 0
+   * (the DE driver's null model), kept here for a numeric variable. For a categorical one the
+   * double's bytes replace two level codes, which the reference then reads out of range; the
+   * codes are left as loaded. */
+  if (!o->gpv && o->vc[p - 1] == 1) o->varbase[p - 1][0] = 199.0;
   /* level codes must index an existing column (the reference does not check) */
-  for (int j = 1; j < p - 1; j++)
+  for (int j = 1; j <= n_var; j++)
     if (o->vc[j] != 1)
       for (int i = 0; i < N; i++)
         if (o->varcat[j][i] < 0 || o->varcat[j][i] >= o->vc[j] * o->vv[j]) { orc_destroy(o); return NULL; }
@@ -235,10 +245,11 @@ orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene
 
 void orc_destroy(orc_ctx* o) {
   if (!o) return;
+  const int nv_end = o->p - o->gpv; /* the file's variables are 1 .. nv_end - 1 */
   if (o->varbase)
-    for (int j = 1; j < o->p - 1; j++) free(o->varbase[j]);
+    for (int j = 1; j < nv_end; j++) free(o->varbase[j]);
   if (o->varcat)
-    for (int j = 1; j < o->p - 1; j++) free(o->varcat[j]);
+    for (int j = 1; j < nv_end; j++) free(o->varcat[j]);
   void* bufs[] = {o->ci, o->gp, o->cx, o->vc, o->vv, o->nh, o->mc, o->mv, o->mk, o->numcol, o->catcol,
                   o->varbase, o->varcat, o->ones, o->Knm, o->Omega, o->delta, o->X, o->T, o->rho, o->phi,
                   o->ls, o->zeta, o->Kmm, o->Kinv, o->KinvKmn, o->titsias, o->DeltaInv, o->W, o->Nu, o->Psi,
@@ -257,7 +268,7 @@ void orc_init_params(orc_ctx* o) {
   const int p = o->p;
   o->delta[0] = 1.5;
   for (int i = 1; i < p - 1; i++) o->delta[i] = 0.01;
-  o->delta[p - 1] = 0.3;
+  o->delta[p - 1] = o->gpv ? 0.3 : 0.01;
   for (int i = 0; i < o->N; i++) o->Omega[i] = 1.0;
   for (int j = 0; j < o->J; j++) o->phi[j] = 1.0;
   o->rho[0] = 5.0;
@@ -277,38 +288,39 @@ void orc_set_params(orc_ctx* o, const double* Omega, const double* delta, const 
 
 void orc_set_beta(orc_ctx* o, const double* beta) { memcpy(o->Beta, beta, sizeof(double) * (size_t)o->P * o->J); }
 
-/* ---- kernel matrices: kernel_funcs.cu:61-97, 139-162 ------------------------------ */
+/* ---- kernel matrices: kernel_funcs.cu:61-97, 101-135, 139-162 ---------------------- */
 
-void orc_kernel_mats(orc_ctx* o) {
+/* Squared distance term of one cell/inducing pair (or inducing/inducing pair): all latent
+ * dimensions (getKernelMatsWithPer, kernel_funcs.cu:61-97: periodic dim 0, ARD dims >= 1)
+ * when lv < 0, dimension lv alone otherwise (getKernelMatsWithPerSpecificLV,
+ * kernel_funcs.cu:101-135). a and b index the two point sets with leading sizes na, nb. */
+static double kern_sum(const double* A, int na, int a, const double* B, int nb, int b, const double* rho, int Q,
+                       int lv) {
+  double sum = 0.0, t;
+  if (lv <= 0) {
+    t = sin((A[a] - B[b]) / 2.0);
+    sum += t * t / rho[0];
+  }
+  for (int k = 1; k < Q; k++) {
+    if (lv >= 0 && k != lv) continue;
+    t = A[a + (size_t)k * na] - B[b + (size_t)k * nb];
+    sum += t * t / 2.0 / rho[k];
+  }
+  return sum;
+}
+
+static void kernel_mats_lv(orc_ctx* o, int lv) {
   const int N = o->N, M = o->M, Q = o->Q;
   const double *X = o->X, *T = o->T, *rho = o->rho;
-  /* getKernelMatsWithPer: periodic dim 0, ARD squared-exponential dims >= 1 */
 #pragma omp parallel for schedule(static)
-  for (int j = 0; j < M; j++) {
-    for (int i = 0; i < N; i++) {
-      double sum = 0.0, t = sin((X[i] - T[j]) / 2.0);
-      sum += t * t / rho[0];
-      for (int k = 1; k < Q; k++) {
-        t = X[i + k * N] - T[j + k * M];
-        sum += t * t / 2.0 / rho[k];
-      }
-      o->Knm[i + (size_t)j * N] = exp(-sum);
-    }
-  }
+  for (int j = 0; j < M; j++)
+    for (int i = 0; i < N; i++) o->Knm[i + (size_t)j * N] = exp(-kern_sum(X, N, i, T, M, j, rho, Q, lv));
   for (int j = 0; j < M; j++) {
     for (int ii = 0; ii < M; ii++) {
       double val;
       if (ii == j) val = 1.0;
       else if (ii > j) val = 0.0;
-      else {
-        double sum = 0.0, t = sin((T[ii] - T[j]) / 2.0);
-        sum += t * t / rho[0];
-        for (int k = 1; k < Q; k++) {
-          t = T[ii + k * M] - T[j + k * M];
-          sum += t * t / 2.0 / rho[k];
-        }
-        val = exp(-sum);
-      }
+      else val = exp(-kern_sum(T, M, ii, T, M, j, rho, Q, lv));
       o->Kmm[ii + j * M] = val;
       o->Kinv[ii + j * M] = val;
     }
@@ -326,10 +338,21 @@ void orc_kernel_mats(orc_ctx* o) {
   }
 }
 
+void orc_kernel_mats(orc_ctx* o) { kernel_mats_lv(o, -1); }
+
+/* getKernelMats(..., q, ...) (kernel_funcs.cu:17-19): the GP over latent dimension q alone,
+ * then cholKmm and getKinvKmn as for the full kernel (ggplvm_de.cu:1129-1133). */
+void orc_kernel_mats_lv(orc_ctx* o, int q) { kernel_mats_lv(o, q < 0 ? -1 : q); }
+
 /* expandDelta_k (util_cuda.cu:249-269): prior precision blockdiag(1/delta_k I, Kmm/delta_GP), upper. */
 void orc_expand_delta(orc_ctx* o) {
   const int p = o->p, P = o->P, M = o->M;
   memset(o->DeltaInv, 0, sizeof(double) * (size_t)P * P);
+  if (!o->gpv) { /* expandDeltaWOK_k (util_cuda.cu:235-246): no GP block */
+    for (int i = 0; i < p; i++)
+      for (int j = o->nh[i]; j < o->nh[i + 1]; j++) o->DeltaInv[j + j * P] = 1.0 / o->delta[i];
+    return;
+  }
   for (int i = 0; i < p - 1; i++)
     for (int j = o->nh[i]; j < o->nh[i + 1]; j++) o->DeltaInv[j + j * P] = 1.0 / o->delta[i];
   for (int j = 0; j < M; j++) {
@@ -1068,6 +1091,155 @@ void orc_score_stats(orc_ctx* o, int L, const double* G, double* S) {
     free(tmp);
     free(tmp2);
   }
+}
+
+/* ---- the differential-expression driver's model comparison: ggplvm_de.cu ----------- */
+/* The DE driver (ggplvm_de.cu:886-1237) refits the GLM part by IRLS, at the fitted Omega,
+ * delta, X and rho, for a null model without the GP (Z0), one reduced model per latent
+ * dimension (GP over that dimension alone, Mredc equispaced inducing points) and the full
+ * model (Mfull inducing points, the fitted T), and keeps every model's per-gene
+ * log-likelihood ("BFs", ggplvm_de.cu:1107,1200,1203-1207). Its kernels differ from the fit
+ * driver's in the places restated below. */
+
+/* getZeta (ggplvm_de.cu:34-47): the 1/phi-weighted mean coefficient over genes. */
+static void de_zeta(orc_ctx* o) {
+  const int J = o->J, P = o->P;
+  for (int k = 0; k < P; k++) {
+    double sum = 0.0, den = 0.0;
+    for (int j = 0; j < J; j++) {
+      sum += o->Beta[k + (size_t)j * P] / o->phi[j];
+      den += 1.0 / o->phi[j];
+    }
+    o->zeta[k] = sum / den;
+  }
+}
+
+/* getWForBeta of the DE driver (ggplvm_de.cu:442-486): the Titsias factor enters W with
+ * weight 1, and nu = z.(beta - zeta) + (y - W)/W at a count, z.(beta - zeta) - 1 elsewhere. */
+static void de_w_nu(orc_ctx* o) {
+  const int N = o->N, J = o->J, p = o->p, P = o->P;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int j = 0; j < J; j++) {
+    const double* bj = o->Beta + (size_t)j * P;
+    double* Wj = o->W + (size_t)j * N;
+    double* nj = o->Nu + (size_t)j * N;
+    int l = o->gp[j], lmax = o->gp[j + 1];
+    for (int i = 0; i < N; i++) {
+      double sum = 0.0, sum2 = 0.0;
+      for (int k = 0; k < p; k++) {
+        if (o->vc[k] == 1) {
+          const double* pd = o->varbase[k];
+          for (int m = 0; m < o->vv[k]; m++) {
+            sum += pd[i + (size_t)m * N] * bj[o->nh[k] + m];
+            sum2 += pd[i + (size_t)m * N] * (bj[o->nh[k] + m] - o->zeta[o->nh[k] + m]);
+          }
+        } else {
+          int lev = o->varcat[k][i];
+          sum += bj[o->nh[k] + lev];
+          sum2 += (bj[o->nh[k] + lev] - o->zeta[o->nh[k] + lev]);
+        }
+      }
+      Wj[i] = exp(sum) * o->ls[i] * exp(o->delta[p - 1] * o->titsias[i]);
+      if (l < lmax && o->ci[l] == i) {
+        nj[i] = sum2 + (o->cx[l] - Wj[i]) / Wj[i];
+        l++;
+      } else {
+        nj[i] = sum2 - 1.0;
+      }
+    }
+  }
+}
+
+/* getBetaPhi of the DE driver (ggplvm_de.cu:413-438): undamped, beta = Psi^{-1} b + zeta,
+ * phi = (sum nu^2 W/Omega - b . Psi^{-1} b) / N with clamps NaN -> 1, < 0 -> 100,
+ * < 0.01 -> 0.01, > 100 -> 100. */
+static void de_beta_phi(orc_ctx* o) {
+  const int N = o->N, J = o->J, P = o->P;
+#pragma omp parallel
+  {
+    double* b = (double*)xcalloc(P, sizeof(double));
+#pragma omp for schedule(dynamic, 4)
+    for (int j = 0; j < J; j++) {
+      const double* Wj = o->W + (size_t)j * N;
+      const double* nj = o->Nu + (size_t)j * N;
+      double* bj = o->Beta + (size_t)j * P;
+      double phij = 0.0;
+      zt_oinv_nu(o, Wj, nj, b);
+      for (int i = 0; i < N; i++) phij += nj[i] * nj[i] * Wj[i] / o->Omega[i];
+      cholsl(o->Psi + (size_t)j * P * P, P, b, bj);
+      for (int k = 0; k < P; k++) {
+        phij -= bj[k] * b[k];
+        bj[k] += o->zeta[k];
+      }
+      double ph = phij / (double)N;
+      if (isnan(ph)) ph = 1.0;
+      if (ph < 0.0) ph = 100.0;
+      if (ph < 0.01) ph = 0.01;
+      if (ph > 100.0) ph = 100.0;
+      o->phi[j] = ph;
+    }
+    free(b);
+  }
+}
+
+/* getLkhdPois of the DE driver (ggplvm_de.cu:667-693): per gene
+ * (sum_i [(log W - delta_{p-1} titsias) y - W] / Omega - sum_k log L_kk) / phi + P log(2 pi') / 2
+ * with the reference's pi' = 3.1415926535. */
+static void de_lkhd(orc_ctx* o) {
+  const int N = o->N, J = o->J, p = o->p, P = o->P;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int j = 0; j < J; j++) {
+    const double* Wj = o->W + (size_t)j * N;
+    const double* Pj = o->Psi + (size_t)j * P * P;
+    int l = o->gp[j], lmax = o->gp[j + 1];
+    double sum = 0.0;
+    for (int i = 0; i < N; i++) {
+      if (l < lmax && o->ci[l] == i) {
+        sum += ((log(Wj[i]) - o->delta[p - 1] * o->titsias[i]) * o->cx[l] - Wj[i]) / o->Omega[i];
+        l++;
+      } else {
+        sum -= Wj[i] / o->Omega[i];
+      }
+    }
+    for (int k = 0; k < P; k++) sum -= log(Pj[k + k * P]);
+    o->lkhds[j] = sum / o->phi[j] + log(2 * 3.1415926535) * ((double)P) / 2.0;
+  }
+}
+
+/* One model of the DE driver: the GLM initialisation (initPsi, initPsi2, initBeta) and
+ * getZeta (ggplvm_de.cu:1071-1077, 1135-1140), then IRLS sweeps of getWForBeta, getPsi,
+ * cholPsi, getBetaPhi, getZeta, getLkhdPois and collectLkhd(N = 0, Q = 0), which sums the
+ * per-gene values (ggplvm_de.cu:1079-1104, 1142-1177), stopping at a NaN/inf sum, at
+ * jtr_max sweeps or when the relative change falls below tol (1e-5 for the null model,
+ * 1e-8 for the others). Kernel matrices are set beforehand (orc_kernel_mats[_lv]); with
+ * M = 0 there are none and titsias is 0 (initTitsias). Returns the number of sweeps; the
+ * per-gene values are left in "lkhds", the sums in "lkhd". */
+int orc_de_irls(orc_ctx* o, int jtr_max, double tol) {
+  orc_glm_init(o);
+  de_zeta(o);
+  int jtr;
+  for (jtr = 0; jtr < jtr_max; jtr++) {
+    de_w_nu(o);
+    gram_chol(o);
+    de_beta_phi(o);
+    de_zeta(o);
+    de_lkhd(o);
+    double sum = 0.0;
+    for (int k = 0; k < o->J; k++) sum += o->lkhds[k];
+    o->lkhd[jtr] = sum;
+    if (jtr > 0) {
+      if (isinf(sum) || isnan(sum)) { jtr++; break; }
+      if (jtr == jtr_max - 1 || fabs(o->lkhd[jtr - 1] - sum) / fabs(sum) < tol) { jtr++; break; }
+    }
+  }
+  return jtr;
+}
+
+/* initTaEquispaced (util.c:57-71): dim 0 on (0, 2 pi), dims >= 1 on (-3, 3). */
+void orc_ta_equispaced(int M, int Q, double* T) {
+  for (int i = 0; i < M; i++) T[i] = ((double)(i + 1) / (double)(M + 1)) * 2.0 * 3.14159265358979;
+  for (int k = 1; k < Q; k++)
+    for (int i = 0; i < M; i++) T[i + (size_t)k * M] = ((double)(i + 1) / (double)(M + 1) - 0.5) * 6.0;
 }
 
 long orc_get(orc_ctx* o, const char* name, double* out) {

@@ -20,7 +20,8 @@ typedef struct orc_ctx orc_ctx;
 
 /* N cells, J genes, counts in gene-major CSR (SparseMat.cuh:3-10); the design as the file
  * part of a DataFrame (DataFrame.cu:88-149): n_var variables, c[] levels, v[] widths, and
- * the raw body bytes; M inducing points, Q latent dimensions. Returns NULL on bad input. */
+ * the raw body bytes; M inducing points (0: no GP variable, the DE driver's null model),
+ * Q latent dimensions. Returns NULL on bad input. */
 orc_ctx* orc_create(int N, int J, long nnz, const int* cell_idx, const int* gene_ptr, const double* counts,
                     int n_var, const int* c, const int* v, const void* body, long body_bytes, int M, int Q,
                     const double* ls, const double* X0);
@@ -46,6 +47,11 @@ void orc_beta_from_tilde(orc_ctx* o);
 int orc_fit(orc_ctx* o, int itr_max, int lbfgs_budget, int* stats, double* trace, int trace_cap);
 long orc_get(orc_ctx* o, const char* name, double* out);
 void orc_score_stats(orc_ctx* o, int L, const double* G, double* S); /* getScoreStats */
+/* the DE driver's model comparison (ggplvm_de.cu): kernel over one latent dimension
+ * (q < 0: all), one model's IRLS with its stopping rule, initTaEquispaced */
+void orc_kernel_mats_lv(orc_ctx* o, int q);
+int orc_de_irls(orc_ctx* o, int jtr_max, double tol);
+void orc_ta_equispaced(int M, int Q, double* T);
 void orc_set_threads(int n);
 
 #ifdef __cplusplus

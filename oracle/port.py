@@ -57,6 +57,10 @@ def lib():
         L.orc_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _dp]
         L.orc_score_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_kernel_mats_lv.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_de_irls.restype = ctypes.c_int
+        L.orc_de_irls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.orc_ta_equispaced.argtypes = [ctypes.c_int, ctypes.c_int, _dp]
         _lib = L
     return _lib
 
@@ -172,3 +176,53 @@ class OracleModel:
         out = np.zeros(n)
         lib().orc_get(self.h, name.encode(), _dptr(out))
         return out
+
+
+def ta_equispaced(M: int, Q: int) -> np.ndarray:
+    """initTaEquispaced (util.c:57-71): M x Q inducing points, column-major."""
+    T = np.zeros(M * Q)
+    lib().orc_ta_equispaced(int(M), int(Q), _dptr(T))
+    return T.reshape(Q, M).T.copy()
+
+
+def de_bfs(ds, prm, Mredc: int, Mfull: int, jtr_max: int = 1000):
+    """The DE driver's model comparison (ggplvm_de.cu:1067-1207) on the oracle: per-gene
+    log-likelihoods J x (Q + 2) of the null model, the Q one-dimension GP models (Mredc
+    equispaced inducing points) and the full model (Mfull inducing points, prm.T), each
+    refitted by the DE driver's IRLS at prm's Omega, delta, X and rho; phi starts at 1 and
+    carries from model to model. Returns (BFs, sweeps per model, full-model beta P x J, phi)."""
+    Q, J = ds.Q, ds.J
+    BFs = np.zeros((J, Q + 2))
+    sweeps = []
+    phi = np.ones(J)
+    delta = np.asarray(prm.delta, np.float64)
+
+    def run(M, T, delta_m, lv, tol):
+        nonlocal phi
+        m = OracleModel(ds.y, ds.z, ds.ls, prm.X, M, Q)
+        try:
+            lib().orc_set_params(m.h, _dptr(np.ascontiguousarray(prm.Omega, np.float64)),
+                                 _dptr(np.ascontiguousarray(delta_m)), _dptr(np.ascontiguousarray(
+                                     np.asarray(prm.X, np.float64).ravel(order="F"))),
+                                 _dptr(None if T is None else np.ascontiguousarray(np.asarray(T).ravel(order="F"))),
+                                 _dptr(np.ascontiguousarray(prm.rho, np.float64)), _dptr(phi.copy()))
+            if M > 0:
+                lib().orc_kernel_mats_lv(m.h, int(lv))
+            n = lib().orc_de_irls(m.h, int(jtr_max), float(tol))
+            out = m.get("lkhds").copy()
+            phi = m.get("phi").copy()
+            beta = m.get("Beta").reshape(J, m.P).T.copy()
+            return n, out, beta
+        finally:
+            m.close()
+
+    n, BFs[:, 0], _ = run(0, None, delta[:-1].copy(), -1, 1e-5)
+    sweeps.append(n)
+    Tr = ta_equispaced(Mredc, Q)
+    beta = None
+    for q in range(Q):
+        n, BFs[:, q + 1], _ = run(Mredc, Tr, delta, q, 1e-8)
+        sweeps.append(n)
+    n, BFs[:, Q + 1], beta = run(Mfull, np.asarray(prm.T), delta, -1, 1e-8)
+    sweeps.append(n)
+    return BFs, sweeps, beta, phi

@@ -70,6 +70,20 @@ void LBFGS(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K
 void getScoreStats(int L, SparseMat* Y, DataFrame* Z, double* G, double* Psi, double* W, double* Omega,
                    double* phi, double* Work, double* S);
 
+/* the DE driver's own versions of six kernels (ggplvm_de.cu), built into namespace de */
+namespace de {
+void getZeta(int J, int P, double* Beta, double* phi, double* zeta);
+void getBetaPhi(int J, DataFrame* Z, double* ls, double* Psi, double* Omega, double* zeta, double* Nu, double* W,
+                double* Work, double* Beta, double* phi);
+void getWForBeta(SparseMat* Y, DataFrame* Z, double* ls, double* Beta, double* zeta, double* delta, double* titsias,
+                 double* W, double* Nu);
+void getPsi(int J, DataFrame* Z, double* Omega, double* DeltaInv, double* W, double* Psi);
+void getLkhdPois(SparseMat* Y, DataFrame* Z, double* W, double* delta, double* titsias, double* Psi, double* Omega,
+                 double* phi, double* lkhds);
+void collectLkhd(int N, int J, int Q, double* Omega, double* lkhds, int itr, int jtr, DataFrame* Z, double* delta,
+                 double* Xi, double* Ta, double* W, double* titsias, double wt, double* lkhd_d);
+}  // namespace de
+
 namespace {
 
 struct RefCtx {
@@ -458,6 +472,151 @@ void ref_score_stats(void* h, int L, const double* G, double* S) {
     getScoreStats(L, c->Y, c->Z, g.data(), c->Psi, c->W, c->Omega, c->phi, work.data(), s.data());
   });
   std::memcpy(S, s.data(), sizeof(double) * s.size());
+}
+
+/* The model comparison of the differential-expression driver (ggplvm_de.cu:886-1207),
+ * from its loaders to the per-gene log-likelihood table "BFs" (J x (Q + 2), gene fastest:
+ * column 0 the null model Z0, column q + 1 the GP over latent dimension q alone with Mredc
+ * inducing points, column Q + 1 the full model with Mfull), with main's allocations, grid
+ * shapes and stopping rules, under a budget of jtr_max IRLS sweeps per model (main: 1000).
+ * The fitted Omega, delta, X, T (Mfull x Q) and rho arrive as readParams would read them
+ * (ggplvm_de.cu:1040-1043); phi restarts at 1 (initPhi) and titsias at 0 (initTitsias).
+ * initTaEquispaced (util.c:57-71, in the GSL-dependent util.c) is restated for the reduced
+ * models' inducing points. sweeps[Q + 2] receives each model's IRLS count; beta_full (P1 x J)
+ * and phi_out (J) the last model's coefficients and dispersions (either may be NULL).
+ * Returns P1, or -1 on a file error. */
+int ref_de_bfs(const char* y_path, const char* z_path, const char* ls_path, int Q, int Mredc, int Mfull,
+               const double* Omega_in, const double* delta_in, const double* X_in, const double* Tfull_in,
+               const double* rho_in, int jtr_max, double* BFs_out, int* sweeps, double* beta_full, double* phi_out) {
+  FILE* probe;
+  for (const char* pth : {y_path, z_path, ls_path}) {
+    if (!(probe = fopen(pth, "rb"))) return -1;
+    fclose(probe);
+  }
+  std::string yp(y_path), zp(z_path);
+  SparseMat* Y_h = loadSparseMat(&yp[0]);
+  const int N = Y_h->N, J = Y_h->J;
+  SparseMat* Y = newSparseMatOnDevice(Y_h);
+  DataFrame* Z_h = loadDataFrame(&zp[0], Mredc);
+  DataFrame* Z0_h = loadDataFrame(&zp[0]);
+  DataFrame* Z1_h = loadDataFrame(&zp[0], Mfull);
+  DataFrame* Z = newDataFrameOnDevice(Z_h);
+  DataFrame* Z0 = newDataFrameOnDevice(Z0_h);
+  DataFrame* Z1 = newDataFrameOnDevice(Z1_h);
+  const int P0 = Z0_h->P, P1 = Z1_h->P, p = Z_h->p;
+  int P = P1, M = Mfull;
+  const int JTRMAX = jtr_max;
+  const double wt = 0.0; /* ggplvm_de.cu:20 */
+
+  double* Psi = dalloc((size_t)J * P * P * 2);
+  double* W = dalloc((size_t)N * (J + 1));
+  double* Nu = dalloc((size_t)N * J);
+  size_t lwork = (size_t)(N < M * M ? M * M : N);
+  lwork *= (2 * P);
+  double* Work = dalloc(lwork);
+  double* ls = dalloc(N);
+  double* Omega = dalloc((size_t)N * 2);
+  double* DeltaInv = dalloc((size_t)P * P);
+  double* delta = dalloc((size_t)p * 2);
+  double* phi = dalloc(J);
+  double* zeta = dalloc(P);
+  double* Beta = dalloc((size_t)P * J);
+  double* lkhds = dalloc(J);
+  double* BFs = dalloc((size_t)J * (Q + 2));
+  double* lkhd_d = dalloc(JTRMAX);
+  double* rho = dalloc((size_t)Q * 2);
+  double* Xi = dalloc((size_t)N * Q * 2);
+  double* Ta1 = dalloc((size_t)Mfull * Q * 2);
+  double* Ta = dalloc((size_t)Mredc * Q * 2);
+  double* K = dalloc((size_t)M * M);
+  double* Kinv = dalloc((size_t)M * M);
+  double* KinvKmn = dalloc((size_t)N * M);
+  double* titsias = dalloc(N);
+  std::vector<double> lkhd_h(JTRMAX);
+
+  for (int i = 0; i < Mredc; i++) Ta[i] = ((double)(i + 1) / (double)(Mredc + 1)) * 2.0 * 3.14159265358979;
+  for (int k = 1; k < Q; k++)
+    for (int i = 0; i < Mredc; i++) Ta[i + k * Mredc] = ((double)(i + 1) / (double)(Mredc + 1) - 0.5) * 6.0;
+  if (!read_doubles(ls_path, ls, N)) return -1;
+  memcpy(Omega, Omega_in, sizeof(double) * N);
+  memcpy(delta, delta_in, sizeof(double) * p);
+  memcpy(Xi, X_in, sizeof(double) * (size_t)N * Q);
+  memcpy(Ta1, Tfull_in, sizeof(double) * (size_t)Mfull * Q);
+  memcpy(rho, rho_in, sizeof(double) * Q);
+
+  const dim3 gridJ(J, 1), block1(1, 1), gridPsi0(J, P0), blockPsi0(1, P0), gridPP0(P0, P0);
+  const int sN = (int)(sqrt((double)N) / 4) + 1;
+  const dim3 gridN(sN, sN), blockN(4, 4);
+  int q = 0, jtr = 0;
+
+  /* null model (ggplvm_de.cu:1067-1107) */
+  ref_launch(dim3(1), block1, [&] { initPhi(J, phi); });
+  ref_launch(dim3(1), block1, [&] { initTitsias(N, titsias); });
+  ref_launch(dim3(1), block1, [&] { expandDeltaWOK_k(Z0, delta, DeltaInv); });
+  ref_launch(gridPP0, block1, [&] { initPsi(Z0, DeltaInv, Psi); });
+  ref_launch(dim3(1), block1, [&] { initPsi2(P0, Psi); });
+  ref_launch(gridJ, block1, [&] { initBeta(Y, ls, Z0, Psi, Work, Beta); });
+  ref_launch(dim3(P0), block1, [&] { de::getZeta(J, P0, Beta, phi, zeta); });
+  for (jtr = 0; jtr < JTRMAX; jtr++) {
+    ref_launch(gridJ, block1, [&] { de::getWForBeta(Y, Z0, ls, Beta, zeta, delta, titsias, W, Nu); });
+    ref_launch(gridPsi0, blockPsi0, [&] { de::getPsi(J, Z0, Omega, DeltaInv, W, Psi); });
+    ref_launch(gridJ, block1, [&] { cholPsi(J, P0, Psi); });
+    ref_launch(gridJ, block1, [&] { de::getBetaPhi(J, Z0, ls, Psi, Omega, zeta, Nu, W, Work, Beta, phi); });
+    ref_launch(dim3(P0), block1, [&] { de::getZeta(J, P0, Beta, phi, zeta); });
+    ref_launch(gridJ, block1, [&] { de::getLkhdPois(Y, Z0, W, delta, titsias, Psi, Omega, phi, lkhds); });
+    ref_launch(dim3(1), block1, [&] {
+      de::collectLkhd(0, J, 0, Omega, lkhds, q, jtr, Z0, delta, Xi, Ta, W, titsias, wt, lkhd_d);
+    });
+    lkhd_h[jtr] = lkhd_d[jtr];
+    if (jtr > 0) {
+      if (std::isinf(lkhd_h[jtr]) || std::isnan(lkhd_h[jtr])) break;
+      if (jtr == (JTRMAX - 1) || fabs(lkhd_h[jtr - 1] - lkhd_h[jtr]) / fabs(lkhd_h[jtr]) < 1e-5) break;
+    }
+  }
+  if (sweeps) sweeps[0] = jtr < JTRMAX ? jtr + 1 : JTRMAX;
+  memcpy(BFs, lkhds, sizeof(double) * J);
+
+  /* reduced models q = 0..Q-1 and the full model q = Q (ggplvm_de.cu:1110-1207) */
+  for (q = 0; q < Q + 1; q++) {
+    DataFrame *pZ, *pZ_h;
+    double* pT;
+    if (q == Q) {
+      pZ = Z1; pZ_h = Z1_h; pT = Ta1; P = P1; M = Mfull;
+      ref_launch(dim3(N + Mfull, Mfull), block1, [&] { getKernelMats(Q, Xi, pT, rho, pZ, K, Kinv, KinvKmn); });
+    } else {
+      M = Mredc; P = Z_h->P; pZ = Z; pZ_h = Z_h; pT = Ta;
+      ref_launch(dim3(N + Mredc, Mredc), block1, [&] { getKernelMats(Q, Xi, pT, rho, pZ, q, K, Kinv, KinvKmn); });
+    }
+    ref_launch(dim3(1), block1, [&] { cholKmm(M, Kinv); });
+    ref_launch(gridN, blockN, [&] { getKinvKmn(Kinv, pZ, KinvKmn, titsias); });
+    ref_launch(dim3(1), block1, [&] { expandDelta_k(pZ, delta, K, DeltaInv); });
+    ref_launch(dim3(pZ_h->P, pZ_h->P), block1, [&] { initPsi(pZ, DeltaInv, Psi); });
+    ref_launch(dim3(1), block1, [&] { initPsi2(P, Psi); });
+    ref_launch(gridJ, block1, [&] { initBeta(Y, ls, pZ, Psi, Work, Beta); });
+    ref_launch(dim3(pZ_h->P), block1, [&] { de::getZeta(J, P, Beta, phi, zeta); });
+    for (jtr = 0; jtr < JTRMAX; jtr++) {
+      ref_launch(gridJ, block1, [&] { de::getWForBeta(Y, pZ, ls, Beta, zeta, delta, titsias, W, Nu); });
+      ref_launch(dim3(J, P), dim3(1, P), [&] { de::getPsi(J, pZ, Omega, DeltaInv, W, Psi); });
+      ref_launch(gridJ, block1, [&] { cholPsi(J, P, Psi); });
+      ref_launch(gridJ, block1, [&] { de::getBetaPhi(J, pZ, ls, Psi, Omega, zeta, Nu, W, Work, Beta, phi); });
+      ref_launch(dim3(pZ_h->P), block1, [&] { de::getZeta(J, P, Beta, phi, zeta); });
+      ref_launch(gridJ, block1, [&] { de::getLkhdPois(Y, pZ, W, delta, titsias, Psi, Omega, phi, lkhds); });
+      ref_launch(dim3(1), block1, [&] {
+        de::collectLkhd(0, J, 0, Omega, lkhds, q, jtr, pZ, delta, Xi, pT, W, titsias, wt, lkhd_d);
+      });
+      lkhd_h[jtr] = lkhd_d[jtr];
+      if (jtr > 0) {
+        if (std::isinf(lkhd_h[jtr]) || std::isnan(lkhd_h[jtr])) break;
+        if (jtr == (JTRMAX - 1) || fabs(lkhd_h[jtr - 1] - lkhd_h[jtr]) / fabs(lkhd_h[jtr]) < 1e-8) break;
+      }
+    }
+    if (sweeps) sweeps[q + 1] = jtr < JTRMAX ? jtr + 1 : JTRMAX;
+    memcpy(BFs + (size_t)J * (q + 1), lkhds, sizeof(double) * J);
+  }
+  memcpy(BFs_out, BFs, sizeof(double) * J * (Q + 2));
+  if (beta_full) memcpy(beta_full, Beta, sizeof(double) * (size_t)P1 * J);
+  if (phi_out) memcpy(phi_out, phi, sizeof(double) * J);
+  return P1;
 }
 
 }  // extern "C"

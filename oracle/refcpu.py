@@ -61,6 +61,9 @@ def lib():
         L.ref_model_meta.argtypes = [ctypes.c_void_p, _ip, _ip, _ip, _ip]
         L.ref_set_verbose.argtypes = [ctypes.c_int]
         L.ref_score_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ref_de_bfs.restype = ctypes.c_int
+        L.ref_de_bfs.argtypes = [ctypes.c_char_p] * 3 + [ctypes.c_int] * 3 + [_dp] * 5 + [ctypes.c_int, _dp, _ip,
+                                                                                        _dp, _dp]
         _lib = L
     return _lib
 
@@ -176,3 +179,26 @@ class RefModel:
         mk = (ctypes.c_int * self.P)()
         lib().ref_model_meta(self.h, nh, mc, mv, mk)
         return np.array(nh), np.array(mc), np.array(mv), np.array(mk)
+
+
+def de_bfs(ds, prm, Mredc: int, Mfull: int, jtr_max: int = 1000, workdir: Optional[str] = None):
+    """The reference's own DE model comparison (ggplvm_de.cu:886-1207, through ref_de_bfs)
+    on the dataset's files at prm's fitted Omega, delta, X, T (Mfull x Q) and rho.
+    Returns (BFs J x (Q + 2), sweeps per model, full-model beta P x J, phi)."""
+    from gaspacho2_b200.formats import write_dataset
+
+    wd = workdir or tempfile.mkdtemp(prefix="gpl_ref_de_")
+    paths = write_dataset(wd, ds.y, ds.z, ds.ls, ds.X0)
+    Q, J = ds.Q, ds.J
+    arr = [np.ascontiguousarray(np.asarray(a, np.float64).ravel(order="F"))
+           for a in (prm.Omega, prm.delta, prm.X, prm.T, prm.rho)]
+    BFs = np.zeros(J * (Q + 2))
+    sweeps = (ctypes.c_int * (Q + 2))()
+    P1 = 1 + int(sum(int(c) * int(v) for c, v in zip(ds.z.c, ds.z.v))) + int(Mfull)  # nh[p] (DataFrame.cu:77-89)
+    beta = np.zeros(P1 * J)
+    phi = np.zeros(J)
+    P1r = lib().ref_de_bfs(paths["Y"].encode(), paths["Z"].encode(), paths["ls"].encode(), Q, int(Mredc), int(Mfull),
+                           *[_ptr(a) for a in arr], int(jtr_max), _ptr(BFs), sweeps, _ptr(beta), _ptr(phi))
+    if P1r < 0:
+        raise IOError("reference could not open its input files")
+    return BFs.reshape(Q + 2, J).T.copy(), list(sweeps), beta[:P1r * J].reshape(J, P1r).T.copy(), phi

@@ -130,15 +130,73 @@ def make_case(name: str, spec: dict) -> dict:
     return out
 
 
+# The DE driver's model comparison (ggplvm_de.cu:886-1207) at parameters from a short
+# reference fit: Mfull = the fit's M, Mredc reduced inducing points, budgets of 3 sweeps per
+# model and of the driver's own 1000. "de_icpt" has no design variables (the null model is
+# the intercept alone, whose first cell the reference's loader sets to 199.0).
+DE_CASES = {
+    "de_c1": dict(config=1, seed=5, N=300, G=24, M=8, Q=3, Mredc=4),
+    "de_icpt": dict(config=0, seed=6, N=250, G=20, M=6, Q=2, Mredc=3, no_vars=True),
+}
+
+
+def make_de_case(name: str, spec: dict) -> dict:
+    from gaspacho2_b200.formats import Design
+
+    kw = dict(spec)
+    cfg, seed, Mredc = kw.pop("config"), kw.pop("seed"), kw.pop("Mredc")
+    no_vars = kw.pop("no_vars", False)
+    ds = synth.make(cfg, seed, **kw)
+    if no_vars:
+        ds.z = Design(ds.N, np.zeros(0, np.int32), np.zeros(0, np.int32), [])
+        p = 2
+        ds.init.delta = ds.init.delta[[0, -1]].copy()
+        assert ds.init.delta.shape[0] == p
+    m = refcpu.RefModel.from_dataset(ds)
+    m.set_params(ds.init)
+    m.kernel_mats()
+    m.glm_init()
+    m.fit(1, 6)
+    prm = type(ds.init)(*(m.get(k).copy() for k in ("Omega", "delta", "X", "T", "rho", "phi")))
+    prm.X = prm.X.reshape(ds.Q, ds.N).T.copy()
+    prm.T = prm.T.reshape(ds.Q, ds.M).T.copy()
+    m.close()
+    out = {
+        "in_N": np.array(ds.y.N), "in_J": np.array(ds.y.J), "in_M": np.array(ds.M), "in_Q": np.array(ds.Q),
+        "in_y_i": ds.y.i, "in_y_p": ds.y.p, "in_y_x": ds.y.x, "in_z_c": ds.z.c, "in_z_v": ds.z.v,
+        "in_z_body": np.frombuffer(ds.z.body_bytes(), np.uint8), "in_ls": ds.ls, "in_X0": ds.X0,
+        "in_Mredc": np.array(Mredc),
+    }
+    for k, a in zip(("Omega", "delta", "X", "T", "rho", "phi"), prm.flat()):
+        out["in_init_" + k] = a
+    for tag, jt in (("j3", 3), ("conv", 1000)):
+        bfs, sweeps, beta, phi = refcpu.de_bfs(ds, prm, Mredc, ds.M, jt)
+        out[f"de_{tag}_BFs"] = bfs
+        out[f"de_{tag}_sweeps"] = np.array(sweeps)
+        out[f"de_{tag}_phi"] = phi
+        out[f"de_{tag}_beta_full"] = beta
+    return out
+
+
 def main():
     if not refcpu.available():
         raise SystemExit("build the reference first: make -C oracle ref")
+    only = set(sys.argv[1:])
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         out = make_case(name, spec)
         path = os.path.join(OUT, f"{name}.npz")
         np.savez_compressed(path, **out)
         print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, irls sweeps {int(out['irls_n'])}, "
               f"fit {out['fit_stats'].tolist()}")
+    for name, spec in DE_CASES.items():
+        if only and name not in only:
+            continue
+        out = make_de_case(name, spec)
+        path = os.path.join(OUT, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, DE sweeps {out['de_conv_sweeps'].tolist()}")
 
 
 if __name__ == "__main__":

@@ -8,6 +8,7 @@ from gaspacho2_b200.formats import Counts, Design, Params
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ("c0_small", "c2_cats", "edges")
+DE_CASES = ("de_c1", "de_icpt")  # the DE driver's model comparison (make_golden.make_de_case)
 
 
 @dataclasses.dataclass
