@@ -57,6 +57,7 @@ struct PairState {
   int smem_gram = 0, smem_v = 0, smem_vu = 0;
   int2* pairs = nullptr;
   double *rOm = nullptr, *Sp = nullptr, *V = nullptr;
+  double* Gacc = nullptr;  // pairs x genes Gram accumulator when the cells need several ranges
 };
 
 struct TcState {

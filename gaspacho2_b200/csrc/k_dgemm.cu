@@ -3,13 +3,15 @@
 // model columns, which turns the per-gene P x P products into two plain GEMMs and uses the
 // symmetry of Psi_j and Psi_j^{-1} to halve the work.
 //
-//   k_pair_gram   G[p, j] = sum_i (D_ia D_ib / Omega_i) W_ij, written straight into Psi_j
-//                 (both triangles, plus DeltaInv) at model columns (dcol a, dcol b): the dense
-//                 block of getPsi (ggplvm.cu:621-680). M = pairs, N = genes, K = cells.
-//                 The weights, the dense columns and 1/Omega of every 16-cell slice arrive by
-//                 cp.async (three stages); the pair products are formed from them in shared
-//                 memory one slice ahead of the MMAs.
-//                 Work: N*J*n_d*(n_d+1) flops.
+//   k_pair_products  A[i, p] = D_ia D_ib / Omega_i for a range of cells, row-major with the
+//                 pairs contiguous (the layout of V): the Gram's K-major A operand, written once
+//                 per range (N * pairs doubles in all; a few ms of HBM writes per Gram).
+//   k_pair_gram   G[p, j] = sum_i A[i, p] W_ij over a range of cells (M = pairs, N = genes,
+//                 K = cells), both operands by cp.async (three stages, one barrier per slice),
+//                 written straight into Psi_j (both triangles, plus DeltaInv) at model columns
+//                 (dcol a, dcol b) when one range covers all cells: the dense block of getPsi
+//                 (ggplvm.cu:621-680); otherwise added up range by range in a pairs x genes
+//                 buffer that k_pair_scatter moves into Psi. Work: N*J*n_d*(n_d+1) flops.
 //   k_pair_v      V[i, p] = (1/Omega_i) sum_j W_ij S_j[a, b] for a cell range, S_j = Psi_j^{-1}
 //                 gathered per pair (k_gather_spair). M = cells, N = pairs, K = genes; both
 //                 operands by cp.async. Work: N*J*n_d*(n_d+1) flops.
@@ -22,6 +24,7 @@
 // c0,c1 = C[g][2t, 2t+1], c2,c3 = C[g+8][2t, 2t+1]. Shared rows are padded so that the
 // 16 lanes of each half-warp hit 16 distinct 8-byte bank pairs.
 #include <algorithm>
+#include <cstdlib>
 
 #include "dmma_common.cuh"
 #include "gpl_internal.cuh"
@@ -33,7 +36,6 @@ constexpr int BM = 128, BN = 128, BK = 16;
 constexpr int SA = BM + 4;   // As[k][m]
 constexpr int SBT = BK + 4;  // Bs[n][k] (weights, k contiguous)
 constexpr int SBN = BN + 4;  // Bs[k][n] (S pairs, n contiguous)
-constexpr int SD = BK + 2;   // Ds[col][k] (dense columns of a slice, k contiguous, 16-byte rows)
 constexpr int kThreads = 256;
 }  // namespace
 
@@ -65,62 +67,79 @@ __device__ __forceinline__ void warp_slice(const double* __restrict__ As, const 
 // ---------------------------------------------------------------------------------------------
 // Gram over the dense column pairs
 // ---------------------------------------------------------------------------------------------
+// A[(i - c0) * pairs_pad + p] for cells [c0, c1): 8 cells per block, their dense-column
+// values and 1/Omega staged in shared memory, stores along the pairs (coalesced). Padding
+// pairs and cells past N (1/Omega = 0 there) give 0.
+constexpr int kProdCells = 8;
+
+__global__ void __launch_bounds__(256) k_pair_products(int ldN, int n_d, int c0, int c1, int n_pairs, int pairs_pad,
+                                                       const int2* __restrict__ pairs, const double* __restrict__ D,
+                                                       const double* __restrict__ rOm, double* __restrict__ A) {
+  extern __shared__ double dsh[];  // [n_d][kProdCells] then rOm[kProdCells]
+  const int i0 = c0 + blockIdx.x * kProdCells;
+  const int nc = min(kProdCells, c1 - i0);
+  for (int e = threadIdx.x; e < n_d * kProdCells; e += blockDim.x) {
+    const int a = e / kProdCells, r = e - a * kProdCells;
+    dsh[e] = r < nc ? D[(size_t)a * ldN + i0 + r] : 0.0;
+  }
+  if (threadIdx.x < kProdCells) dsh[n_d * kProdCells + threadIdx.x] = threadIdx.x < nc ? rOm[i0 + threadIdx.x] : 0.0;
+  __syncthreads();
+  const double* ro = dsh + n_d * kProdCells;
+  for (int p = threadIdx.x; p < pairs_pad; p += blockDim.x) {
+    double v[kProdCells];
+    if (p < n_pairs) {
+      const int2 q = pairs[p];
+      const double* da = dsh + q.x * kProdCells;
+      const double* db = dsh + q.y * kProdCells;
+#pragma unroll
+      for (int r = 0; r < kProdCells; r++) v[r] = da[r] * db[r] * ro[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < kProdCells; r++) v[r] = 0.0;
+    }
+    for (int r = 0; r < nc; r++) A[(size_t)(i0 - c0 + r) * pairs_pad + p] = v[r];
+  }
+}
+
+// epilogue modes of k_pair_gram
+constexpr int kGramPsi = 0;  // one range: Psi_j[mk, ml] = Psi_j[ml, mk] = G + DeltaInv
+constexpr int kGramSet = 1;  // first of several ranges: Gacc[p * J + j] = G
+constexpr int kGramAdd = 2;  // later ranges: Gacc[p * J + j] += G
+
 __global__ void __launch_bounds__(kThreads, 1)
-    k_pair_gram(int N, int ldN, int J, int P, int n_d, const double* __restrict__ D, const int2* __restrict__ pairs,
-                int n_pairs, const int* __restrict__ dcol, const double* __restrict__ rOm,
-                const double* __restrict__ W, const double* __restrict__ Dinv, double* __restrict__ Psi) {
+    k_pair_gram(int N, int ldN, int J, int P, int c0, int c1, int pairs_pad, int n_pairs, int mode,
+                const double* __restrict__ A, const int2* __restrict__ pairs, const int* __restrict__ dcol,
+                const double* __restrict__ W, const double* __restrict__ Dinv, double* __restrict__ Psi,
+                double* __restrict__ Gacc) {
   extern __shared__ __align__(16) double smem_d[];
-  double* As = smem_d;                          // [2][BK][SA]   pair products
-  double* Bs = As + 2 * BK * SA;                // [3][BN][SBT]  weights
-  double* Rs = Bs + 3 * BN * SBT;               // [3][BK]       1/Omega
-  double* Ds = Rs + 3 * BK;                     // [3][n_d][SD]  dense columns
+  double* As = smem_d;              // [3][BK][SA]   pair products (pairs contiguous)
+  double* Bs = As + 3 * BK * SA;    // [3][BN][SBT]  weights (cells contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
   const int p0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
-  const int nsl = (N + BK - 1) / BK;
+  const int nsl = (c1 - c0 + BK - 1) / BK;
 
-  // producer role for the A slice: pair m, cells [8h, 8h + 8) of the slice
-  const int pm = tid & (BM - 1), ph = tid >> 7;
-  const int2 ab = (p0 + pm < n_pairs) ? pairs[p0 + pm] : make_int2(-1, -1);
-
-  // slice s of the weights (cp.async 16 B), the dense columns and 1/Omega (8 B) into stage st
+  // slice s: cells [c0 + 16 s, c0 + 16 s + 16) of both operands (16-byte copies; rows of A
+  // past the range and weights past N arrive as zeros)
   auto load = [&](int s, int st) {
-    const int i0 = s * BK;
+    const int kb = s * BK;
+#pragma unroll
+    for (int r = 0; r < (BM * BK / 2) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int k = ch >> 6, part = ch & 63;
+      const int row = kb + k;
+      const int nb = (c0 + row < c1) ? 16 : 0;
+      const double* src = A + (size_t)min(row, c1 - c0 - 1) * pairs_pad + p0 + part * 2;
+      cp_async16(As + st * BK * SA + k * SA + part * 2, src, nb);
+    }
 #pragma unroll
     for (int r = 0; r < (BN * BK / 2) / kThreads; r++) {
       const int ch = tid + r * kThreads;
       const int n = ch >> 3, part = ch & 7;
-      const int j = j0 + n, i = i0 + part * 2;
-      const int nb = (j < J) ? 8 * max(0, min(2, N - i)) : 0;
+      const int j = j0 + n, i = c0 + kb + part * 2;
+      const int nb = (j < J) ? 8 * max(0, min(2, min(N, c1) - i)) : 0;
       const double* src = W + (size_t)min(j, J - 1) * ldN + min(i, ldN - 2);
       cp_async16(Bs + st * BN * SBT + n * SBT + part * 2, src, nb);
-    }
-    for (int e = tid; e < (BK / 2) * n_d; e += kThreads) {  // 16-byte chunks: 2 cells of a column
-      const int col = e / (BK / 2), part = e - col * (BK / 2);
-      const int i = i0 + part * 2;
-      const int nb = 8 * max(0, min(2, N - i));
-      cp_async16(Ds + (size_t)st * n_d * SD + col * SD + part * 2, D + (size_t)col * ldN + min(i, ldN - 2), nb);
-    }
-    if (tid < BK) {
-      const int i = i0 + tid;
-      cp_async8(Rs + st * BK + tid, rOm + min(i, ldN - 1), i < N ? 8 : 0);
-    }
-  };
-  auto fill_a = [&](int st, int buf) {
-    const double* r = Rs + st * BK + ph * 8;
-    double* dst = As + buf * BK * SA + (ph * 8) * SA + pm;
-    if (ab.x < 0) {
-#pragma unroll
-      for (int k = 0; k < 8; k++) dst[k * SA] = 0.0;
-      return;
-    }
-    const double2* da = reinterpret_cast<const double2*>(Ds + (size_t)st * n_d * SD + ab.x * SD + ph * 8);
-    const double2* db = reinterpret_cast<const double2*>(Ds + (size_t)st * n_d * SD + ab.y * SD + ph * 8);
-#pragma unroll
-    for (int k2 = 0; k2 < 4; k2++) {
-      const double2 x = da[k2], y = db[k2];
-      dst[(2 * k2) * SA] = x.x * y.x * r[2 * k2];
-      dst[(2 * k2 + 1) * SA] = x.y * y.y * r[2 * k2 + 1];
     }
   };
 
@@ -132,49 +151,68 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
 
-  // One barrier per slice. At the top of iteration s: slice s + 1 has landed (its copies were
-  // issued one iteration earlier) and, after the barrier, every warp is done with iteration
-  // s - 1, so stage (s + 2) % 3 and pair-product buffer (s + 1) & 1 are free. The products of
-  // slice s + 1 are formed after this warp's MMAs of slice s are issued, overlapping them.
+  // three stages, one barrier per slice (as k_pair_v)
   load(0, 0);
   cp_async_commit();
   if (nsl > 1) load(1, 1);
   cp_async_commit();
-  cp_async_wait<1>();
-  __syncthreads();
-  fill_a(0, 0);
   for (int s = 0; s < nsl; s++) {
-    cp_async_wait<0>();  // slice s + 1 landed
+    cp_async_wait<1>();  // slice s landed
     __syncthreads();
     if (s + 2 < nsl) load(s + 2, (s + 2) % 3);
     cp_async_commit();
-    warp_slice<true>(As + (s & 1) * BK * SA, Bs + (s % 3) * BN * SBT, wm, wn, g, t, acc);
-    if (s + 1 < nsl) fill_a((s + 1) % 3, (s + 1) & 1);
+    warp_slice<true>(As + (s % 3) * BK * SA, Bs + (s % 3) * BN * SBT, wm, wn, g, t, acc);
   }
   cp_async_wait<0>();
 
-  // epilogue: both triangles of Psi_j plus DeltaInv
 #pragma unroll
   for (int mt = 0; mt < 4; mt++)
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const int p = p0 + wm * 64 + mt * 16 + g + h * 8;
       if (p >= n_pairs) continue;
-      const int2 q = pairs[p];
-      const size_t mk = dcol[q.x], ml = dcol[q.y];
-      const double dv = Dinv[mk + ml * P];
+      size_t mk = 0, ml = 0;
+      double dv = 0.0;
+      if (mode == kGramPsi) {
+        const int2 q = pairs[p];
+        mk = dcol[q.x];
+        ml = dcol[q.y];
+        dv = Dinv[mk + ml * P];
+      }
 #pragma unroll
       for (int nt = 0; nt < 4; nt++)
 #pragma unroll
         for (int e = 0; e < 2; e++) {
           const int j = j0 + wn * 32 + nt * 8 + 2 * t + e;
           if (j >= J) continue;
-          double* Pj = Psi + (size_t)j * P * P;
-          const double v = acc[mt][nt][h * 2 + e] + dv;
-          Pj[mk + ml * P] = v;
-          Pj[ml + mk * P] = v;
+          const double v = acc[mt][nt][h * 2 + e];
+          if (mode == kGramPsi) {
+            double* Pj = Psi + (size_t)j * P * P;
+            Pj[mk + ml * P] = v + dv;
+            Pj[ml + mk * P] = v + dv;
+          } else if (mode == kGramSet) {
+            Gacc[(size_t)p * J + j] = v;
+          } else {
+            Gacc[(size_t)p * J + j] += v;
+          }
         }
     }
+}
+
+// Psi_j[mk, ml] = Psi_j[ml, mk] = Gacc[p * J + j] + DeltaInv[mk, ml] after several ranges
+__global__ void k_pair_scatter(int J, int P, int n_pairs, const int2* __restrict__ pairs,
+                               const int* __restrict__ dcol, const double* __restrict__ Gacc,
+                               const double* __restrict__ Dinv, double* __restrict__ Psi) {
+  const int p = blockIdx.x;
+  const int2 q = pairs[p];
+  const size_t mk = dcol[q.x], ml = dcol[q.y];
+  const double dv = Dinv[mk + ml * P];
+  for (int j = threadIdx.x; j < J; j += blockDim.x) {
+    const double v = Gacc[(size_t)p * J + j] + dv;
+    double* Pj = Psi + (size_t)j * P * P;
+    Pj[mk + ml * P] = v;
+    Pj[ml + mk * P] = v;
+  }
 }
 
 __global__ void k_recip_omega(int N, int cpad, const double* __restrict__ Omega, double* __restrict__ rOm) {
@@ -309,9 +347,16 @@ int pair_prepare(Ctx* c) {
   s.n_pairs = (int)pairs.size();
   s.pairs_pad = (s.n_pairs + BN - 1) / BN * BN;
   s.cpad = (c->N + BM - 1) / BM * BM;
-  // V holds a range of cells at a time: at most 2 GiB or all cells
+  // V (the gradient's V rows, or the Gram's pair products) holds a range of cells at a time:
+  // all cells when that fits in 8 GiB (one range: the Gram writes Psi directly), else ranges
+  // of at most 8 GiB. GPL_PAIR_RANGE_CELLS sets a smaller range (tests of the multi-range path).
   const size_t row = (size_t)s.pairs_pad * sizeof(double);
-  s.v_cells = (int)std::min<size_t>((size_t)s.cpad, std::max<size_t>(BM, ((size_t)2 << 30) / row / BM * BM));
+  size_t cap = std::max<size_t>(BM, ((size_t)8 << 30) / row / BM * BM);
+  if (const char* e = getenv("GPL_PAIR_RANGE_CELLS")) {
+    const long v = atol(e);
+    if (v >= BM) cap = std::min<size_t>(cap, (size_t)v / BM * BM);
+  }
+  s.v_cells = (int)std::min<size_t>((size_t)s.cpad, cap);
   if (cudaMalloc((void**)&s.pairs, sizeof(int2) * pairs.size()) != cudaSuccess ||
       cudaMalloc((void**)&s.rOm, sizeof(double) * s.cpad) != cudaSuccess ||
       cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess ||
@@ -321,7 +366,13 @@ int pair_prepare(Ctx* c) {
     return GPL_ERR_ALLOC;
   }
   GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  s.smem_gram = (int)sizeof(double) * (2 * BK * SA + 3 * BN * SBT + 3 * BK + 3 * n_d * SD);
+  if (s.v_cells < c->N &&
+      cudaMalloc((void**)&s.Gacc, sizeof(double) * (size_t)s.n_pairs * c->J) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "device allocation failed: pair Gram accumulator";
+    return GPL_ERR_ALLOC;
+  }
+  s.smem_gram = (int)sizeof(double) * 3 * (BK * SA + BN * SBT);
   s.smem_v = (int)sizeof(double) * 3 * (BK * SA + BK * SBN);
   s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
   if (s.smem_vu > 200 * 1024) {
@@ -337,7 +388,7 @@ int pair_prepare(Ctx* c) {
 
 void pair_release(Ctx* c) {
   PairState& s = c->pr;
-  void* bufs[] = {s.pairs, s.rOm, s.Sp, s.V};
+  void* bufs[] = {s.pairs, s.rOm, s.Sp, s.V, s.Gacc};
   for (void* p : bufs)
     if (p) cudaFree(p);
   s = PairState();
@@ -366,10 +417,25 @@ int launch_pair_gram(Ctx* c) {
   PairState& s = c->pr;
   if ((rc = launch_recip(c))) return rc;
   ProfScope ps(c, "gram");
-  dim3 g(div_up(s.n_pairs, BM), div_up(c->J, BN));
-  k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c->n_d, c->Dm, s.pairs, s.n_pairs,
-                                                      c->dcol_d, s.rOm, c->W, c->DeltaInv, c->Psi);
-  GPL_LAUNCHED(c, "k_pair_gram");
+  const bool one = s.v_cells >= c->N;
+  for (int c0 = 0; c0 < c->N; c0 += s.v_cells) {
+    const int c1 = std::min(c->N, c0 + s.v_cells);
+    const int smem_p = (int)sizeof(double) * (c->n_d + 1) * kProdCells;
+    k_pair_products<<<div_up(c1 - c0, kProdCells), 256, smem_p, c->stream>>>(
+        c->ldN, c->n_d, c0, c1, s.n_pairs, s.pairs_pad, s.pairs, c->Dm, s.rOm, s.V);
+    GPL_LAUNCHED(c, "k_pair_products");
+    const int mode = one ? kGramPsi : (c0 == 0 ? kGramSet : kGramAdd);
+    dim3 g(div_up(s.n_pairs, BM), div_up(c->J, BN));
+    k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c0, c1, s.pairs_pad, s.n_pairs,
+                                                        mode, s.V, s.pairs, c->dcol_d, c->W, c->DeltaInv, c->Psi,
+                                                        s.Gacc);
+    GPL_LAUNCHED(c, "k_pair_gram");
+  }
+  if (!one) {
+    k_pair_scatter<<<s.n_pairs, 256, 0, c->stream>>>(c->J, c->P, s.n_pairs, s.pairs, c->dcol_d, s.Gacc,
+                                                    c->DeltaInv, c->Psi);
+    GPL_LAUNCHED(c, "k_pair_scatter");
+  }
   return GPL_OK;
 }
 

@@ -146,3 +146,31 @@ def test_against_oracle_synthetic(cfg, kw):
         if not e <= tol:
             bad.append(f"{k}: {e:.2e} > {tol:.2e}")
     assert not bad, "; ".join(bad)
+
+
+def test_gram_over_cell_ranges():
+    """The Gram over several cell ranges (pair products of one range at a time, partial Grams
+    added in a pairs x genes buffer, then scattered into Psi) against the one-range form: the
+    same products, summed in a different grouping."""
+    import os
+
+    from gaspacho2_b200 import synth
+
+    ds = synth.make(2, 7, N=3000, G=150, M=24, Q=4)
+    psi = []
+    for cells in (None, "640"):
+        if cells:
+            os.environ["GPL_PAIR_RANGE_CELLS"] = cells
+        try:
+            with GPLVM.from_dataset(ds) as m:
+                m.set_params(ds.init)
+                m.kernel_mats()
+                m.glm_init()
+                m.irls_sweep(0, 0)
+                m.gram()
+                psi.append(m.get("Psi").copy())
+        finally:
+            os.environ.pop("GPL_PAIR_RANGE_CELLS", None)
+    e = gu.rel_err(psi[1], psi[0])
+    print(f"Psi over 5 ranges vs one range: {e:.2e}")
+    assert e <= 1e-13
