@@ -304,10 +304,8 @@ def de_leg(args, ds, stream, device):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the dominant FP64
 # kernel, from a single-pass ncu capture of this bench's own command at the full workload (the
-# metric is not available inside the timed run): k_pair_gram at config 2 read 18.16 GB and wrote
-# 1.51 GB per launch, against 9.5 GB of algorithmic operand bytes (W 8.0 GB, the dense columns
-# 0.1 GB, both triangles of the Psi dense blocks 1.4 GB): W is read about 2.2 times.
-TRAFFIC_BYTES = {("gram", 2, 100000, 10000, 128, 10): 18.16e9 + 1.51e9}
+# metric is not available inside the timed run). Entries are added per kernel version.
+TRAFFIC_BYTES = {}
 
 
 def measured_traffic(kernel, ds, args):
