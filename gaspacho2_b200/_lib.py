@@ -52,6 +52,7 @@ SIGNATURES = {
     "gpl_fit_outer": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int]),
     "gpl_score_stats": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
     "gpl_de_model": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gpl_vc_fit": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int, _ip]),
     "gpl_de_irls": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _dp, _ip, _dp, ctypes.c_int]),
     "gpl_ta_equispaced": (None, [ctypes.c_int, ctypes.c_int, _dp]),
     "gpl_evaluate": (ctypes.c_int, [_vp, _dp, ctypes.c_int64, _dp, _dp]),

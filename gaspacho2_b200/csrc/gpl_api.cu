@@ -301,6 +301,129 @@ static int de_irls(Ctx* c, int jtr_max, double tol, int* n_sweeps, double* trace
   return GPL_OK;
 }
 
+// ---- the variance-component driver (ggplvm_delta.cu) ------------------------------------------
+// Host state of its one-variable L-BFGS (LBFGS, Downdate: ggplvm_delta.cu:707-782): the step
+// history S, the gradient-change history Y (10 slots), the current step and the backup of
+// delta[p-2].
+struct VcLbfgs {
+  double S[10] = {0}, Y[10] = {0}, ss = 0.0, g0 = 0.0, backup = 0.0;
+};
+
+// lbfgs (util_cuda.cu:187-232) for one variable: the two-loop recursion over the history, the
+// initial scaling s.y / y.y, the clamp to [-1, 1] and the sign flip.
+static double lbfgs_scalar(const VcLbfgs& h, double g, int itr) {
+  const int m = 10, pt = (itr - 1) % m, lo = itr > m ? pt - m + 1 : 0;
+  double a[10], q = g;
+  for (int i = pt; i >= lo; i--) {
+    const int ii = (i + m) % m;
+    a[ii] = (0.0 + h.S[ii] * q) / (0.0 + h.S[ii] * h.Y[ii]);
+    q -= a[ii] * h.Y[ii];
+  }
+  double z = (0.0 + h.S[pt] * h.Y[pt]) / (0.0 + h.Y[pt] * h.Y[pt]) * q;
+  for (int i = lo; i <= pt; i++) {
+    const int ii = (i + m) % m;
+    z += h.S[ii] * (a[ii] - (0.0 + h.Y[ii] * z) / (0.0 + h.S[ii] * h.Y[ii]));
+  }
+  if (z > 1.0) z = 1.0;
+  if (z < (-1.0)) z = -1.0;
+  return -z;
+}
+
+static int set_delta_dg(Ctx* c, double v) {
+  GPL_TRY(c, cudaMemcpyAsync(c->delta + (c->p - 2), &v, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  return GPL_OK;
+}
+
+// The driver's loop (ggplvm_delta.cu:962-1097) from the parameters set: per outer iteration an
+// IRLS phase in the DE driver's forms (at most 30 sweeps, relative change 1e-5), the Laplace
+// objective, then L-BFGS on log delta[p-2] with the backtracking line search (at most
+// lbfgs_max steps, relative change 1e-8), and beta = tilde-beta + zeta. The gradient is only
+// the delta block (getTildeBeta, getGradLogDelta, collectGradLogDelta); the reference's
+// one-variable lbfgs reads grad[0], the gradient of log delta[0], as its current gradient
+// while its history holds delta[p-2]'s steps and gradient changes, and so does this one.
+static int vc_fit(Ctx* c, int itr_max, int lbfgs_max, double* dg, double* obj, int cap, int* n_itr) {
+  const int p = c->p, N = c->N;
+  const int64_t PP = (int64_t)c->P * c->P;
+  GPL_RUN(launch_kernel_mats(c));
+  GPL_RUN(glm_init(c));
+  GPL_RUN(launch_de_zeta(c));
+  VcLbfgs h;
+  double dgv = 0.0;
+  GPL_TRY(c, cudaMemcpy(&dgv, c->delta + (p - 2), sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<double> l((size_t)lbfgs_max + 2, 0.0);
+  int itr;
+  for (itr = 0; itr < itr_max; itr++) {
+    double prev = 0.0;
+    for (int jtr = 0; jtr < 30; jtr++) {
+      GPL_RUN(launch_w_nu(c));
+      GPL_RUN(launch_gram(c, false));
+      GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, PP));
+      GPL_RUN(launch_zt_u(c, 0));
+      GPL_RUN(launch_de_beta_phi(c));
+      GPL_RUN(launch_de_zeta(c));
+      GPL_RUN(launch_lkhd_pois(c));
+      GPL_RUN(launch_collect_lkhd(c, 0, 0));
+      double cur = 0.0;
+      GPL_RUN(read_slot(c, 0, &cur));
+      if (jtr > 0 && (jtr == 29 || fabs(prev - cur) / fabs(cur) < 1e-5)) break;
+      prev = cur;
+    }
+    GPL_RUN(objective_after_irls(c, &l[0]));
+    int jtr;
+    for (jtr = 0; jtr < lbfgs_max; jtr++) {
+      GPL_RUN(launch_expand_delta(c));
+      GPL_RUN(launch_oinvt(c));
+      GPL_RUN(launch_zt_u(c, 0));
+      GPL_RUN(solve_refined(c, c->bvec, c->tBeta));
+      GPL_RUN(launch_inverse_batched(c));
+      GPL_RUN(launch_grad_delta(c));
+      double g[2];  // d/dlog delta[0] and d/dlog delta[p-2]
+      GPL_TRY(c, cudaMemcpyAsync(&g[0], c->grad + N, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      GPL_TRY(c, cudaMemcpyAsync(&g[1], c->grad + N + (p - 2), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      GPL_TRY(c, cudaStreamSynchronize(c->stream));
+      // LBFGS (ggplvm_delta.cu:734-782)
+      const int pt = (jtr - 1) % 10, ptp1 = jtr % 10;
+      if (jtr == 0) {
+        h.ss = -g[1] / 10000.0;
+        if (h.ss > 1.0) h.ss = 0.01;
+        if (h.ss < (-1.0)) h.ss = -0.01;
+      } else {
+        h.Y[pt] = g[1] - h.g0;
+        h.ss = lbfgs_scalar(h, g[0], jtr);
+      }
+      h.g0 = g[1];
+      h.backup = dgv;
+      dgv = exp(log(dgv) - h.ss);
+      h.S[ptp1] = h.ss;
+      GPL_RUN(set_delta_dg(c, dgv));
+      double sr = 1.0;
+      for (int ktr = 1; ktr < 8; ktr++) {
+        GPL_RUN(objective_launch(c, 1));
+        GPL_RUN(read_slot(c, 1, &l[jtr + 1]));
+        if (l[jtr + 1] > l[jtr] || ktr == 7) break;
+        else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
+        else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
+        // Downdate (ggplvm_delta.cu:707-731)
+        dgv = exp(log(h.backup) - sr * h.ss);
+        h.S[ptp1] = sr * h.ss;
+        GPL_RUN(set_delta_dg(c, dgv));
+      }
+      if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) {
+        jtr++;
+        break;
+      }
+    }
+    if (obj && itr < cap) obj[itr] = l[jtr];
+    GPL_RUN(launch_expand_delta(c));
+    GPL_RUN(launch_beta_from_tilde(c));
+    GPL_RUN(launch_de_zeta(c));
+    if (dg && itr < cap) dg[itr] = dgv;
+  }
+  *n_itr = itr;
+  return GPL_OK;
+}
+
 // The reference's loader leaves 199.0 in the first cell of the last design variable of a
 // design without GP (DataFrame.cu:112-113, 131): the null model sees it, the GP models do not.
 static int de_loader_value(Ctx* c, bool on) {
@@ -985,6 +1108,33 @@ int gpl_de_irls(gpl_ctx* h, int jtr_max, double tol, double* lkhds, int32_t* swe
   if (rc) return rc;
   if (lkhds) GPL_TRY(c, cudaMemcpy(lkhds, c->lkhds, sizeof(double) * c->J, cudaMemcpyDeviceToHost));
   if (sweeps) *sweeps = n;
+  return GPL_OK;
+}
+
+int gpl_vc_fit(gpl_ctx* h, int itr_max, int lbfgs_max, double* dg, double* obj, int cap, int32_t* n_itr) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (itr_max < 1 || lbfgs_max < 1 || lbfgs_max + 2 >= kLkhdSlots || c->p < 3 || ((dg || obj) && cap < 0)) {
+    c->err = "itr_max and lbfgs_max must be >= 1 and the design needs a variable besides intercept and GP";
+    return GPL_ERR_ARG;
+  }
+  const int prec = c->precision;
+  const bool de = c->de, vcf = c->vcomp;
+  const int lv = c->kernel_lv;
+  GPL_RUN(de_loader_value(c, false));
+  c->precision = GPL_PREC_FP64;
+  c->de = true;
+  c->vcomp = true;
+  c->kernel_lv = kLvAll;
+  int n = 0;
+  const int rc = vc_fit(c, itr_max, lbfgs_max, dg, obj, (dg || obj) ? cap : 0, &n);
+  c->precision = prec;
+  c->de = de;
+  c->vcomp = vcf;
+  c->kernel_lv = lv;
+  if (rc) return rc;
+  if (n_itr) *n_itr = n;
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
   return GPL_OK;
 }
 

@@ -93,6 +93,7 @@ struct Ctx {
   // the differential-expression driver's model comparison (ggplvm_de.cu)
   int kernel_lv = kLvAll;  // GP over all latent dimensions, one dimension (>= 0), or none (kLvNone)
   bool de = false;         // IRLS in the DE driver's forms (W/nu, beta/phi, zeta, per-gene likelihood)
+  bool vcomp = false;      // the variance-component driver's likelihood constants (ggplvm_delta.cu)
   double* e0 = nullptr;    // z_i . zeta per cell (DE working response)
   double* zeta = nullptr;  // the DE driver's zeta (P)
   int de_quirk_col = -1;   // dense column whose first cell holds the null model's loader value

@@ -39,6 +39,19 @@ constexpr int SBN = BN + 4;  // Bs[k][n] (S pairs, n contiguous)
 constexpr int kThreads = 256;
 }  // namespace
 
+// Grouped tile order: a 1-D grid of tm x tn output tiles in which consecutive blocks walk
+// kGroupM tile rows down one tile column before moving to the next column, so that the ~148
+// resident blocks cover a kGroupM x ~12 patch and share both operands' tiles through L2
+// (row-major order would re-read one operand from DRAM for nearly every block).
+constexpr int kGroupM = 12;
+__device__ __forceinline__ int2 grouped_tile(int id, int tm, int tn) {
+  const int per = kGroupM * tn;
+  const int grp = id / per, first = grp * kGroupM;
+  const int gm = min(tm - first, kGroupM);
+  const int r = id - grp * per;
+  return make_int2(first + r % gm, r / gm);
+}
+
 // One 16-deep K slice of the warp tile. kNT: B stored [n][k] (true) or [k][n] (false).
 template <bool kNT>
 __device__ __forceinline__ void warp_slice(const double* __restrict__ As, const double* __restrict__ Bs, int wm,
@@ -116,7 +129,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   double* Bs = As + 3 * BK * SA;    // [3][BN][SBT]  weights (cells contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
-  const int p0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+  const int2 tile = grouped_tile(blockIdx.x, (n_pairs + BM - 1) / BM, (J + BN - 1) / BN);
+  const int p0 = tile.x * BM, j0 = tile.y * BN;
   const int nsl = (c1 - c0 + BK - 1) / BK;
 
   // slice s: cells [c0 + 16 s, c0 + 16 s + 16) of both operands (16-byte copies; rows of A
@@ -245,7 +259,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   double* Bs = smem_d + 3 * BK * SA;  // [3][BK][SBN] S pairs (pairs contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
-  const int i0 = c0 + blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int2 tile = grouped_tile(blockIdx.x, (c1 - c0 + BM - 1) / BM, pairs_pad / BN);
+  const int i0 = c0 + tile.x * BM, n0 = tile.y * BN;
   const int nsl = (J + BK - 1) / BK;
 
   auto load = [&](int s, int buf) {
@@ -425,7 +440,7 @@ int launch_pair_gram(Ctx* c) {
         c->ldN, c->n_d, c0, c1, s.n_pairs, s.pairs_pad, s.pairs, c->Dm, s.rOm, s.V);
     GPL_LAUNCHED(c, "k_pair_products");
     const int mode = one ? kGramPsi : (c0 == 0 ? kGramSet : kGramAdd);
-    dim3 g(div_up(s.n_pairs, BM), div_up(c->J, BN));
+    const int g = div_up(s.n_pairs, BM) * div_up(c->J, BN);
     k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c0, c1, s.pairs_pad, s.n_pairs,
                                                         mode, s.V, s.pairs, c->dcol_d, c->W, c->DeltaInv, c->Psi,
                                                         s.Gacc);
@@ -455,7 +470,7 @@ int launch_pair_uq(Ctx* c) {
     const int c1 = std::min(c->N, c0 + s.v_cells);
     {
       ProfScope ps(c, "uq");
-      dim3 g(div_up(c1 - c0, BM), s.pairs_pad / BN);
+      const int g = div_up(c1 - c0, BM) * (s.pairs_pad / BN);
       k_pair_v<<<g, kThreads, s.smem_v, c->stream>>>(c->N, c->ldN, c->J, c0, c1, s.pairs_pad, c->W, s.Sp, s.rOm,
                                                      s.V);
       GPL_LAUNCHED(c, "k_pair_v");

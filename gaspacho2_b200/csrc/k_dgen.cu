@@ -38,6 +38,24 @@ constexpr int kSplitK = 8;
 
 }  // namespace
 
+// A loader whose element combines several loaded values (a product, a scaled value) declares
+// `Raw`, `load()` returning the loaded values and `finish()` doing the arithmetic: the kernel
+// keeps the raw values in registers until it stores the slice into shared memory, so the next
+// slice's loads stay in flight while the current slice's MMAs run. Other loaders return the
+// element itself. finish(Raw{}) is 0 (the padding outside the matrix).
+template <class L, class = void>
+struct Staged {
+  using Raw = double;
+  __device__ static Raw load(const L& l, int a, int b, int z) { return l(a, b, z); }
+  __device__ static double finish(const L&, const Raw& v) { return v; }
+};
+template <class L>
+struct Staged<L, decltype((void)sizeof(typename L::Raw))> {
+  using Raw = typename L::Raw;
+  __device__ static Raw load(const L& l, int a, int b, int z) { return l.load(a, b, z); }
+  __device__ static double finish(const L& l, const Raw& v) { return l.finish(v); }
+};
+
 // KR(z) -> [kbeg, kend); A(r, k, z); B(k, c, z); E(r, c, z, v). kFastK: the loader's K index
 // is the contiguous one in memory (threads sweep k first).
 template <class T, class LA, class LB, class KR, class Epi>
@@ -51,7 +69,10 @@ __global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr
   const int m0 = blockIdx.x * T::BM, n0 = blockIdx.y * T::BN, z = blockIdx.z;
   const int2 kk = kr(z);
   const int nsl = kk.y > kk.x ? (kk.y - kk.x + BK - 1) / BK : 0;
-  double ra[T::NA], rb[T::NB];
+  using SA_ = Staged<LA>;
+  using SB_ = Staged<LB>;
+  typename SA_::Raw ra[T::NA];
+  typename SB_::Raw rb[T::NB];
 
   auto fetch = [&](int s) {
     const int k0 = kk.x + s * BK;
@@ -60,14 +81,14 @@ __global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr
       const int e = tid + q * 256;
       int r, k;
       if (LA::kFastK) { k = e % BK; r = e / BK; } else { r = e % T::BM; k = e / T::BM; }
-      ra[q] = (m0 + r < m && k0 + k < kk.y) ? A(m0 + r, k0 + k, z) : 0.0;
+      ra[q] = (m0 + r < m && k0 + k < kk.y) ? SA_::load(A, m0 + r, k0 + k, z) : typename SA_::Raw{};
     }
 #pragma unroll
     for (int q = 0; q < T::NB; q++) {
       const int e = tid + q * 256;
       int c, k;
       if (LB::kFastK) { k = e % BK; c = e / BK; } else { c = e % T::BN; k = e / T::BN; }
-      rb[q] = (n0 + c < n && k0 + k < kk.y) ? B(k0 + k, n0 + c, z) : 0.0;
+      rb[q] = (n0 + c < n && k0 + k < kk.y) ? SB_::load(B, k0 + k, n0 + c, z) : typename SB_::Raw{};
     }
   };
   auto stash = [&](int buf) {
@@ -78,14 +99,14 @@ __global__ void __launch_bounds__(256, 1) k_dgen(int m, int n, LA A, LB B, KR kr
       const int e = tid + q * 256;
       int r, k;
       if (LA::kFastK) { k = e % BK; r = e / BK; } else { r = e % T::BM; k = e / T::BM; }
-      as[k * T::SA + r] = ra[q];
+      as[k * T::SA + r] = SA_::finish(A, ra[q]);
     }
 #pragma unroll
     for (int q = 0; q < T::NB; q++) {
       const int e = tid + q * 256;
       int c, k;
       if (LB::kFastK) { k = e % BK; c = e / BK; } else { c = e % T::BN; k = e / T::BN; }
-      bs[k * T::SB + c] = rb[q];
+      bs[k * T::SB + c] = SB_::finish(B, rb[q]);
     }
   };
 
@@ -165,19 +186,30 @@ struct LdU {  // B(k = cell, c = gene): mode 0 W u / Omega, 1 u (y0), 2 W g / Om
   static constexpr bool kFastK = true;
   const double *W, *Nu, *rOm;
   int ldN, mode;
-  __device__ double operator()(int k, int c, int) const {
+  struct Raw {
+    double w, r, u;
+  };
+  __device__ Raw load(int k, int c, int) const {
     const size_t e = (size_t)c * ldN + k;
-    return mode == 0 ? W[e] * rOm[k] * Nu[e] : mode == 1 ? Nu[e] : W[e] * rOm[k] * Nu[k];
+    if (mode == 1) return Raw{1.0, 1.0, Nu[e]};
+    return Raw{W[e], rOm[k], mode == 0 ? Nu[e] : Nu[k]};
   }
+  __device__ double finish(const Raw& v) const { return v.w * v.r * v.u; }
 };
 struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega (1/phi given)
   static constexpr bool kFastK = false;
   const double *W, *Nu, *E, *rOm, *rphi;
   int ldN;
-  __device__ double operator()(int r, int k, int) const {
+  struct Raw {
+    double w, r, u, e, f;
+  };
+  __device__ Raw load(int r, int k, int) const {
     const size_t e = (size_t)k * ldN + r;
-    const double o = W[e] * rOm[r];
-    return (o * Nu[e] - o * E[e]) * rphi[k];
+    return Raw{W[e], rOm[r], Nu[e], E[e], rphi[k]};
+  }
+  __device__ double finish(const Raw& v) const {
+    const double o = v.w * v.r;
+    return (o * v.u - o * v.e) * v.f;
   }
 };
 struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
@@ -198,11 +230,15 @@ struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) o
   const double *W, *rOm;
   const int *gcells, *gstart;
   int ldN, mode;
-  __device__ double operator()(int k, int c, int z) const {
-    if (mode == 1) return 1.0;
+  struct Raw {
+    double w, r;
+  };
+  __device__ Raw load(int k, int c, int z) const {
+    if (mode == 1) return Raw{1.0, 1.0};
     const int i = gcells[gstart[z] + k];
-    return W[(size_t)c * ldN + i] * rOm[i];
+    return Raw{W[(size_t)c * ldN + i], rOm[i]};
   }
+  __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
 struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the tile list
   static constexpr bool kFastK = false;
@@ -218,10 +254,14 @@ struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cel
   const double *W, *rOm;
   const int* cells;  // 128 slots per tile
   int ldN;
-  __device__ double operator()(int k, int c, int z) const {
+  struct Raw {
+    double w, r;
+  };
+  __device__ Raw load(int k, int c, int z) const {
     const int i = cells[(size_t)z * 128 + c];
-    return i < 0 ? 0.0 : W[(size_t)k * ldN + i] * rOm[i];
+    return i < 0 ? Raw{0.0, 0.0} : Raw{W[(size_t)k * ldN + i], rOm[i]};
   }
+  __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
 
 // ---- epilogues -------------------------------------------------------------------------------

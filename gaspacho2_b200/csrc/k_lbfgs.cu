@@ -229,9 +229,23 @@ int launch_downdate(Ctx* c, int itr, double r, int rhoflag) {
   return apply(c, itr, r, 0, rhoflag);
 }
 
+// Beta = tBeta + zeta (getBetaFromTildeBeta): zeta is 0 in the fit driver, the DE driver's
+// zeta in the variance-component driver
+__global__ void k_add_zeta(int P, int64_t n, const double* __restrict__ tB, const double* __restrict__ zeta,
+                           double* __restrict__ B) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) B[e] = tB[e] + zeta[e % P];
+}
+
 int launch_beta_from_tilde(Ctx* c) {
-  GPL_TRY(c, cudaMemcpyAsync(c->Beta, c->tBeta, sizeof(double) * (size_t)c->P * c->J, cudaMemcpyDeviceToDevice,
-                             c->stream));
+  if (!c->de) {
+    GPL_TRY(c, cudaMemcpyAsync(c->Beta, c->tBeta, sizeof(double) * (size_t)c->P * c->J, cudaMemcpyDeviceToDevice,
+                               c->stream));
+    return GPL_OK;
+  }
+  const int64_t n = (int64_t)c->P * c->J;
+  k_add_zeta<<<div_up(n, 256), 256, 0, c->stream>>>(c->P, n, c->tBeta, c->zeta, c->Beta);
+  GPL_LAUNCHED(c, "k_add_zeta");
   return GPL_OK;
 }
 

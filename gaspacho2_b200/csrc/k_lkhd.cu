@@ -9,6 +9,7 @@
 //   k_lkhd_pois   per gene: sum over matched counts of (log W - delta_GP titsias wt) y, minus sum W
 //   k_lkhd_genes  per gene: the Laplace/PQL marginal l_j
 //   k_collect     sum_j l_j - wt delta_GP sum_i Oinvt_i titsias_i - inverse-gamma prior on Omega
+//                 (and the variance-component driver's N(0, 1) priors on X and T)
 #include "gpl_internal.cuh"
 
 namespace gpl {
@@ -195,7 +196,7 @@ int launch_beta_phi(Ctx* c, int jtr) {
   return GPL_OK;
 }
 
-__global__ void __launch_bounds__(256) k_lkhd_pois(int N, int ldN, int pvars, const double* __restrict__ W,
+__global__ void __launch_bounds__(256) k_lkhd_pois(int N, int ldN, int pvars, double wt, const double* __restrict__ W,
                                                    const double* __restrict__ delta, const double* __restrict__ titsias,
                                                    const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
                                                    const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256) k_lkhd_pois(int N, int ldN, int pvars, co
   const double dgp = delta[pvars - 1];
   for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
     const int i = cell[l];
-    part += (log(Wj[i]) - dgp * titsias[i] * kWt) * cnt[l];
+    part += (log(Wj[i]) - dgp * titsias[i] * wt) * cnt[l];
   }
   const double s = block_sum(part, sh);
   if (threadIdx.x == 0) lkhds[j] = s;
@@ -217,7 +218,8 @@ __global__ void __launch_bounds__(256) k_lkhd_pois(int N, int ldN, int pvars, co
 
 int launch_lkhd_pois(Ctx* c) {
   ProfScope ps(c, "lkhd_pois");
-  k_lkhd_pois<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->W, c->delta, c->titsias, c->cell, c->gptr,
+  // the variance-component driver takes the Titsias factor at weight 1 (ggplvm_delta.cu:610-631)
+  k_lkhd_pois<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->vcomp ? 1.0 : kWt, c->W, c->delta, c->titsias, c->cell, c->gptr,
                                            c->gvalid, c->cnt, c->lkhds);
   GPL_LAUNCHED(c, "k_lkhd_pois");
   return GPL_OK;
@@ -267,29 +269,41 @@ int launch_lkhd_genes(Ctx* c) {
   return GPL_OK;
 }
 
-__global__ void __launch_bounds__(1024) k_collect(int J, int n, int ldN, int pvars, const double* __restrict__ lkhds,
+// sum_j l_j - Q-prior - wt delta_GP sum_i Oinvt_i titsias_i - sum_i (igb/Omega_i + iga log Omega_i);
+// Q-prior: N(0, 1) on X and T in dimensions 1..qp-1 (qp = 0 for none). The fit driver:
+// wt = 0.1, igb = iga = 100, qp = 0 (ggplvm.cu:788-815); the variance-component driver: wt = 0,
+// 30, 30 and qp = Q (ggplvm_delta.cu:677-704).
+__global__ void __launch_bounds__(1024) k_collect(int J, int n, int ldN, int pvars, double wt, double igb, double iga,
+                                                  int qp, int M, const double* __restrict__ X,
+                                                  const double* __restrict__ T, const double* __restrict__ lkhds,
                                                   const double* __restrict__ W, const double* __restrict__ titsias,
                                                   const double* __restrict__ Omega, const double* __restrict__ delta,
                                                   double* __restrict__ out) {
   __shared__ double sh[32];
-  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
   for (int k = threadIdx.x; k < J; k += blockDim.x) s1 += lkhds[k];
   const double* Oinvt = W + (size_t)J * ldN;
   const double dgp = delta[pvars - 1];
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    s2 += kWt * dgp * Oinvt[i] * titsias[i];
-    s3 += kIgb / Omega[i] + kIgap1 * log(Omega[i]);
+    s2 += wt * dgp * Oinvt[i] * titsias[i];
+    s3 += igb / Omega[i] + iga * log(Omega[i]);
+    for (int k = 1; k < qp; k++) s4 += X[i + (size_t)k * n] * X[i + (size_t)k * n] / 2.0;
   }
+  for (int i = threadIdx.x; i < M && qp > 1; i += blockDim.x)
+    for (int k = 1; k < qp; k++) s4 += T[i + (size_t)k * M] * T[i + (size_t)k * M] / 2.0;
   s1 = block_sum(s1, sh);
   s2 = block_sum(s2, sh);
   s3 = block_sum(s3, sh);
-  if (threadIdx.x == 0) out[0] = s1 - s2 - s3;
+  s4 = block_sum(s4, sh);
+  if (threadIdx.x == 0) out[0] = s1 - s4 - s2 - s3;
 }
 
 int launch_collect_lkhd(Ctx* c, int n_cells, int slot) {
   ProfScope ps(c, "collect");
-  k_collect<<<1, 1024, 0, c->stream>>>(c->J, n_cells, c->ldN, c->p, c->lkhds, c->W, c->titsias, c->Omega, c->delta,
-                                       c->lkhd_dev + slot);
+  const int qp = (c->vcomp && n_cells > 0) ? c->Q : 0;
+  k_collect<<<1, 1024, 0, c->stream>>>(c->J, n_cells, c->ldN, c->p, c->vcomp ? 0.0 : kWt, c->vcomp ? 30.0 : kIgb,
+                                       c->vcomp ? 30.0 : kIgap1, qp, c->M, c->X, c->T, c->lkhds, c->W, c->titsias,
+                                       c->Omega, c->delta, c->lkhd_dev + slot);
   GPL_LAUNCHED(c, "k_collect");
   return GPL_OK;
 }

@@ -172,6 +172,16 @@ class GPLVM:
                                     _d(tr) if trace_cap else None, int(trace_cap)), "gpl_de_irls")
         return lk, n.value, tr[:min(n.value, trace_cap)].copy()
 
+    def vc_fit(self, itr_max: int = 100, lbfgs_max: int = 100):
+        """The variance-component driver (ggplvm_delta.cu) from the parameters set: refits
+        delta[p-2]; returns (delta[p-2], objective) after each outer iteration."""
+        dg = np.zeros(itr_max)
+        obj = np.zeros(itr_max)
+        n = ctypes.c_int32()
+        self._c(self._L.gpl_vc_fit(self.h, int(itr_max), int(lbfgs_max), _d(dg), _d(obj), int(itr_max),
+                                   ctypes.byref(n)), "gpl_vc_fit")
+        return dg[:n.value].copy(), obj[:n.value].copy()
+
     def evaluate(self, params: np.ndarray, grad_out: Optional[np.ndarray] = None):
         """Objective and gradient at natural-scale params [Omega | delta | X | T | rho]."""
         params = np.ascontiguousarray(params, np.float64)

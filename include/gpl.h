@@ -204,6 +204,19 @@ GPL_API int gpl_de_model(gpl_ctx* ctx, int model);
 GPL_API int gpl_de_irls(gpl_ctx* ctx, int jtr_max, double tol, double* lkhds, int32_t* sweeps, double* trace,
                         int trace_cap);
 
+/* The variance-component driver (ggplvm_delta.cu:784-1097; the reference's main does not
+ * compile): refits the prior variance delta[p-2] of the design's last variable (the genotype,
+ * when Z.bin ends with it) at the parameters set, alternating IRLS phases in the DE driver's
+ * forms (at most 30 sweeps, relative change 1e-5) with L-BFGS on log delta[p-2] under the
+ * Laplace objective with N(0, 1) priors on X and T (dimensions >= 1) and an inverse-gamma
+ * (30, 30) prior on Omega, at most lbfgs_max steps per outer iteration (the reference: 100),
+ * itr_max outer iterations (the reference: 100). The reference's main reads params.bin with
+ * p - 1 deltas, sets delta[p-2] to its --init-deltaG (default 0.01) and leaves delta[p-1] at
+ * initParams' 0.3; callers that must match it set delta so. dg[itr] receives delta[p-2] and
+ * obj[itr] the objective after each outer iteration (up to cap), *n_itr the iterations run.
+ * Always FP64; the context's IRLS forms are restored afterwards. */
+GPL_API int gpl_vc_fit(gpl_ctx* ctx, int itr_max, int lbfgs_max, double* dg, double* obj, int cap, int32_t* n_itr);
+
 /* initTaEquispaced (util.c:57-71): M x Q inducing points (column-major), dim 0 equispaced on
  * (0, 2 pi), dims >= 1 on (-3, 3): the DE driver's points for the per-dimension models. */
 GPL_API void gpl_ta_equispaced(int M, int Q, double* T);

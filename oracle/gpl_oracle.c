@@ -672,12 +672,11 @@ double orc_objective(orc_ctx* o, int slot) {
 
 /* ---- gradient: ggplvm.cu:46-281, 301-376, 406-414 --------------------------------- */
 
-void orc_gradient(orc_ctx* o, double* grad_out) {
-  const int N = o->N, J = o->J, M = o->M, Q = o->Q, P = o->P, p = o->p;
+/* getTildeBeta (ggplvm.cu:406-414), getGradLogDelta (ggplvm.cu:210-253) and
+ * collectGradLogDelta (ggplvm.cu:256-281) with Titsias weight wt: d/dlog delta into out[0..p). */
+static void grad_log_delta(orc_ctx* o, double wt, double* out) {
+  const int N = o->N, J = o->J, M = o->M, P = o->P, p = o->p;
   const int g0 = o->nh[p - 1];
-  double* grad = o->grad;
-  orc_expand_delta(o);
-  oinvt(o);
   /* getTildeBeta (ggplvm.cu:406-414) */
 #pragma omp parallel
   {
@@ -727,10 +726,19 @@ void orc_gradient(orc_ctx* o, double* grad_out) {
       for (int j = 0; j < J; j++)
         for (int k = o->nh[l]; k < o->nh[l + 1]; k++) sum += o->gdtmp[k + (size_t)j * P];
       if (l == p - 1)
-        for (int i = 0; i < N; i++) sum -= WT * Oinvt[i] * o->titsias[i] * o->delta[p - 1];
-      grad[N + l] = sum;
+        for (int i = 0; i < N; i++) sum -= wt * Oinvt[i] * o->titsias[i] * o->delta[p - 1];
+      out[l] = sum;
     }
   }
+}
+
+void orc_gradient(orc_ctx* o, double* grad_out) {
+  const int N = o->N, J = o->J, M = o->M, Q = o->Q, P = o->P, p = o->p;
+  const int g0 = o->nh[p - 1];
+  double* grad = o->grad;
+  orc_expand_delta(o);
+  oinvt(o);
+  grad_log_delta(o, WT, grad + N);
   /* getGradLogOmega (ggplvm.cu:301-376): d/dlog Omega, adjoint C1, d/dX */
   {
     double* gO = grad;
@@ -1240,6 +1248,146 @@ void orc_ta_equispaced(int M, int Q, double* T) {
   for (int i = 0; i < M; i++) T[i] = ((double)(i + 1) / (double)(M + 1)) * 2.0 * 3.14159265358979;
   for (int k = 1; k < Q; k++)
     for (int i = 0; i < M; i++) T[i + (size_t)k * M] = ((double)(i + 1) / (double)(M + 1) - 0.5) * 6.0;
+}
+
+/* ---- the variance-component driver: ggplvm_delta.cu --------------------------------- */
+/* ggplvm_delta.cu re-optimises one prior variance, delta[p-2] (that of the last design
+ * variable: the genotype when Z.bin ends with it), by L-BFGS on its log, at a fit's Omega, X,
+ * T and rho, alternating with IRLS. Its IRLS uses the DE driver's forms (de_w_nu,
+ * de_beta_phi, de_zeta); the rest differs from the fit driver as restated here. */
+
+/* getLkhdPois of ggplvm_delta.cu (:610-631): the Titsias factor at weight 1. */
+static void vc_lkhd_pois(orc_ctx* o) {
+  const int N = o->N, J = o->J, p = o->p;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int j = 0; j < J; j++) {
+    const double* Wj = o->W + (size_t)j * N;
+    int l = o->gp[j], lmax = o->gp[j + 1];
+    double sum = 0.0;
+    for (int i = 0; i < N; i++) {
+      if (l < lmax && o->ci[l] == i) {
+        sum += (log(Wj[i]) - o->delta[p - 1] * o->titsias[i]) * o->cx[l] - Wj[i];
+        l++;
+      } else {
+        sum -= Wj[i];
+      }
+    }
+    o->lkhds[j] = sum;
+  }
+}
+
+/* collectLkhd of ggplvm_delta.cu (:677-704): the genes' sum, N(0, 1) priors on X and T in
+ * dimensions >= 1, the Titsias term at weight 0 and an inverse-gamma(30, 30) prior on Omega,
+ * over n cells and Q dimensions (0 and 0 in the IRLS). */
+static double vc_collect(orc_ctx* o, int n, int Q, int slot) {
+  const int J = o->J, p = o->p, M = o->M;
+  const double* Oinvt = o->W + (size_t)n * J;
+  double sum = 0.0;
+  for (int k = 0; k < J; k++) sum += o->lkhds[k];
+  for (int i = 0; i < n; i++)
+    for (int k = 1; k < Q; k++) sum -= o->X[i + (size_t)k * n] * o->X[i + (size_t)k * n] / 2.0;
+  for (int i = 0; i < M; i++)
+    for (int k = 1; k < Q; k++) sum -= o->T[i + (size_t)k * M] * o->T[i + (size_t)k * M] / 2.0;
+  for (int i = 0; i < n; i++) sum -= 0.0 * o->delta[p - 1] * Oinvt[i] * o->titsias[i];
+  for (int i = 0; i < n; i++) sum = sum - 30.0 / o->Omega[i] - 30.0 * log(o->Omega[i]);
+  o->lkhd[slot] = sum;
+  return sum;
+}
+
+/* The objective after an IRLS phase (ggplvm_delta.cu:1012-1020) and at a line-search point
+ * (:1047-1070: kernel matrices, DeltaInv, Gram and both factorisations again). */
+static double vc_objective(orc_ctx* o, int slot, int full) {
+  oinvt(o);
+  if (full) {
+    orc_kernel_mats(o);
+    orc_expand_delta(o);
+    gram_chol(o);
+  }
+  choldc(o->DeltaInv, o->P);
+  lkhd_genes(o);
+  return vc_collect(o, o->N, o->Q, slot);
+}
+
+/* LBFGS of ggplvm_delta.cu (:734-782) on the single variable log delta[p-2]: the first step is
+ * -g/10000 (clamped to +-0.01 beyond +-1); later ones run lbfgs (util_cuda.cu:187-232) with a
+ * one-element history of that variable's steps and gradient changes but with grad[0], the
+ * gradient of log delta[0], as the current gradient, as the reference does. */
+static void vc_lbfgs(orc_ctx* o, int itr) {
+  const int p = o->p, pt = (itr - 1) % 10, ptp1 = itr % 10;
+  double *grad = o->grad, *ss = o->ss;
+  if (itr == 0) {
+    ss[0] = -grad[p - 2] / 10000.0;
+    if (ss[0] > 1.0) ss[0] = 0.01;
+    if (ss[0] < (-1.0)) ss[0] = -0.01;
+    o->grad0[p - 2] = grad[p - 2];
+  } else {
+    o->XX[pt] = grad[p - 2] - o->grad0[p - 2];
+    o->grad0[p - 2] = grad[p - 2];
+    lbfgs_dir(o->SS, o->XX, grad, 1, 10, itr, ss);
+  }
+  o->delta[p - 2 + p] = o->delta[p - 2];
+  o->delta[p - 2] = exp(log(o->delta[p - 2]) - ss[0]);
+  o->SS[ptp1] = ss[0];
+}
+
+/* Downdate of ggplvm_delta.cu (:707-731): back along the step by the factor r. */
+static void vc_downdate(orc_ctx* o, int itr, double r) {
+  const int p = o->p, ptp1 = itr % 10;
+  o->delta[p - 2] = exp(log(o->delta[p - 2 + p]) - r * o->ss[0]);
+  o->SS[ptp1] = r * o->ss[0];
+}
+
+/* The driver (ggplvm_delta.cu:962-1097) from the parameters set (delta[p-2] the initial
+ * variance), under budgets: itr_max outer iterations (the reference: 100), each an IRLS phase
+ * of at most 30 sweeps (stopping at a relative change below 1e-5), the objective, and at most
+ * lbfgs_max L-BFGS steps (the reference: 100) with the backtracking line search, stopping at a
+ * relative change below 1e-8; then tilde-beta + zeta becomes beta and zeta is recomputed.
+ * dg[itr] receives delta[p-2] after each outer iteration and obj[itr] the objective after its
+ * last accepted step (up to cap). Returns the outer iterations run. */
+int orc_vc_fit(orc_ctx* o, int itr_max, int lbfgs_max, double* dg, double* obj, int cap) {
+  const int N = o->N, J = o->J, P = o->P, p = o->p;
+  orc_kernel_mats(o);
+  orc_glm_init(o);
+  de_zeta(o);
+  int itr;
+  for (itr = 0; itr < itr_max; itr++) {
+    const int JT = 30;
+    for (int jtr = 0; jtr < JT; jtr++) {
+      de_w_nu(o);
+      gram_chol(o);
+      de_beta_phi(o);
+      de_zeta(o);
+      vc_lkhd_pois(o);
+      vc_collect(o, 0, 0, jtr);
+      if (jtr > 0 && (jtr == JT - 1 || fabs(o->lkhd[jtr - 1] - o->lkhd[jtr]) / fabs(o->lkhd[jtr]) < 1e-5)) break;
+    }
+    vc_objective(o, 0, 0);
+    double* l = o->lkhd;
+    int jtr;
+    for (jtr = 0; jtr < lbfgs_max; jtr++) {
+      orc_expand_delta(o);
+      oinvt(o);
+      grad_log_delta(o, 0.0, o->grad);
+      vc_lbfgs(o, jtr);
+      double sr = 1.0;
+      for (int ktr = 1; ktr < 8; ktr++) {
+        vc_objective(o, jtr + 1, 1);
+        if (l[jtr + 1] > l[jtr] || ktr == 7) break;
+        else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
+        else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
+        vc_downdate(o, jtr, sr);
+      }
+      if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) { jtr++; break; }
+    }
+    if (obj && itr < cap) obj[itr] = l[jtr < lbfgs_max ? jtr : lbfgs_max];
+    orc_expand_delta(o);
+    for (int j = 0; j < J; j++) /* getBetaFromTildeBeta (ggplvm_delta.cu:380-389) */
+      for (int k = 0; k < P; k++) o->Beta[k + (size_t)j * P] = o->tBeta[k + (size_t)j * P] + o->zeta[k];
+    de_zeta(o);
+    if (dg && itr < cap) dg[itr] = o->delta[p - 2];
+  }
+  (void)N;
+  return itr;
 }
 
 long orc_get(orc_ctx* o, const char* name, double* out) {

@@ -52,6 +52,8 @@ void orc_score_stats(orc_ctx* o, int L, const double* G, double* S); /* getScore
 void orc_kernel_mats_lv(orc_ctx* o, int q);
 int orc_de_irls(orc_ctx* o, int jtr_max, double tol);
 void orc_ta_equispaced(int M, int Q, double* T);
+/* the variance-component driver (ggplvm_delta.cu): L-BFGS on log delta[p-2] with IRLS phases */
+int orc_vc_fit(orc_ctx* o, int itr_max, int lbfgs_max, double* dg, double* obj, int cap);
 void orc_set_threads(int n);
 
 #ifdef __cplusplus

@@ -61,6 +61,8 @@ def lib():
         L.orc_de_irls.restype = ctypes.c_int
         L.orc_de_irls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.orc_ta_equispaced.argtypes = [ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_vc_fit.restype = ctypes.c_int
+        L.orc_vc_fit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -226,3 +228,28 @@ def de_bfs(ds, prm, Mredc: int, Mfull: int, jtr_max: int = 1000):
     n, BFs[:, Q + 1], beta = run(Mfull, np.asarray(prm.T), delta, -1, 1e-8)
     sweeps.append(n)
     return BFs, sweeps, beta, phi
+
+
+def vc_fit(ds, prm, init_dg: float = 0.01, itr_max: int = 100, lbfgs_max: int = 100):
+    """The variance-component driver (ggplvm_delta.cu:784-1097) on the oracle. ``ds`` holds the
+    design with the extra variable last (its variance is refitted); ``prm`` the fit's Omega,
+    X, T, rho and its p - 1 deltas (without the extra variable), as the driver reads them from
+    params.bin. delta[p-2] starts at init_dg and delta[p-1] keeps initParams' value, as the
+    driver leaves them. Returns (delta[p-2] after each outer iteration, the objective after
+    each outer iteration)."""
+    m = OracleModel(ds.y, ds.z, ds.ls, prm.X, ds.M, ds.Q)
+    try:
+        p = m.p
+        d = m.get("delta")[:p].copy()  # initParams' values (init.cu:27-48)
+        dfile = np.asarray(prm.delta, np.float64)
+        d[:p - 2] = dfile[:p - 2]
+        d[p - 2] = init_dg
+        arr = [np.ascontiguousarray(np.asarray(a, np.float64).ravel(order="F")) for a in (prm.Omega, prm.X, prm.T, prm.rho)]
+        lib().orc_set_params(m.h, _dptr(arr[0]), _dptr(np.ascontiguousarray(d)), _dptr(arr[1]), _dptr(arr[2]),
+                             _dptr(arr[3]), None)
+        dg = np.zeros(itr_max)
+        obj = np.zeros(itr_max)
+        n = lib().orc_vc_fit(m.h, int(itr_max), int(lbfgs_max), _dptr(dg), _dptr(obj), int(itr_max))
+        return dg[:n].copy(), obj[:n].copy()
+    finally:
+        m.close()

@@ -84,6 +84,35 @@ void collectLkhd(int N, int J, int Q, double* Omega, double* lkhds, int itr, int
                  double* Xi, double* Ta, double* W, double* titsias, double wt, double* lkhd_d);
 }  // namespace de
 
+/* the variance-component driver's kernels (ggplvm_delta.cu), built into namespace vc */
+namespace vc {
+void getZeta(int J, int P, double* Beta, double* phi, double* zeta);
+void getBetaPhi(int J, DataFrame* Z, double* ls, double* Psi, double* Omega, double* zeta, double* Nu, double* W,
+                double* Work, double* Beta, double* phi);
+void getWForBeta(SparseMat* Y, DataFrame* Z, double* ls, double* Beta, double* zeta, double* delta, double* titsias,
+                 double* W, double* Nu);
+void getPsi(int J, DataFrame* Z, double* Omega, double* DeltaInv, double* W, double* Psi);
+void cholPsi(int J, int P, double* Psi);
+void cholDeltaInv(int P, double* DeltaInv);
+void getLkhdPois(SparseMat* Y, DataFrame* Z, double* W, double* delta, double* titsias, double* lkhds);
+void getLkhd(int J, DataFrame* Z, double* Omega, double* DeltaInv, double* phi, double* Nu, double* Psi, double* W,
+             double* Work, double* lkhds);
+void collectLkhd(int N, int J, int Q, double* Omega, double* lkhds, int itr, int jtr, DataFrame* Z, double* delta,
+                 double* Xi, double* Ta, double* W, double* titsias, double wt, double* lkhd_d);
+void getOinvt(int N, int J, double* Omega, double* W);
+void getTildeBeta(int J, DataFrame* Z, double* ls, double* Psi, double* Omega, double* Nu, double* W, double* Work,
+                  double* tBeta);
+void getGradLogDelta(int J, DataFrame* Z, double* DeltaInv, double* delta, double* K, double* Psi, double* tBeta,
+                     double* phi, double* Work, double* gradDeltaTmp);
+void collectGradLogDelta(int J, DataFrame* Z, double* delta, double* gradDeltaTmp, double* W, double* titsias,
+                         double wt, double* grad);
+void getBetaFromTildeBeta(int J, DataFrame* Z, double* tBeta, double* zeta, double* Beta);
+void LBFGS(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K, double* Xi, double* Ta, double* rho,
+           double* grad, double* grad0, double* SS, double* XX, double* ss, double* Work, int rhoflag);
+void Downdate(int itr, int Q, DataFrame* Z, double* Omega, double* delta, double* K, double* Xi, double* Ta,
+              double* rho, double* grad, double* grad0, double* SS, double* XX, double* ss, double r, int rhoflag);
+}  // namespace vc
+
 namespace {
 
 struct RefCtx {
@@ -617,6 +646,161 @@ int ref_de_bfs(const char* y_path, const char* z_path, const char* ls_path, int 
   if (beta_full) memcpy(beta_full, Beta, sizeof(double) * (size_t)P1 * J);
   if (phi_out) memcpy(phi_out, phi, sizeof(double) * J);
   return P1;
+}
+
+/* The variance-component driver (ggplvm_delta.cu:784-1097; its main does not compile in the
+ * reference because it calls a __global__ printMetaDataFrame from the host at :823): main's
+ * allocations, initialisation and loops, with the parameters given as arrays instead of the
+ * params.bin its main reads from the working directory (ggplvm_delta.cu:944-956): Omega (N),
+ * delta_file (the p - 1 values main reads), X (N x Q), T (M x Q), rho (Q). As main, delta[p-2]
+ * becomes init_dg and delta[p-1] keeps initParams' value (main copies p - 1 values to the
+ * device). Budgets: itr_max outer iterations (main: 100) and lbfgs_max L-BFGS steps per outer
+ * iteration (main: 100). dg[itr] receives delta[p-2] after each outer iteration and obj[itr]
+ * the objective after its last accepted step (up to cap). Returns the outer iterations run, or
+ * -1 on a file error. */
+int ref_vc_fit(const char* y_path, const char* z_path, const char* ls_path, int M, int Q, const double* Omega_in,
+               const double* delta_file, const double* X_in, const double* T_in, const double* rho_in, double init_dg,
+               int itr_max, int lbfgs_max, double* dg, double* obj, int cap) {
+  FILE* probe;
+  for (const char* pth : {y_path, z_path, ls_path}) {
+    if (!(probe = fopen(pth, "rb"))) return -1;
+    fclose(probe);
+  }
+  std::string yp(y_path), zp(z_path);
+  SparseMat* Y_h = loadSparseMat(&yp[0]);
+  const int N = Y_h->N, J = Y_h->J;
+  SparseMat* Y = newSparseMatOnDevice(Y_h);
+  DataFrame* Z_h = loadDataFrame(&zp[0], M);
+  DataFrame* Z = newDataFrameOnDevice(Z_h);
+  const int P = Z_h->P, p = Z_h->p;
+  const double wt = 0.0; /* ggplvm_delta.cu:20 */
+  const int JTRMAX = 1000;
+  const size_t tot = (size_t)N + p + (size_t)(N + M + 1) * Q;
+  double* Psi = dalloc((size_t)J * P * P * 2);
+  double* W = dalloc((size_t)N * (J + 1));
+  double* Nu = dalloc((size_t)N * J);
+  double* grad = dalloc(tot);
+  double* grad0 = dalloc(tot);
+  double* SS = dalloc(tot * 10);
+  double* XX = dalloc(tot * 10);
+  double* ss = dalloc(tot);
+  size_t lwork = (size_t)(N < M * M ? M * M : N) * (2 * P);
+  if ((size_t)N < (size_t)J * P) lwork = (size_t)((size_t)J * P < (size_t)M * M ? (size_t)M * M : (size_t)J * P) * (2 * P);
+  double* Work = dalloc(lwork);
+  double* IdenP = dalloc((size_t)P * P);
+  double* ls = dalloc(N);
+  double* Omega = dalloc((size_t)N * 2);
+  double* DeltaInv = dalloc((size_t)P * P);
+  double* delta = dalloc((size_t)p * 2);
+  double* phi = dalloc(J);
+  double* gradDeltaTmp = dalloc((size_t)P * J);
+  double* zeta = dalloc(P);
+  double* Beta = dalloc((size_t)P * J);
+  double* tBeta = dalloc((size_t)P * J);
+  double* lkhds = dalloc(J);
+  double* lkhd_d = dalloc(JTRMAX);
+  double* rho = dalloc((size_t)Q * 2);
+  double* Xi = dalloc((size_t)N * Q * 2);
+  double* Ta = dalloc((size_t)M * Q * 2);
+  double* K = dalloc((size_t)M * M);
+  double* Kinv = dalloc((size_t)M * M);
+  double* KinvKmn = dalloc((size_t)N * M);
+  double* titsias = dalloc(N);
+  std::vector<double> lkhd_h(JTRMAX);
+  if (!read_doubles(ls_path, ls, N)) return -1;
+
+  const dim3 gridJ(J, 1), gridJP(J, P), gridPsi(J, P), blockPsi(1, P), gridPP(P, P), gridP(P, 1), gridDel(p, 1),
+      block1(1, 1), gridNpMM(N + M, M);
+  const int sN = (int)(sqrt((double)N) / 4) + 1;
+  const dim3 gridN(sN, sN), blockN(4, 4);
+
+  ref_launch(dim3(1), block1, [&] { initParams(N, J, P, p, Q, delta, Omega, phi, rho, IdenP); });
+  /* params.bin (ggplvm_delta.cu:944-956): p - 1 deltas, delta[p-2] <- init_dg, p - 1 copied */
+  std::vector<double> delta_h(p);
+  for (int k = 0; k < p - 1; k++) delta_h[k] = delta_file[k];
+  delta_h[p - 1] = delta_h[p - 2];
+  delta_h[p - 2] = init_dg;
+  memcpy(Omega, Omega_in, sizeof(double) * N);
+  memcpy(delta, delta_h.data(), sizeof(double) * (p - 1));
+  memcpy(Xi, X_in, sizeof(double) * (size_t)N * Q);
+  memcpy(Ta, T_in, sizeof(double) * (size_t)M * Q);
+  memcpy(rho, rho_in, sizeof(double) * Q);
+
+  ref_launch(gridNpMM, block1, [&] { getKernelMats(Q, Xi, Ta, rho, Z, K, Kinv, KinvKmn); });
+  ref_launch(dim3(1), block1, [&] { cholKmm(M, Kinv); });
+  ref_launch(gridN, blockN, [&] { getKinvKmn(Kinv, Z, KinvKmn, titsias); });
+  ref_launch(dim3(1), block1, [&] { expandDelta_k(Z, delta, K, DeltaInv); });
+  ref_launch(gridPP, block1, [&] { initPsi(Z, DeltaInv, Psi); });
+  ref_launch(dim3(1), block1, [&] { initPsi2(P, Psi); });
+  ref_launch(gridJ, block1, [&] { initBeta(Y, ls, Z, Psi, Work, Beta); });
+  ref_launch(gridP, block1, [&] { vc::getZeta(J, P, Beta, phi, zeta); });
+
+  int rhoflag = 0, itr, jtr;
+  for (itr = 0; itr < itr_max; itr++) {
+    const int JT = 30;
+    for (jtr = 0; jtr < JT; jtr++) {
+      ref_launch(gridJ, block1, [&] { vc::getWForBeta(Y, Z, ls, Beta, zeta, delta, titsias, W, Nu); });
+      ref_launch(gridPsi, blockPsi, [&] { vc::getPsi(J, Z, Omega, DeltaInv, W, Psi); });
+      ref_launch(gridJ, block1, [&] { vc::cholPsi(J, P, Psi); });
+      ref_launch(gridJ, block1, [&] { vc::getBetaPhi(J, Z, ls, Psi, Omega, zeta, Nu, W, Work, Beta, phi); });
+      ref_launch(gridP, block1, [&] { vc::getZeta(J, P, Beta, phi, zeta); });
+      ref_launch(gridJ, block1, [&] { vc::getLkhdPois(Y, Z, W, delta, titsias, lkhds); });
+      ref_launch(dim3(1), block1, [&] {
+        vc::collectLkhd(0, J, 0, Omega, lkhds, itr, jtr, Z, delta, Xi, Ta, W, titsias, wt, lkhd_d);
+      });
+      lkhd_h[jtr] = lkhd_d[jtr];
+      if (jtr > 0 && (jtr == (JT - 1) || fabs(lkhd_h[jtr - 1] - lkhd_h[jtr]) / fabs(lkhd_h[jtr]) < 1e-5)) break;
+    }
+    ref_launch(gridN, blockN, [&] { vc::getOinvt(N, J, Omega, W); });
+    ref_launch(dim3(1), block1, [&] { vc::cholDeltaInv(P, DeltaInv); });
+    ref_launch(gridJ, block1, [&] { vc::getLkhd(J, Z, Omega, DeltaInv, phi, Nu, Psi, W, Work, lkhds); });
+    ref_launch(dim3(1), block1, [&] {
+      vc::collectLkhd(N, J, Q, Omega, lkhds, itr, 0, Z, delta, Xi, Ta, W, titsias, wt, lkhd_d);
+    });
+    lkhd_h[0] = lkhd_d[0];
+    if (itr > 10) rhoflag = 1;
+    for (jtr = 0; jtr < lbfgs_max; jtr++) {
+      ref_launch(dim3(1), block1, [&] { expandDelta_k(Z, delta, K, DeltaInv); });
+      ref_launch(gridN, blockN, [&] { vc::getOinvt(N, J, Omega, W); });
+      ref_launch(gridJ, block1, [&] { vc::getTildeBeta(J, Z, ls, Psi, Omega, Nu, W, Work, tBeta); });
+      ref_launch(gridJP, block1, [&] {
+        vc::getGradLogDelta(J, Z, DeltaInv, delta, K, Psi, tBeta, phi, Work, gradDeltaTmp);
+      });
+      ref_launch(gridDel, block1, [&] { vc::collectGradLogDelta(J, Z, delta, gradDeltaTmp, W, titsias, wt, grad); });
+      ref_launch(dim3(1), block1, [&] {
+        vc::LBFGS(jtr, Q, Z, Omega, delta, K, Xi, Ta, rho, grad, grad0, SS, XX, ss, Work, rhoflag);
+      });
+      double sr = 1.0;
+      for (int ktr = 1; ktr < 8; ktr++) {
+        ref_launch(gridN, blockN, [&] { vc::getOinvt(N, J, Omega, W); });
+        ref_launch(gridNpMM, block1, [&] { getKernelMats(Q, Xi, Ta, rho, Z, K, Kinv, KinvKmn); });
+        ref_launch(dim3(1), block1, [&] { expandDelta_k(Z, delta, K, DeltaInv); });
+        ref_launch(dim3(1), block1, [&] { cholKmm(M, Kinv); });
+        ref_launch(gridN, blockN, [&] { getKinvKmn(Kinv, Z, KinvKmn, titsias); });
+        ref_launch(gridPsi, blockPsi, [&] { vc::getPsi(J, Z, Omega, DeltaInv, W, Psi); });
+        ref_launch(gridJ, block1, [&] { vc::cholPsi(J, P, Psi); });
+        ref_launch(dim3(1), block1, [&] { vc::cholDeltaInv(P, DeltaInv); });
+        ref_launch(gridJ, block1, [&] { vc::getLkhd(J, Z, Omega, DeltaInv, phi, Nu, Psi, W, Work, lkhds); });
+        ref_launch(dim3(1), block1, [&] {
+          vc::collectLkhd(N, J, Q, Omega, lkhds, itr, jtr + 1, Z, delta, Xi, Ta, W, titsias, wt, lkhd_d);
+        });
+        for (int k = 0; k < jtr + 2; k++) lkhd_h[k] = lkhd_d[k];
+        if (lkhd_h[jtr + 1] > lkhd_h[jtr] || ktr == 7) break;
+        else if (std::isnan(lkhd_h[jtr + 1]) || std::isinf(lkhd_h[jtr + 1])) sr *= 0.01;
+        else if (lkhd_h[jtr + 1] < lkhd_h[jtr]) sr *= 0.1;
+        ref_launch(dim3(1), block1, [&] {
+          vc::Downdate(jtr, Q, Z, Omega, delta, K, Xi, Ta, rho, grad, grad0, SS, XX, ss, sr, rhoflag);
+        });
+      }
+      if (jtr > 0 && fabs(lkhd_h[jtr + 1] - lkhd_h[jtr]) < fabs(lkhd_h[jtr + 1]) * 1e-8) { jtr++; break; }
+    }
+    if (obj && itr < cap) obj[itr] = lkhd_h[jtr];
+    ref_launch(dim3(1), block1, [&] { expandDelta_k(Z, delta, K, DeltaInv); });
+    ref_launch(gridJ, dim3(1), [&] { vc::getBetaFromTildeBeta(J, Z, tBeta, zeta, Beta); });
+    ref_launch(gridP, block1, [&] { vc::getZeta(J, P, Beta, phi, zeta); });
+    if (dg && itr < cap) dg[itr] = delta[p - 2];
+  }
+  return itr;
 }
 
 }  // extern "C"

@@ -61,6 +61,9 @@ def lib():
         L.ref_model_meta.argtypes = [ctypes.c_void_p, _ip, _ip, _ip, _ip]
         L.ref_set_verbose.argtypes = [ctypes.c_int]
         L.ref_score_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.ref_vc_fit.restype = ctypes.c_int
+        L.ref_vc_fit.argtypes = [ctypes.c_char_p] * 3 + [ctypes.c_int] * 2 + [_dp] * 5 + [ctypes.c_double] + \
+            [ctypes.c_int] * 2 + [_dp, _dp, ctypes.c_int]
         L.ref_de_bfs.restype = ctypes.c_int
         L.ref_de_bfs.argtypes = [ctypes.c_char_p] * 3 + [ctypes.c_int] * 3 + [_dp] * 5 + [ctypes.c_int, _dp, _ip,
                                                                                         _dp, _dp]
@@ -202,3 +205,24 @@ def de_bfs(ds, prm, Mredc: int, Mfull: int, jtr_max: int = 1000, workdir: Option
     if P1r < 0:
         raise IOError("reference could not open its input files")
     return BFs.reshape(Q + 2, J).T.copy(), list(sweeps), beta[:P1r * J].reshape(J, P1r).T.copy(), phi
+
+
+def vc_fit(ds, prm, init_dg: float = 0.01, itr_max: int = 100, lbfgs_max: int = 100,
+           workdir: Optional[str] = None):
+    """The reference's own variance-component driver (ggplvm_delta.cu:784-1097, through
+    ref_vc_fit) on the dataset's files; ``prm`` as for oracle.port.vc_fit. Returns (delta[p-2]
+    after each outer iteration, the objective after each outer iteration)."""
+    from gaspacho2_b200.formats import write_dataset
+
+    wd = workdir or tempfile.mkdtemp(prefix="gpl_ref_vc_")
+    paths = write_dataset(wd, ds.y, ds.z, ds.ls, ds.X0)
+    arr = [np.ascontiguousarray(np.asarray(a, np.float64).ravel(order="F"))
+           for a in (prm.Omega, prm.delta, prm.X, prm.T, prm.rho)]
+    dg = np.zeros(itr_max)
+    obj = np.zeros(itr_max)
+    n = lib().ref_vc_fit(paths["Y"].encode(), paths["Z"].encode(), paths["ls"].encode(), int(ds.M), int(ds.Q),
+                         *[_ptr(a) for a in arr], float(init_dg), int(itr_max), int(lbfgs_max), _ptr(dg), _ptr(obj),
+                         int(itr_max))
+    if n < 0:
+        raise IOError("reference could not open its input files")
+    return dg[:n].copy(), obj[:n].copy()

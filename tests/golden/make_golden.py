@@ -178,6 +178,51 @@ def make_de_case(name: str, spec: dict) -> dict:
     return out
 
 
+# The variance-component driver (ggplvm_delta.cu:784-1097): a fit (6 L-BFGS steps of the
+# reference) of the design without its last numeric covariate, which has a real effect in
+# the counts, then that covariate's variance delta[p-2] refitted on the full design from
+# 0.01 under budgets of (3 outer iterations, 100 L-BFGS steps) and (8, 100).
+VC_CASES = {
+    "vc_c1": dict(config=1, seed=8, N=300, G=24, M=8, Q=2),
+}
+
+
+def make_vc_case(name: str, spec: dict) -> dict:
+    import dataclasses
+
+    from gaspacho2_b200.formats import Design
+
+    kw = dict(spec)
+    cfg, seed = kw.pop("config"), kw.pop("seed")
+    ds = synth.make(cfg, seed, **kw)
+    z = ds.z
+    assert z.c[-1] == 1
+    zfit = Design(z.N, z.c[:-1].copy(), z.v[:-1].copy(), list(z.columns[:-1]))
+    dfit = dataclasses.replace(ds, z=zfit, init=dataclasses.replace(ds.init, delta=ds.init.delta[1:].copy()))
+    m = refcpu.RefModel.from_dataset(dfit)
+    m.set_params(dfit.init)
+    m.kernel_mats()
+    m.glm_init()
+    m.fit(1, 6)
+    prm = type(ds.init)(*(m.get(k).copy() for k in ("Omega", "delta", "X", "T", "rho", "phi")))
+    prm.X = prm.X.reshape(ds.Q, ds.N).T.copy()
+    prm.T = prm.T.reshape(ds.Q, ds.M).T.copy()
+    m.close()
+    out = {
+        "in_N": np.array(ds.y.N), "in_J": np.array(ds.y.J), "in_M": np.array(ds.M), "in_Q": np.array(ds.Q),
+        "in_y_i": ds.y.i, "in_y_p": ds.y.p, "in_y_x": ds.y.x, "in_z_c": ds.z.c, "in_z_v": ds.z.v,
+        "in_z_body": np.frombuffer(ds.z.body_bytes(), np.uint8), "in_ls": ds.ls, "in_X0": ds.X0,
+        "in_init_dg": np.array(0.01),
+    }
+    for k, a in zip(("Omega", "delta", "X", "T", "rho", "phi"), prm.flat()):
+        out["fit_" + k] = a
+    for tag, it in (("i3", 3), ("i8", 8)):
+        dg, obj = refcpu.vc_fit(ds, prm, 0.01, it, 100)
+        out[f"vc_{tag}_dg"] = dg
+        out[f"vc_{tag}_obj"] = obj
+    return out
+
+
 def main():
     if not refcpu.available():
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -190,6 +235,13 @@ def main():
         np.savez_compressed(path, **out)
         print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, irls sweeps {int(out['irls_n'])}, "
               f"fit {out['fit_stats'].tolist()}")
+    for name, spec in VC_CASES.items():
+        if only and name not in only:
+            continue
+        out = make_vc_case(name, spec)
+        path = os.path.join(OUT, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, delta_G {out['vc_i8_dg'].tolist()}")
     for name, spec in DE_CASES.items():
         if only and name not in only:
             continue

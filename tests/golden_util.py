@@ -9,6 +9,30 @@ from gaspacho2_b200.formats import Counts, Design, Params
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ("c0_small", "c2_cats", "edges")
 DE_CASES = ("de_c1", "de_icpt")  # the DE driver's model comparison (make_golden.make_de_case)
+VC_CASES = ("vc_c1",)  # the variance-component driver (make_golden.make_vc_case)
+
+
+def load_vc(name: str):
+    """A variance-component fixture: (dataset with the full design, the fit's parameters)."""
+    g = dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+    N, J, M, Q = (int(g[k]) for k in ("in_N", "in_J", "in_M", "in_Q"))
+    y = Counts(N, J, g["in_y_i"].astype(np.int32), g["in_y_p"].astype(np.int32), g["in_y_x"])
+    c, v = g["in_z_c"].astype(np.int32), g["in_z_v"].astype(np.int32)
+    body = g["in_z_body"].tobytes()
+    cols, off = [], 0
+    for k in range(c.shape[0]):
+        nb = (8 if c[k] == 1 else 4) * N * int(v[k])
+        if c[k] == 1:
+            cols.append(np.frombuffer(body[off:off + nb], np.float64).reshape(int(v[k]), N).T.copy())
+        else:
+            cols.append(np.frombuffer(body[off:off + nb], np.int32)[:N].copy())
+        off += nb
+    z = Design(N, c, v, cols)
+    prm = Params(g["fit_Omega"], g["fit_delta"], g["fit_X"].reshape(Q, N).T.copy(), g["fit_T"].reshape(Q, M).T.copy(),
+                 g["fit_rho"], g["fit_phi"])
+    init = Params(g["fit_Omega"], np.zeros(c.shape[0] + 2), prm.X, prm.T, g["fit_rho"], g["fit_phi"])
+    ds = GoldenData(y, z, g["in_ls"], g["in_X0"].reshape(N, Q) if g["in_X0"].ndim == 1 else g["in_X0"], init, M, Q, g)
+    return ds, prm
 
 
 @dataclasses.dataclass

@@ -74,3 +74,51 @@ def test_cli_de_matches_reference(cli, tmp_path):
     assert np.allclose(np.array(beta[-gd.J:]).T, gd.g["de_j3_beta_full"], rtol=1e-6, atol=1e-5)
     knm = _rows(out / "Knm_de.gz")
     assert len(knm) == gd.Q * (gd.N + Mr) + gd.N + gd.M
+
+
+# ---- ggplvm_delta: the variance-component driver's command line (ggplvm_delta.cu:784-1097) ----
+@pytest.fixture(scope="module")
+def cli_vc():
+    gbuild.build()
+    exe = os.path.join(gbuild.PKG, "bin", "ggplvm_delta")
+    assert os.path.exists(exe), "ggplvm_delta was not built"
+    return exe
+
+
+def test_vc_usage_errors(cli_vc, tmp_path):
+    r = _run(cli_vc, [], tmp_path)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = _run(cli_vc, ["a", "b", "c", "d", "--init-deltaG", "-1"], tmp_path)
+    assert r.returncode == 2
+    r = _run(cli_vc, ["a", "b", "c", "d", "--bogus"], tmp_path)
+    assert r.returncode == 2
+
+
+def _vc_inputs(tmp_path):
+    ds, prm = gu.load_vc("vc_c1")
+    p = formats.write_dataset(str(tmp_path), ds.y, ds.z, ds.ls, ds.X0)
+    # params.bin as the driver reads it: Omega, the fit's p - 1 deltas, X, T, rho (and phi)
+    with open(tmp_path / "params.bin", "wb") as f:
+        for a in (prm.Omega, prm.delta, prm.X.ravel(order="F"), prm.T.ravel(order="F"), prm.rho, prm.phi):
+            np.asarray(a, np.float64).tofile(f)
+    return ds, p
+
+
+def test_vc_missing_params_file(cli_vc, tmp_path):
+    ds, p = _vc_inputs(tmp_path)
+    os.remove(tmp_path / "params.bin")
+    r = _run(cli_vc, [p["Y"], p["Z"], p["ls"], p["Xi"], "-M", ds.M, "-Q", ds.Q], tmp_path)
+    assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_vc_matches_reference(cli_vc, tmp_path):
+    ds, p = _vc_inputs(tmp_path)
+    r = _run(cli_vc, [p["Y"], p["Z"], p["ls"], p["Xi"], "-M", ds.M, "-Q", ds.Q, "--max-outer", 3, "--quiet"],
+             tmp_path)
+    assert r.returncode == 0, r.stderr
+    rows = [line.split() for line in r.stdout.splitlines() if line.startswith("itr=")]
+    dg = np.array([float(x[1].split("=")[1]) for x in rows])
+    obj = np.array([float(x[2].split("=")[1]) for x in rows])
+    assert np.allclose(dg, ds.g["vc_i3_dg"], rtol=1e-9, atol=0)
+    assert np.allclose(obj, ds.g["vc_i3_obj"], rtol=1e-9, atol=0)
