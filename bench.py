@@ -302,10 +302,13 @@ def de_leg(args, ds, stream, device):
     return res
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the dominant FP64
-# kernel, from a single-pass ncu capture of this bench's own command at the full workload (the
-# metric is not available inside the timed run). Entries are added per kernel version.
-TRAFFIC_BYTES = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one Gram (the pair products
+# written once, then the GEMM), from a single-pass ncu capture of this bench's own command at
+# config 2 (the metric is not available inside the timed run): k_pair_products read 0.11 GB and
+# wrote 7.00 GB, k_pair_gram read 174.40 GB and wrote 1.73 GB, against 16.6 GB of algorithmic
+# bytes (products 7.1 GB written and read once, W 8.0 GB read, Psi dense blocks 1.4 GB written):
+# the grouped tile order leaves each operand tile read from DRAM about 11 times, at 0.3 TB/s.
+TRAFFIC_BYTES = {("gram", 2, 100000, 10000, 128, 10): 0.11e9 + 7.00e9 + 174.40e9 + 1.73e9}
 
 
 def measured_traffic(kernel, ds, args):
