@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "obj+grad evals/s (100K cells x 10K genes, M=128, Q=10)"
 FALLBACK_BF16_SUSTAINED = 1400.0  # TFLOP/s, earlier measurement on this hardware pool
+FALLBACK_HBM_GBS = 6650.0  # GB/s, earlier copy measurement on this hardware pool
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -122,9 +123,15 @@ def measured_peaks():
         return {}
 
 
+_FP64_PEAK = []
+
+
 def fp64_peak_tflops(torch) -> float:
     """Dense FP64 GEMM rate on this GPU (torch.matmul float64 8192^3, best of 5), the FP64
-    counterpart of the bf16 figure in MEASURED_PEAKS.json, which has no FP64 entry."""
+    counterpart of the bf16 figure in MEASURED_PEAKS.json, which has no FP64 entry; measured
+    once per run."""
+    if _FP64_PEAK:
+        return _FP64_PEAK[0]
     n = 8192
     a = torch.randn(n, n, dtype=torch.float64, device="cuda")
     b = torch.randn(n, n, dtype=torch.float64, device="cuda")
@@ -140,7 +147,8 @@ def fp64_peak_tflops(torch) -> float:
         best = min(best, s.elapsed_time(e) / 1e3)
     del a, b
     torch.cuda.empty_cache()
-    return 2.0 * n ** 3 / best / 1e12
+    _FP64_PEAK.append(2.0 * n ** 3 / best / 1e12)
+    return _FP64_PEAK[0]
 
 
 def flops_table(N, J, M, P, n_dense):
@@ -315,6 +323,49 @@ def measured_traffic(kernel, ds, args):
     return TRAFFIC_BYTES.get((kernel, args.config, ds.N, ds.J, ds.M, ds.Q))
 
 
+def irls_leg(m, ds, args, stream, torch):
+    """IRLS sweeps (getWForBeta, getPsi, cholPsi, getBetaPhi, getLkhdPois: ggplvm.cu:1156-1181)
+    at the bench state: 3 sweeps timed with CUDA events, their phases from the library's
+    profile, and the W / nu kernel against its two bounds: the HBM bytes it must move (W and
+    nu written, the counts and dense columns read) at the measured copy bandwidth, and the
+    FP64 multiply-adds of the linear predictor (2 N J n_d) at the measured FP64 GEMM rate; the
+    larger of the two times is the bound it is measured against."""
+    m.profile(True)
+    m.profile_reset()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 3
+    s.record(stream)
+    for j in range(n):
+        m.irls_sweep(0, args.irls_sweeps + j)
+    e.record(stream)
+    torch.cuda.synchronize()
+    t = s.elapsed_time(e) / 1e3 / n
+    ph = {}
+    for name in ("w_nu", "gram", "group_sums", "assemble_psi", "chol", "zt_u", "solve", "beta_phi", "lkhd_pois",
+                 "collect"):
+        ms, k = m.profile_read(name)
+        if k:
+            ph[name] = ms / n
+    m.profile(False)
+    N, J, n_d = m.N, m.J, m.n_dense()
+    nnz = int(ds.y.L)
+    bytes_w_nu = 2.0 * 8 * N * J + 12.0 * nnz + 8.0 * N * n_d + 8.0 * N
+    flops_w_nu = 2.0 * N * J * n_d
+    hbm = (measured_peaks().get("hbm_gbs") or FALLBACK_HBM_GBS) * 1e9
+    f64 = fp64_peak_tflops(torch) * 1e12
+    t_w = ph.get("w_nu", 0.0) / 1e3
+    bound = "hbm" if bytes_w_nu / hbm >= flops_w_nu / f64 else "fp64"
+    t_bound = max(bytes_w_nu / hbm, flops_w_nu / f64)
+    return {"ms_per_sweep": t * 1e3, "phase_ms_per_sweep": ph,
+            "w_nu_roofline": {"bound": bound, "algorithmic_bytes": bytes_w_nu, "flops": flops_w_nu,
+                              "achieved_gbs": bytes_w_nu / t_w / 1e9 if t_w else None,
+                              "achieved_tflops": flops_w_nu / t_w / 1e12 if t_w else None,
+                              "frac": t_bound / t_w if t_w else None,
+                              "note": "bound = the larger of bytes / measured copy bandwidth and flops / measured "
+                                      "FP64 GEMM rate; frac = that time / the kernel's time"}}
+
+
 def precision_leg(args, ds, stream, device):
     """The precision form (tensor-core Gram and gradient contraction over whitened columns,
     FP64 elsewhere, refined solves) on the same workload and state as the FP64 line: its
@@ -473,6 +524,8 @@ def run_ours(args):
     e2e = {"value": world * args.steps / dt2, "unit": "evals/s", "h2d_bytes_per_step": int(params.nbytes),
            "d2h_bytes_per_step": int(grad.nbytes + 8)}
 
+    irls = irls_leg(m, ds, args, stream, torch) if rank == 0 else None
+
     line = None
     if rank == 0:
         total_prof = sum(v[0] for v in prof.values())
@@ -515,6 +568,7 @@ def run_ours(args):
             "gpu_launches": int(launches), "roofline": roof, "clocks": ck,
             "phase_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
             "hbm_gbs_measured": peaks.get("hbm_gbs"), "bf16_tflops_measured": peaks.get("bf16_tflops"),
+            "irls_sweep": irls,
         }
     m.close()
     if rank == 0 and args.precision == "fp64" and not args.no_precision_leg:
