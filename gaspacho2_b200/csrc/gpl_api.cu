@@ -204,11 +204,20 @@ static int objective_launch(Ctx* c, int slot) {
   return GPL_OK;
 }
 
-static int gradient_launch(Ctx* c) {
+// after_objective: the objective was just evaluated at this state (objective_launch or
+// objective_after_irls), so Oinvt is current and getTildeBeta's solve Psi_j x = Z^T diag(W/Omega)
+// nu_j (ggplvm.cu:406-414) is the one getLkhd already made with the same factor and right-hand
+// side (ggplvm.cu:744-784): tilde-beta is that solution, copied instead of solved again.
+static int gradient_launch(Ctx* c, bool after_objective = false) {
   GPL_RUN(launch_expand_delta(c));
-  GPL_RUN(launch_oinvt(c));
-  GPL_RUN(launch_zt_u(c, 0));
-  GPL_RUN(solve_refined(c, c->bvec, c->tBeta));
+  if (after_objective) {
+    GPL_TRY(c, cudaMemcpyAsync(c->tBeta, c->sol, sizeof(double) * (size_t)c->P * c->J, cudaMemcpyDeviceToDevice,
+                               c->stream));
+  } else {
+    GPL_RUN(launch_oinvt(c));
+    GPL_RUN(launch_zt_u(c, 0));
+    GPL_RUN(solve_refined(c, c->bvec, c->tBeta));
+  }
   GPL_RUN(launch_inverse_batched(c));
   GPL_RUN(launch_grad_delta(c));
   GPL_RUN(launch_grad_omega(c));
@@ -235,7 +244,7 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
   const int rhoflag = itr > 20 ? 1 : 0;
   if (itr == 30) JTRMAX = 10000;
   for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
-    GPL_RUN(gradient_launch(c));
+    GPL_RUN(gradient_launch(c, true));  // the last objective (after the IRLS or the accepted step) is here
     GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
     double sr = 1.0;
     std::vector<double>& l = c->lkhd;
@@ -1164,7 +1173,7 @@ int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkh
   p += (size_t)c->M * c->Q;
   GPL_TRY(c, cudaMemcpyAsync(c->rho, p, sizeof(double) * c->Q, cudaMemcpyHostToDevice, c->stream));
   GPL_RUN(objective_launch(c, 1));
-  GPL_RUN(gradient_launch(c));
+  GPL_RUN(gradient_launch(c, true));
   if (grad) GPL_TRY(c, cudaMemcpyAsync(grad, c->grad, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
   double v = 0.0;
   GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1178,7 +1187,7 @@ int gpl_evaluate_device(gpl_ctx* h) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));
   GPL_RUN(objective_launch(c, 1));
-  GPL_RUN(gradient_launch(c));
+  GPL_RUN(gradient_launch(c, true));
   return GPL_OK;
 }
 
