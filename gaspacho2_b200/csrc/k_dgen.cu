@@ -12,8 +12,9 @@
 //
 // Tile: 8 warps as WARPS_M x WARPS_N, each warp WM x WN DMMA tiles of 16 x 8, K slices of 16
 // staged through registers (the next slice's global loads are in flight during the current
-// slice's MMAs) into double-buffered shared memory laid out [k][m] and [k][n] with rows padded
-// to 4 mod 16 doubles (conflict-free fragment loads).
+// slice's MMAs; operands computed from several loads keep the raw values in registers and do
+// their arithmetic only when the slice is stored) into double-buffered shared memory laid out
+// [k][m] and [k][n] with rows padded to 4 mod 16 doubles (conflict-free fragment loads).
 #include <algorithm>
 
 #include "dmma_common.cuh"
