@@ -129,76 +129,53 @@ __device__ __forceinline__ double add_levels(double dense, int i, int j, int ldN
 }
 
 // ---- W / Nu -----------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int P, int J, int pvars, int n_d, int n_cv,
-                                              const double* __restrict__ D, const int* __restrict__ dcol,
-                                              const int* __restrict__ cv_nh, const int* __restrict__ codes,
-                                              const double* __restrict__ Beta, const double* __restrict__ ls,
-                                              const double* __restrict__ delta, const double* __restrict__ titsias,
-                                              const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
-                                              const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
-                                              int de, const double* __restrict__ e0, double* __restrict__ W,
-                                              double* __restrict__ Nu) {
-  // the GEMM tiles and the count tile are live at different times: overlay them
-  __shared__ __align__(16) unsigned char raw[TN * (TM + 1) * sizeof(double) + TN * TM];
-  double(*As)[TM + 1] = reinterpret_cast<double(*)[TM + 1]>(raw);
-  double(*Bs)[TN + 1] = reinterpret_cast<double(*)[TN + 1]>(raw + TK * (TM + 1) * sizeof(double));
-  double(*ys)[TM + 1] = reinterpret_cast<double(*)[TM + 1]>(raw);
-  unsigned char(*yf)[TM] = reinterpret_cast<unsigned char(*)[TM]>(raw + TN * (TM + 1) * sizeof(double));
-  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
-  double acc[4][4];
-  gemm_tile(m0, n0, n_d, LoadD{D, ldN, N, n_d}, LoadBetaDense{Beta, dcol, P, n_d, J}, acc, As, Bs);
-  // counts of this tile
-  for (int e = threadIdx.x; e < TN * TM; e += 256) yf[e / TM][e % TM] = 0;
-  __syncthreads();
-  if (threadIdx.x < TN) {
-    const int j = n0 + threadIdx.x;
-    if (j < J) {
-      int64_t lo = gptr[j], hi = gptr[j] + gvalid[j];
-      while (lo < hi) {  // first entry with cell >= m0
-        const int64_t mid = (lo + hi) >> 1;
-        if (cell[mid] < m0) lo = mid + 1; else hi = mid;
-      }
-      const int64_t end = gptr[j] + gvalid[j];
-      for (int64_t l = lo; l < end && cell[l] < m0 + TM; l++) {
-        ys[threadIdx.x][cell[l] - m0] = cnt[l];
-        yf[threadIdx.x][cell[l] - m0] = 1;
-      }
-    }
+// getWForBeta (ggplvm.cu:468-514) from the linear predictor eta = z_i . beta_j (k_eta, FFMA
+// tile GEMM with the cells' level coefficients, written to a cell x gene buffer first), one
+// block per gene: every cell gets W = exp(eta) s_i exp(dgp titsias_i wt) and the working
+// response of a zero count; then the counts that the reference's merge walk matches (the first
+// gvalid entries of the gene) replace their cells' working response. The barrier orders the
+// two writes of such a cell. The DE driver takes the Titsias factor at weight 1 and
+// nu = z.(beta - zeta) + (y - W)/W (ggplvm_de.cu:442-486); the fit driver has zeta = 0.
+__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int pvars, const double* __restrict__ E,
+                                              const double* __restrict__ ls, const double* __restrict__ delta,
+                                              const double* __restrict__ titsias, const int32_t* __restrict__ cell,
+                                              const int64_t* __restrict__ gptr, const int32_t* __restrict__ gvalid,
+                                              const double* __restrict__ cnt, int de, const double* __restrict__ e0,
+                                              double* __restrict__ W, double* __restrict__ Nu) {
+  const int j = blockIdx.x;
+  const double dgp = delta[pvars - 1];
+  const double wt = de ? 1.0 : kWt;
+  const double* Ej = E + (size_t)j * ldN;
+  double* Wj = W + (size_t)j * ldN;
+  double* Nj = Nu + (size_t)j * ldN;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double eta = Ej[i], lsi = ls[i], tt = dgp * titsias[i] * wt;
+    Wj[i] = exp(eta) * lsi * exp(tt);
+    Nj[i] = de ? (eta - e0[i]) - 1.0 : eta - 1.0;
   }
   __syncthreads();
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const double dgp = delta[pvars - 1];
-#pragma unroll
-  for (int x = 0; x < 4; x++) {
-    const int r = tx + 16 * x, i = m0 + r;
-    if (i >= N) continue;
-    // the DE driver takes the Titsias factor at weight 1 and nu = z.(beta - zeta) + (y - W)/W
-    // (ggplvm_de.cu:442-486); the fit driver weights it by wt and has zeta = 0
-    const double lsi = ls[i], tt = de ? dgp * titsias[i] : dgp * titsias[i] * kWt;
-    const double lls = log(lsi), ez = de ? e0[i] : 0.0;
-#pragma unroll
-    for (int y = 0; y < 4; y++) {
-      const int cc = ty + 16 * y, j = n0 + cc;
-      if (j >= J) continue;
-      const double eta = add_levels(acc[x][y], i, j, ldN, P, n_cv, cv_nh, codes, Beta);
-      const double logW = eta + lls + tt;
-      const double w = exp(eta) * lsi * exp(tt);
-      double nu;
-      if (de) nu = yf[cc][r] ? (eta - ez) + (ys[cc][r] - w) / w : (eta - ez) - 1.0;
-      else if (yf[cc][r]) nu = eta + exp(log(ys[cc][r]) - logW) - 1.0;
-      else nu = eta - 1.0;
-      W[(size_t)j * ldN + i] = w;
-      Nu[(size_t)j * ldN + i] = nu;
-    }
+  const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
+  for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
+    const int i = cell[l];
+    const double eta = Ej[i], lsi = ls[i], tt = dgp * titsias[i] * wt, y = cnt[l];
+    const double w = exp(eta) * lsi * exp(tt);
+    Nj[i] = de ? (eta - e0[i]) + (y - w) / w : eta + exp(log(y) - (eta + log(lsi) + tt)) - 1.0;
   }
 }
+
+__global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n_d, int n_cv,
+                                             const double* __restrict__ D, const int* __restrict__ dcol,
+                                             const int* __restrict__ cv_nh, const int* __restrict__ codes,
+                                             const double* __restrict__ B, double* __restrict__ out);
 
 int launch_w_nu(Ctx* c) {
   ProfScope ps(c, "w_nu");
   dim3 g(div_up(c->N, TM), div_up(c->J, TN));
-  k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->p, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
-                                   c->codes_d, c->Beta, c->ls, c->delta, c->titsias, c->cell, c->gptr, c->gvalid,
-                                   c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
+  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                  c->codes_d, c->Beta, c->scratch);
+  GPL_LAUNCHED(c, "k_eta");
+  k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->scratch, c->ls, c->delta, c->titsias, c->cell, c->gptr,
+                                      c->gvalid, c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
   return GPL_OK;
 }
