@@ -84,7 +84,8 @@ static void free_state(Ctx* c) {
   tc_release(c);
   pair_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
-                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d};
+                   c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d,
+                   c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d};
   for (void* q : extra)
     if (q) cudaFree(q);
   c->hk_tiles128_d = nullptr;
@@ -94,6 +95,8 @@ static void free_state(Ctx* c) {
   c->part_n = 0;
   c->Dm = c->gsum = c->gT = c->HK = nullptr;
   c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
+  c->lvl_cc_d = c->lvl_v_d = c->lvl_ptr_d = c->lvl_grp_d = nullptr;
+  c->n_lvl = 0;
   c->hk_tiles_d = nullptr;
   c->n_grp = c->n_cv = 0;
   void* bufs[] = {c->Z,      c->W,      c->Nu,      c->Psi,     c->PsiInv, c->Beta,   c->tBeta,  c->scratch,
@@ -798,6 +801,26 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_TRY(c, cudaMemcpy(c->glev_d, glev.data(), sizeof(int32_t) * glev.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->gcells_d, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
+    // per level of each grouped variable: its model column, its variable, its groups in order
+    std::vector<int32_t> lvl_cc, lvl_v, lvl_ptr(1, 0), lvl_grp;
+    for (int v = 0; v < ncat; v++)
+      for (int L = 0; L < c->cv_nlev[v]; L++) {
+        lvl_cc.push_back(c->cv_nh[v] + L);
+        lvl_v.push_back(v);
+        for (int g = 0; g < n_grp; g++)
+          if (glev[(size_t)g * ncat + v] == L) lvl_grp.push_back(g);
+        lvl_ptr.push_back((int32_t)lvl_grp.size());
+      }
+    c->n_lvl = (int)lvl_cc.size();
+    GPL_RUN(dalloc(c, &c->lvl_cc_d, lvl_cc.size(), "level columns"));
+    GPL_RUN(dalloc(c, &c->lvl_v_d, lvl_v.size(), "level variables"));
+    GPL_RUN(dalloc(c, &c->lvl_ptr_d, lvl_ptr.size(), "level offsets"));
+    GPL_RUN(dalloc(c, &c->lvl_grp_d, std::max<size_t>(1, lvl_grp.size()), "level groups"));
+    GPL_TRY(c, cudaMemcpy(c->lvl_cc_d, lvl_cc.data(), sizeof(int32_t) * lvl_cc.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->lvl_v_d, lvl_v.data(), sizeof(int32_t) * lvl_v.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->lvl_ptr_d, lvl_ptr.data(), sizeof(int32_t) * lvl_ptr.size(), cudaMemcpyHostToDevice));
+    if (!lvl_grp.empty())
+      GPL_TRY(c, cudaMemcpy(c->lvl_grp_d, lvl_grp.data(), sizeof(int32_t) * lvl_grp.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles_d, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles128_d, tiles128.data(), sizeof(int2) * tiles128.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_cells_d, tile_cells.data(), sizeof(int32_t) * tile_cells.size(),

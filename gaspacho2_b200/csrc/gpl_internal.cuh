@@ -117,6 +117,10 @@ struct Ctx {
   std::vector<int> cv_nh, cv_nlev;  // first model column and level count of each grouped variable
   int *dcol_d = nullptr, *cv_nh_d = nullptr, *cv_nlev_d = nullptr, *gid_d = nullptr, *glev_d = nullptr;
   int *gcells_d = nullptr, *gstart_d = nullptr, *codes_d = nullptr;
+  // levels of the grouped variables: model column, variable, and the groups at that level
+  // (ascending) as offsets into a list
+  int n_lvl = 0;
+  int *lvl_cc_d = nullptr, *lvl_v_d = nullptr, *lvl_ptr_d = nullptr, *lvl_grp_d = nullptr;
   int2* hk_tiles_d = nullptr;       // (group, first row) of every 64-cell tile of the group lists
   int n_hk_tiles = 0;
   int2* hk_tiles128_d = nullptr;    // the same for 128-cell tiles

@@ -153,70 +153,58 @@ int launch_group_sums(Ctx* c, int mode) {
 }
 
 // Categorical rows and columns of Psi_j (both triangles) from the group sums, plus the
-// prior's diagonal on them; the dense x dense entries are written by the Gram kernel.
-__global__ void __launch_bounds__(256) k_assemble_psi(int P, int n_d, int n_cv, int n_grp,
-                                                      const int* __restrict__ dcol, const int* __restrict__ cv_nh,
-                                                      const int* __restrict__ cv_nlev, const int* __restrict__ glev,
-                                                      const double* __restrict__ S, const double* __restrict__ Dinv,
-                                                      double* __restrict__ Psi) {
+// prior's diagonal on them; the dense x dense entries are written by the Gram kernel. Every
+// categorical entry is written once, as a sum over the groups at its level(s) taken in group
+// order (the order of getPsi's case analysis, ggplvm.cu:628-674, over the cells of each group):
+//   (level l, dense column a)   sum_{g at l} S[g][a]
+//   (level l, level l)          sum_{g at l} S[g][0] + DeltaInv (S[.][0]: the intercept = sum w)
+//   (level l, other level of the same variable)   0
+//   (level l of v, level l2 of v2 != v)           sum_{g at l and l2} S[g][0]
+__global__ void __launch_bounds__(256) k_assemble_psi(int P, int n_d, int NL, int n_cv, int n_grp,
+                                                      const int* __restrict__ dcol, const int* __restrict__ lvl_cc,
+                                                      const int* __restrict__ lvl_v, const int* __restrict__ lvl_ptr,
+                                                      const int* __restrict__ lvl_grp, const int* __restrict__ cv_nh,
+                                                      const int* __restrict__ glev, const double* __restrict__ S,
+                                                      const double* __restrict__ Dinv, double* __restrict__ Psi) {
   const int j = blockIdx.x;
   double* Pj = Psi + (size_t)j * P * P;
   const double* Sj = S + (size_t)j * n_grp * (n_d + 1);
-  // zero every row and column of a grouped categorical variable
-  for (int v = 0; v < n_cv; v++)
-    for (int e = threadIdx.x; e < cv_nlev[v] * P; e += blockDim.x) {
-      const int cidx = cv_nh[v] + e / P, r = e % P;
-      Pj[cidx + (size_t)r * P] = 0.0;
-      Pj[r + (size_t)cidx * P] = 0.0;
-    }
-  __syncthreads();
-  // level x dense column: thread owns dense column a
-  for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
-    const size_t col = (size_t)dcol[a] * P;
-    for (int g = 0; g < n_grp; g++) {
-      const double s = Sj[(size_t)g * (n_d + 1) + a];
-      for (int v = 0; v < n_cv; v++) Pj[cv_nh[v] + glev[g * n_cv + v] + col] += s;
-    }
+  const int ld = n_d + 1;
+  for (int e = threadIdx.x; e < NL * n_d; e += blockDim.x) {
+    const int l = e / n_d, a = e - l * n_d;
+    double s = 0.0;
+    for (int q = lvl_ptr[l]; q < lvl_ptr[l + 1]; q++) s += Sj[(size_t)lvl_grp[q] * ld + a];
+    const size_t cc = lvl_cc[l], dc = dcol[a];
+    Pj[cc + dc * P] = s;
+    Pj[dc + cc * P] = s;
   }
-  // level x level (different variables) and the diagonal: one thread, groups in order
-  if (threadIdx.x == 0) {
-    for (int g = 0; g < n_grp; g++) {
-      const double s = Sj[(size_t)g * (n_d + 1) + 0];  // dense column 0 is the intercept: sum w
-      for (int v = 0; v < n_cv; v++) {
-        const int cv = cv_nh[v] + glev[g * n_cv + v];
-        Pj[cv + (size_t)cv * P] += s;
-        for (int v2 = v + 1; v2 < n_cv; v2++) Pj[cv + (size_t)(cv_nh[v2] + glev[g * n_cv + v2]) * P] += s;
+  for (int e = threadIdx.x; e < NL * NL; e += blockDim.x) {
+    const int l1 = e / NL, l2 = e - l1 * NL;
+    const int v1 = lvl_v[l1], v2 = lvl_v[l2];
+    const size_t c1 = lvl_cc[l1], c2 = lvl_cc[l2];
+    double s = 0.0;
+    if (v1 == v2) {
+      if (l1 == l2) {
+        for (int q = lvl_ptr[l1]; q < lvl_ptr[l1 + 1]; q++) s += Sj[(size_t)lvl_grp[q] * ld];
+        s += Dinv[c1 + c1 * P];
+      }
+    } else {
+      const int L2 = (int)c2 - cv_nh[v2];
+      for (int q = lvl_ptr[l1]; q < lvl_ptr[l1 + 1]; q++) {
+        const int g = lvl_grp[q];
+        if (glev[(size_t)g * n_cv + v2] == L2) s += Sj[(size_t)g * ld];
       }
     }
-    for (int v = 0; v < n_cv; v++)
-      for (int L = 0; L < cv_nlev[v]; L++) {
-        const int cc = cv_nh[v] + L;
-        Pj[cc + (size_t)cc * P] += Dinv[cc + (size_t)cc * P];
-      }
+    Pj[c1 + c2 * P] = s;
   }
-  __syncthreads();
-  // mirror: (dense column, level) and (level, later variable's level)
-  for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
-    const int dc = dcol[a];
-    for (int v = 0; v < n_cv; v++)
-      for (int L = 0; L < cv_nlev[v]; L++) {
-        const int cc = cv_nh[v] + L;
-        Pj[dc + (size_t)cc * P] = Pj[cc + (size_t)dc * P];
-      }
-  }
-  for (int v = 0; v < n_cv; v++)
-    for (int v2 = v + 1; v2 < n_cv; v2++)
-      for (int e = threadIdx.x; e < cv_nlev[v] * cv_nlev[v2]; e += blockDim.x) {
-        const int c1 = cv_nh[v] + e / cv_nlev[v2], c2 = cv_nh[v2] + e % cv_nlev[v2];
-        Pj[c2 + (size_t)c1 * P] = Pj[c1 + (size_t)c2 * P];
-      }
 }
 
 int launch_assemble_psi(Ctx* c, int J) {
   if (c->n_grp == 0) return GPL_OK;
   ProfScope ps(c, "assemble_psi");
-  k_assemble_psi<<<J, 256, 0, c->stream>>>(c->P, c->n_d, c->n_cv, c->n_grp, c->dcol_d, c->cv_nh_d, c->cv_nlev_d,
-                                           c->glev_d, c->gsum, c->DeltaInv, c->Psi);
+  k_assemble_psi<<<J, 256, 0, c->stream>>>(c->P, c->n_d, c->n_lvl, c->n_cv, c->n_grp, c->dcol_d, c->lvl_cc_d,
+                                           c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d, c->cv_nh_d, c->glev_d, c->gsum,
+                                           c->DeltaInv, c->Psi);
   GPL_LAUNCHED(c, "k_assemble_psi");
   return GPL_OK;
 }
