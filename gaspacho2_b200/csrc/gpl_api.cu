@@ -104,7 +104,7 @@ static void free_state(Ctx* c) {
                   c->X,      c->T,      c->rho,     c->phi,     c->ls,     c->lkhds,  c->lkhd_dev, c->grad,
                   c->grad0,  c->ss,     c->SS,      c->XX,      c->gdtmp,  c->C1,     c->C2,     c->grtmp,
                   c->KmmInv, c->bvec,   c->sol,     c->red,     c->lb_work, c->mc_d,  c->mv_d,   c->mk_d,
-                  c->nh_d,   c->rres,   c->bx,      c->rphi,    c->e0,      c->zeta,  c->eta_bd};
+                  c->nh_d,   c->rres,   c->bx,      c->rphi,    c->e0,      c->zeta};
   for (void* p : bufs)
     if (p) cudaFree(p);
   c->Z = c->W = c->Nu = c->Psi = c->PsiInv = c->Beta = c->tBeta = c->scratch = c->U = nullptr;
@@ -112,7 +112,7 @@ static void free_state(Ctx* c) {
   c->rho = c->phi = c->ls = c->lkhds = c->lkhd_dev = c->grad = c->grad0 = c->ss = c->SS = c->XX = nullptr;
   c->gdtmp = c->C1 = c->C2 = c->grtmp = c->KmmInv = c->bvec = c->sol = c->red = c->lb_work = nullptr;
   c->mc_d = c->mv_d = c->mk_d = c->nh_d = nullptr;
-  c->rres = c->bx = c->rphi = c->e0 = c->zeta = c->eta_bd = nullptr;
+  c->rres = c->bx = c->rphi = c->e0 = c->zeta = nullptr;
   c->have_design = false;
 }
 

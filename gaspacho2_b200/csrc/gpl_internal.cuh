@@ -96,7 +96,6 @@ struct Ctx {
   bool vcomp = false;      // the variance-component driver's likelihood constants (ggplvm_delta.cu)
   double* e0 = nullptr;    // z_i . zeta per cell (DE working response)
   double* zeta = nullptr;  // the DE driver's zeta (P)
-  double* eta_bd = nullptr;  // dense rows of a coefficient matrix, gene-contiguous (k_eta_dmma)
   int de_quirk_col = -1;   // dense column whose first cell holds the null model's loader value
   double de_quirk_orig = 0.0;
   bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
@@ -217,7 +216,6 @@ int solve_refined(Ctx* c, const double* b, double* x, bool dinv_factored = false
 int launch_init_response(Ctx* c);        // scratch = log((y+0.05)/ls) or log(0.05/ls)
 int launch_zbeta(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B
 int launch_eta_one(Ctx* c, const double* b, double* out);  // out[N] = Z * b for one coefficient vector
-int launch_eta_dmma(Ctx* c, const double* B, double* out);  // out[ldN x J] = Z * B on DMMA (n_d <= 136)
 int launch_c1_tn(Ctx* c);                // C1 partial from tn/phi and tBeta GP block
 // k_gram.cu
 int launch_gram(Ctx* c, bool unweighted);  // Psi (full symmetric) = Z^T diag(W/Omega) Z + DeltaInv

@@ -168,23 +168,12 @@ __global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n
                                              const int* __restrict__ cv_nh, const int* __restrict__ codes,
                                              const double* __restrict__ B, double* __restrict__ out);
 
-// E = Z B (ldN x J): the DMMA GEMM, or the FFMA tile GEMM when the dense columns are too many
-static int eta_all(Ctx* c, const double* B, double* out) {
-  if (!c->simt_fp64) {
-    const int rc = launch_eta_dmma(c, B, out);
-    if (rc != GPL_ERR_ARG) return rc;
-  }
-  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
-  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
-                                  c->codes_d, B, out);
-  GPL_LAUNCHED(c, "k_eta");
-  return GPL_OK;
-}
-
 int launch_w_nu(Ctx* c) {
   ProfScope ps(c, "w_nu");
-  const int rc = eta_all(c, c->Beta, c->scratch);
-  if (rc) return rc;
+  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                  c->codes_d, c->Beta, c->scratch);
+  GPL_LAUNCHED(c, "k_eta");
   k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->scratch, c->ls, c->delta, c->titsias, c->cell, c->gptr,
                                       c->gvalid, c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
@@ -216,7 +205,11 @@ __global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n
 
 int launch_zbeta(Ctx* c, const double* B, double* out) {
   ProfScope ps(c, "zbeta");
-  return eta_all(c, B, out);
+  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                  c->codes_d, B, out);
+  GPL_LAUNCHED(c, "k_eta");
+  return GPL_OK;
 }
 
 int launch_eta_one(Ctx* c, const double* b, double* out) {
