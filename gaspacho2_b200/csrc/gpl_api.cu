@@ -85,7 +85,7 @@ static void free_state(Ctx* c) {
   pair_release(c);
   void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
                    c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d,
-                   c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d};
+                   c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d, c->hk_pos_d, c->Wg, c->Dg, c->rOmg};
   for (void* q : extra)
     if (q) cudaFree(q);
   c->hk_tiles128_d = nullptr;
@@ -95,7 +95,8 @@ static void free_state(Ctx* c) {
   c->part_n = 0;
   c->Dm = c->gsum = c->gT = c->HK = nullptr;
   c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
-  c->lvl_cc_d = c->lvl_v_d = c->lvl_ptr_d = c->lvl_grp_d = nullptr;
+  c->lvl_cc_d = c->lvl_v_d = c->lvl_ptr_d = c->lvl_grp_d = c->hk_pos_d = nullptr;
+  c->Wg = c->Dg = c->rOmg = nullptr;
   c->n_lvl = 0;
   c->hk_tiles_d = nullptr;
   c->n_grp = c->n_cv = 0;
@@ -723,12 +724,16 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   c->n_hk_tiles = (int)tiles.size();
   std::vector<int2> tiles128;
   std::vector<int32_t> tile_cells;  // the cell of each of the 128 slots of every tile, -1 past the group
+  std::vector<int32_t> tile_pos;    // the same slots as positions in group order
   if (grouped)
     for (int g = 0; g < n_grp; g++)
       for (int r0 = 0; r0 < gstart[g + 1] - gstart[g]; r0 += 128) {
         tiles128.push_back(make_int2(g, r0));
-        for (int q = 0; q < 128; q++)
-          tile_cells.push_back(r0 + q < gstart[g + 1] - gstart[g] ? order[gstart[g] + r0 + q] : -1);
+        for (int q = 0; q < 128; q++) {
+          const bool in = r0 + q < gstart[g + 1] - gstart[g];
+          tile_cells.push_back(in ? order[gstart[g] + r0 + q] : -1);
+          tile_pos.push_back(in ? gstart[g] + r0 + q : -1);
+        }
       }
   c->n_hk_tiles128 = (int)tiles128.size();
   c->tot_max = tot_len(c, 1);
@@ -792,6 +797,11 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->hk_tiles128_d, tiles128.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->hk_cells_d, tile_cells.size(), "group tile cells"));
+    GPL_RUN(dalloc(c, &c->hk_pos_d, tile_pos.size(), "group tile positions"));
+    GPL_RUN(dalloc(c, &c->Wg, ldN * (size_t)J, "W in group order"));
+    GPL_RUN(dalloc(c, &c->Dg, ldN * (size_t)n_d, "dense columns in group order"));
+    GPL_RUN(dalloc(c, &c->rOmg, ldN, "1/Omega in group order"));
+    GPL_TRY(c, cudaMemset(c->Wg, 0, sizeof(double) * ldN * (size_t)J));
     GPL_RUN(dalloc(c, &c->gsum, (size_t)J * n_grp * (n_d + 1), "group sums"));
     GPL_RUN(dalloc(c, &c->gT, (size_t)J * n_grp, "group response sums"));
     GPL_RUN(dalloc(c, &c->HK, ldN * (n_d + 1), "HK"));
@@ -823,6 +833,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
       GPL_TRY(c, cudaMemcpy(c->lvl_grp_d, lvl_grp.data(), sizeof(int32_t) * lvl_grp.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles_d, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_tiles128_d, tiles128.data(), sizeof(int2) * tiles128.size(), cudaMemcpyHostToDevice));
+    GPL_TRY(c, cudaMemcpy(c->hk_pos_d, tile_pos.data(), sizeof(int32_t) * tile_pos.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->hk_cells_d, tile_cells.data(), sizeof(int32_t) * tile_cells.size(),
                           cudaMemcpyHostToDevice));
   }

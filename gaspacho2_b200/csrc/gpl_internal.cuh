@@ -125,6 +125,10 @@ struct Ctx {
   int n_hk_tiles = 0;
   int2* hk_tiles128_d = nullptr;    // the same for 128-cell tiles
   int* hk_cells_d = nullptr;        // the cell of each slot of those tiles (-1 past the group)
+  int* hk_pos_d = nullptr;          // the same slots as positions in group order (-1 past the group)
+  // cells in group order (the cells of each group contiguous): W (refreshed with W), the dense
+  // columns and 1/Omega (refreshed per use), so that the group-sum GEMMs read contiguous rows
+  double *Wg = nullptr, *Dg = nullptr, *rOmg = nullptr;
   int n_hk_tiles128 = 0;
   double* part = nullptr;           // split-K partial sums
   size_t part_n = 0;
@@ -206,6 +210,7 @@ int launch_assemble_psi(Ctx* c, int J);   // categorical rows/columns of Psi fro
 int launch_assemble_b(Ctx* c, double* out);  // categorical entries of Z^T u (P x J) from the group sums
 int launch_group_tables(Ctx* c);          // per (gene, group) categorical blocks of Psi^{-1}
 int launch_hk(Ctx* c);                    // HK[i] = sum_j O_ij [h_{j,g(i)} | kappa_{j,g(i)}]
+int launch_group_order(Ctx* c, const double* src, int ncols, double* dst);  // dst[col][pos] = src[col][cell(pos)]
 // k_gemm.cu
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response

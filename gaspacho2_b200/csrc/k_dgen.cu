@@ -219,25 +219,25 @@ struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
   int P, g0;
   __device__ double operator()(int k, int c, int) const { return tB[g0 + c + (size_t)k * P]; }
 };
-struct LdGroupD {  // A(r = dense column, k = k-th cell of group z) = D[r*ldN + cell]
+struct LdGroupD {  // A(r = dense column, k = k-th cell of group z) = Dg[r*ldN + gstart[z] + k] (group order)
   static constexpr bool kFastK = true;
-  const double* D;
-  const int *gcells, *gstart;
+  const double* Dg;
+  const int* gstart;
   int ldN;
-  __device__ double operator()(int r, int k, int z) const { return D[(size_t)r * ldN + gcells[gstart[z] + k]]; }
+  __device__ double operator()(int r, int k, int z) const { return Dg[(size_t)r * ldN + gstart[z] + k]; }
 };
-struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) or 1 (mode 1)
+struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) or 1 (mode 1), group order
   static constexpr bool kFastK = true;
-  const double *W, *rOm;
-  const int *gcells, *gstart;
+  const double *Wg, *rOmg;
+  const int* gstart;
   int ldN, mode;
   struct Raw {
     double w, r;
   };
   __device__ Raw load(int k, int c, int z) const {
     if (mode == 1) return Raw{1.0, 1.0};
-    const int i = gcells[gstart[z] + k];
-    return Raw{W[(size_t)c * ldN + i], rOm[i]};
+    const int pos = gstart[z] + k;
+    return Raw{Wg[(size_t)c * ldN + pos], rOmg[pos]};
   }
   __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
@@ -250,17 +250,17 @@ struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the ti
     return tab[((size_t)k * n_grp + tiles[z].x) * ld + r];
   }
 };
-struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell
+struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell, group order
   static constexpr bool kFastK = false;
-  const double *W, *rOm;
-  const int* cells;  // 128 slots per tile
+  const double *Wg, *rOmg;
+  const int* pos;  // 128 slots per tile, positions in group order (-1 past the group)
   int ldN;
   struct Raw {
     double w, r;
   };
   __device__ Raw load(int k, int c, int z) const {
-    const int i = cells[(size_t)z * 128 + c];
-    return i < 0 ? Raw{0.0, 0.0} : Raw{W[(size_t)k * ldN + i], rOm[i]};
+    const int q = pos[(size_t)z * 128 + c];
+    return q < 0 ? Raw{0.0, 0.0} : Raw{Wg[(size_t)k * ldN + q], rOmg[q]};
   }
   __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
@@ -431,15 +431,17 @@ int dgen_c1_tn(Ctx* c) {
 int dgen_group_sums(Ctx* c, int mode) {
   using T = TileTall;
   if (c->n_d > T::BM) return GPL_ERR_ARG;
-  const double* rOm = nullptr;
+  int rc;
   if (mode == 0) {
-    int rc = recip_omega(c, &rOm);
-    if (rc) return rc;
+    const double* rOm = nullptr;
+    if ((rc = recip_omega(c, &rOm))) return rc;
+    if ((rc = launch_group_order(c, rOm, 1, c->rOmg))) return rc;
   }
+  if ((rc = launch_group_order(c, c->Dm, c->n_d, c->Dg))) return rc;
   const int J = mode == 1 ? 1 : c->J;
   dim3 g(1, div_up(J, T::BN), c->n_grp);
-  return launch_dgen<T>(c, g, c->n_d, J, LdGroupD{c->Dm, c->gcells_d, c->gstart_d, c->ldN},
-                        LdGroupW{c->W, rOm, c->gcells_d, c->gstart_d, c->ldN, mode}, KGroup{c->gstart_d},
+  return launch_dgen<T>(c, g, c->n_d, J, LdGroupD{c->Dg, c->gstart_d, c->ldN},
+                        LdGroupW{c->Wg, c->rOmg, c->gstart_d, c->ldN, mode}, KGroup{c->gstart_d},
                         EpGroup{c->gsum, c->n_grp, c->n_d + 1}, "k_dgen(group_sums)");
 }
 
@@ -450,9 +452,10 @@ int dgen_hk(Ctx* c) {
   const double* rOm = nullptr;
   int rc = recip_omega(c, &rOm);
   if (rc) return rc;
+  if ((rc = launch_group_order(c, rOm, 1, c->rOmg))) return rc;
   dim3 g(1, 1, c->n_hk_tiles128);
   return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
-                        LdTileO{c->W, rOm, c->hk_cells_d, c->ldN}, KAll{c->J}, EpHK{c->HK, c->hk_cells_d, c->ldN},
+                        LdTileO{c->Wg, c->rOmg, c->hk_pos_d, c->ldN}, KAll{c->J}, EpHK{c->HK, c->hk_cells_d, c->ldN},
                         "k_dgen(hk)");
 }
 

@@ -177,6 +177,8 @@ int launch_w_nu(Ctx* c) {
   k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->scratch, c->ls, c->delta, c->titsias, c->cell, c->gptr,
                                       c->gvalid, c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
+  // W in group order for the group-sum GEMMs (W changes only here)
+  if (c->Wg) return launch_group_order(c, c->W, c->J, c->Wg);
   return GPL_OK;
 }
 

@@ -19,6 +19,8 @@
 // so that z_i^T S_j z_i = d_i^T S_DD d_i + 2 d_i . h + kappa for a cell of group g.
 // The group sums and HK are FP64 GEMMs over the gathered cells of one group (the shared
 // register-tiled tile of k_gemm.cu's scheme), N*J*n_d multiply-adds each.
+#include <algorithm>
+
 #include "gpl_internal.cuh"
 
 namespace gpl {
@@ -197,6 +199,22 @@ __global__ void __launch_bounds__(256) k_assemble_psi(int P, int n_d, int NL, in
     }
     Pj[c1 + c2 * P] = s;
   }
+}
+
+// dst[col * ldN + pos] = src[col * ldN + cell(pos)]: the cells in group order (gcells)
+__global__ void k_group_order(int N, int ldN, int ncols, const int* __restrict__ gcells, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= N) return;
+  const int i = gcells[pos];
+  for (int col = blockIdx.y; col < ncols; col += gridDim.y) dst[(size_t)col * ldN + pos] = src[(size_t)col * ldN + i];
+}
+
+int launch_group_order(Ctx* c, const double* src, int ncols, double* dst) {
+  dim3 g(div_up(c->N, 256), std::min(ncols, 65535));
+  k_group_order<<<g, 256, 0, c->stream>>>(c->N, c->ldN, ncols, c->gcells_d, src, dst);
+  GPL_LAUNCHED(c, "k_group_order");
+  return GPL_OK;
 }
 
 int launch_assemble_psi(Ctx* c, int J) {
