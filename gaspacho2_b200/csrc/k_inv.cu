@@ -250,34 +250,54 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
       }
     }
     __syncthreads();
-    // the diagonal block, one warp: lane = row
+    // The diagonal block, one warp, right-looking with row `lane` in registers; then the rows
+    // below it, thread per row, the same way. Entry (r, q) still takes its products
+    // l_rk l_qk in increasing k and is scaled by 1/l_qq last, as choldc's sums: the same
+    // operations in the same order as the entry-by-entry form, with independent FMAs in place
+    // of one dependent chain per entry.
     if (warp == 0) {
-      for (int cc = 0; cc < ncol; cc++) {
-        if (lane == cc) {
-          double piv = Ap[cc * IS + cc];
-          for (int q = 0; q < cc; q++) piv -= Ap[cc * IS + q] * Ap[cc * IS + q];
-          if (piv <= 0.0) fail = 1;  // a NaN pivot passes, as in choldc
+      double a[IB];
+#pragma unroll
+      for (int q = 0; q < IB; q++) a[q] = Ap[lane * IS + q];
+#pragma unroll
+      for (int cc = 0; cc < IB; cc++) {
+        if (cc < ncol) {
+          const double piv = __shfl_sync(0xffffffffu, a[cc], cc);
           const double l = sqrt(piv);
-          Ap[cc * IS + cc] = l;
-          Rd[cc] = 1.0 / l;
+          const double rd = 1.0 / l;
+          if (lane == cc) {
+            if (piv <= 0.0) fail = 1;  // a NaN pivot passes, as in choldc
+            a[cc] = l;
+            Rd[cc] = rd;
+          } else if (lane > cc) {
+            a[cc] = a[cc] * rd;
+          }
+#pragma unroll
+          for (int q = cc + 1; q < IB; q++) {
+            const double lq = __shfl_sync(0xffffffffu, a[cc], q);
+            a[q] -= a[cc] * lq;
+          }
         }
-        __syncwarp();
-        if (lane > cc && lane < ncol) {
-          double sacc = Ap[lane * IS + cc];
-          for (int q = 0; q < cc; q++) sacc -= Ap[lane * IS + q] * Ap[cc * IS + q];
-          Ap[lane * IS + cc] = sacc * Rd[cc];
-        }
-        __syncwarp();
       }
+#pragma unroll
+      for (int q = 0; q < IB; q++) Ap[lane * IS + q] = a[q];
     }
     __syncthreads();
-    // rows below the block: L[r][0..32) against the factored block, thread per row
     for (int r = IB + tid; r < rows; r += blockDim.x) {
-      for (int cc = 0; cc < ncol; cc++) {
-        double sacc = Ap[r * IS + cc];
-        for (int q = 0; q < cc; q++) sacc -= Ap[r * IS + q] * Ap[cc * IS + q];
-        Ap[r * IS + cc] = sacc * Rd[cc];
+      double a[IB];
+#pragma unroll
+      for (int q = 0; q < IB; q++) a[q] = Ap[r * IS + q];
+#pragma unroll
+      for (int cc = 0; cc < IB; cc++) {
+        if (cc < ncol) {
+          const double x = a[cc] * Rd[cc];
+          a[cc] = x;
+#pragma unroll
+          for (int q = cc + 1; q < IB; q++) a[q] -= x * Ap[q * IS + cc];
+        }
       }
+#pragma unroll
+      for (int q = 0; q < IB; q++) Ap[r * IS + q] = a[q];
     }
     __syncthreads();
     for (int e = tid; e < rows * IB; e += blockDim.x) {
