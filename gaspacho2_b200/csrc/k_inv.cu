@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256, 1)
     }
     cp_async_commit();
     for (int e = tid; e < IB * IB; e += blockDim.x) {
-      const int m = e >> 5, q = e & 31;
+      const int q = e >> 5, m = e & 31;
       const int row = rb + m, col = rb + q;
       double v;
       if (row < P && col < P) v = q <= m ? L[row + (size_t)col * P] : 0.0;
@@ -122,8 +122,8 @@ __global__ void __launch_bounds__(256, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int m0 = (warp >> 2) * 16, n0 = (warp & 3) * 8;
   const int kb_rows = (P - c0 + 3) / 4 * 4;
-  for (int e = tid; e < kb_rows * IB; e += blockDim.x) {
-    const int k = e >> 5, n = e & 31;
+  for (int e = tid; e < kb_rows * IB; e += blockDim.x) {  // rows fastest: coalesced columns
+    const int n = e / kb_rows, k = e - n * kb_rows;
     const int row = c0 + k, col = c0 + n;
     const bool ok = row < P && col < P;
     cp_async8(Vb + k * IS + n, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(256, 1)
     const int a0 = a * IB;
     const int K = (P - a0 + 3) / 4 * 4;
     for (int e = tid; e < K * IB; e += blockDim.x) {
-      const int k = e >> 5, m = e & 31;
+      const int m = e / K, k = e - m * K;
       const int row = a0 + k, col = a0 + m;
       const bool ok = row < P && col < P;
       cp_async8(Ak + k * IS + m, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
@@ -187,8 +187,8 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
     const int c0 = kp * IB, rows = P - c0, ncol = min(IB, rows);
     const int rpad = (rows + 15) / 16 * 16;
     // the panel's lower part: rows c0.., columns c0..c0+ncol
-    for (int e = tid; e < rpad * IB; e += blockDim.x) {
-      const int r = e >> 5, cc = e & 31;
+    for (int e = tid; e < rpad * IB; e += blockDim.x) {  // rows fastest: coalesced columns
+      const int cc = e / rpad, r = e - cc * rpad;
       Ap[r * IS + cc] = (r < rows && cc < ncol) ? A[(size_t)(c0 + r) + (size_t)(c0 + cc) * P] : 0.0;
     }
     if (kp > 0) {
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
     }
     __syncthreads();
     for (int e = tid; e < rows * IB; e += blockDim.x) {
-      const int r = e >> 5, cc = e & 31;
+      const int cc = e / rows, r = e - cc * rows;
       if (cc < ncol && r >= cc) A[(size_t)(c0 + r) + (size_t)(c0 + cc) * P] = Ap[r * IS + cc];
     }
     __threadfence_block();
