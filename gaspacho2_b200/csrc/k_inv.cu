@@ -8,10 +8,12 @@
 //                  the finished rows, R = E - L[i, jb..i) Y[jb..i) (DMMA), then solves
 //                  L[i,i] Y_i = R by column-oriented substitution: one warp per 4 right-hand
 //                  sides, lanes over rows, y_q = r_q * (1/L[q,q]) broadcast by shuffle, each
-//                  row's sum taken in increasing q as in cholsl. The panel stays in shared memory.
-//                  Work: P^3/6 multiply-adds per gene.
+//                  row's sum taken in increasing q as in cholsl. The panel stays in shared memory;
+//                  L's rows stream through two 32-column buffers. Work: P^3/6 multiply-adds per gene.
 //   k_lauum_panel  one CTA per (panel b, gene): S[a, b] = sum_{k >= a} V[k, a]^T V[k, b]
-//                  for the blocks a >= b, written to both triangles. Work: P^3/6 per gene.
+//                  for the blocks a >= b, written to both triangles; the rows of block column a
+//                  stream through two 32-row buffers. Work: P^3/6 per gene.
+// Both fit two CTAs per SM up to P = 256 (the panel's rows plus the two buffers).
 //
 // L is the lower triangle (with diagonal) of the factored Psi_j (column-major, ld P); V is
 // written column-major (ld P) below and on the diagonal of each panel, the strict upper part of
@@ -26,9 +28,10 @@ namespace {
 constexpr int IB = 32;  // block size
 constexpr int IS = 36;  // shared row stride (doubles): conflict-free fragment loads
 constexpr int LS = 33;  // shared row stride of the 32 x 32 diagonal and right-hand-side blocks
+constexpr int CW = 8;   // finished columns per chunk of the Cholesky's panel update
 }  // namespace
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
     k_trtri_panel(const double* __restrict__ Psi, int P, int64_t stride, double* __restrict__ V) {
   extern __shared__ __align__(16) double sm[];
   const int nb = (P + IB - 1) / IB;
@@ -37,8 +40,8 @@ __global__ void __launch_bounds__(256, 1)
   double* Vm = V + (size_t)blockIdx.y * stride;
   const int r0 = jb * IB;
   double* Yp = sm;                            // [nb*32][IS], local row r = global row r0 + r
-  double* As = Yp + (size_t)nb * IB * IS;     // [nb*32][IS], As[k][m] = L[rb + m][r0 + k]
-  double* Ld = As + (size_t)nb * IB * IS;     // [32][LS] diagonal block
+  double* As = Yp + (size_t)nb * IB * IS;     // [2][32][IS]: As[k][m] = L[rb + m][r0 + 32 ch + k]
+  double* Ld = As + 2 * IB * IS;              // [32][LS] diagonal block
   double* Rs = Ld + IB * LS;                  // [32][LS] right-hand sides
   double* Rd = Rs + IB * LS;                  // [32] reciprocals of the diagonal
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
@@ -46,13 +49,18 @@ __global__ void __launch_bounds__(256, 1)
 
   for (int ib = jb; ib < nb; ib++) {
     const int rb = ib * IB;
-    const int K = rb - r0;
-    for (int e = tid; e < K * IB; e += blockDim.x) {
-      const int k = e >> 5, m = e & 31;
-      const int row = rb + m;
-      cp_async8(As + k * IS + m, L + (size_t)min(row, P - 1) + (size_t)(r0 + k) * P, row < P ? 8 : 0);
-    }
-    cp_async_commit();
+    const int nch = ib - jb;  // 32-column chunks of the finished rows
+    // L[rb.., r0 + 32 ch ..] streamed through two buffers, 32 columns at a time
+    auto stage = [&](int ch, int buf) {
+      double* dst = As + buf * IB * IS;
+      for (int e = tid; e < IB * IB; e += blockDim.x) {
+        const int k = e >> 5, m = e & 31;
+        const int row = rb + m;
+        cp_async8(dst + k * IS + m, L + (size_t)min(row, P - 1) + (size_t)(r0 + ch * IB + k) * P, row < P ? 8 : 0);
+      }
+      cp_async_commit();
+    };
+    if (nch > 0) stage(0, 0);
     for (int e = tid; e < IB * IB; e += blockDim.x) {
       const int q = e >> 5, m = e & 31;
       const int row = rb + m, col = rb + q;
@@ -61,16 +69,30 @@ __global__ void __launch_bounds__(256, 1)
       else v = (m == q) ? 1.0 : 0.0;
       Ld[m * LS + q] = v;
     }
-    cp_async_wait<0>();
-    __syncthreads();
 
-    // two accumulators over alternating K steps (K is a multiple of 32) break the DMMA chain
+    // two accumulators over alternating K steps break the DMMA chain; the K order is that of
+    // one pass over all the finished rows
     double acc[4] = {0.0, 0.0, 0.0, 0.0}, acc2[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int kb = 0; kb < K; kb += 8) {
-      dmma_16x8x4(acc, As[(kb + t) * IS + m0 + g], As[(kb + t) * IS + m0 + g + 8], Yp[(kb + t) * IS + n0 + g]);
-      dmma_16x8x4(acc2, As[(kb + 4 + t) * IS + m0 + g], As[(kb + 4 + t) * IS + m0 + g + 8],
-                  Yp[(kb + 4 + t) * IS + n0 + g]);
+    for (int ch = 0; ch < nch; ch++) {
+      if (ch + 1 < nch) {
+        stage(ch + 1, (ch + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      const double* as = As + (ch & 1) * IB * IS;
+      const double* yp = Yp + (size_t)ch * IB * IS;
+#pragma unroll
+      for (int kb = 0; kb < IB; kb += 8) {
+        dmma_16x8x4(acc, as[(kb + t) * IS + m0 + g], as[(kb + t) * IS + m0 + g + 8], yp[(kb + t) * IS + n0 + g]);
+        dmma_16x8x4(acc2, as[(kb + 4 + t) * IS + m0 + g], as[(kb + 4 + t) * IS + m0 + g + 8],
+                    yp[(kb + 4 + t) * IS + n0 + g]);
+      }
+      __syncthreads();  // the buffer is refilled two chunks on
     }
+    __syncthreads();  // Ld complete
+    const int K = nch * IB;
 #pragma unroll
     for (int h = 0; h < 2; h++)
 #pragma unroll
@@ -108,7 +130,7 @@ __global__ void __launch_bounds__(256, 1)
   }
 }
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
     k_lauum_panel(const double* __restrict__ V, int P, int64_t stride, double* __restrict__ S) {
   extern __shared__ __align__(16) double sm[];
   const int nb = (P + IB - 1) / IB;
@@ -118,7 +140,7 @@ __global__ void __launch_bounds__(256, 1)
   const int c0 = b * IB;
   const int ncol = min(IB, P - c0);
   double* Vb = sm;                          // [nb*32][IS]: Vb[k][n] = V[c0 + k][c0 + n]
-  double* Ak = Vb + (size_t)nb * IB * IS;   // [nb*32][IS]: Ak[k][m] = V[a0 + k][a0 + m]
+  double* Ak = Vb + (size_t)nb * IB * IS;   // [2][32][IS]: Ak[k][m] = V[a0 + 32 ch + k][a0 + m]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int m0 = (warp >> 2) * 16, n0 = (warp & 3) * 8;
   const int kb_rows = (P - c0 + 3) / 4 * 4;
@@ -132,22 +154,40 @@ __global__ void __launch_bounds__(256, 1)
   for (int a = b; a < nb; a++) {
     const int a0 = a * IB;
     const int K = (P - a0 + 3) / 4 * 4;
-    for (int e = tid; e < K * IB; e += blockDim.x) {
-      const int m = e / K, k = e - m * K;
-      const int row = a0 + k, col = a0 + m;
-      const bool ok = row < P && col < P;
-      cp_async8(Ak + k * IS + m, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();
+    const int nch = (K + IB - 1) / IB;
+    // the rows of block column a streamed through two buffers, 32 rows at a time
+    auto stage = [&](int ch, int buf) {
+      double* dst = Ak + buf * IB * IS;
+      const int k0 = ch * IB, kn = min(IB, K - k0);
+      for (int e = tid; e < kn * IB; e += blockDim.x) {
+        const int m = e / kn, k = e - m * kn;
+        const int row = a0 + k0 + k, col = a0 + m;
+        const bool ok = row < P && col < P;
+        cp_async8(dst + k * IS + m, Vm + (ok ? (size_t)row + (size_t)col * P : 0), ok ? 8 : 0);
+      }
+      cp_async_commit();
+    };
+    stage(0, 0);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int off = a0 - c0;
-    for (int kb = 0; kb < K; kb += 4) {
-      const double a0v = Ak[(kb + t) * IS + m0 + g];
-      const double a1v = Ak[(kb + t) * IS + m0 + g + 8];
-      const double b0v = Vb[(off + kb + t) * IS + n0 + g];
-      dmma_16x8x4(acc, a0v, a1v, b0v);
+    for (int ch = 0; ch < nch; ch++) {
+      if (ch + 1 < nch) {
+        stage(ch + 1, (ch + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      const double* ak = Ak + (ch & 1) * IB * IS;
+      const double* vb = Vb + (size_t)(off + ch * IB) * IS;
+      const int kn = min(IB, K - ch * IB);  // a multiple of 4
+      for (int kb = 0; kb < kn; kb += 4) {
+        const double a0v = ak[(kb + t) * IS + m0 + g];
+        const double a1v = ak[(kb + t) * IS + m0 + g + 8];
+        const double b0v = vb[(kb + t) * IS + n0 + g];
+        dmma_16x8x4(acc, a0v, a1v, b0v);
+      }
+      __syncthreads();  // the buffer is refilled two chunks on
     }
 #pragma unroll
     for (int h = 0; h < 2; h++)
@@ -160,24 +200,23 @@ __global__ void __launch_bounds__(256, 1)
           Sm[(size_t)col + (size_t)row * P] = acc[2 * h + e];
         }
       }
-    __syncthreads();
   }
 }
 
 // Batched Cholesky (cholPsi, ggplvm.cu:683-692), one CTA per gene, 32-column panels left to
 // right (left-looking): the panel is loaded into shared memory, takes the product of the
-// finished columns (DMMA, the finished part streamed through shared memory 32 columns at a
-// time), then its 32 x 32 diagonal block is factored by one warp (lane = row; each entry's sum
+// finished columns (DMMA, the finished part streamed through shared memory 8 columns at a
+// time, so that two CTAs share an SM), then its 32 x 32 diagonal block is factored by one warp (lane = row; each entry's sum
 // in increasing column order as in choldc) and the rows below solve against it (thread per
 // row). A non-positive pivot zero-fills the matrix, as choldc does. Reads the lower triangle,
 // writes the factor over it; the strict upper triangle is left as it was.
-__global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi, int P, int64_t stride) {
+__global__ void __launch_bounds__(256, 2) k_potrf_panel(double* __restrict__ Psi, int P, int64_t stride) {
   extern __shared__ __align__(16) double sm[];
   const int rows_pad = (P + 15) / 16 * 16;
   const int SA = rows_pad + 4;                 // La[q][r]: rows contiguous, 4 mod 16
   double* Ap = sm;                             // [rows_pad][IS]: the panel, Ap[r][c]
-  double* La = Ap + (size_t)rows_pad * IS;     // [2][32][SA]: finished columns, one 32-chunk
-  double* Rd = La + 2 * (size_t)IB * SA;       // [32] reciprocals of the diagonal
+  double* La = Ap + (size_t)rows_pad * IS;     // [2][CW][SA]: finished columns, one CW-chunk
+  double* Rd = La + 2 * (size_t)CW * SA;       // [32] reciprocals of the diagonal
   __shared__ int fail;
   double* A = Psi + (size_t)blockIdx.x * stride;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
@@ -192,7 +231,7 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
       Ap[r * IS + cc] = (r < rows && cc < ncol) ? A[(size_t)(c0 + r) + (size_t)(c0 + cc) * P] : 0.0;
     }
     if (kp > 0) {
-      // Ap -= L[c0.., 0..c0) L[c0..c0+32, 0..c0)^T, 32 finished columns per chunk
+      // Ap -= L[c0.., 0..c0) L[c0..c0+32, 0..c0)^T, CW finished columns per chunk
       double acc[2][4][4];
 #pragma unroll
       for (int x = 0; x < 2; x++)
@@ -201,26 +240,27 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
 #pragma unroll
           for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
       auto stage = [&](int ch, int buf) {
-        double* dst = La + (size_t)buf * IB * SA;
-        for (int e = tid; e < IB * rpad; e += blockDim.x) {
+        double* dst = La + (size_t)buf * CW * SA;
+        for (int e = tid; e < CW * rpad; e += blockDim.x) {
           const int q = e / rpad, r = e - q * rpad;
           const bool ok = r < rows;
-          cp_async8(dst + q * SA + r, A + (ok ? (size_t)(c0 + r) + (size_t)(ch * IB + q) * P : 0), ok ? 8 : 0);
+          cp_async8(dst + q * SA + r, A + (ok ? (size_t)(c0 + r) + (size_t)(ch * CW + q) * P : 0), ok ? 8 : 0);
         }
         cp_async_commit();
       };
       stage(0, 0);
-      for (int ch = 0; ch < kp; ch++) {
-        if (ch + 1 < kp) {
+      const int nch = c0 / CW;
+      for (int ch = 0; ch < nch; ch++) {
+        if (ch + 1 < nch) {
           stage(ch + 1, (ch + 1) & 1);
           cp_async_wait<1>();
         } else {
           cp_async_wait<0>();
         }
         __syncthreads();
-        const double* la = La + (size_t)(ch & 1) * IB * SA;
+        const double* la = La + (size_t)(ch & 1) * CW * SA;
 #pragma unroll
-        for (int k4 = 0; k4 < IB / 4; k4++) {
+        for (int k4 = 0; k4 < CW / 4; k4++) {
           const double* lr = la + (k4 * 4 + t) * SA;
           double b[4];
 #pragma unroll
@@ -256,9 +296,11 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
     // operations in the same order as the entry-by-entry form, with independent FMAs in place
     // of one dependent chain per entry.
     if (warp == 0) {
+      // rows past the panel (ncol < 32 only when P - c0 < 32, where the panel may hold 16 rows)
+      // are zeros in registers and never touch shared memory
       double a[IB];
 #pragma unroll
-      for (int q = 0; q < IB; q++) a[q] = Ap[lane * IS + q];
+      for (int q = 0; q < IB; q++) a[q] = lane < ncol ? Ap[lane * IS + q] : 0.0;
 #pragma unroll
       for (int cc = 0; cc < IB; cc++) {
         if (cc < ncol) {
@@ -279,8 +321,9 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
           }
         }
       }
+      if (lane < ncol)
 #pragma unroll
-      for (int q = 0; q < IB; q++) Ap[lane * IS + q] = a[q];
+        for (int q = 0; q < IB; q++) Ap[lane * IS + q] = a[q];
     }
     __syncthreads();
     for (int r = IB + tid; r < rows; r += blockDim.x) {
@@ -313,21 +356,24 @@ __global__ void __launch_bounds__(256, 1) k_potrf_panel(double* __restrict__ Psi
 
 int potrf_panel_smem(int P) {
   const int rows_pad = (P + 15) / 16 * 16;
-  return (int)sizeof(double) * (rows_pad * IS + 2 * IB * (rows_pad + 4) + IB);
+  return (int)sizeof(double) * (rows_pad * IS + 2 * CW * (rows_pad + 4) + IB);
 }
 
 int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride) {
   const int smem = potrf_panel_smem(n);
   if (smem > 220 * 1024) return GPL_ERR_ARG;
   GPL_TRY(c, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  GPL_TRY(c, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   k_potrf_panel<<<batch, 256, smem, c->stream>>>(A, n, stride);
   GPL_LAUNCHED(c, "k_potrf_panel");
   return GPL_OK;
 }
 
+// trtri: the panel's rows, two 32-column chunks of L, the diagonal and right-hand-side blocks;
+// lauum needs less (the panel's rows and two chunks). About 107 KB at P = 236: two CTAs per SM.
 int inverse_panel_smem(int P) {
   const int nb = (P + IB - 1) / IB;
-  return (int)sizeof(double) * (2 * nb * IB * IS + 2 * IB * LS + IB);
+  return (int)sizeof(double) * (nb * IB * IS + 2 * IB * IS + 2 * IB * LS + IB);
 }
 
 // Returns GPL_ERR_ARG when P is beyond the shared-memory budget of the panel kernels.
@@ -337,6 +383,8 @@ int launch_inverse_panels(Ctx* c) {
   if (smem > 220 * 1024) return GPL_ERR_ARG;
   GPL_TRY(c, cudaFuncSetAttribute(k_trtri_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   GPL_TRY(c, cudaFuncSetAttribute(k_lauum_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  GPL_TRY(c, cudaFuncSetAttribute(k_trtri_panel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  GPL_TRY(c, cudaFuncSetAttribute(k_lauum_panel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   const int64_t st = (int64_t)P * P;
   const int nb = (P + IB - 1) / IB;
   dim3 g(nb, c->J);
