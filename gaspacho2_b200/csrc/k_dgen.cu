@@ -1,14 +1,15 @@
 // FP64 tensor-core (DMMA) forms of the cell x gene contractions around the Gram: one
 // register-staged GEMM template whose operand loaders apply the element-wise prologues
-// (W/Omega, products with nu, the gathers of a cell group) and whose epilogues scatter the
-// results.
+// (W/Omega, products with nu, a cell group's slice) and whose epilogues scatter the results.
 //
 //   zt_u      bvec[dcol a, j] = sum_i D_ia u_ij (getZtOinvjnj util_cuda.cu:462-487 with
 //             u = W nu / Omega; initBeta init.cu:193-221 with u = y0), split over the cells
 //             into 8 ranges whose partial sums are added in order.  2*N*J*n_d flops.
 //   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
-//   group     S[j][g][a] = sum_{i in g} w_ij D_ia over the gathered cells of each group.
-//   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for the cells of each group.
+//   group     S[j][g][a] = sum_{i in g} w_ij D_ia, K = the group's cells, read from copies of
+//             W, D and 1/Omega in group order (each group a contiguous run of rows).
+//   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for 128-cell tiles of each group, O read
+//             from the group-ordered copies and HK scattered back to the cells.
 //
 // Tile: 8 warps as WARPS_M x WARPS_N, each warp WM x WN DMMA tiles of 16 x 8, K slices of 16
 // staged through registers (the next slice's global loads are in flight during the current
