@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) k_group_sums(int N, int ldN, int J, int n
 // mode 2: w = 1, u = y0 (scratch).
 template <int MODE>
 __global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gcells, const int* __restrict__ gstart,
-                          const double* __restrict__ W, const double* __restrict__ Omega,
+                          const double* __restrict__ Wg, const double* __restrict__ Omega,
                           const double* __restrict__ U, double* __restrict__ T) {
   const int g = blockIdx.x;
   const int j = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -111,7 +111,12 @@ __global__ void k_group_t(int ldN, int J, int n_grp, const int* __restrict__ gce
   for (int k = c0 + lane; k < c1; k += 32) {
     const int i = gcells[k];
     const size_t e = (size_t)j * ldN + i;
-    s += MODE == 0 ? W[e] / Omega[i] * U[e] : MODE == 4 ? W[e] / Omega[i] * U[i] : U[e];
+    if (MODE == 2) {
+      s += U[e];
+    } else {
+      const double w = Wg[(size_t)j * ldN + k];  // W of cell i, read in group order
+      s += MODE == 0 ? w / Omega[i] * U[e] : w / Omega[i] * U[i];
+    }
   }
   s = warp_sum(s);
   if (lane == 0) T[(size_t)j * n_grp + g] = s;
@@ -142,13 +147,13 @@ int launch_group_sums(Ctx* c, int mode) {
   ProfScope pt(c, "group_t");
   dim3 g(c->n_grp, div_up(c->J, 8));
   if (mode == 2)
-    k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+    k_group_t<2><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->Wg, c->Omega,
                                            c->scratch, c->gT);
   else if (mode == 4)  // u per cell, the same for every gene
-    k_group_t<4><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+    k_group_t<4><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->Wg, c->Omega,
                                            c->zt_u_src, c->gT);
   else
-    k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->W, c->Omega,
+    k_group_t<0><<<g, 256, 0, c->stream>>>(c->ldN, c->J, c->n_grp, c->gcells_d, c->gstart_d, c->Wg, c->Omega,
                                            c->zt_u_src ? c->zt_u_src : c->Nu, c->gT);
   GPL_LAUNCHED(c, "k_group_t");
   return GPL_OK;
