@@ -183,6 +183,7 @@ class CpuSample:
         from oracle import port, refcpu
 
         sub = synth.gene_subset(ds, genes)
+        self.sub = sub
         self.threads = os.cpu_count() or 1
         if refcpu.available():
             self.m = refcpu.RefModel.from_dataset(sub)
@@ -208,6 +209,45 @@ class CpuSample:
         self.m.objective(0, self.slot)
         self.slot += 1
         return (time.perf_counter() - t0) * self.scale
+
+
+PARITY_TOL = 1e-8  # per-buffer relative error of the FP64 path against the reference's kernels
+
+
+def bench_parity(cs, device, stream):
+    """The CUDA path against the reference's kernels built for the host at the bench's shape:
+    the CPU sample's genes with all cells (M, Q, P and the cell ranges of the full workload),
+    the same call sequence on a context over those genes (GLM initialisation, one IRLS sweep,
+    the objective, then one gradient and one objective as the CPU step runs them), compared
+    per gene (the Laplace objective pieces l_j, tilde-beta_j, the diagonal of each factored
+    Psi_j) and on the whole gradient (every cell-summed block over those genes) and the
+    objective. Errors are max |a - b| / max |b| per buffer."""
+    from gaspacho2_b200 import GPLVM
+
+    sub, ref = cs.sub, cs.m
+    with GPLVM.from_dataset(sub, device=device, stream=stream.cuda_stream, precision="fp64") as m:
+        m.set_params(sub.init)
+        m.kernel_mats()
+        m.glm_init()
+        m.irls_sweep(0, 0)
+        m.objective_after_irls(0)
+        g = m.gradient()
+        v = m.objective(0, 1)
+        P, J = m.P, m.J
+        got = {"objective": np.array([v]), "grad": g, "lkhds": m.get("lkhds"), "tBeta": m.get("tBeta"),
+               "Psi_diag": m.get("Psi").reshape(J, P, P)[:, np.arange(P), np.arange(P)].ravel()}
+    want = {"objective": np.array([ref.get("lkhd")[cs.slot - 1]]), "grad": ref.get("grad")[:g.shape[0]],
+            "lkhds": ref.get("lkhds"), "tBeta": ref.get("tBeta"),
+            "Psi_diag": ref.get("Psi")[:J * P * P].reshape(J, P, P)[:, np.arange(P), np.arange(P)].ravel()}
+    errs = {}
+    for k in got:
+        a, b = np.asarray(got[k], np.float64), np.asarray(want[k], np.float64)
+        fin = np.isfinite(b)
+        errs[k] = float("inf") if not np.array_equal(fin, np.isfinite(a)) else \
+            float(np.abs(a[fin] - b[fin]).max() / max(np.abs(b[fin]).max(), 1e-300))
+    return {"against": f"the reference's kernels built for the host ({cs.kind}), same state and call sequence",
+            "genes": int(J), "cells": int(sub.N), "max_rel_err": errs, "tol": PARITY_TOL,
+            "pass": bool(all(e <= PARITY_TOL for e in errs.values()))}
 
 
 def dataset(args):
@@ -533,7 +573,7 @@ def run_ours(args):
         P = m.P
         ft = flops_table(m.N, m.J, m.M, P, m.n_dense())
         peaks = measured_peaks()
-        tc_kernels = ("gram",) if os.environ.get("GPL_TC_GRAD", "1") == "0" else ("gram", "uq")
+        tc_kernels = ("gram", "uq") if m.get_option("tc_grad") else ("gram",)
         if dom in ft and args.precision == "bf16x3" and dom in tc_kernels:
             # useful flops of the contraction; the hi/lo split issues 3 BF16 products per useful MAC
             tflops = ft[dom]
@@ -583,6 +623,7 @@ def run_ours(args):
         t = cs.step()
         line["cpu_baseline"] = {"value": 1.0 / t, "unit": "evals/s", "cores": cs.threads, "kind": cs.kind,
                                 "sample": cs.desc}
+        line["parity"] = bench_parity(cs, local, stream)
     if rank == 0:
         print(json.dumps(line), flush=True)
     rep.close()

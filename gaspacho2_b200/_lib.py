@@ -26,6 +26,8 @@ SIGNATURES = {
     "gpl_destroy": (ctypes.c_int, [_vp]),
     "gpl_last_error": (ctypes.c_char_p, [_vp]),
     "gpl_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gpl_set_option": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+    "gpl_get_option": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_load_counts": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp]),
     "gpl_load_design": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _ip, _vp, ctypes.c_int64, ctypes.c_int,
                                        ctypes.c_int]),

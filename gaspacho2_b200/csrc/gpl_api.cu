@@ -521,10 +521,48 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
     return GPL_ERR_ARG;
   }
   c->precision = precision;
-  c->tc.check_each = getenv("GPL_TC_CHECK") != nullptr;
-  c->simt_fp64 = getenv("GPL_FP64_SIMT") != nullptr;
-  if (const char* tg = getenv("GPL_TC_GRAD")) c->tc_grad = atoi(tg) != 0;
-  if (const char* rs = getenv("GPL_REFINE")) c->refine_steps = atoi(rs);
+  return GPL_OK;
+}
+
+int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
+  if (!h || !name) return GPL_ERR_ARG;
+  Ctx* c = C(h);
+  const std::string s(name);
+  if (s == "tc_grad") {
+    c->tc_grad = value != 0;
+  } else if (s == "refine_steps") {
+    if (value < 0 || value > 16) { c->err = "refine_steps must be in 0..16"; return GPL_ERR_ARG; }
+    c->refine_steps = (int)value;
+  } else if (s == "tc_run") {
+    if (value < 1 || value > 64) { c->err = "tc_run must be in 1..64"; return GPL_ERR_ARG; }
+    c->tc_run = (int)value;
+    c->tc.run = (int)value;
+  } else if (s == "tc_check") {
+    c->tc_check = value != 0;
+  } else if (s == "pair_range_cells") {
+    if (value < 0) { c->err = "pair_range_cells must be >= 0"; return GPL_ERR_ARG; }
+    if (value != c->pair_range_cells) {
+      GPL_TRY(c, cudaStreamSynchronize(c->stream));
+      pair_release(c);  // the range size fixes the buffers: sized again on next use
+    }
+    c->pair_range_cells = value;
+  } else {
+    c->err = "unknown option: " + s;
+    return GPL_ERR_ARG;
+  }
+  return GPL_OK;
+}
+
+int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
+  if (!h || !name || !value) return GPL_ERR_ARG;
+  const Ctx* c = &h->c;
+  const std::string s(name);
+  if (s == "tc_grad") *value = c->tc_grad ? 1 : 0;
+  else if (s == "refine_steps") *value = c->refine_steps;
+  else if (s == "tc_run") *value = c->tc_run;
+  else if (s == "tc_check") *value = c->tc_check ? 1 : 0;
+  else if (s == "pair_range_cells") *value = c->pair_range_cells;
+  else return GPL_ERR_ARG;
   return GPL_OK;
 }
 

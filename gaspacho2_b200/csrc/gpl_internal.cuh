@@ -52,7 +52,7 @@ struct DevBuf {
 // Column-pair FP64 GEMM state (k_dgemm.cu): the pair list (a <= b over the dense columns),
 // 1/Omega, the gathered Psi^{-1} pairs per gene and a range of V rows.
 struct PairState {
-  bool ready = false;
+  bool ready = false, wide = false;  // wide: more dense columns than the pair GEMMs stage
   int n_pairs = 0, pairs_pad = 0, cpad = 0, v_cells = 0;
   int smem_gram = 0, smem_v = 0, smem_vu = 0;
   int2* pairs = nullptr;
@@ -61,7 +61,7 @@ struct PairState {
 };
 
 struct TcState {
-  bool ready = false, check_each = false;
+  bool ready = false;
   int cpad = 0, chunks_cells = 0, gram_tiles_n = 0, Jpad = 0;
   int n_pairs = 0, pair_tiles = 0;
   int smem_gram = 0, smem_whiten = 0, run = 4;  // run: K chunks per FP32 accumulator run
@@ -98,7 +98,10 @@ struct Ctx {
   double* zeta = nullptr;  // the DE driver's zeta (P)
   int de_quirk_col = -1;   // dense column whose first cell holds the null model's loader value
   double de_quirk_orig = 0.0;
-  bool simt_fp64 = false;  // FP64 Gram/gradient contraction on the FFMA kernels instead of DMMA
+  // options (gpl_set_option)
+  bool tc_check = false;      // read the tensor-core error flag after every tensor-core launch
+  int tc_run = 4;             // precision form: K chunks per FP32 accumulator run before the FP64 fold
+  int64_t pair_range_cells = 0;  // cells per range of the pair GEMMs (0: as many as 8 GiB holds)
   std::string err;
 
   // sizes
@@ -232,7 +235,7 @@ int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride);  /
 int launch_inverse_panels(Ctx* c);       // the same in 32-column panels with DMMA block products
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA
-void launch_chol_exact_raw(cudaStream_t st, double* A, int n);
+cudaError_t launch_chol_exact_raw(cudaStream_t st, double* A, int n);  // the launch's own status
 int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
                            const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork);
 // k_tc.cu (precision form)

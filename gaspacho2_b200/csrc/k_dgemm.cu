@@ -364,39 +364,39 @@ int pair_prepare(Ctx* c) {
   s.cpad = (c->N + BM - 1) / BM * BM;
   // V (the gradient's V rows, or the Gram's pair products) holds a range of cells at a time:
   // all cells when that fits in 8 GiB (one range: the Gram writes Psi directly), else ranges
-  // of at most 8 GiB. GPL_PAIR_RANGE_CELLS sets a smaller range (tests of the multi-range path).
+  // of at most 8 GiB. The option pair_range_cells sets a smaller range (tests of the multi-range path).
   const size_t row = (size_t)s.pairs_pad * sizeof(double);
   size_t cap = std::max<size_t>(BM, ((size_t)8 << 30) / row / BM * BM);
-  if (const char* e = getenv("GPL_PAIR_RANGE_CELLS")) {
-    const long v = atol(e);
-    if (v >= BM) cap = std::min<size_t>(cap, (size_t)v / BM * BM);
-  }
+  if (c->pair_range_cells >= BM) cap = std::min<size_t>(cap, (size_t)c->pair_range_cells / BM * BM);
   s.v_cells = (int)std::min<size_t>((size_t)s.cpad, cap);
+  s.smem_gram = (int)sizeof(double) * 3 * (BK * SA + BN * SBT);
+  s.smem_v = (int)sizeof(double) * 3 * (BK * SA + BK * SBN);
+  s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
+  // more dense columns than k_v_to_u stages per cell: the pair GEMMs are not used (their
+  // callers take the FFMA forms); the pair list and 1/Omega still serve the other kernels
+  s.wide = s.smem_vu > 200 * 1024;
   if (cudaMalloc((void**)&s.pairs, sizeof(int2) * pairs.size()) != cudaSuccess ||
       cudaMalloc((void**)&s.rOm, sizeof(double) * s.cpad) != cudaSuccess ||
-      cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess ||
-      cudaMalloc((void**)&s.V, sizeof(double) * (size_t)s.v_cells * s.pairs_pad) != cudaSuccess) {
+      (!s.wide && cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess) ||
+      (!s.wide && cudaMalloc((void**)&s.V, sizeof(double) * (size_t)s.v_cells * s.pairs_pad) != cudaSuccess)) {
     cudaGetLastError();
+    pair_release(c);
     c->err = "device allocation failed: pair GEMM buffers";
     return GPL_ERR_ALLOC;
   }
   GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  if (s.v_cells < c->N &&
+  if (!s.wide && s.v_cells < c->N &&
       cudaMalloc((void**)&s.Gacc, sizeof(double) * (size_t)s.n_pairs * c->J) != cudaSuccess) {
     cudaGetLastError();
+    pair_release(c);
     c->err = "device allocation failed: pair Gram accumulator";
     return GPL_ERR_ALLOC;
   }
-  s.smem_gram = (int)sizeof(double) * 3 * (BK * SA + BN * SBT);
-  s.smem_v = (int)sizeof(double) * 3 * (BK * SA + BK * SBN);
-  s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
-  if (s.smem_vu > 200 * 1024) {
-    c->err = "too many dense model columns for the staged pair contraction";
-    return GPL_ERR_ARG;
+  if (!s.wide) {
+    GPL_TRY(c, cudaFuncSetAttribute(k_pair_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_gram));
+    GPL_TRY(c, cudaFuncSetAttribute(k_pair_v, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_v));
+    GPL_TRY(c, cudaFuncSetAttribute(k_v_to_u, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_vu));
   }
-  GPL_TRY(c, cudaFuncSetAttribute(k_pair_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_gram));
-  GPL_TRY(c, cudaFuncSetAttribute(k_pair_v, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_v));
-  GPL_TRY(c, cudaFuncSetAttribute(k_v_to_u, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_vu));
   s.ready = true;
   return GPL_OK;
 }
@@ -430,6 +430,7 @@ int launch_pair_gram(Ctx* c) {
   int rc = pair_prepare(c);
   if (rc) return rc;
   PairState& s = c->pr;
+  if (s.wide) return GPL_ERR_ARG;
   if ((rc = launch_recip(c))) return rc;
   ProfScope ps(c, "gram");
   const bool one = s.v_cells >= c->N;
@@ -457,6 +458,7 @@ int launch_pair_gram(Ctx* c) {
 int launch_pair_uq(Ctx* c) {
   int rc = pair_prepare(c);
   if (rc) return rc;
+  if (c->pr.wide) return GPL_ERR_ARG;
   PairState& s = c->pr;
   if ((rc = launch_recip(c))) return rc;
   {

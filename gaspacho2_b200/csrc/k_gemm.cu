@@ -282,13 +282,13 @@ int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out) {
     ProfScope ps(c, "zt_u");
     dim3 g(div_up(c->n_d, TM), div_up(c->J, TN));
     LoadDt A{c->Dm, c->ldN, c->N, c->n_d};
-    const int rc = c->simt_fp64 ? GPL_ERR_ARG : dgen_zt_u(c, mode, u, out);
+    const int rc = dgen_zt_u(c, mode, u, out);
     if (rc != GPL_OK && rc != GPL_ERR_ARG) return rc;
     if (rc == GPL_ERR_ARG && mode == 2) {
       c->err = "per-cell Z^T u needs the DMMA form (at most 144 dense columns)";
       return GPL_ERR_ARG;
     }
-    if (rc == GPL_ERR_ARG) {  // the FFMA form: forced, or more dense columns than one DMMA tile
+    if (rc == GPL_ERR_ARG) {  // the FFMA form: more dense columns than one DMMA tile
       if (mode == 0)
         k_gemm_store<<<g, 256, 0, c->stream>>>(c->n_d, c->J, c->N, A,
                                                LoadOinvNu{c->W, u, c->Omega, c->ldN, c->N, c->J}, out,
@@ -309,7 +309,10 @@ int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out) {
 // C1 <- sum_j (tn_ij/phi_j) tBeta_j[GP]   (stored cell-fastest, ld ldN)
 int launch_c1_tn(Ctx* c) {
   ProfScope ps(c, "c1_tn");
-  if (!c->simt_fp64) return dgen_c1_tn(c);
+  {
+    const int rc = dgen_c1_tn(c);
+    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: more dense columns than one DMMA tile
+  }
   const int g0 = c->nh[c->p - 1];
   dim3 g(div_up(c->N, TM), div_up(c->M, TN));
   k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->M, c->J,

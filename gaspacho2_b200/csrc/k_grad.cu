@@ -250,10 +250,9 @@ int launch_grad_omega(Ctx* c) {
   if (c->precision == GPL_PREC_BF16X3 && c->tc_grad) {
     rc = launch_tc_grad(c);
     if (rc) return rc;
-  } else if (!c->simt_fp64) {
-    rc = launch_pair_uq(c);
+  } else if ((rc = launch_pair_uq(c)) != GPL_ERR_ARG) {
     if (rc) return rc;
-  } else {
+  } else {  // more dense columns than the staged pair contraction holds
     ProfScope ps(c, "uq");
     const int n_dp = div_up(c->n_d, TK) * TK;
     dim3 g(div_up(c->N, TM), div_up(c->n_d, TN));

@@ -257,29 +257,28 @@ int launch_gram(Ctx* c, bool unweighted) {
   const int nb = div_up(c->n_d, GB);
   const int npairs = nb * (nb + 1) / 2;
   const int J = unweighted ? 1 : c->J;
-  if (!unweighted && c->precision == GPL_PREC_BF16X3) {
-    int rc = launch_tc_gram(c);
-    if (rc) return rc;
-  } else if (!unweighted && !c->simt_fp64) {
-    int rc = launch_pair_gram(c);
-    if (rc) return rc;
-  } else {
+  int rc = GPL_ERR_ARG;
+  if (!unweighted) rc = c->precision == GPL_PREC_BF16X3 ? launch_tc_gram(c) : launch_pair_gram(c);
+  if (rc != GPL_OK && !(rc == GPL_ERR_ARG && c->precision == GPL_PREC_FP64)) return rc;
+  if (rc == GPL_ERR_ARG) {
+    // the unweighted Gram of one gene (GLM initialisation), or more dense columns than the
+    // staged pair contraction holds
     ProfScope ps(c, "gram");
     dim3 g(npairs, div_up(J, GG));
     k_gram<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->n_d, c->P, J, c->Dm, c->dcol_d, c->W, c->Omega, c->DeltaInv,
                                      c->Psi, unweighted ? 1 : 0);
     GPL_LAUNCHED(c, "k_gram");
   }
-  int rc = launch_group_sums(c, unweighted ? 1 : 0);
+  rc = launch_group_sums(c, unweighted ? 1 : 0);
   if (rc) return rc;
   return launch_assemble_psi(c, J);
 }
 
 int launch_chol_batched(Ctx* c, double* A, int n, int batch, int64_t stride) {
   ProfScope ps(c, "chol");
-  if (!c->simt_fp64) {
+  {
     const int rc = launch_potrf_panels(c, A, n, batch, stride);
-    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: n beyond the panel kernel's shared memory
+    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: n beyond the panel kernel's checked range
   }
   k_chol<<<batch, 256, 0, c->stream>>>(A, n, stride, 0);
   GPL_LAUNCHED(c, "k_chol");
@@ -298,7 +297,10 @@ int launch_chol_single(Ctx* c, double* A, int n) {
   return GPL_OK;
 }
 
-void launch_chol_exact_raw(cudaStream_t st, double* A, int n) { k_chol_exact<<<1, 256, 0, st>>>(A, n); }
+cudaError_t launch_chol_exact_raw(cudaStream_t st, double* A, int n) {
+  void* args[] = {&A, &n};
+  return cudaLaunchKernel((const void*)k_chol_exact, dim3(1), dim3(256), args, 0, st);
+}
 
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out) {
   k_cholinv_exact<<<div_up(n, 64), 64, 0, c->stream>>>(L, n, out);
@@ -322,9 +324,9 @@ int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const 
 int launch_inverse_batched(Ctx* c) {
   const int64_t st = (int64_t)c->P * c->P;
   ProfScope ps(c, "inverse");
-  if (!c->simt_fp64) {
+  {
     const int rc = launch_inverse_panels(c);
-    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: P beyond the panel kernels' shared memory
+    if (rc != GPL_ERR_ARG) return rc;  // GPL_ERR_ARG: P beyond the panel kernels' checked range
   }
   k_trtri<<<c->J, 256, 0, c->stream>>>(c->Psi, c->P, st, c->scratch);
   GPL_LAUNCHED(c, "k_trtri");

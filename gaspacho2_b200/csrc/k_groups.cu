@@ -129,7 +129,7 @@ int launch_group_sums(Ctx* c, int mode) {
   if (c->n_grp == 0) return GPL_OK;
   if (mode == 0 || mode == 1) {
     ProfScope ps(c, "group_sums");
-    if (!c->simt_fp64) {
+    {
       const int rc = dgen_group_sums(c, mode);
       if (rc != GPL_ERR_ARG) return rc;
     }
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256) k_hk(int ldN, int J, int n_d, int n_grp, 
 int launch_hk(Ctx* c) {
   if (c->n_grp == 0) return GPL_OK;
   ProfScope ps(c, "hk");
-  if (!c->simt_fp64) {
+  {
     const int rc = dgen_hk(c);
     if (rc != GPL_ERR_ARG) return rc;
   }

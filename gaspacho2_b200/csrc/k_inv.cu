@@ -29,6 +29,13 @@ constexpr int IB = 32;  // block size
 constexpr int IS = 36;  // shared row stride (doubles): conflict-free fragment loads
 constexpr int LS = 33;  // shared row stride of the 32 x 32 diagonal and right-hand-side blocks
 constexpr int CW = 8;   // finished columns per chunk of the Cholesky's panel update
+// Largest P each kernel is launched for. k_potrf_panel's update covers 256 rows of a panel
+// (8 warps x 2 row tiles of 16), so its panels below the first may hold at most 256 rows:
+// P <= 288. The inverse panels hold any P their shared memory admits (P <= 640 within 220 KiB).
+// tests/index_mirror/k_inv_mirror.c replays every shared- and global-memory index of the
+// three kernels on the CPU for every P up to these limits.
+constexpr int kPotrfMaxP = 288;
+constexpr int kInverseMaxP = 640;
 }  // namespace
 
 __global__ void __launch_bounds__(256, 2)
@@ -361,7 +368,7 @@ int potrf_panel_smem(int P) {
 
 int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride) {
   const int smem = potrf_panel_smem(n);
-  if (smem > 220 * 1024) return GPL_ERR_ARG;
+  if (n > kPotrfMaxP || smem > 220 * 1024) return GPL_ERR_ARG;
   GPL_TRY(c, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   GPL_TRY(c, cudaFuncSetAttribute(k_potrf_panel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   k_potrf_panel<<<batch, 256, smem, c->stream>>>(A, n, stride);
@@ -376,11 +383,11 @@ int inverse_panel_smem(int P) {
   return (int)sizeof(double) * (nb * IB * IS + 2 * IB * IS + 2 * IB * LS + IB);
 }
 
-// Returns GPL_ERR_ARG when P is beyond the shared-memory budget of the panel kernels.
+// Returns GPL_ERR_ARG when P is beyond the panel kernels' checked range.
 int launch_inverse_panels(Ctx* c) {
   const int P = c->P;
   const int smem = inverse_panel_smem(P);
-  if (smem > 220 * 1024) return GPL_ERR_ARG;
+  if (P > kInverseMaxP || smem > 220 * 1024) return GPL_ERR_ARG;
   GPL_TRY(c, cudaFuncSetAttribute(k_trtri_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   GPL_TRY(c, cudaFuncSetAttribute(k_lauum_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   GPL_TRY(c, cudaFuncSetAttribute(k_trtri_panel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));

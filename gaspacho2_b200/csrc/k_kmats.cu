@@ -54,7 +54,7 @@ __global__ void k_kmm(int M, int Q, int lv, const double* __restrict__ T, const 
   else if (ii > j) val = 0.0;
   else val = exp(-kern_sum(T, (size_t)M, ii, T, M, j, rho, Q, lv));
   K[ii + j * M] = val;
-  Kinv[ii + j * M] = val;
+  if (Kinv) Kinv[ii + j * M] = val;  // no copy when the caller needs Kmm once (Kinv == nullptr)
 }
 
 // The DE driver's null model as a design whose GP block is inert: Knm = 0, Kmm = Kinv = I,
@@ -148,16 +148,26 @@ int launch_expand_delta(Ctx* c) {
 
 // The kernel-matrix sequence on caller-supplied buffers, without a context: Knm and the
 // cell-fastest Kmm^{-1} k_n (both N x M, ld N), titsias (N), and an M x M work matrix that
-// receives Kmm and then its factor. Returns a cudaError_t.
+// receives Kmm and then its factor. Each launch goes through cudaLaunchKernel, whose return
+// value is that launch's own status (an error left on the thread by earlier, unrelated work is
+// neither reported nor cleared). Returns the first failing launch's cudaError_t, else
+// cudaSuccess.
 int launch_kernel_mats_raw(cudaStream_t st, int N, int M, int Q, const double* X, const double* T,
                            const double* rho, double* Knm, double* KinvKmn, double* titsias, double* Lwork) {
-  dim3 g(div_up(N, 128), M);
-  k_knm<<<g, 128, 0, st>>>(N, N, M, Q, -1, X, T, rho, Knm);
-  dim3 g2(div_up(M, 64), M);
-  k_kmm<<<g2, 64, 0, st>>>(M, Q, -1, T, rho, Lwork, Lwork);
-  launch_chol_exact_raw(st, Lwork, M);
-  k_kinvkmn<<<div_up(N, 128), 128, 0, st>>>(N, N, M, Lwork, Knm, KinvKmn, titsias);
-  return (int)cudaGetLastError();
+  int ldN = N, lv = kLvAll;
+  double* no_copy = nullptr;
+  void* a_knm[] = {&N, &ldN, &M, &Q, &lv, &X, &T, &rho, &Knm};
+  cudaError_t e = cudaLaunchKernel((const void*)k_knm, dim3(div_up(N, 128), M), dim3(128), a_knm, 0, st);
+  if (e != cudaSuccess) return (int)e;
+  void* a_kmm[] = {&M, &Q, &lv, &T, &rho, &Lwork, &no_copy};
+  e = cudaLaunchKernel((const void*)k_kmm, dim3(div_up(M, 64), M), dim3(64), a_kmm, 0, st);
+  if (e != cudaSuccess) return (int)e;
+  e = launch_chol_exact_raw(st, Lwork, M);
+  if (e != cudaSuccess) return (int)e;
+  const double* L = Lwork;
+  void* a_kk[] = {&N, &ldN, &M, &L, &Knm, &KinvKmn, &titsias};
+  e = cudaLaunchKernel((const void*)k_kinvkmn, dim3(div_up(N, 128)), dim3(128), a_kk, 0, st);
+  return (int)e;
 }
 
 }  // namespace gpl

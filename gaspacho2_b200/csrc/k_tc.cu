@@ -52,7 +52,7 @@ constexpr int kThreadsGram = 192;       // TMA, MMA and 4 drain warps
 constexpr int kStagesGram = 3;          // pipeline depth (192 KB of operand tiles)
 constexpr int kMaxStages = 3;
 constexpr int kGramN = 128;             // genes per Gram tile
-constexpr int kSBGram = 4;              // chunks per FP32 run (default; GPL_TC_RUN overrides)
+constexpr int kSBGram = 4;              // chunks per FP32 run (default; the option tc_run overrides)
 constexpr int kTileA = 128 * 128;       // 128 rows x 64 BF16
 constexpr int kTileBG = kGramN * 128;   // 128 gene rows x 64 BF16
 constexpr int kMaxWhiten = 160;         // dense columns the whitened rows kernel holds per cell
@@ -483,8 +483,7 @@ int tc_prepare(Ctx* c) {
     c->err = "cuTensorMapEncodeTiled failed";
     return GPL_ERR_CUDA;
   }
-  t.run = kSBGram;
-  if (const char* r = getenv("GPL_TC_RUN")) t.run = std::max(1, atoi(r));
+  t.run = c->tc_run > 0 ? c->tc_run : kSBGram;
   t.smem_gram = 1024 + kStagesGram * (2 * kTileA + 2 * kTileBG) + (int)sizeof(TcShared) + 128 * (int)sizeof(int2);
   GPL_TRY(c, cudaFuncSetAttribute(k_tc_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_gram));
   t.ready = true;
@@ -497,9 +496,7 @@ void tc_release(Ctx* c) {
                   t.ohi, t.olo};
   for (void* p : bufs)
     if (p) cudaFree(p);
-  const bool keep = t.check_each;
   t = TcState();
-  t.check_each = keep;
 }
 
 static int tc_check_flag(Ctx* c) {
@@ -553,7 +550,7 @@ int launch_tc_gram(Ctx* c) {
     ProfScope ps(c, "unwhiten");
     if ((rc = dgen_unwhiten(c, t.Gt, t.Tt, t.Lw))) return rc;
   }
-  return c->tc.check_each ? tc_check_flag(c) : GPL_OK;
+  return c->tc_check ? tc_check_flag(c) : GPL_OK;
 }
 
 // The gradient contraction on tensor cores, over the column pairs of the whitened columns:
@@ -594,7 +591,7 @@ int launch_tc_grad(Ctx* c) {
     k_unwhiten_u<<<div_up(c->N, 128), 128, t.smem_whiten, c->stream>>>(c->N, c->ldN, c->n_d, t.Lw, c->U);
     GPL_LAUNCHED(c, "k_unwhiten_u");
   }
-  return c->tc.check_each ? tc_check_flag(c) : GPL_OK;
+  return c->tc_check ? tc_check_flag(c) : GPL_OK;
 }
 
 int tc_error_flag(Ctx* c) { return c->tc.ready ? tc_check_flag(c) : GPL_OK; }

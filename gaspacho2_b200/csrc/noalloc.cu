@@ -17,9 +17,15 @@
 //     call overwrites the M x M block it uses before reading it, so nothing needs clearing,
 //     but two calls whose kernels overlap on the GPU (different streams, or host threads
 //     racing) corrupt each other's factor: serialise them, e.g. on one stream.
-//   - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current) and caches it; make that first call before any stream
-//     capture begins. Later calls on the device only launch kernels.
+//   - Every call on a stream that is not being captured looks up the array's device address
+//     (cudaGetSymbolAddress, with the caller's device current) and remembers it per device;
+//     a call made while its stream is being captured uses the remembered address, so make
+//     one call on the device before any capture begins (a capture with none yet is refused
+//     with GPL_ERR_STATE). Looking the address up again outside capture keeps it right after
+//     a cudaDeviceReset or in another context, where the module is loaded anew.
+//   - A Kmm that is not positive definite (non-positive pivot) leaves its factor zero-filled,
+//     as the reference's choldc does; Kmm^-1 k_n and titsias are then inf/NaN and the call
+//     still returns GPL_OK (it only enqueues work and never reads results back).
 #include <mutex>
 
 #include "gpl_internal.cuh"
@@ -36,20 +42,19 @@ std::mutex g_mu;
 double* g_work_ptr[kMaxDevices] = {nullptr};
 
 // Device address of g_kmm_work on the current device (host code cannot use the symbol's
-// name as a pointer: on the host it only stands in for the device object).
-int work_pointer(double** out) {
+// name as a pointer: on the host it only stands in for the device object). Looked up anew
+// unless `capturing`, when the address remembered from an earlier call is used.
+int work_pointer(bool capturing, double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return GPL_ERR_CUDA;
   if (dev < 0 || dev >= kMaxDevices) return GPL_ERR_LIMIT;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_work_ptr[dev]) {
+  if (!capturing) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_kmm_work) != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return GPL_ERR_CUDA;
-    }
+    if (cudaGetSymbolAddress(&p, g_kmm_work) != cudaSuccess || p == nullptr) return GPL_ERR_CUDA;
     g_work_ptr[dev] = static_cast<double*>(p);
   }
+  if (!g_work_ptr[dev]) return GPL_ERR_STATE;
   *out = g_work_ptr[dev];
   return GPL_OK;
 }
@@ -60,10 +65,12 @@ extern "C" int gpl_kernel_mats_noalloc(int N, int M, int Q, const double* X, con
                                        double* Knm, double* KinvKmn, double* titsias, void* stream) {
   if (N <= 0 || M <= 0 || Q <= 0 || !X || !T || !rho || !Knm || !KinvKmn || !titsias) return GPL_ERR_ARG;
   if (M > kMaxM) return GPL_ERR_LIMIT;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return GPL_ERR_CUDA;
   double* work = nullptr;
-  const int rc = work_pointer(&work);
+  const int rc = work_pointer(cap != cudaStreamCaptureStatusNone, &work);
   if (rc != GPL_OK) return rc;
-  const int e = gpl::launch_kernel_mats_raw(static_cast<cudaStream_t>(stream), N, M, Q, X, T, rho, Knm, KinvKmn,
-                                            titsias, work);
+  const int e = gpl::launch_kernel_mats_raw(st, N, M, Q, X, T, rho, Knm, KinvKmn, titsias, work);
   return e == 0 ? GPL_OK : GPL_ERR_CUDA;
 }

@@ -83,6 +83,15 @@ class GPLVM:
     def set_precision(self, precision: str):
         self._c(self._L.gpl_set_precision(self.h, _lib.PREC[precision]), "gpl_set_precision")
 
+    def set_option(self, name: str, value: int) -> None:
+        """A named integer option of the context (gpl_set_option)."""
+        self._c(self._L.gpl_set_option(self.h, name.encode(), int(value)), f"gpl_set_option({name})")
+
+    def get_option(self, name: str) -> int:
+        v = ctypes.c_int64()
+        self._c(self._L.gpl_get_option(self.h, name.encode(), ctypes.byref(v)), f"gpl_get_option({name})")
+        return v.value
+
     def set_params(self, prm) -> None:
         flat = [np.ascontiguousarray(a, dtype=np.float64) for a in prm.flat()]
         self._keep = flat

@@ -64,6 +64,20 @@ GPL_API const char* gpl_last_error(const gpl_ctx* ctx);
 /* Selects GPL_PREC_FP64 (default) or GPL_PREC_BF16X3 for the following calls. */
 GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
 
+/* Named integer options of a context (no reference counterpart; the reference hard-codes its
+ * schedule). Unknown names and out-of-range values give GPL_ERR_ARG.
+ *   "tc_grad"           precision form: the gradient contraction on tensor cores (1, default)
+ *                       or in FP64 (0)
+ *   "refine_steps"      precision form: FP64-residual refinement steps per solve (0..16, default 1)
+ *   "tc_run"            precision form: K chunks an FP32 accumulator collects before its fold
+ *                       into the FP64 sum (1..64, default 4)
+ *   "tc_check"          read the tensor-core kernels' error flag after each of their launches
+ *                       (1) or only when a result is read back (0, default)
+ *   "pair_range_cells"  cells per range of the FP64 pair GEMMs (0, default: as many as 8 GiB
+ *                       of pair products holds; smaller values exercise the multi-range path) */
+GPL_API int gpl_set_option(gpl_ctx* ctx, const char* name, int64_t value);
+GPL_API int gpl_get_option(const gpl_ctx* ctx, const char* name, int64_t* value);
+
 /* Gene-major CSR counts: replaces loadSparseMat + newSparseMatOnDevice
  * (SparseMat.cu:37-52,127-142). Gene j owns entries gene_ptr[j]..gene_ptr[j+1]-1.
  * Count matching keeps the reference's merge-walk rule (ggplvm.cu:505-511): within a
@@ -247,9 +261,13 @@ GPL_API int gpl_launch_count(const gpl_ctx* ctx, int64_t* launches);
  * KinvKmn (N x M, cell fastest: the transpose of the reference's M x N buffer) and titsias (N)
  * out, computed as gpl_kernel_mats computes them. The M x M work matrix lives in a fixed
  * 512 KiB array inside the library (M <= GPL_NOALLOC_MAX_M, else GPL_ERR_LIMIT), shared by all
- * calls on a device: calls that overlap on the GPU race, so serialise them. The first call on
- * a device looks the array up (make it before any stream capture). stream: a cudaStream_t or
- * NULL for the default stream; the call only enqueues work. */
+ * calls on a device: calls that overlap on the GPU race, so serialise them. Each call outside
+ * stream capture looks the array's device address up (with the caller's device current) and
+ * remembers it; a call under capture uses the remembered one, so make one call on the device
+ * before any capture (GPL_ERR_STATE otherwise). stream: a cudaStream_t or NULL for the default
+ * stream; the call only enqueues work and reports its own launches' status (GPL_ERR_CUDA), not
+ * errors of earlier work. A Kmm that is not positive definite zero-fills its factor as the
+ * reference's choldc does: KinvKmn and titsias are then inf/NaN and the call returns GPL_OK. */
 #define GPL_NOALLOC_MAX_M 256
 GPL_API int gpl_kernel_mats_noalloc(int N, int M, int Q, const double* X, const double* T, const double* rho,
                                     double* Knm, double* KinvKmn, double* titsias, void* stream);

@@ -223,6 +223,72 @@ def make_vc_case(name: str, spec: dict) -> dict:
     return out
 
 
+# The benchmark's shape at a size the reference's host build finishes in minutes: M = 128
+# inducing points, Q = 10 latent dimensions and the 100-donor design (batch 4 levels, 3
+# numerics, donor 100 levels: P = 236 model columns, 132 of them dense), with N and G cut.
+# The large buffers are kept as a seeded sample of entries (idx_<key>) with the full buffer's
+# largest magnitude (scale_<key>); sens_<key> is the reference's own change when X and T move
+# by a fraction of an ulp (two perturbed runs), the rounding floor any reordering reaches.
+HEAD_CASES = {
+    "c2_head": dict(config=2, seed=21, N=2000, G=16, M=128, Q=10),
+}
+HEAD_SAMPLED = ("kmats_Knm", "kmats_KinvKmn", "sweep0_Psi3", "grad0_C1")
+
+
+def make_head_case(name: str, spec: dict) -> dict:
+    import dataclasses
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import golden_util as gu  # noqa: E402
+
+    kw = dict(spec)
+    cfg, seed = kw.pop("config"), kw.pop("seed")
+    ds = synth.make(cfg, seed, **kw)
+
+    def run(d):
+        m = refcpu.RefModel.from_dataset(d)
+        o = gu.run_phases(m, d)
+        m.close()
+        m = refcpu.RefModel.from_dataset(d)
+        o.update(gu.run_fit(m, d))
+        m.close()
+        return o
+
+    base = run(ds)
+    sens = {}
+    same_decisions = True  # the perturbed runs took the same discrete decisions
+    for sd in (0, 1):
+        rng = np.random.default_rng(sd)
+        X2 = ds.init.X * (1 + 2e-16 * rng.standard_normal(ds.init.X.shape))
+        T2 = ds.init.T * (1 + 2e-16 * rng.standard_normal(ds.init.T.shape))
+        d2 = dataclasses.replace(ds, init=dataclasses.replace(ds.init, X=X2, T=T2))
+        pert = run(d2)
+        same_decisions &= int(pert["irls_n"]) == int(base["irls_n"]) and \
+            np.array_equal(np.asarray(pert["fit_stats"]), np.asarray(base["fit_stats"]))
+        for k in base:
+            if k not in ("irls_n", "fit_rc", "fit_stats"):
+                sens[k] = max(sens.get(k, 0.0), gu.rel_err(np.atleast_1d(pert[k]), np.atleast_1d(base[k])))
+    out = {
+        "in_N": np.array(ds.y.N), "in_J": np.array(ds.y.J), "in_M": np.array(ds.M), "in_Q": np.array(ds.Q),
+        "in_y_i": ds.y.i, "in_y_p": ds.y.p, "in_y_x": ds.y.x, "in_z_c": ds.z.c, "in_z_v": ds.z.v,
+        "in_z_body": np.frombuffer(ds.z.body_bytes(), np.uint8), "in_ls": ds.ls, "in_X0": ds.X0,
+        "same_decisions": np.array(same_decisions),
+    }
+    for k, a in zip(("Omega", "delta", "X", "T", "rho", "phi"), ds.init.flat()):
+        out["in_init_" + k] = a
+    for k, v in base.items():
+        v = np.atleast_1d(np.asarray(v))
+        if k in HEAD_SAMPLED:
+            idx = np.sort(np.random.default_rng(7).choice(v.shape[0], 8192, replace=False))
+            out["idx_" + k] = idx.astype(np.int64)
+            out["scale_" + k] = np.array(np.abs(v[np.isfinite(v)]).max())
+            v = v[idx]
+        out[k] = v
+        if k in sens:
+            out["sens_" + k] = np.array(sens[k])
+    return out
+
+
 def main():
     if not refcpu.available():
         raise SystemExit("build the reference first: make -C oracle ref")
@@ -231,6 +297,14 @@ def main():
         if only and name not in only:
             continue
         out = make_case(name, spec)
+        path = os.path.join(OUT, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, irls sweeps {int(out['irls_n'])}, "
+              f"fit {out['fit_stats'].tolist()}")
+    for name, spec in HEAD_CASES.items():
+        if only and name not in only:
+            continue
+        out = make_head_case(name, spec)
         path = os.path.join(OUT, f"{name}.npz")
         np.savez_compressed(path, **out)
         print(f"{path}: {os.path.getsize(path) / 1024:.0f} KiB, irls sweeps {int(out['irls_n'])}, "

@@ -92,6 +92,51 @@ def test_fit_matches_reference_golden(case):
     assert not bad, "; ".join(bad)
 
 
+def test_headline_shape_against_reference():
+    """The benchmark's shape against the reference's own kernels (tests/golden/c2_head.npz):
+    M = 128, Q = 10 and the 100-donor design, so P = 236 with 132 dense columns (8,778 column
+    pairs: the DMMA pair GEMMs' full tile grid, the 32-column panel Cholesky and inverse at
+    P = 236, the group sums over 400 batch x donor cell groups), with N = 2,000 cells and
+    G = 16 genes. Every phase buffer within max(1e-8, 20x the reference's own sub-ulp
+    sensitivity) of the golden values (large buffers on a seeded sample of 8,192 entries,
+    relative to the whole buffer's largest magnitude), the objective values within 1e-6; the
+    12-step fit with the same decisions, its trace within 1e-6, its parameters within
+    max(1e-6, 20x sensitivity)."""
+    gd = gu.load("c2_head")
+    g = gd.g
+    with GPLVM.from_dataset(gd) as m:
+        assert (m.P, m.M, m.Q) == (236, 128, 10)
+        assert m.n_dense() == 132
+        out = gu.run_phases(m, gd)
+    with GPLVM.from_dataset(gd) as m:
+        out.update(gu.run_fit(m, gd))
+    bad = []
+    for k, v in out.items():
+        if k in ("irls_n", "fit_rc", "fit_stats"):
+            if not np.array_equal(np.asarray(v), np.asarray(g[k])):
+                if bool(g["same_decisions"]) or k == "fit_rc":
+                    bad.append(f"{k}: {v} != {g[k]}")
+            continue
+        v = np.atleast_1d(np.asarray(v, np.float64))
+        ref = np.atleast_1d(g[k])
+        if "idx_" + k in g:
+            a = v[g["idx_" + k]]
+            fin = np.isfinite(ref)
+            e = float("inf") if not np.array_equal(fin, np.isfinite(a)) else \
+                float(np.abs(a[fin] - ref[fin]).max() / float(g["scale_" + k]))
+        else:
+            e = gu.rel_err(v, ref)
+        sens = float(g.get("sens_" + k, 0.0))
+        fit = k.startswith("fit_")
+        tol = max(TOL_FIT if fit else TOL_PHASE, 20.0 * sens)
+        if k in ("obj0", "obj1", "sweep0_lkhd", "fit_trace"):
+            tol = min(tol, TOL_FIT)
+        print(f"{k:16s} err {e:.2e} sensitivity {sens:.2e} tol {tol:.1e}")
+        if not e <= tol:
+            bad.append(f"{k}: {e:.2e} > {tol:.2e}")
+    assert not bad, "; ".join(bad)
+
+
 def test_count_walk_on_device():
     gd = gu.load("edges")
     with GPLVM.from_dataset(gd) as m:
@@ -152,25 +197,20 @@ def test_gram_over_cell_ranges():
     """The Gram over several cell ranges (pair products of one range at a time, partial Grams
     added in a pairs x genes buffer, then scattered into Psi) against the one-range form: the
     same products, summed in a different grouping."""
-    import os
-
     from gaspacho2_b200 import synth
 
     ds = synth.make(2, 7, N=3000, G=150, M=24, Q=4)
     psi = []
-    for cells in (None, "640"):
-        if cells:
-            os.environ["GPL_PAIR_RANGE_CELLS"] = cells
-        try:
-            with GPLVM.from_dataset(ds) as m:
-                m.set_params(ds.init)
-                m.kernel_mats()
-                m.glm_init()
-                m.irls_sweep(0, 0)
-                m.gram()
-                psi.append(m.get("Psi").copy())
-        finally:
-            os.environ.pop("GPL_PAIR_RANGE_CELLS", None)
+    for cells in (0, 640):
+        with GPLVM.from_dataset(ds) as m:
+            m.set_option("pair_range_cells", cells)
+            assert m.get_option("pair_range_cells") == cells
+            m.set_params(ds.init)
+            m.kernel_mats()
+            m.glm_init()
+            m.irls_sweep(0, 0)
+            m.gram()
+            psi.append(m.get("Psi").copy())
     e = gu.rel_err(psi[1], psi[0])
     print(f"Psi over 5 ranges vs one range: {e:.2e}")
     assert e <= 1e-13

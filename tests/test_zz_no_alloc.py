@@ -65,6 +65,26 @@ def test_noalloc_matches_context_path_on_consecutive_calls():
             assert e <= TOL, f"{name}: rel err {e:.3e}"
 
 
+def test_noalloc_fills_the_whole_scratch_at_its_limit():
+    """M = GPL_NOALLOC_MAX_M uses every element of the fixed 256 x 256 array; twice in a row,
+    after a smaller M left other contents in it."""
+    torch = pytest.importorskip("torch")
+    from gaspacho2_b200 import synth
+
+    gd = synth.make(2, 3, N=700, G=12, M=256, Q=10)
+    ref = _through_context(gd)
+    for _ in range(2):
+        rc, got = _without_allocation(torch, gd)
+        assert rc == 0, _lib.ERRORS.get(rc, rc)
+        for name, a, b in zip(("Knm", "KinvKmn", "titsias"), got, ref):
+            assert np.all(np.isfinite(a)), f"{name}: unwritten or non-finite elements"
+            e = gu.rel_err(a, b)
+            assert e <= TOL, f"{name}: rel err {e:.3e}"
+        small = gu.load("c0_small")
+        rc, _ = _without_allocation(torch, small)
+        assert rc == 0
+
+
 def test_noalloc_rejects_m_beyond_its_fixed_scratch():
     torch = pytest.importorskip("torch")
     gd = gu.load("c0_small")
