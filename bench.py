@@ -42,6 +42,17 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--plain", action="store_true",
+                    help="time the plain launches (no graphs, separate IRLS tail kernels, no autotuning)")
+    ap.add_argument("--profile-steps", type=int, default=1,
+                    help="eager evaluations after the timed region for the per-kernel profile")
+    ap.add_argument("--no-encoder-leg", action="store_true", help="skip the amortised encoder's experiment")
+    ap.add_argument("--enc-config", type=int, default=1)
+    ap.add_argument("--enc-train", type=int, default=16384)
+    ap.add_argument("--enc-test", type=int, default=4096)
+    ap.add_argument("--enc-fit-lbfgs", type=int, default=60)
+    ap.add_argument("--enc-epochs", type=int, default=40)
+    ap.add_argument("--enc-genes", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
@@ -505,24 +516,33 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     m = GPLVM.from_dataset(ds, device=local, stream=stream.cuda_stream, precision=args.precision)
+    batched = not args.plain
+    if batched:
+        # the batched form: the IRLS tail as one persistent launch, evaluations replayed from
+        # captured CUDA graphs, tile orders chosen by the autotuner (all give the plain path's bits)
+        for k in ("fused_tail", "autotune", "graph"):
+            m.set_option(k, 1)
     m.set_params(ds.init)
     m.kernel_mats()
     m.glm_init()
     for j in range(args.irls_sweeps):
         m.irls_sweep(0, j)
     m.objective_after_irls(0)
-    for _ in range(args.warmup):
+    warm = 0
+    while warm < args.warmup or (batched and warm < 40 and m.get_option("graph_replays") < 2 and
+                                 m.get_option("graph") == 1):
         m.evaluate_device()
+        m.sync()
+        warm += 1
     torch.cuda.synchronize()
 
     barrier = rep.barrier
 
     # device-resident throughput
-    m.profile(True)
-    m.profile_reset()
     clocks = ClockSampler(local)
     clocks.start()
     l0 = m.launches()
+    r0 = m.get_option("graph_replays")
     barrier()
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -534,7 +554,19 @@ def run_ours(args):
     barrier()
     dt = s.elapsed_time(e) / 1e3
     launches = m.launches() - l0
+    replays = m.get_option("graph_replays") - r0
     ck = clocks.stop()
+    # per-kernel device times: the same evaluation run eagerly with CUDA events around each kernel
+    # (profiling runs outside the graphs), after the timed region
+    m.profile(True)
+    m.profile_reset()
+    s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s3.record(stream)
+    for _ in range(args.profile_steps):
+        m.evaluate_device()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = s3.elapsed_time(e3) / args.profile_steps
     prof = {}
     for name in ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
                  "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
@@ -607,11 +639,24 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3+f64",
             "data": "synthetic", "config": workload_config(ds, args, args.precision), "e2e": e2e,
             "gpu_launches": int(launches), "roofline": roof, "clocks": ck,
-            "phase_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "phase_ms_per_step": {k: v[0] / args.profile_steps
+                                  for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "phase_note": f"per-kernel CUDA-event times of {args.profile_steps} eager evaluations after the timed "
+                          f"region ({eager_ms:.1f} ms each, profiling on)",
             "hbm_gbs_measured": peaks.get("hbm_gbs"), "bf16_tflops_measured": peaks.get("bf16_tflops"),
             "irls_sweep": irls,
+            "batched_form": {"graph": bool(m.get_option("graph")), "graph_replays_timed": int(replays),
+                             "fused_tail": bool(m.get_option("fused_tail")),
+                             "autotune": {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail")},
+                             "eager_profiled_ms_per_step": eager_ms, "warmup_evaluations": warm} if batched else None,
         }
     m.close()
+    if rank == 0 and world == 1 and not args.no_encoder_leg:
+        from gaspacho2_b200.encoder import amortised_placement
+
+        line["encoder"] = amortised_placement(args.enc_config, args.enc_train, args.enc_test, args.enc_fit_lbfgs,
+                                              args.enc_epochs, n_genes=args.enc_genes, device=local,
+                                              stream=stream.cuda_stream)
     if rank == 0 and args.precision == "fp64" and not args.no_precision_leg:
         line["precision_form"] = precision_leg(args, ds, stream, local)
     if rank == 0 and args.precision == "fp64" and not args.no_de_leg:

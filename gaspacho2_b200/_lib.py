@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(PKG, "libgpl_b200.so")
 GPL_OK = 0
 ERRORS = {-1: "GPL_ERR_ARG", -2: "GPL_ERR_CUDA", -3: "GPL_ERR_ALLOC", -4: "GPL_ERR_STATE", -5: "GPL_ERR_NAN",
           -6: "GPL_ERR_FORMAT", -7: "GPL_ERR_IO",
-          -8: "GPL_ERR_LIMIT"}
+          -8: "GPL_ERR_LIMIT", -9: "GPL_ERR_TIMEOUT"}
 PREC = {"fp64": 0, "bf16x3": 1}
 DE_NULL, DE_FULL = -2, -1  # gpl_de_model's model codes besides a latent dimension
 
@@ -28,6 +28,7 @@ SIGNATURES = {
     "gpl_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gpl_set_option": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
     "gpl_get_option": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gpl_tuning": (ctypes.c_int, [_vp, ctypes.c_char_p, _ip, _ip, _dp, ctypes.c_int, _ip]),
     "gpl_load_counts": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp]),
     "gpl_load_design": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, _ip, _vp, ctypes.c_int64, ctypes.c_int,
                                        ctypes.c_int]),
@@ -65,6 +66,23 @@ SIGNATURES = {
     "gpl_profile_read": (ctypes.c_int, [_vp, ctypes.c_char_p, _dp, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_sync": (ctypes.c_int, [_vp]),
+    "gpl_wait_probe": (ctypes.c_int, [_vp, ctypes.c_int64]),
+    "gpl_place_cells": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _ip]),
+    "gpl_cell_objective": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "gpl_enc_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_uint64]),
+    "gpl_enc_destroy": (ctypes.c_int, [_vp]),
+    "gpl_enc_last_error": (ctypes.c_char_p, [_vp]),
+    "gpl_enc_set_cells": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64, _ip, _ip, _dp,
+                                         _dp, _ip, _ip]),
+    "gpl_enc_set_targets": (ctypes.c_int, [_vp, _dp]),
+    "gpl_enc_n_params": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "gpl_enc_get_params": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "gpl_enc_set_params": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "gpl_enc_grads": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_float)]),
+    "gpl_enc_train": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_uint64, _dp]),
+    "gpl_enc_predict": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
+    "gpl_enc_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "gpl_kernel_mats_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                                _vp, _vp]),
 }

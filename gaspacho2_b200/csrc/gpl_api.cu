@@ -118,6 +118,9 @@ static void free_state(Ctx* c) {
 }
 
 static void free_counts(Ctx* c) {
+  if (c->gene_order_d) cudaFree(c->gene_order_d);
+  if (c->queue_head_d) cudaFree(c->queue_head_d);
+  c->gene_order_d = c->queue_head_d = nullptr;
   if (c->cell) cudaFree(c->cell);
   if (c->gptr) cudaFree(c->gptr);
   if (c->gvalid) cudaFree(c->gvalid);
@@ -148,19 +151,34 @@ static int read_slot(Ctx* c, int slot, double* out) {
   GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + slot, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
   GPL_RUN(tc_error_flag(c));
+  tune_harvest(c);
   c->lkhd[slot] = v;
   if (out) *out = v;
   return GPL_OK;
 }
 
 // ---- phases -------------------------------------------------------------------------------
+// With the fused tail (FP64, the main driver's forms), Z^T diag(W/Omega) nu comes first (it does
+// not read the factor) and one persistent launch does every gene's Cholesky, solve, coefficient
+// update and Poisson likelihood; the results are the same bits as the separate kernels'.
 static int irls_sweep(Ctx* c, int jtr, double* lk) {
   GPL_RUN(launch_w_nu(c));
   GPL_RUN(launch_gram(c, false));
-  GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, (int64_t)c->P * c->P));
-  GPL_RUN(launch_zt_u(c, 0));
-  GPL_RUN(launch_beta_phi(c, jtr));
-  GPL_RUN(launch_lkhd_pois(c));
+  bool fused = false;
+  if (c->fused_tail && c->precision == GPL_PREC_FP64 && !c->de) {
+    GPL_RUN(launch_zt_u(c, 0));
+    const int rc = launch_irls_tail(c, jtr, c->tail_ctas_per_sm);
+    if (rc != GPL_OK && rc != GPL_ERR_ARG) return rc;
+    fused = rc == GPL_OK;
+    if (!fused) GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, (int64_t)c->P * c->P));
+  } else {
+    GPL_RUN(launch_chol_batched(c, c->Psi, c->P, c->J, (int64_t)c->P * c->P));
+    GPL_RUN(launch_zt_u(c, 0));
+  }
+  if (!fused) {
+    GPL_RUN(launch_beta_phi(c, jtr));
+    GPL_RUN(launch_lkhd_pois(c));
+  }
   GPL_RUN(launch_collect_lkhd(c, 0, jtr));
   return read_slot(c, jtr, lk);
 }
@@ -230,6 +248,83 @@ static int gradient_launch(Ctx* c, bool after_objective = false) {
   return GPL_OK;
 }
 
+// ---- evaluations as CUDA graphs ----------------------------------------------------------------
+// The objective (about 40 launches) and the gradient after it (about 100) are captured once into
+// graphs and replayed: one launch each instead of one per kernel, and no host work per kernel in
+// the L-BFGS loop. The objective graph writes its value to a fixed slot, copied on the device to
+// the slot the caller asked for. Capture needs every lazily sized buffer to exist already, so the
+// first call runs eagerly and captures afterwards; if capture is refused (a call that a captured
+// stream does not allow), the context stays eager and says why in graph_note.
+constexpr int kGraphSlot = kLkhdSlots - 1;
+
+void graph_reset(Ctx* c) {
+  if (c->g_obj) cudaGraphExecDestroy(c->g_obj);
+  if (c->g_grad) cudaGraphExecDestroy(c->g_grad);
+  c->g_obj = c->g_grad = nullptr;
+}
+
+static bool graph_ok(const Ctx* c) {
+  return c->use_graph && !c->prof && !c->tc_check && (!c->autotune || tune_settled(c));
+}
+
+template <class F>
+static int capture(Ctx* c, cudaGraphExec_t* out, int64_t* n_kernels, F body) {
+  cudaGraph_t g = nullptr;
+  const int64_t l0 = c->launches;
+  GPL_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  *n_kernels = c->launches - l0;
+  c->launches = l0;  // captured, not run
+  if (rc != GPL_OK || e != cudaSuccess || g == nullptr) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (rc != GPL_OK) return rc;
+    c->use_graph = false;
+    c->graph_note = std::string("stream capture refused: ") + cudaGetErrorString(e);
+    return GPL_OK;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    c->use_graph = false;
+    c->graph_note = std::string("graph instantiation failed: ") + cudaGetErrorString(ei);
+  }
+  return GPL_OK;
+}
+
+// objective_launch(c, slot), through the objective graph when graphs are on.
+static int objective_run(Ctx* c, int slot) {
+  if (!graph_ok(c)) return objective_launch(c, slot);
+  if (!c->g_obj) {
+    GPL_RUN(objective_launch(c, slot));
+    return capture(c, &c->g_obj, &c->g_obj_kernels, [&] { return objective_launch(c, kGraphSlot); });
+  }
+  GPL_TRY(c, cudaGraphLaunch(c->g_obj, c->stream));
+  c->launches += c->g_obj_kernels;
+  c->graph_replays++;
+  if (slot != kGraphSlot)
+    GPL_TRY(c, cudaMemcpyAsync(c->lkhd_dev + slot, c->lkhd_dev + kGraphSlot, sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+  return GPL_OK;
+}
+
+// gradient_launch(c, true) (the gradient at the point of the last objective), through the
+// gradient graph when graphs are on.
+static int gradient_run(Ctx* c) {
+  if (!graph_ok(c)) return gradient_launch(c, true);
+  if (!c->g_grad) {
+    GPL_RUN(gradient_launch(c, true));
+    return capture(c, &c->g_grad, &c->g_grad_kernels, [&] { return gradient_launch(c, true); });
+  }
+  GPL_TRY(c, cudaGraphLaunch(c->g_grad, c->stream));
+  c->launches += c->g_grad_kernels;
+  c->graph_replays++;
+  return GPL_OK;
+}
+
 // One outer iteration `itr` of the driver (ggplvm.cu:1146-1330): IRLS to convergence
 // (JTRMAX 200 on the first iteration, 100 after), the objective, then L-BFGS steps with the
 // backtracking line search (rhoflag once itr > 20; a 10000-step limit on itr 30), and the
@@ -248,12 +343,12 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
   const int rhoflag = itr > 20 ? 1 : 0;
   if (itr == 30) JTRMAX = 10000;
   for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
-    GPL_RUN(gradient_launch(c, true));  // the last objective (after the IRLS or the accepted step) is here
+    GPL_RUN(gradient_run(c));  // the last objective (after the IRLS or the accepted step) is here
     GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
     double sr = 1.0;
     std::vector<double>& l = c->lkhd;
     for (int ktr = 1; ktr < 8; ktr++) {
-      GPL_RUN(objective_launch(c, jtr + 1));
+      GPL_RUN(objective_run(c, jtr + 1));
       GPL_RUN(read_slot(c, jtr + 1, nullptr));
       st[2]++;
       if (l[jtr + 1] > l[jtr] || ktr == 7) break;
@@ -494,6 +589,9 @@ int gpl_create(gpl_ctx** out, int device, void* stream) {
     c->own_stream = true;
   }
   c->lkhd.assign(kLkhdSlots, 0.0);
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && nsm > 0)
+    c->sm_count = nsm;
   *out = h;
   return GPL_OK;
 }
@@ -503,6 +601,8 @@ int gpl_destroy(gpl_ctx* h) {
   Ctx* c = C(h);
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  graph_reset(c);
+  tune_release(c);
   drain_profile(c);
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   free_state(c);
@@ -520,6 +620,7 @@ int gpl_set_precision(gpl_ctx* h, int precision) {
     c->err = "unknown precision";
     return GPL_ERR_ARG;
   }
+  if (precision != c->precision) graph_reset(c);
   c->precision = precision;
   return GPL_OK;
 }
@@ -528,6 +629,7 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
   if (!h || !name) return GPL_ERR_ARG;
   Ctx* c = C(h);
   const std::string s(name);
+  graph_reset(c);  // the captured graphs hold the old option's launches
   if (s == "tc_grad") {
     c->tc_grad = value != 0;
   } else if (s == "refine_steps") {
@@ -539,6 +641,16 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
     c->tc.run = (int)value;
   } else if (s == "tc_check") {
     c->tc_check = value != 0;
+  } else if (s == "autotune") {
+    c->autotune = value != 0;
+  } else if (s == "fused_tail") {
+    c->fused_tail = value != 0;
+  } else if (s == "tail_ctas_per_sm") {
+    if (value < 1 || value > 2) { c->err = "tail_ctas_per_sm must be 1 or 2"; return GPL_ERR_ARG; }
+    c->tail_ctas_per_sm = (int)value;
+  } else if (s == "graph") {
+    c->use_graph = value != 0;
+    c->graph_note.clear();
   } else if (s == "pair_range_cells") {
     if (value < 0) { c->err = "pair_range_cells must be >= 0"; return GPL_ERR_ARG; }
     if (value != c->pair_range_cells) {
@@ -562,6 +674,11 @@ int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
   else if (s == "tc_run") *value = c->tc_run;
   else if (s == "tc_check") *value = c->tc_check ? 1 : 0;
   else if (s == "pair_range_cells") *value = c->pair_range_cells;
+  else if (s == "graph") *value = c->use_graph ? 1 : 0;
+  else if (s == "fused_tail") *value = c->fused_tail ? 1 : 0;
+  else if (s == "autotune") *value = c->autotune ? 1 : 0;
+  else if (s == "tail_ctas_per_sm") *value = c->tail_ctas_per_sm;
+  else if (s == "graph_replays") *value = c->graph_replays;
   else return GPL_ERR_ARG;
   return GPL_OK;
 }
@@ -607,6 +724,13 @@ int gpl_load_counts(gpl_ctx* h, int N, int J, int64_t nnz, const int32_t* cell_i
   }
   GPL_TRY(c, cudaMemcpy(c->gptr, gp.data(), sizeof(int64_t) * (J + 1), cudaMemcpyHostToDevice));
   GPL_TRY(c, cudaMemcpy(c->gvalid, gv.data(), sizeof(int32_t) * J, cudaMemcpyHostToDevice));
+  // the persistent IRLS tail's gene queue: decreasing matched count (ties by gene index)
+  std::vector<int32_t> order(J);
+  for (int j = 0; j < J; j++) order[j] = j;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return gv[a] > gv[b]; });
+  GPL_RUN(dalloc(c, &c->gene_order_d, (size_t)J, "gene queue"));
+  GPL_RUN(dalloc(c, &c->queue_head_d, 1, "gene queue head"));
+  GPL_TRY(c, cudaMemcpy(c->gene_order_d, order.data(), sizeof(int32_t) * J, cudaMemcpyHostToDevice));
   c->N = N;
   c->J = J;
   c->nnz = nnz;
@@ -1030,8 +1154,8 @@ int gpl_objective_after_irls(gpl_ctx* h, double* lkhd) {
 int gpl_objective(gpl_ctx* h, int slot, double* lkhd) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));
-  if (slot < 0 || slot >= kLkhdSlots) return GPL_ERR_ARG;
-  GPL_RUN(objective_launch(c, slot));
+  if (slot < 0 || slot >= kGraphSlot) return GPL_ERR_ARG;
+  GPL_RUN(objective_run(c, slot));
   return read_slot(c, slot, lkhd);
 }
 
@@ -1162,6 +1286,7 @@ int gpl_de_model(gpl_ctx* h, int model) {
     c->err = "model must be GPL_DE_NULL, GPL_DE_FULL or a latent dimension in [0, Q)";
     return GPL_ERR_ARG;
   }
+  graph_reset(c);  // the model changes the kernels an evaluation launches
   GPL_RUN(de_loader_value(c, model == GPL_DE_NULL));
   c->de = true;
   c->kernel_lv = model == GPL_DE_NULL ? kLvNone : (model == GPL_DE_FULL ? kLvAll : model);
@@ -1199,6 +1324,7 @@ int gpl_vc_fit(gpl_ctx* h, int itr_max, int lbfgs_max, double* dg, double* obj, 
     c->err = "itr_max and lbfgs_max must be >= 1 and the design needs a variable besides intercept and GP";
     return GPL_ERR_ARG;
   }
+  graph_reset(c);  // the driver's constants change the objective's launches
   const int prec = c->precision;
   const bool de = c->de, vcf = c->vcomp;
   const int lv = c->kernel_lv;
@@ -1244,8 +1370,8 @@ int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkh
   GPL_TRY(c, cudaMemcpyAsync(c->T, p, sizeof(double) * (size_t)c->M * c->Q, cudaMemcpyHostToDevice, c->stream));
   p += (size_t)c->M * c->Q;
   GPL_TRY(c, cudaMemcpyAsync(c->rho, p, sizeof(double) * c->Q, cudaMemcpyHostToDevice, c->stream));
-  GPL_RUN(objective_launch(c, 1));
-  GPL_RUN(gradient_launch(c, true));
+  GPL_RUN(objective_run(c, 1));
+  GPL_RUN(gradient_run(c));
   if (grad) GPL_TRY(c, cudaMemcpyAsync(grad, c->grad, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
   double v = 0.0;
   GPL_TRY(c, cudaMemcpyAsync(&v, c->lkhd_dev + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1258,8 +1384,8 @@ int gpl_evaluate(gpl_ctx* h, const double* params, int64_t n_params, double* lkh
 int gpl_evaluate_device(gpl_ctx* h) {
   Ctx* c = C(h);
   GPL_RUN(need_state(c));
-  GPL_RUN(objective_launch(c, 1));
-  GPL_RUN(gradient_launch(c, true));
+  GPL_RUN(objective_run(c, 1));
+  GPL_RUN(gradient_run(c));
   return GPL_OK;
 }
 
@@ -1375,7 +1501,56 @@ int gpl_launch_count(const gpl_ctx* h, int64_t* launches) {
 int gpl_sync(gpl_ctx* h) {
   Ctx* c = C(h);
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  tune_harvest(c);
   return tc_error_flag(c);
+}
+
+int gpl_wait_probe(gpl_ctx* h, int64_t limit_ns) {
+  if (!h || limit_ns <= 0) return GPL_ERR_ARG;
+  Ctx* c = C(h);
+  return wait_probe(c, limit_ns);
+}
+
+int gpl_tuning(gpl_ctx* h, const char* name, int32_t* chosen, int32_t* cands, double* best_ms, int cap,
+               int32_t* n_cands) {
+  if (!h || !name) return GPL_ERR_ARG;
+  Ctx* c = C(h);
+  GPL_TRY(c, cudaStreamSynchronize(c->stream));
+  tune_harvest(c);
+  Tunable* t = tune_find(c, name);
+  if (!t) {
+    if (n_cands) *n_cands = 0;
+    if (chosen) *chosen = -1;
+    return GPL_OK;
+  }
+  const int n = (int)t->cands.size();
+  if (n_cands) *n_cands = n;
+  if (chosen) *chosen = t->best >= 0 ? t->cands[t->best] : -1;
+  for (int k = 0; k < n && k < cap; k++) {
+    if (cands) cands[k] = t->cands[k];
+    if (best_ms) best_ms[k] = t->n[k] > 0 ? t->best_ms[k] : (t->from_cache ? -2.0 : -1.0);
+  }
+  return GPL_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int gpl_place_cells(gpl_ctx* h, int iters, double* X, double* obj, int32_t* stats) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (iters < 0 || !X) return GPL_ERR_ARG;
+  cudaSetDevice(c->device);
+  return place_cells(c, iters, X, obj, stats);
+}
+
+int gpl_cell_objective(gpl_ctx* h, const double* X, double* obj, double* grad) {
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  if (!X || !obj) return GPL_ERR_ARG;
+  cudaSetDevice(c->device);
+  return cell_objective(c, X, obj, grad);
 }
 
 }  // extern "C"

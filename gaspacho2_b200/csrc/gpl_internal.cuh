@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -77,6 +78,22 @@ struct TcState {
   CUtensorMap map_whi, map_wlo, map_ahi, map_alo, map_shi, map_slo, map_ohi, map_olo;
 };
 
+// One open or settled choice of the autotuner (tune.cu): candidate values, each one's best
+// time so far and number of timings, the launches whose events are not read yet.
+struct Tunable {
+  struct Pending {
+    int cand;
+    cudaEvent_t a, b;
+  };
+  std::string name;
+  std::vector<int> cands;
+  std::vector<double> best_ms;
+  std::vector<int> n;
+  std::vector<Pending> pending;
+  int best = -1, cur = 0;
+  bool from_cache = false;
+};
+
 constexpr int kLvAll = -1;   // kernel over every latent dimension
 constexpr int kLvNone = -2;  // no GP (inert GP block): the DE driver's null model
 
@@ -102,6 +119,23 @@ struct Ctx {
   bool tc_check = false;      // read the tensor-core error flag after every tensor-core launch
   int tc_run = 4;             // precision form: K chunks per FP32 accumulator run before the FP64 fold
   int64_t pair_range_cells = 0;  // cells per range of the pair GEMMs (0: as many as 8 GiB holds)
+  // CUDA graphs of one objective evaluation and of the gradient that follows it (option
+  // "graph"): captured on first use, replayed after; dropped whenever a buffer they captured
+  // is reallocated or an option or the precision changes (graph_reset)
+  bool use_graph = false;
+  // the IRLS sweep's per-gene tail (Cholesky, solve, coefficient update, Poisson likelihood) as
+  // one persistent launch over a gene queue (option "fused_tail"), with this many CTAs per SM
+  bool fused_tail = false;
+  int tail_ctas_per_sm = 2;
+  int sm_count = 148;
+  int* gene_order_d = nullptr;   // genes by decreasing matched count (the queue's order)
+  int* queue_head_d = nullptr;   // the queue's head, reset before each launch
+  // the autotuner (option "autotune"): open and settled choices (tune.cu)
+  bool autotune = false;
+  std::deque<Tunable> tun;
+  cudaGraphExec_t g_obj = nullptr, g_grad = nullptr;
+  int64_t g_obj_kernels = 0, g_grad_kernels = 0, graph_replays = 0;
+  std::string graph_note;  // why capture was given up, when it was
   std::string err;
 
   // sizes
@@ -195,6 +229,26 @@ struct ProfScope {
   ~ProfScope();
 };
 
+// Drops the captured evaluation graphs (before any buffer they reference is freed or resized).
+void graph_reset(Ctx* c);
+
+// The autotuner (tune.cu). tune_pick returns the candidate value for this launch (`fallback`
+// when tuning is off) and, while the choice is open, the Tunable to time the launch with a
+// TuneScope around it; tune_harvest reads finished timings (after a host synchronisation);
+// tune_settled: no choice of the context is open.
+int tune_pick(Ctx* c, const char* name, const std::vector<int>& cands, int fallback, Tunable** slot);
+Tunable* tune_find(Ctx* c, const char* name);
+void tune_harvest(Ctx* c);
+bool tune_settled(const Ctx* c);
+void tune_release(Ctx* c);
+struct TuneScope {
+  Ctx* c;
+  Tunable* t;
+  cudaEvent_t a = nullptr, b = nullptr;
+  TuneScope(Ctx* c_, Tunable* t_);
+  ~TuneScope();
+};
+
 inline int64_t tot_len(const Ctx* c, int rhoflag) {
   return (int64_t)c->N + c->p + (int64_t)c->N * c->Q + (int64_t)c->M * c->Q + rhoflag;
 }
@@ -233,6 +287,8 @@ int launch_solve_batched(Ctx* c, const double* L, int n, int64_t lstride, const 
 int launch_inverse_batched(Ctx* c);      // PsiInv from Psi's factor
 int launch_potrf_panels(Ctx* c, double* A, int n, int batch, int64_t stride);  // 32-column panels, DMMA
 int launch_inverse_panels(Ctx* c);       // the same in 32-column panels with DMMA block products
+int launch_irls_tail(Ctx* c, int jtr, int ctas_per_sm);  // persistent per-gene IRLS tail; GPL_ERR_ARG:
+                                                          // P beyond the panel Cholesky's range
 int launch_inverse_single(Ctx* c, const double* L, int n, double* tmp, double* out);
 int launch_cholinv_exact(Ctx* c, const double* L, int n, double* out);  // cholsl order, no FMA
 cudaError_t launch_chol_exact_raw(cudaStream_t st, double* A, int n);  // the launch's own status
@@ -255,7 +311,11 @@ int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St);  // S
 int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D);  // U from the V rows of cells [c0, c1)
 int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tensor cores
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
-int tc_error_flag(Ctx* c);                // GPL_ERR_CUDA if a tensor-core kernel gave up waiting
+int tc_error_flag(Ctx* c);                // GPL_ERR_TIMEOUT if a tensor-core kernel gave up waiting
+int wait_probe(Ctx* c, int64_t limit_ns); // the bounded wait against a barrier nothing completes
+// k_place.cu (per-cell placement at a fitted model)
+int place_cells(Ctx* c, int iters, double* X_host, double* obj_host, int32_t* stats);
+int cell_objective(Ctx* c, const double* X_host, double* obj_host, double* grad_host);
 void tc_release(Ctx* c);
 // k_lkhd.cu
 int launch_oinvt(Ctx* c);

@@ -40,14 +40,16 @@ constexpr int kThreads = 256;
 }  // namespace
 
 // Grouped tile order: a 1-D grid of tm x tn output tiles in which consecutive blocks walk
-// kGroupM tile rows down one tile column before moving to the next column, so that the ~148
-// resident blocks cover a kGroupM x ~12 patch and share both operands' tiles through L2
-// (row-major order would re-read one operand from DRAM for nearly every block).
+// group_m tile rows down one tile column before moving to the next column, so that the ~148
+// resident blocks cover a group_m x ~(148 / group_m) patch and share both operands' tiles
+// through L2 (row-major order would re-read one operand from DRAM for nearly every block).
+// group_m is the autotuner's choice (default 12); it changes only which block computes which
+// tile, never a tile's sums.
 constexpr int kGroupM = 12;
-__device__ __forceinline__ int2 grouped_tile(int id, int tm, int tn) {
-  const int per = kGroupM * tn;
-  const int grp = id / per, first = grp * kGroupM;
-  const int gm = min(tm - first, kGroupM);
+__device__ __forceinline__ int2 grouped_tile(int id, int tm, int tn, int group_m) {
+  const int per = group_m * tn;
+  const int grp = id / per, first = grp * group_m;
+  const int gm = min(tm - first, group_m);
   const int r = id - grp * per;
   return make_int2(first + r % gm, r / gm);
 }
@@ -123,13 +125,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_pair_gram(int N, int ldN, int J, int P, int c0, int c1, int pairs_pad, int n_pairs, int mode,
                 const double* __restrict__ A, const int2* __restrict__ pairs, const int* __restrict__ dcol,
                 const double* __restrict__ W, const double* __restrict__ Dinv, double* __restrict__ Psi,
-                double* __restrict__ Gacc) {
+                double* __restrict__ Gacc, int group_m) {
   extern __shared__ __align__(16) double smem_d[];
   double* As = smem_d;              // [3][BK][SA]   pair products (pairs contiguous)
   double* Bs = As + 3 * BK * SA;    // [3][BN][SBT]  weights (cells contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
-  const int2 tile = grouped_tile(blockIdx.x, (n_pairs + BM - 1) / BM, (J + BN - 1) / BN);
+  const int2 tile = grouped_tile(blockIdx.x, (n_pairs + BM - 1) / BM, (J + BN - 1) / BN, group_m);
   const int p0 = tile.x * BM, j0 = tile.y * BN;
   const int nsl = (c1 - c0 + BK - 1) / BK;
 
@@ -253,13 +255,13 @@ __global__ void k_gather_spair(int J, int P, int n_pairs, int pairs_pad, const i
 
 __global__ void __launch_bounds__(kThreads, 1)
     k_pair_v(int N, int ldN, int J, int c0, int c1, int pairs_pad, const double* __restrict__ W,
-             const double* __restrict__ Sp, const double* __restrict__ rOm, double* __restrict__ V) {
+             const double* __restrict__ Sp, const double* __restrict__ rOm, double* __restrict__ V, int group_m) {
   extern __shared__ __align__(16) double smem_d[];
   double* As = smem_d;                // [3][BK][SA]  W rows (cells contiguous)
   double* Bs = smem_d + 3 * BK * SA;  // [3][BK][SBN] S pairs (pairs contiguous)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
-  const int2 tile = grouped_tile(blockIdx.x, (c1 - c0 + BM - 1) / BM, pairs_pad / BN);
+  const int2 tile = grouped_tile(blockIdx.x, (c1 - c0 + BM - 1) / BM, pairs_pad / BN, group_m);
   const int i0 = c0 + tile.x * BM, n0 = tile.y * BN;
   const int nsl = (J + BK - 1) / BK;
 
@@ -402,6 +404,7 @@ int pair_prepare(Ctx* c) {
 }
 
 void pair_release(Ctx* c) {
+  graph_reset(c);
   PairState& s = c->pr;
   void* bufs[] = {s.pairs, s.rOm, s.Sp, s.V, s.Gacc};
   for (void* p : bufs)
@@ -442,9 +445,12 @@ int launch_pair_gram(Ctx* c) {
     GPL_LAUNCHED(c, "k_pair_products");
     const int mode = one ? kGramPsi : (c0 == 0 ? kGramSet : kGramAdd);
     const int g = div_up(s.n_pairs, BM) * div_up(c->J, BN);
+    Tunable* tu = nullptr;
+    const int gm = tune_pick(c, "pair_gram", {4, 8, 12, 16, 32}, kGroupM, &tu);
+    TuneScope ts(c, one ? tu : nullptr);
     k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c0, c1, s.pairs_pad, s.n_pairs,
                                                         mode, s.V, s.pairs, c->dcol_d, c->W, c->DeltaInv, c->Psi,
-                                                        s.Gacc);
+                                                        s.Gacc, gm);
     GPL_LAUNCHED(c, "k_pair_gram");
   }
   if (!one) {
@@ -473,8 +479,11 @@ int launch_pair_uq(Ctx* c) {
     {
       ProfScope ps(c, "uq");
       const int g = div_up(c1 - c0, BM) * (s.pairs_pad / BN);
+      Tunable* tu = nullptr;
+      const int gm = tune_pick(c, "pair_v", {4, 8, 12, 16, 32}, kGroupM, &tu);
+      TuneScope ts(c, c1 - c0 == c->N ? tu : nullptr);
       k_pair_v<<<g, kThreads, s.smem_v, c->stream>>>(c->N, c->ldN, c->J, c0, c1, s.pairs_pad, c->W, s.Sp, s.rOm,
-                                                     s.V);
+                                                     s.V, gm);
       GPL_LAUNCHED(c, "k_pair_v");
     }
     if ((rc = launch_v_to_u_cells(c, c0, c1, c->Dm))) return rc;

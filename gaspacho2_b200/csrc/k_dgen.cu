@@ -384,6 +384,7 @@ static int launch_dgen(Ctx* c, dim3 grid, int m, int n, LA A, LB B, KR kr, Epi e
 
 static int ensure_part(Ctx* c, size_t n) {
   if (c->part_n >= n) return GPL_OK;
+  graph_reset(c);
   if (c->part) cudaFree(c->part);
   c->part = nullptr;
   c->part_n = 0;

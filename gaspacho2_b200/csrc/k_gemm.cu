@@ -70,6 +70,12 @@ struct LoadTn {  // A(r = cell, k = gene) = tn / phi, tn = O*nu - O*E, O = W/Ome
     return tn / phi[k];
   }
 };
+struct LoadCellGeneA {  // A(r = cell, k = gene) = S[k*ldN + r]
+  static constexpr bool kFastK = false;
+  const double* S;
+  int ldN, N, J;
+  __device__ double operator()(int r, int k) const { return (r < N && k < J) ? S[(size_t)k * ldN + r] : 0.0; }
+};
 struct LoadTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + a + k*P]
   static constexpr bool kFastK = false;
   const double* tB;
@@ -320,6 +326,22 @@ int launch_c1_tn(Ctx* c) {
                                          LoadTBetaGP{c->tBeta, c->P, g0, c->M, c->J}, c->C1, (int64_t)c->ldN,
                                          (const int*)nullptr);
   GPL_LAUNCHED(c, "k_gemm_store(c1_tn)");
+  return GPL_OK;
+}
+
+}  // namespace gpl
+
+namespace gpl {
+
+// G[i, a] = sum_j R_ij B[g0 + a, j]: a cell x gene matrix R (cell fastest, ld ldN) against the GP
+// block of coefficients (P x J), into G (cell fastest, ld ldN). FFMA tile GEMM.
+int launch_resid_gp(Ctx* c, const double* R, const double* B, double* G) {
+  const int g0 = c->nh[c->p - 1];
+  dim3 g(div_up(c->N, TM), div_up(c->M, TN));
+  k_gemm_store<<<g, 256, 0, c->stream>>>(c->N, c->M, c->J, LoadCellGeneA{R, c->ldN, c->N, c->J},
+                                         LoadTBetaGP{B, c->P, g0, c->M, c->J}, G, (int64_t)c->ldN,
+                                         (const int*)nullptr);
+  GPL_LAUNCHED(c, "k_gemm_store(resid_gp)");
   return GPL_OK;
 }
 

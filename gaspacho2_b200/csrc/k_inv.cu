@@ -19,6 +19,8 @@
 // written column-major (ld P) below and on the diagonal of each panel, the strict upper part of
 // the diagonal blocks holding exact zeros. A factor zero-filled by a failed Cholesky gives
 // infinities and NaNs, as in the reference.
+#include <algorithm>
+
 #include "dmma_common.cuh"
 #include "gpl_internal.cuh"
 
@@ -217,15 +219,15 @@ __global__ void __launch_bounds__(256, 2)
 // in increasing column order as in choldc) and the rows below solve against it (thread per
 // row). A non-positive pivot zero-fills the matrix, as choldc does. Reads the lower triangle,
 // writes the factor over it; the strict upper triangle is left as it was.
-__global__ void __launch_bounds__(256, 2) k_potrf_panel(double* __restrict__ Psi, int P, int64_t stride) {
-  extern __shared__ __align__(16) double sm[];
+// The factorization of one matrix A (P x P, ld P) by the CTA (256 threads); `sm` is the dynamic
+// shared memory (potrf_panel_smem(P) bytes), `fail` a shared flag. Used by k_potrf_panel (one
+// matrix per CTA) and by the persistent IRLS tail (k_irls_tail, matrices from a queue).
+__device__ __forceinline__ void potrf_panel_one(double* __restrict__ A, int P, double* sm, int& fail) {
   const int rows_pad = (P + 15) / 16 * 16;
   const int SA = rows_pad + 4;                 // La[q][r]: rows contiguous, 4 mod 16
   double* Ap = sm;                             // [rows_pad][IS]: the panel, Ap[r][c]
   double* La = Ap + (size_t)rows_pad * IS;     // [2][CW][SA]: finished columns, one CW-chunk
   double* Rd = La + 2 * (size_t)CW * SA;       // [32] reciprocals of the diagonal
-  __shared__ int fail;
-  double* A = Psi + (size_t)blockIdx.x * stride;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int nb = (P + IB - 1) / IB;
   if (tid == 0) fail = 0;
@@ -361,6 +363,12 @@ __global__ void __launch_bounds__(256, 2) k_potrf_panel(double* __restrict__ Psi
     for (int e = tid; e < P * P; e += blockDim.x) A[e] = 0.0;
 }
 
+__global__ void __launch_bounds__(256, 2) k_potrf_panel(double* __restrict__ Psi, int P, int64_t stride) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ int fail;
+  potrf_panel_one(Psi + (size_t)blockIdx.x * stride, P, sm, fail);
+}
+
 int potrf_panel_smem(int P) {
   const int rows_pad = (P + 15) / 16 * 16;
   return (int)sizeof(double) * (rows_pad * IS + 2 * CW * (rows_pad + 4) + IB);
@@ -399,6 +407,142 @@ int launch_inverse_panels(Ctx* c) {
   GPL_LAUNCHED(c, "k_trtri_panel");
   k_lauum_panel<<<g, 256, smem, c->stream>>>(c->scratch, P, st, c->PsiInv);
   GPL_LAUNCHED(c, "k_lauum_panel");
+  return GPL_OK;
+}
+
+}  // namespace gpl
+
+namespace gpl {
+
+// The per-gene tail of one IRLS sweep as ONE persistent launch (getBetaPhi's cholPsi, cholsl and
+// coefficient update, then getLkhdPois: ggplvm.cu:683-692, 418-464, 703-724). Each CTA takes
+// genes from a queue (an atomic head over `order`, the genes by decreasing matched count, so that
+// the genes with the most counts start first and the short ones fill the end) and for each gene:
+//   1. factors Psi_j in place (potrf_panel_one, as k_potrf_panel);
+//   2. solves L L^T x = b_j with one warp, in k_solve's operation order, and stores x (sol);
+//   3. beta_j <- (1 - r) beta_j + r x and phi_j from nu^T diag(W/Omega) nu - |L^T beta_j|^2 with
+//      the reference's clamps, in k_beta_phi's order;
+//   4. the Poisson log-likelihood of the gene's matched counts, in k_lkhd_pois's order.
+// Every sum is taken in the same per-thread order and reduced by the same block tree as in the
+// separate kernels, so the results are the same bits; which CTA takes which gene changes nothing.
+// The W and nu columns are read once for steps 3 and 4 together.
+__global__ void __launch_bounds__(256, 2)
+    k_irls_tail(int J, int N, int ldN, int P, int pvars, double r, double wt, double* __restrict__ Psi,
+                const double* __restrict__ bvec, double* __restrict__ sol, double* __restrict__ Beta,
+                double* __restrict__ phi, const double* __restrict__ W, const double* __restrict__ Nu,
+                const double* __restrict__ Omega, const double* __restrict__ delta,
+                const double* __restrict__ titsias, const int32_t* __restrict__ cell,
+                const int64_t* __restrict__ gptr, const int32_t* __restrict__ gvalid,
+                const double* __restrict__ cnt, double* __restrict__ lkhds, const int* __restrict__ order,
+                int* __restrict__ head) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ int fail, next;
+  __shared__ double sh[32];
+  const int rows_pad = (P + 15) / 16 * 16;
+  double* y = sm + (size_t)rows_pad * IS + 2 * (size_t)CW * (rows_pad + 4) + IB;  // past the panel's space
+  double* sb = y + P;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const int64_t PP = (int64_t)P * P;
+  for (;;) {
+    __syncthreads();  // the previous gene's shared values are no longer read
+    if (tid == 0) next = atomicAdd(head, 1);
+    __syncthreads();
+    const int q = next;
+    if (q >= J) break;
+    const int j = order[q];
+    double* L = Psi + (size_t)j * PP;
+    potrf_panel_one(L, P, sm, fail);
+    __syncthreads();
+    // 2. (L L^T) x = b_j, one warp (k_solve)
+    if (wid == 0) {
+      const double* rhs = bvec + (size_t)j * P;
+      for (int i = lane; i < P; i += 32) y[i] = rhs[i];
+      __syncwarp();
+      for (int k = 0; k < P; k++) {
+        const double xk = y[k] / L[k + (size_t)k * P];
+        __syncwarp();
+        if (lane == 0) y[k] = xk;
+        for (int i = k + 1 + lane; i < P; i += 32) y[i] -= L[i + (size_t)k * P] * xk;
+        __syncwarp();
+      }
+      for (int i = P - 1; i >= 0; i--) {
+        double part = 0.0;
+        for (int k = i + 1 + lane; k < P; k += 32) part += L[k + (size_t)i * P] * y[k];
+        part = warp_sum(part);
+        const double xi = (y[i] - part) / L[i + (size_t)i * P];
+        __syncwarp();
+        if (lane == 0) y[i] = xi;
+        __syncwarp();
+      }
+      double* x = sol + (size_t)j * P;
+      for (int i = lane; i < P; i += 32) x[i] = y[i];
+    }
+    // 3. and 4.: one pass over the gene's cells for both per-cell sums
+    const double* Wj = W + (size_t)j * ldN;
+    const double* nj = Nu + (size_t)j * ldN;
+    double qpart = 0.0, lpart = 0.0;
+    for (int i = tid; i < N; i += blockDim.x) {
+      qpart += nj[i] * nj[i] * Wj[i] / Omega[i];
+      lpart -= Wj[i];
+    }
+    const int64_t b0 = gptr[j], b1 = gptr[j] + gvalid[j];
+    const double dgp = delta[pvars - 1];
+    for (int64_t l = b0 + tid; l < b1; l += blockDim.x) {
+      const int i = cell[l];
+      lpart += (log(Wj[i]) - dgp * titsias[i] * wt) * cnt[l];
+    }
+    const double quad = block_sum(qpart, sh);  // syncs: the solution y is complete
+    double* bj = Beta + (size_t)j * P;
+    for (int k = tid; k < P; k += blockDim.x) {
+      const double nb = bj[k] * (1 - r) + y[k] * r;
+      bj[k] = nb;
+      sb[k] = nb;
+    }
+    __syncthreads();
+    double sq = 0.0;
+    for (int k = wid; k < P; k += nw) {
+      double t = 0.0;
+      for (int i = k + lane; i < P; i += 32) t += L[i + (size_t)k * P] * sb[i];
+      t = warp_sum(t);
+      sq += t * t;
+    }
+    if (lane != 0) sq = 0.0;
+    const double s2 = block_sum(sq, sh);
+    const double lk = block_sum(lpart, sh);
+    if (tid == 0) {
+      double ph = (quad - s2) / (double)N;
+      if (isnan(ph)) ph = 1.0;
+      if (ph < 0.0) ph = 1.0;
+      if (ph < 0.01) ph = 0.01;
+      if (ph > 1000.0) ph = 1000.0;
+      phi[j] = ph;
+      lkhds[j] = lk;
+    }
+  }
+}
+
+int irls_tail_smem(int P) { return potrf_panel_smem(P) + 2 * (int)sizeof(double) * P; }
+
+// GPL_ERR_ARG when the fused tail does not apply (P beyond the panel Cholesky's range).
+int launch_irls_tail(Ctx* c, int jtr, int ctas_per_sm) {
+  const int P = c->P;
+  const int smem = irls_tail_smem(P);
+  if (P > kPotrfMaxP || smem > 220 * 1024 || !c->gene_order_d) return GPL_ERR_ARG;
+  GPL_TRY(c, cudaFuncSetAttribute(k_irls_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  GPL_TRY(c, cudaFuncSetAttribute(k_irls_tail, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  double r = (double)(jtr + 1) / 100.0;  // the damping of getBetaPhi (ggplvm.cu:426)
+  if (jtr > 100) r = 1.0;
+  Tunable* tu = nullptr;
+  ctas_per_sm = tune_pick(c, "irls_tail", {1, 2}, ctas_per_sm, &tu);
+  const int grid = std::max(1, std::min(c->J, std::max(1, ctas_per_sm) * c->sm_count));
+  GPL_TRY(c, cudaMemsetAsync(c->queue_head_d, 0, sizeof(int), c->stream));
+  ProfScope ps(c, "irls_tail");
+  TuneScope ts(c, tu);
+  k_irls_tail<<<grid, 256, smem, c->stream>>>(c->J, c->N, c->ldN, P, c->p, r, c->vcomp ? 1.0 : kWt, c->Psi, c->bvec,
+                                              c->sol, c->Beta, c->phi, c->W, c->Nu, c->Omega, c->delta,
+                                              c->titsias, c->cell, c->gptr, c->gvalid, c->cnt, c->lkhds,
+                                              c->gene_order_d, c->queue_head_d);
+  GPL_LAUNCHED(c, "k_irls_tail");
   return GPL_OK;
 }
 

@@ -491,6 +491,7 @@ int tc_prepare(Ctx* c) {
 }
 
 void tc_release(Ctx* c) {
+  graph_reset(c);
   TcState& t = c->tc;
   void* bufs[] = {t.whi, t.wlo, t.pairs, t.err, t.Lw, t.Gt, t.Tt, t.DtC, t.DwC, t.ahi, t.alo, t.shi, t.slo,
                   t.ohi, t.olo};
@@ -505,7 +506,45 @@ static int tc_check_flag(Ctx* c) {
   GPL_TRY(c, cudaStreamSynchronize(c->stream));
   if (flag) {
     c->err = "tensor-core kernel gave up waiting (code " + std::to_string(flag) + ")";
-    return GPL_ERR_CUDA;
+    return GPL_ERR_TIMEOUT;
+  }
+  return GPL_OK;
+}
+
+// The bounded wait of the tensor-core kernels (mbar_wait) against a barrier whose phase nothing
+// completes: the wait runs out after limit_ns and the CTA records code 99 in the flag and
+// returns. No copy, MMA or TMEM allocation is in flight, so giving up leaves nothing behind.
+__global__ void k_wait_probe(uint64_t limit_ns, int* __restrict__ flag) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, nullptr, limit_ns)) atomicCAS(flag, 0, 99);
+}
+
+int wait_probe(Ctx* c, int64_t limit_ns) {
+  int* flag = nullptr;
+  if (cudaMalloc((void**)&flag, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    c->err = "device allocation failed: probe flag";
+    return GPL_ERR_ALLOC;
+  }
+  int v = 0;
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess) {
+    k_wait_probe<<<1, 32, 0, c->stream>>>((uint64_t)limit_ns, flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&v, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(flag);
+  GPL_TRY(c, e);
+  c->launches++;
+  if (v) {
+    c->err = "device wait gave up after " + std::to_string(limit_ns) + " ns (code " + std::to_string(v) + ")";
+    return GPL_ERR_TIMEOUT;
   }
   return GPL_OK;
 }

@@ -66,15 +66,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity: false when kWaitLimitNs passed or (when
+// Bounded wait for the phase with the given parity: false when `limit_ns` passed or (when
 // `err` is given) another thread has raised the error flag.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err,
+                                          uint64_t limit_ns = kWaitLimitNs) {
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 127u) == 127u) {
       if (err && *(const volatile int*)err != 0) return false;
-      if (global_ns() - t0 > kWaitLimitNs) return false;
+      if (global_ns() - t0 > limit_ns) return false;
     }
   }
 }

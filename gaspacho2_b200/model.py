@@ -92,6 +92,18 @@ class GPLVM:
         self._c(self._L.gpl_get_option(self.h, name.encode(), ctypes.byref(v)), f"gpl_get_option({name})")
         return v.value
 
+    def tuning(self, name: str) -> dict:
+        """The autotuner's record of one choice: the chosen value (None while open) and each
+        candidate's best measured launch time in ms (None if untimed)."""
+        chosen = ctypes.c_int32()
+        n = ctypes.c_int32()
+        cands = (ctypes.c_int32 * 16)()
+        ms = (ctypes.c_double * 16)()
+        self._c(self._L.gpl_tuning(self.h, name.encode(), ctypes.byref(chosen), cands, ms, 16, ctypes.byref(n)),
+                f"gpl_tuning({name})")
+        return {"chosen": None if chosen.value < 0 else chosen.value,
+                "candidates_ms": {int(cands[k]): (ms[k] if ms[k] >= 0 else None) for k in range(n.value)}}
+
     def set_params(self, prm) -> None:
         flat = [np.ascontiguousarray(a, dtype=np.float64) for a in prm.flat()]
         self._keep = flat

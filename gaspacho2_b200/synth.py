@@ -198,6 +198,35 @@ def make(config: int = 0, seed: int = 0, N: Optional[int] = None, G: Optional[in
     return Dataset(cfg, seed, y, z, s, X0, prm, M, Q, X)
 
 
+def cell_subset(ds: Dataset, cells: np.ndarray, init: bool = True) -> Dataset:
+    """The cells ``cells`` of ``ds`` (in that order) with every gene: the counts, covariates, size
+    factors and true coordinates of those cells, drawn from the same gene parameters. With
+    ``init`` the start is computed on the subset as ``make`` computes it (PCA of log1p, k-means)."""
+    cells = np.asarray(cells, np.int64)
+    y = ds.y
+    new = np.full(y.N, -1, np.int64)
+    new[cells] = np.arange(cells.shape[0])
+    gene = np.repeat(np.arange(y.J), np.diff(np.asarray(y.p, np.int64)))
+    keep = new[y.i] >= 0
+    ni, ng, nx = new[y.i][keep], gene[keep], y.x[keep]
+    o = np.lexsort((ni, ng))  # gene-major, cells ascending within a gene
+    p = np.zeros(y.J + 1, np.int64)
+    p[1:] = np.cumsum(np.bincount(ng, minlength=y.J))
+    ys = Counts(int(cells.shape[0]), y.J, ni[o].astype(np.int32), p.astype(np.int32), nx[o].copy())
+    cols = [np.asarray(col)[cells].copy() for col in ds.z.columns]
+    z = Design(int(cells.shape[0]), ds.z.c.copy(), ds.z.v.copy(), cols)
+    s = np.asarray(ds.ls)[cells].copy()
+    Xt = np.asarray(ds.X_true)[cells].copy()
+    if init:
+        X0 = _pca_scores(ys, s, ds.Q, ds.seed)
+        T0 = _kmeans(X0, ds.M, np.random.default_rng([ds.seed, 7]))
+    else:
+        X0 = np.asarray(ds.X0)[cells].copy()
+        T0 = np.asarray(ds.init.T).copy()
+    prm = default_params(ys.N, ys.J, len(ds.z.c) + 2, ds.M, ds.Q, X0, T0)
+    return Dataset(ds.config, ds.seed, ys, z, s, X0, prm, ds.M, ds.Q, Xt)
+
+
 def gene_subset(ds: Dataset, n_genes: int) -> Dataset:
     """The first ``n_genes`` genes of ``ds`` (cells and covariates unchanged)."""
     y = ds.y

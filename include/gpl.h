@@ -44,6 +44,7 @@ extern "C" {
 #define GPL_ERR_FORMAT (-6)   /* malformed input data (level code out of range, bad CSR offsets) */
 #define GPL_ERR_IO (-7)       /* file could not be read or written */
 #define GPL_ERR_LIMIT (-8)    /* size beyond a fixed limit of the allocation-free entry point */
+#define GPL_ERR_TIMEOUT (-9)  /* a bounded device wait ran out; the kernel gave up and the context stays usable */
 
 #define GPL_PREC_FP64 0       /* plain double precision: the drop-in path */
 /* The precision form (no reference counterpart): the Gram and the gradient contraction on
@@ -74,9 +75,35 @@ GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
  *   "tc_check"          read the tensor-core kernels' error flag after each of their launches
  *                       (1) or only when a result is read back (0, default)
  *   "pair_range_cells"  cells per range of the FP64 pair GEMMs (0, default: as many as 8 GiB
- *                       of pair products holds; smaller values exercise the multi-range path) */
+ *                       of pair products holds; smaller values exercise the multi-range path)
+ *   "graph"             1: each objective evaluation and each gradient after it (in gpl_fit,
+ *                       gpl_fit_outer, gpl_objective, gpl_evaluate, gpl_evaluate_device) runs as
+ *                       a CUDA graph, captured on its first use and replayed after (one launch
+ *                       per evaluation instead of one per kernel; the same kernels and results).
+ *                       Not while profiling or tc_check is on. Reads back as 0 if the capture
+ *                       was refused; the context then runs eagerly. Default 0.
+ *   "graph_replays"     (read only) graph launches so far
+ *   "fused_tail"        1: each IRLS sweep's per-gene tail (cholPsi, the solve and coefficient
+ *                       update of getBetaPhi, getLkhdPois: ggplvm.cu:683-692, 418-464, 703-724)
+ *                       runs as one persistent launch whose CTAs take genes from a queue ordered
+ *                       by decreasing count (FP64 path, P <= 288; else the separate kernels).
+ *                       Same results bit for bit. Default 0.
+ *   "tail_ctas_per_sm"  CTAs per SM of that launch (1 or 2, default 2)
+ *   "autotune"          1: the tile orders of the FP64 pair GEMMs and the CTAs per SM of the
+ *                       fused tail are chosen by timing each candidate on the context's own
+ *                       launches (every candidate gives the same bits); the choices are kept for
+ *                       the process per problem shape. Graphs are captured once all are chosen.
+ *                       Default 0. */
 GPL_API int gpl_set_option(gpl_ctx* ctx, const char* name, int64_t value);
 GPL_API int gpl_get_option(const gpl_ctx* ctx, const char* name, int64_t* value);
+
+/* The autotuner's record of one choice ("pair_gram", "pair_v", "irls_tail", "tc_gram",
+ * "tc_grad"): *chosen = the chosen candidate value (-1 while open), cands[k] the candidate
+ * values and best_ms[k] each one's best measured launch time (-1 untimed, -2 chosen from the
+ * process-wide record without timing), up to cap entries; *n_cands the number of candidates
+ * (0 if the choice never came up). No reference counterpart. */
+GPL_API int gpl_tuning(gpl_ctx* ctx, const char* name, int32_t* chosen, int32_t* cands, double* best_ms, int cap,
+                       int32_t* n_cands);
 
 /* Gene-major CSR counts: replaces loadSparseMat + newSparseMatOnDevice
  * (SparseMat.cu:37-52,127-142). Gene j owns entries gene_ptr[j]..gene_ptr[j+1]-1.
@@ -271,6 +298,64 @@ GPL_API int gpl_launch_count(const gpl_ctx* ctx, int64_t* launches);
 #define GPL_NOALLOC_MAX_M 256
 GPL_API int gpl_kernel_mats_noalloc(int N, int M, int Q, const double* X, const double* T, const double* rho,
                                     double* Knm, double* KinvKmn, double* titsias, void* stream);
+
+/* Failure detection of the device waits: runs the bounded wait that the tensor-core kernels use
+ * on every barrier, against a barrier whose phase nothing completes, with a limit of limit_ns
+ * (> 0). The wait gives up, the kernel records it and returns, and this call reports
+ * GPL_ERR_TIMEOUT, exactly as a tensor-core kernel whose wait ran out would; the context stays
+ * usable. No reference counterpart (the reference's kernels never wait). */
+GPL_API int gpl_wait_probe(gpl_ctx* ctx, int64_t limit_ns);
+
+/* Per-cell placement at a fitted model: the per-cell slice of the reference's L-BFGS phase
+ * (ggplvm.cu:1214-1301) for cells whose counts and covariates this context holds, with every
+ * gene's coefficients (gpl_set_beta: the fit's beta), T, rho and delta (gpl_set_params) fixed.
+ * Each cell's X_i maximises its Poisson log-likelihood over all genes (getLkhdPois,
+ * ggplvm.cu:703-724, with getWForBeta's mean W = s exp(z(X_i).beta + wt delta_GP titsias_i),
+ * ggplvm.cu:468-514) by its own L-BFGS under the reference's step rules (lbfgs,
+ * util_cuda.cu:187-232; the backtracking of ggplvm.cu:1278-1289), `iters` steps. X (N x Q,
+ * column-major) is the start in and the result out; obj[N] (may be NULL) the final per-cell
+ * objectives; stats[3] (may be NULL) = steps, objective evaluations, line-search tries. Uses the
+ * context's W, Nu and scratch buffers (an IRLS state there is overwritten). */
+GPL_API int gpl_place_cells(gpl_ctx* ctx, int iters, double* X, double* obj, int32_t* stats);
+/* The per-cell objective above at X (N x Q) into obj[N] and, if grad is not NULL, its gradient
+ * d obj_i / d X_iq into grad (N x Q, column-major). */
+GPL_API int gpl_cell_objective(gpl_ctx* ctx, const double* X, double* obj, double* grad);
+
+/* ---- The amortised encoder (no reference counterpart) -----------------------------------------
+ * The reference places every cell by L-BFGS on its latent coordinates (ggplvm.cu:1214-1301). The
+ * encoder learns that placement: an MLP n_in -> hidden -> hidden -> 2q (GELU; mean and
+ * log-variance of the q latent coordinates) over log1p(y / s) of n_in selected genes, trained on
+ * (cell profile, fitted X) pairs of a plain fit, with FP32 master weights, Adam, and BF16
+ * products on the tensor cores. Its predictions start (or replace) the per-cell refinement
+ * (gpl_place_cells). One encoder runs on one device and stream; hidden is a multiple of 128,
+ * 2q <= 64, batch a multiple of 128. Host arrays throughout; X is N x q column-major. */
+typedef struct gpl_enc gpl_enc;
+GPL_API int gpl_enc_create(gpl_enc** out, int device, void* stream, int n_in, int hidden, int q, int batch,
+                           uint64_t seed);
+GPL_API int gpl_enc_destroy(gpl_enc* enc);
+GPL_API const char* gpl_enc_last_error(const gpl_enc* enc);
+/* A cell set's features (which = 0: training, 1: evaluation) from gene-major CSR counts (the
+ * matched prefix of each gene, as gpl_load_counts reads them), size factors ls[N] and the n_in
+ * feature genes; cell_of_row (a permutation of 0..N-1, or NULL) orders the rows (training
+ * batches are runs of rows). */
+GPL_API int gpl_enc_set_cells(gpl_enc* enc, int which, int N, int J, int64_t nnz, const int32_t* cell_idx,
+                              const int32_t* gene_ptr, const double* counts, const double* ls, const int32_t* genes,
+                              const int32_t* cell_of_row);
+GPL_API int gpl_enc_set_targets(gpl_enc* enc, const double* X);  /* training targets, N x q */
+/* Parameters as one float array: W1 [hidden][n_in], b1, W2 [hidden][hidden], b2, W3 [2q][hidden],
+ * b3 (row-major); gpl_enc_n_params gives its length. */
+GPL_API int gpl_enc_n_params(const gpl_enc* enc, int64_t* n);
+GPL_API int gpl_enc_get_params(gpl_enc* enc, float* params);
+GPL_API int gpl_enc_set_params(gpl_enc* enc, const float* params);
+/* The mean loss of training batch `batch_index` (rows batch_index * batch ..) and every
+ * parameter's gradient (same layout as the parameters), without updating anything. */
+GPL_API int gpl_enc_grads(gpl_enc* enc, int batch_index, double* loss, float* grads);
+/* `epochs` passes over the whole training batches in a seeded random order, one Adam step (lr)
+ * per batch; loss_per_epoch[e] (may be NULL) = the epoch's mean loss. */
+GPL_API int gpl_enc_train(gpl_enc* enc, int epochs, double lr, uint64_t seed, double* loss_per_epoch);
+/* Predicted mean and log-variance (N x q column-major, either may be NULL) of a cell set. */
+GPL_API int gpl_enc_predict(gpl_enc* enc, int which, double* mean, double* logvar);
+GPL_API int gpl_enc_launch_count(const gpl_enc* enc, int64_t* launches);
 
 /* Synchronises the context's stream. */
 GPL_API int gpl_sync(gpl_ctx* ctx);
