@@ -36,6 +36,12 @@ METRIC = "obj+grad evals/s (100K cells x 10K genes, M=128, Q=10)"
 FALLBACK_BF16_SUSTAINED = 1400.0  # TFLOP/s, earlier measurement on this hardware pool
 FALLBACK_HBM_GBS = 6650.0  # GB/s, earlier copy measurement on this hardware pool
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# the library's profile ranges (gpl_profile_read names) reported per evaluation
+PHASES = ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights", "split_sdd", "grad_reduce", "chol",
+          "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes", "solve", "grad_delta", "c2",
+          "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect", "expand_delta", "chol_small", "group_sums",
+          "assemble_psi", "assemble_b", "group_tables", "hk", "group_t", "refine", "unwhiten_u", "irls_tail",
+          "beta_phi", "lkhd_pois", "w_nu")
 
 
 def parse():
@@ -72,6 +78,16 @@ def parse():
     ap.add_argument("--no-de-leg", action="store_true",
                     help="skip the DE driver's model-comparison pass beside the FP64 line")
     ap.add_argument("--de-mredc", type=int, default=5, help="inducing points of the DE per-dimension models")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="instead of the benchmark: the reference's own CUDA build against this project's "
+                         "evaluation on --config (use --config 0)")
+    ap.add_argument("--ref-gpu-steps", type=int, default=20)
+    ap.add_argument("--ref-gpu-seconds", type=float, default=240.0)
+    ap.add_argument("--fit-trace", action="store_true",
+                    help="instead of the benchmark: the --fit-config fit per outer iteration, each precision of "
+                         "--fit-precisions")
+    ap.add_argument("--fit-precisions", default="fp64,bf16x3")
+    ap.add_argument("--fit-max-outer", type=int, default=1000)
     ap.add_argument("--fit-spread", action="store_true",
                     help="instead of the benchmark: the --fit-config fit's end point from starts perturbed by "
                          "1e-12 and 1e-9 (relative, X), FP64 and the precision form")
@@ -451,7 +467,7 @@ def precision_leg(args, ds, stream, device):
     torch.cuda.synchronize()
     dt = s.elapsed_time(e) / 1e3
     phases = {}
-    for name in ("gram", "uq"):
+    for name in PHASES:
         ms, n = m.profile_read(name)
         if n:
             phases[name] = ms / args.steps
@@ -568,9 +584,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     eager_ms = s3.elapsed_time(e3) / args.profile_steps
     prof = {}
-    for name in ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights", "split_sdd", "grad_reduce", "chol", "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes",
-                 "solve", "grad_delta", "c2", "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect",
-                 "expand_delta", "chol_small", "group_sums", "assemble_psi", "assemble_b", "group_tables", "hk", "group_t", "refine", "unwhiten_u"):
+    for name in PHASES:
         ms, n = m.profile_read(name)
         if n:
             prof[name] = (ms, n)
@@ -756,8 +770,117 @@ def precision_report(args):
     return 0
 
 
+def fit_trace(args):
+    """The driver's fit of --fit-config, outer iteration by outer iteration (gpl_fit_outer), for
+    each precision in --fit-precisions, under the --fit-lbfgs step budget: per outer iteration its
+    IRLS sweeps, L-BFGS steps, objective evaluations, first and last accepted objective, why its
+    L-BFGS phase ended and its device time; then the whole fit's time (CUDA events) and final
+    objective. One JSON line per fit."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ds = synth.make(args.fit_config, 0, init=True)
+    for prec in args.fit_precisions.split(","):
+        with GPLVM.from_dataset(ds, stream=stream.cuda_stream, precision=prec) as m:
+            if not args.plain:
+                for k in ("fused_tail", "graph"):
+                    m.set_option(k, 1)
+            m.set_params(ds.init)
+            torch.cuda.synchronize()
+            t0 = time.time()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            m.kernel_mats()
+            m.glm_init()
+            outer, left, itr = [], args.fit_lbfgs, 0
+            while left > 0 and itr < args.fit_max_outer:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                rc, st, tr = m.fit_outer(itr, left)
+                b.record(stream)
+                torch.cuda.synchronize()
+                left -= st["lbfgs"]
+                d = np.abs(np.diff(tr)) / np.abs(tr[1:]) if len(tr) > 1 else np.zeros(0)
+                why = "budget" if left <= 0 else ("stop test" if len(d) and d[-1] < 1e-8 else "step limit")
+                outer.append({"itr": itr, "irls": st["irls"], "lbfgs": st["lbfgs"], "evals": st["evals"],
+                              "first": float(tr[0]) if len(tr) else None, "last": float(tr[-1]) if len(tr) else None,
+                              "ended": why, "seconds": a.elapsed_time(b) / 1e3,
+                              "rejected_tries": int(st["evals"] - 1 - st["lbfgs"]),
+                              "rel_gains": [float(x) for x in (np.diff(tr) / np.abs(tr[1:]))[-5:]] if len(tr) > 1
+                              else []})
+                itr += 1
+                if rc:
+                    break
+            e.record(stream)
+            torch.cuda.synchronize()
+            print(json.dumps({"mode": "fit_trace", "config": args.fit_config, "precision": prec,
+                              "lbfgs_budget": args.fit_lbfgs, "seconds": s.elapsed_time(e) / 1e3,
+                              "wall_seconds": time.time() - t0, "final_objective": outer[-1]["last"] if outer else None,
+                              "outer": outer}), flush=True)
+    return 0
+
+
+def reference_gpu(args):
+    """The reference's own CUDA build (oracle/_ref/ggplvm_gpu, the reference's sources compiled for
+    sm_100a) beside this project's evaluation on the same seeded dataset of --config (use 0): the
+    reference's median seconds per L-BFGS step of its first outer iteration (gradient, update and
+    line-search objectives, from its printed trace), and this project's objective + gradient
+    evaluation after its first IRLS phase, timed with CUDA events. One JSON line."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+    from oracle import ref_gpu
+
+    torch.cuda.set_device(0)
+    kw = {}
+    if args.N:
+        kw["N"] = args.N
+    if args.G:
+        kw["G"] = args.G
+    ds = synth.make(args.config, 0, init=True, **kw)
+    line = {"mode": "reference_gpu", "config": workload_config(ds, args, "fp64")}
+    if not ref_gpu.available():
+        line["reference"] = {"unavailable": "oracle/_ref/ggplvm_gpu not built (make -C oracle ref-gpu)"}
+    else:
+        line["reference"] = ref_gpu.run(ds, steps=args.ref_gpu_steps, seconds=args.ref_gpu_seconds)
+    stream = torch.cuda.Stream()
+    with GPLVM.from_dataset(ds, stream=stream.cuda_stream) as m:
+        for k in ("fused_tail", "graph"):
+            m.set_option(k, 1)
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        m.irls(0, 200)
+        m.objective_after_irls(0)
+        for _ in range(3):
+            m.evaluate_device()
+        n = max(10, args.ref_gpu_steps)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record(stream)
+        for _ in range(n):
+            m.evaluate_device()
+        e.record(stream)
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3 / n
+        line["ours"] = {"seconds_per_evaluation": t, "evaluations_per_second": 1.0 / t,
+                        "note": "objective + gradient after the first IRLS phase, CUDA-graph replay, CUDA events"}
+    ref = line["reference"]
+    if "seconds_per_lbfgs_step_median" in ref:
+        line["reference_seconds_per_step_over_ours_per_evaluation"] = ref["seconds_per_lbfgs_step_median"] / t
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.reference_gpu:
+        return reference_gpu(args)
+    if args.fit_trace:
+        return fit_trace(args)
     if args.precision_report:
         return precision_report(args)
     if args.fit_spread:

@@ -176,6 +176,16 @@ class GPLVM:
         stats = dict(outer=st[0], irls=st[1], lbfgs=st[2], evals=st[3])
         return (1 if rc == -5 else 0), stats, tr[:stats["outer"] + stats["lbfgs"]].copy()
 
+    def fit_outer(self, itr: int, lbfgs_budget: int = 0, trace_cap: int = 20000):
+        """One outer iteration of the driver (gpl_fit_outer): (rc, stats, trace) with stats
+        {irls, lbfgs, evals} of this iteration and its accepted objective values."""
+        st = (ctypes.c_int32 * 4)()
+        tr = np.zeros(trace_cap)
+        rc = self._L.gpl_fit_outer(self.h, int(itr), int(lbfgs_budget), st, _d(tr), int(trace_cap))
+        if rc not in (0, -5):
+            self._c(rc, "gpl_fit_outer")
+        return (1 if rc == -5 else 0), dict(irls=st[0], lbfgs=st[1], evals=st[2]), tr[:st[3]].copy()
+
     # -- the differential-expression driver's model comparison (ggplvm_de.cu) ------------------
     def de_model(self, model) -> None:
         """Select the DE driver's model: "null" (no GP), "full" (the GP over every latent
