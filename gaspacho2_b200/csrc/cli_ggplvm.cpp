@@ -57,13 +57,15 @@ struct Options {
   int M = 100, Q = 51, max_outer = 5000, max_lbfgs = 0, device = 0, L = 0;
   uint64_t seed = 0;
   bool quiet = false;
+  bool init_latent = false;  // compute X (written to Xi.bin) and T from the counts
 };
 
 void usage() {
   fprintf(stderr,
           "usage: ggplvm Y.bin Z.bin ls.bin Xi.bin [-M m] [-Q q] [--init-params params.bin]\n"
           "              [--max-outer n] [--max-lbfgs-iters n] [--precision fp64|bf16x3] [--device d]\n"
-          "              [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--genotypes G.bin -L l] [--quiet]\n");
+          "              [--out-dir dir] [--phi-gz omega|phi] [--seed s] [--genotypes G.bin -L l] [--quiet]\n"
+          "              [--init-latent]   (Xi.bin is then written: PCA of log1p(y/s); T by k-means)\n");
 }
 
 bool parse_int(const char* s, long lo, long hi, long* out) {
@@ -116,6 +118,8 @@ int parse(int argc, char** argv, Options* o) {
       else o->phi_gz = s;
     } else if (a == "--quiet") {
       o->quiet = true;
+    } else if (a == "--init-latent") {
+      o->init_latent = true;
     } else if (a == "-h" || a == "--help") {
       usage();
       return 2;
@@ -221,7 +225,8 @@ int main(int argc, char** argv) {
   }
   const int N = y.N, J = y.J, M = o.M, Q = o.Q;
   std::vector<double> ls(N), Xi((size_t)N * Q);
-  if (!load_doubles(o.ls, ls.data(), N) || !load_doubles(o.xi, Xi.data(), (size_t)N * Q)) return 1;
+  if (!load_doubles(o.ls, ls.data(), N) || (!o.init_latent && !load_doubles(o.xi, Xi.data(), (size_t)N * Q)))
+    return 1;
 
   gpl_ctx* ctx = nullptr;
   int rc = gpl_create(&ctx, o.device, nullptr);
@@ -251,6 +256,12 @@ int main(int argc, char** argv) {
   Normal rng(o.seed);
   for (int k = 1; k < Q; k++)
     for (int i = 0; i < M; i++) q.T[i + (size_t)k * M] = rng();
+  if (o.init_latent) {
+    // X from the principal components of log1p(y / s), T from k-means on X (gpl_init_latent)
+    if ((rc = gpl_init_latent(ctx, 60, 25, o.seed, Xi.data(), q.T.data()))) return fail(ctx, "gpl_init_latent", rc);
+    if (!write_file(o.xi, {{Xi.data(), Xi.size() * 8}})) return 1;
+    if (!o.quiet) printf("Xi written to %s (PCA of log1p counts), T by k-means\n", o.xi.c_str());
+  }
   if (!write_file(join(o.out_dir, "Tau.bin"), {{q.T.data(), q.T.size() * 8}})) return 1;
   q.X = Xi;
   if (!o.init_params.empty()) {

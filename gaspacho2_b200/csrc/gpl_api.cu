@@ -1554,3 +1554,11 @@ int gpl_cell_objective(gpl_ctx* h, const double* X, double* obj, double* grad) {
 }
 
 }  // extern "C"
+
+extern "C" int gpl_init_latent(gpl_ctx* h, int pca_iters, int kmeans_iters, uint64_t seed, double* X, double* T) {
+  if (!h || !X || !T || pca_iters < 1 || kmeans_iters < 0) return GPL_ERR_ARG;
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  cudaSetDevice(c->device);
+  return init_latent(c, pca_iters, kmeans_iters, seed, X, T);
+}

@@ -333,6 +333,21 @@ int launch_c1_tn(Ctx* c) {
 
 namespace gpl {
 
+// C (m x n, column-major, ld ldc) = op(A) B with op(A)(r, k) = A[k * lda + r] (a_trans = false)
+// or A[r * lda + k] (a_trans = true), B(k, c) = B[c * ldb + k]; FFMA tile GEMM.
+int launch_gemm_cm(Ctx* c, int m, int n, int K, const double* A, int lda, bool a_trans, const double* B, int ldb,
+                   double* C, int ldc) {
+  dim3 g(div_up(m, TM), div_up(n, TN));
+  if (a_trans)
+    k_gemm_store<<<g, 256, 0, c->stream>>>(m, n, K, LoadDt{A, lda, K, m}, LoadCellGene{B, ldb, K, n}, C,
+                                           (int64_t)ldc, (const int*)nullptr);
+  else
+    k_gemm_store<<<g, 256, 0, c->stream>>>(m, n, K, LoadD{A, lda, m, K}, LoadCellGene{B, ldb, K, n}, C,
+                                           (int64_t)ldc, (const int*)nullptr);
+  GPL_LAUNCHED(c, "k_gemm_store(cm)");
+  return GPL_OK;
+}
+
 // G[i, a] = sum_j R_ij B[g0 + a, j]: a cell x gene matrix R (cell fastest, ld ldN) against the GP
 // block of coefficients (P x J), into G (cell fastest, ld ldN). FFMA tile GEMM.
 int launch_resid_gp(Ctx* c, const double* R, const double* B, double* G) {

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
               const int2* __restrict__ pairs, int n_pairs,
               int chunks_total, const int* __restrict__ dcol, int P, int J, const double* __restrict__ Dinv,
               double* __restrict__ Psi, double* __restrict__ Gt, int n_d, int n_base, double* __restrict__ V,
-              int v_ld, int run, int* __restrict__ err) {
+              int v_ld, int run, int* __restrict__ err, int group) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* A_hi = base;
@@ -146,7 +146,19 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
   int2* spairs = (int2*)(sh + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ptile = blockIdx.x, n0 = blockIdx.y * kGramN;
+  // tile order: group == 0 takes the launch order (pair tile fastest: the ~148 resident CTAs share
+  // one or two column tiles and every pair tile); group > 0 walks `group` pair tiles down each
+  // column tile before the next, so that the resident CTAs share both operands' tiles through L2.
+  // Either order computes every tile with the same sums.
+  int ptile = blockIdx.x, ntile = blockIdx.y;
+  if (group > 0) {
+    const int id = blockIdx.y * gridDim.x + blockIdx.x, tm = gridDim.x;
+    const int per = group * gridDim.y, grp = id / per, first = grp * group;
+    const int gm = min(tm - first, group), r = id - grp * per;
+    ptile = first + r % gm;
+    ntile = r / gm;
+  }
+  const int n0 = ntile * kGramN;
   const int nch = chunks_total;
   const int nsb = (nch + run - 1) / run;
 
@@ -580,9 +592,13 @@ int launch_tc_gram(Ctx* c) {
   {
     ProfScope ps(c, "gram");
     dim3 g(t.pair_tiles, t.gram_tiles_n);
+    Tunable* tu = nullptr;
+    const int grp = tune_pick(c, "tc_gram", {0, 4, 8, 12, 16}, 0, &tu);
+    TuneScope ts(c, tu);
     k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
                                                            t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
-                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.run, t.err);
+                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.run, t.err,
+                                                           grp);
     GPL_LAUNCHED(c, "k_tc_gram");
   }
   {
@@ -617,10 +633,13 @@ int launch_tc_grad(Ctx* c) {
     {
       ProfScope ps(c, "uq");
       dim3 g(t.pair_tiles, div_up(c1 - c0, kGramN));
+      Tunable* tu = nullptr;
+      const int grp = tune_pick(c, "tc_grad", {0, 4, 8, 12, 16}, 0, &tu);
+      TuneScope ts(c, c1 - c0 == c->N ? tu : nullptr);
       k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
                                                              t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
                                                              c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
-                                                             s.pairs_pad, t.run, t.err);
+                                                             s.pairs_pad, t.run, t.err, grp);
       GPL_LAUNCHED(c, "k_tc_gram(gradient pairs)");
     }
     if ((rc = launch_v_to_u_cells(c, c0, c1, t.DwC))) return rc;

@@ -222,6 +222,15 @@ class GPLVM:
                 "gpl_evaluate")
         return v.value, g
 
+    def init_latent(self, pca_iters: int = 60, kmeans_iters: int = 25, seed: int = 0):
+        """The start from the counts (gpl_init_latent): X (N x Q) PCA scores of log1p(y / s) at unit
+        variance, T (M x Q) k-means centres of X."""
+        X = np.zeros(self.N * self.Q)
+        T = np.zeros(self.M * self.Q)
+        self._c(self._L.gpl_init_latent(self.h, int(pca_iters), int(kmeans_iters), ctypes.c_uint64(seed), _d(X),
+                                        _d(T)), "gpl_init_latent")
+        return X.reshape(self.Q, self.N).T.copy(), T.reshape(self.Q, self.M).T.copy()
+
     def score_stats(self, G: np.ndarray) -> np.ndarray:
         """Genotype score statistics (getScoreStats, ggplvm_de.cu:489-535): G is N x L, the
         result J x L, at the current fitted state."""

@@ -317,6 +317,15 @@ GPL_API int gpl_wait_probe(gpl_ctx* ctx, int64_t limit_ns);
  * objectives; stats[3] (may be NULL) = steps, objective evaluations, line-search tries. Uses the
  * context's W, Nu and scratch buffers (an IRLS state there is overwritten). */
 GPL_API int gpl_place_cells(gpl_ctx* ctx, int iters, double* X, double* obj, int32_t* stats);
+
+/* The start of a fit from the loaded counts and size factors, computed on the device: X (N x Q,
+ * column-major) = the leading Q principal component scores of log1p(y / s) (every gene, centred;
+ * subspace iteration with pca_iters products by the gene covariance), each scaled to unit
+ * variance; T (M x Q) = k-means centres of X after kmeans_iters Lloyd steps from M distinct
+ * seeded cells. The reference reads both from files (X: argv[4], ggplvm.cu:1019-1022; T:
+ * initTaWithPer or --init-params, ggplvm.cu:1011,1103-1106) and ships unused PCA kernels
+ * (init.cu:329-357). Uses the context's scratch buffer. */
+GPL_API int gpl_init_latent(gpl_ctx* ctx, int pca_iters, int kmeans_iters, uint64_t seed, double* X, double* T);
 /* The per-cell objective above at X (N x Q) into obj[N] and, if grad is not NULL, its gradient
  * d obj_i / d X_iq into grad (N x Q, column-major). */
 GPL_API int gpl_cell_objective(gpl_ctx* ctx, const double* X, double* obj, double* grad);
