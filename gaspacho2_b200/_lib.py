@@ -68,6 +68,7 @@ SIGNATURES = {
     "gpl_sync": (ctypes.c_int, [_vp]),
     "gpl_wait_probe": (ctypes.c_int, [_vp, ctypes.c_int64]),
     "gpl_init_latent": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, _dp, _dp]),
+    "gpl_cis_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _dp, _dp]),
     "gpl_place_cells": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _ip]),
     "gpl_cell_objective": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "gpl_enc_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,

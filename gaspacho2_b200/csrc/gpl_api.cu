@@ -1562,3 +1562,12 @@ extern "C" int gpl_init_latent(gpl_ctx* h, int pca_iters, int kmeans_iters, uint
   cudaSetDevice(c->device);
   return init_latent(c, pca_iters, kmeans_iters, seed, X, T);
 }
+
+extern "C" int gpl_cis_stats(gpl_ctx* h, int donor_var, int n_donors, int V, const int8_t* dosages, double* S,
+                             double* LR) {
+  if (!h || !dosages || !S || V < 1 || n_donors < 1) return GPL_ERR_ARG;
+  Ctx* c = C(h);
+  GPL_RUN(need_state(c));
+  cudaSetDevice(c->device);
+  return cis_stats(c, donor_var, n_donors, V, dosages, S, LR);
+}

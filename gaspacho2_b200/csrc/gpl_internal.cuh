@@ -313,6 +313,8 @@ int launch_tc_gram(Ctx* c);               // dense block of every Psi_j on tenso
 int launch_tc_grad(Ctx* c);               // U = sum_j O_ij S_j[DD] d_i on tensor cores
 int tc_error_flag(Ctx* c);                // GPL_ERR_TIMEOUT if a tensor-core kernel gave up waiting
 int wait_probe(Ctx* c, int64_t limit_ns); // the bounded wait against a barrier nothing completes
+// k_cis.cu (per-gene cis genotype statistics through donor-level group sums)
+int cis_stats(Ctx* c, int donor_var, int n_donors, int V, const int8_t* dos_host, double* S_host, double* LR_host);
 // k_init.cu (the start: PCA of log1p(y / s) and k-means inducing points)
 int init_latent(Ctx* c, int pca_iters, int kmeans_iters, uint64_t seed, double* X_host, double* T_host);
 // k_place.cu (per-cell placement at a fitted model)

@@ -231,6 +231,17 @@ class GPLVM:
                                         _d(T)), "gpl_init_latent")
         return X.reshape(self.Q, self.N).T.copy(), T.reshape(self.Q, self.M).T.copy()
 
+    def cis_stats(self, dosages: np.ndarray, donor_var: int):
+        """Per-(gene, variant) statistics (gpl_cis_stats) for donor dosages [donors][genes][variants]:
+        returns (S, LR), both J x V."""
+        dos = np.ascontiguousarray(dosages, np.int8)
+        D, J, V = dos.shape
+        S = np.zeros(J * V)
+        LR = np.zeros(J * V)
+        self._c(self._L.gpl_cis_stats(self.h, int(donor_var), int(D), int(V), dos.ctypes.data_as(ctypes.c_void_p),
+                                      _d(S), _d(LR)), "gpl_cis_stats")
+        return S.reshape(V, J).T.copy(), LR.reshape(V, J).T.copy()
+
     def score_stats(self, G: np.ndarray) -> np.ndarray:
         """Genotype score statistics (getScoreStats, ggplvm_de.cu:489-535): G is N x L, the
         result J x L, at the current fitted state."""

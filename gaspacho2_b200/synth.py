@@ -40,7 +40,8 @@ CONFIGS = {
     0: dict(N=2000, G=500, M=32, Q=2, batch=2, n_num=1, donors=0, mu=(-1.0, 1.0), shift=-1.6),
     1: dict(N=20000, G=2000, M=64, Q=5, batch=4, n_num=3, donors=0, mu=(-1.5, 1.2), shift=-1.75),
     2: dict(N=100000, G=10000, M=128, Q=10, batch=4, n_num=3, donors=100, mu=(-2.0, 1.5), shift=0.0),
-    4: dict(N=500000, G=5000, M=256, Q=10, batch=4, n_num=3, donors=300, mu=(-2.0, 1.5), shift=-0.8),
+    4: dict(N=500000, G=5000, M=256, Q=10, batch=4, n_num=3, donors=300, mu=(-2.0, 1.5), shift=-0.8,
+            variants=20, interaction_frac=0.05),
 }
 
 N_RFF = 256
@@ -58,6 +59,10 @@ class Dataset:
     M: int
     Q: int
     X_true: np.ndarray
+    # genotypes (configurations with cis variants): donor dosages [donors][genes][variants] in
+    # {0, 1, 2} and the truth of their effects (causal variant, main effect, interaction effect)
+    genotypes: Optional[np.ndarray] = None
+    geno_truth: Optional[dict] = None
 
     @property
     def N(self) -> int:
@@ -155,15 +160,35 @@ def make(config: int = 0, seed: int = 0, N: Optional[int] = None, G: Optional[in
     starts = list(range(0, G, chunk))
     child = ss.spawn(len(starts) + 1)[1:]
 
+    # cis genotypes (configurations with `variants`): per gene, that many variants with allele
+    # frequencies U(0.05, 0.5) and donor dosages Binomial(2, p); one causal variant per gene adds a
+    # main effect N(0, 0.1^2) to the log-rate, and on a fraction of genes also an interaction
+    # N(0, 0.1^2) x dosage x f_g(x) with the gene's GP draw f_g
+    V = int(cfg.get("variants", 0))
+    geno = truth = None
+    if V and donors:
+        grng = np.random.default_rng(ss.spawn(5)[4])
+        freq = grng.uniform(0.05, 0.5, (G, V))
+        geno = grng.binomial(2, freq[None, :, :], (donors, G, V)).astype(np.int8)
+        causal = grng.integers(0, V, G)
+        main = grng.normal(0.0, 0.1, G)
+        inter = np.where(grng.random(G) < cfg.get("interaction_frac", 0.0), grng.normal(0.0, 0.1, G), 0.0)
+        dos_c = geno[:, np.arange(G), causal].astype(np.float64)  # donors x genes, the causal dosage
+        truth = {"causal": causal, "main": main, "interaction": inter, "freq": freq}
+
     def gen(ci: int):
         g0 = starts[ci]
         g1 = min(G, g0 + chunk)
         crng = np.random.default_rng(child[ci])
-        lr = Phi @ A_rff[:, g0:g1]
+        f = Phi @ A_rff[:, g0:g1]
+        lr = f.copy()
         lr += mu[g0:g1][None, :] + base[:, None]
         lr += b_batch[batch, g0:g1] + num @ b_num[:, g0:g1]
         if donors:
             lr += d_eff[donor, g0:g1]
+        if geno is not None:
+            dc = dos_c[donor, g0:g1]
+            lr += dc * main[None, g0:g1] + dc * inter[None, g0:g1] * f
         cnt = crng.poisson(np.exp(lr))
         gi, ci_ = np.nonzero(cnt.T)  # gene-major, cells ascending within a gene
         return g1 - g0, gi, ci_.astype(np.int32), cnt.T[gi, ci_].astype(np.float64)
@@ -195,7 +220,7 @@ def make(config: int = 0, seed: int = 0, N: Optional[int] = None, G: Optional[in
         X0 = X.copy()
         T0 = _kmeans(X0, M, np.random.default_rng(ss.spawn(3)[2]), iters=5)
     prm = default_params(N, G, p_vars, M, Q, X0, T0)
-    return Dataset(cfg, seed, y, z, s, X0, prm, M, Q, X)
+    return Dataset(cfg, seed, y, z, s, X0, prm, M, Q, X, geno, truth)
 
 
 def cell_subset(ds: Dataset, cells: np.ndarray, init: bool = True) -> Dataset:

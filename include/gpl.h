@@ -212,6 +212,18 @@ GPL_API int gpl_evaluate(gpl_ctx* ctx, const double* params, int64_t n_params, d
  * phi and factored Psi_j (call after gpl_fit, an IRLS phase or an objective). */
 GPL_API int gpl_score_stats(gpl_ctx* ctx, int L, const double* G, double* S);
 
+/* Cis genotype statistics per (gene, variant): getScoreStats' efficient score (ggplvm_de.cu:489-535)
+ * for a separate set of V variants per gene whose dosages are per donor (every cell carries its
+ * donor's). dosages[(d * J + j) * V + v] (int8, 0/1/2) is donor d's dosage of gene j's variant v;
+ * the donor is design variable donor_var (0-based among the file variables; categorical, with
+ * n_donors levels, handled through cell groups). S[j + v*J] = s / sqrt(phi_j v) as gpl_score_stats
+ * defines s and v for the column g_i = dosage of cell i's donor, and LR[j + v*J] (may be NULL)
+ * = S^2, the likelihood ratio of the IRLS working model for adding that column with every other
+ * coefficient re-estimated. At the current W, nu, phi and factored Psi (after gpl_fit, an IRLS
+ * sweep or an objective). Every sum over cells runs over the cell groups. */
+GPL_API int gpl_cis_stats(gpl_ctx* ctx, int donor_var, int n_donors, int V, const int8_t* dosages, double* S,
+                          double* LR);
+
 /* The model comparison of the differential-expression driver (ggplvm_de.cu:1067-1207), which
  * refits the GLM part by IRLS at the fitted Omega, delta, X, T and rho for several GPs and
  * keeps each model's per-gene log-likelihood ("BFs", J x (Q+2), written to BFs_de.gz). One
