@@ -264,7 +264,7 @@ void graph_reset(Ctx* c) {
 }
 
 static bool graph_ok(const Ctx* c) {
-  return c->use_graph && !c->prof && !c->tc_check && (!c->autotune || tune_settled(c));
+  return c->use_graph && !c->prof && !c->tc_check && (!c->autotune || tune_settled_for_graphs(c));
 }
 
 template <class F>
@@ -272,7 +272,9 @@ static int capture(Ctx* c, cudaGraphExec_t* out, int64_t* n_kernels, F body) {
   cudaGraph_t g = nullptr;
   const int64_t l0 = c->launches;
   GPL_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  c->capturing = true;
   const int rc = body();
+  c->capturing = false;
   const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   *n_kernels = c->launches - l0;
   c->launches = l0;  // captured, not run

@@ -132,6 +132,7 @@ struct Ctx {
   int* queue_head_d = nullptr;   // the queue's head, reset before each launch
   // the autotuner (option "autotune"): open and settled choices (tune.cu)
   bool autotune = false;
+  bool capturing = false;  // a stream capture is in progress (no timing, no lazy allocation)
   std::deque<Tunable> tun;
   cudaGraphExec_t g_obj = nullptr, g_grad = nullptr;
   int64_t g_obj_kernels = 0, g_grad_kernels = 0, graph_replays = 0;
@@ -240,6 +241,7 @@ int tune_pick(Ctx* c, const char* name, const std::vector<int>& cands, int fallb
 Tunable* tune_find(Ctx* c, const char* name);
 void tune_harvest(Ctx* c);
 bool tune_settled(const Ctx* c);
+bool tune_settled_for_graphs(const Ctx* c);  // the choices inside a captured evaluation are made
 void tune_release(Ctx* c);
 struct TuneScope {
   Ctx* c;

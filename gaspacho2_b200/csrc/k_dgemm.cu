@@ -446,7 +446,7 @@ int launch_pair_gram(Ctx* c) {
     const int mode = one ? kGramPsi : (c0 == 0 ? kGramSet : kGramAdd);
     const int g = div_up(s.n_pairs, BM) * div_up(c->J, BN);
     Tunable* tu = nullptr;
-    const int gm = tune_pick(c, "pair_gram", {4, 8, 12, 16, 32}, kGroupM, &tu);
+    const int gm = tune_pick(c, "pair_gram", {8, 12, 16}, kGroupM, &tu);
     TuneScope ts(c, one ? tu : nullptr);
     k_pair_gram<<<g, kThreads, s.smem_gram, c->stream>>>(c->N, c->ldN, c->J, c->P, c0, c1, s.pairs_pad, s.n_pairs,
                                                         mode, s.V, s.pairs, c->dcol_d, c->W, c->DeltaInv, c->Psi,
@@ -480,7 +480,7 @@ int launch_pair_uq(Ctx* c) {
       ProfScope ps(c, "uq");
       const int g = div_up(c1 - c0, BM) * (s.pairs_pad / BN);
       Tunable* tu = nullptr;
-      const int gm = tune_pick(c, "pair_v", {4, 8, 12, 16, 32}, kGroupM, &tu);
+      const int gm = tune_pick(c, "pair_v", {8, 12, 16}, kGroupM, &tu);
       TuneScope ts(c, c1 - c0 == c->N ? tu : nullptr);
       k_pair_v<<<g, kThreads, s.smem_v, c->stream>>>(c->N, c->ldN, c->J, c0, c1, s.pairs_pad, c->W, s.Sp, s.rOm,
                                                      s.V, gm);

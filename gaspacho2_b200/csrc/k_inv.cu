@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(256, 2)
   const int rows_pad = (P + 15) / 16 * 16;
   double* y = sm + (size_t)rows_pad * IS + 2 * (size_t)CW * (rows_pad + 4) + IB;  // past the panel's space
   double* sb = y + P;
+  double* dg = sb + P;  // the factor's diagonal
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int64_t PP = (int64_t)P * P;
   for (;;) {
@@ -453,26 +454,67 @@ __global__ void __launch_bounds__(256, 2)
     double* L = Psi + (size_t)j * PP;
     potrf_panel_one(L, P, sm, fail);
     __syncthreads();
-    // 2. (L L^T) x = b_j, one warp (k_solve)
+    // 2. (L L^T) x = b_j, one warp, in k_solve's operation order (lane l updates the rows
+    // k + 1 + l + 32 m of column k, and sums the rows i + 1 + l + 32 m of row i's column); the
+    // next column's entries are loaded into registers while the current one is applied, so the
+    // dependent chain does not wait on a global load per step
     if (wid == 0) {
+      constexpr int NR = (kPotrfMaxP + 31) / 32;  // rows per lane
       const double* rhs = bvec + (size_t)j * P;
-      for (int i = lane; i < P; i += 32) y[i] = rhs[i];
+      for (int i = lane; i < P; i += 32) {
+        y[i] = rhs[i];
+        dg[i] = L[i + (size_t)i * P];
+      }
       __syncwarp();
+      double cur[NR], nxt[NR];
+#pragma unroll
+      for (int m = 0; m < NR; m++) {
+        const int i = 1 + lane + 32 * m;
+        cur[m] = i < P ? L[i] : 0.0;
+      }
       for (int k = 0; k < P; k++) {
-        const double xk = y[k] / L[k + (size_t)k * P];
+        if (k + 1 < P) {
+#pragma unroll
+          for (int m = 0; m < NR; m++) {
+            const int i = k + 2 + lane + 32 * m;
+            nxt[m] = i < P ? L[i + (size_t)(k + 1) * P] : 0.0;
+          }
+        }
+        const double xk = y[k] / dg[k];
         __syncwarp();
         if (lane == 0) y[k] = xk;
-        for (int i = k + 1 + lane; i < P; i += 32) y[i] -= L[i + (size_t)k * P] * xk;
+#pragma unroll
+        for (int m = 0; m < NR; m++) {
+          const int i = k + 1 + lane + 32 * m;
+          if (i < P) y[i] -= cur[m] * xk;
+        }
         __syncwarp();
+#pragma unroll
+        for (int m = 0; m < NR; m++) cur[m] = nxt[m];
       }
+#pragma unroll
+      for (int m = 0; m < NR; m++) cur[m] = 0.0;  // column P - 1 has no rows below the diagonal
       for (int i = P - 1; i >= 0; i--) {
+        if (i > 0) {
+#pragma unroll
+          for (int m = 0; m < NR; m++) {
+            const int k = i + lane + 32 * m;
+            nxt[m] = k < P ? L[k + (size_t)(i - 1) * P] : 0.0;
+          }
+        }
         double part = 0.0;
-        for (int k = i + 1 + lane; k < P; k += 32) part += L[k + (size_t)i * P] * y[k];
+#pragma unroll
+        for (int m = 0; m < NR; m++) {
+          const int k = i + 1 + lane + 32 * m;
+          if (k < P) part += cur[m] * y[k];
+        }
         part = warp_sum(part);
-        const double xi = (y[i] - part) / L[i + (size_t)i * P];
+        const double xi = (y[i] - part) / dg[i];
         __syncwarp();
         if (lane == 0) y[i] = xi;
         __syncwarp();
+#pragma unroll
+        for (int m = 0; m < NR; m++) cur[m] = nxt[m];
       }
       double* x = sol + (size_t)j * P;
       for (int i = lane; i < P; i += 32) x[i] = y[i];
@@ -521,7 +563,7 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-int irls_tail_smem(int P) { return potrf_panel_smem(P) + 2 * (int)sizeof(double) * P; }
+int irls_tail_smem(int P) { return potrf_panel_smem(P) + 3 * (int)sizeof(double) * P; }
 
 // GPL_ERR_ARG when the fused tail does not apply (P beyond the panel Cholesky's range).
 int launch_irls_tail(Ctx* c, int jtr, int ctas_per_sm) {

@@ -7,15 +7,17 @@
 // [-1, 1]; the backtracking of ggplvm.cu:1278-1289: accept a rise or the 7th try, else shrink by
 // 0.1, by 0.01 after a non-finite value).
 //
-// Per-cell objective: the Poisson log-likelihood of the cell's counts over all genes, as the
-// IRLS's getLkhdPois (ggplvm.cu:703-724) and getWForBeta (ggplvm.cu:468-514) define the mean:
-//     l_i(x) = sum_j y_ij (eta_ij + log s_i) - W_ij,
+// Per-cell objective: the Poisson log-probability of the cell's counts over all genes, with the
+// mean of the IRLS's getLkhdPois (ggplvm.cu:703-724) and getWForBeta (ggplvm.cu:468-514), plus the
+// N(0, 1) prior on the latent dimensions >= 1 that the reference's variance-component driver puts
+// on X (ggplvm_delta.cu) and that keeps a single cell's problem bounded:
+//     l_i(x) = sum_j [y_ij (eta_ij + log s_i) - W_ij - log(y_ij!)] - sum_{q >= 1} x_q^2 / 2,
 //     eta_ij = z_i(x) . beta_j,  W_ij = s_i exp(eta_ij + wt delta_GP titsias_i(x)),
 // where z_i(x) holds the cell's covariates and its kernel row k(x, T), and titsias_i =
 // (1 - k^T Kmm^-1 k) / 2. Its gradient in x: d l / d Knm_ik = sum_j (y_ij - W_ij) beta_j[GP k]
 // + wt delta_GP (sum_j W_ij) (Kmm^-1 k_i)_k, then through the periodic (dimension 0) and ARD
-// kernels. All cells of a context are placed together; every cell keeps its own history, step
-// and line search.
+// kernels, minus x_q for q >= 1. All cells of a context are placed together; every cell keeps its
+// own history, step and line search.
 //
 //   k_place_counts  the dense counts Y (cell x gene, cell fastest) from the CSR's matched prefix
 //   k_place_resid   per cell over all genes: R = y - W (for the gradient GEMM), l_i and sum_j W
@@ -50,10 +52,11 @@ __global__ void k_place_counts(int ldN, const int32_t* __restrict__ cell, const 
   for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) Y[(size_t)j * ldN + cell[l]] = cnt[l];
 }
 
-__global__ void k_place_resid(int N, int ldN, int J, int pvars, const double* __restrict__ E,
+__global__ void k_place_resid(int N, int ldN, int J, int Q, int pvars, const double* __restrict__ E,
                               const double* __restrict__ Y, const double* __restrict__ ls,
                               const double* __restrict__ delta, const double* __restrict__ titsias,
-                              double* __restrict__ R, double* __restrict__ obj, double* __restrict__ wsum) {
+                              const double* __restrict__ X, double* __restrict__ R, double* __restrict__ obj,
+                              double* __restrict__ wsum) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double lsi = ls[i], lls = log(lsi), tt = delta[pvars - 1] * titsias[i] * kWt;
@@ -64,7 +67,12 @@ __global__ void k_place_resid(int N, int ldN, int J, int pvars, const double* __
     const double w = exp(eta) * lsi * exp(tt);
     if (R) R[e] = y - w;
     l += y * (eta + lls) - w;
+    if (y > 0.0) l -= lgamma(y + 1.0);  // the full Poisson log-probability (constant in x)
     ws += w;
+  }
+  for (int q = 1; q < Q; q++) {  // N(0, 1) prior on the ARD dimensions
+    const double x = X[i + (size_t)q * N];
+    l -= 0.5 * x * x;
   }
   obj[i] = l;
   wsum[i] = ws;
@@ -87,6 +95,7 @@ __global__ void k_place_grad(int N, int ldN, int M, int Q, int pvars, const doub
     acc[0] -= C * sin(X[i] - T[k]) / (2.0 * rho[0]);
     for (int q = 1; q < Q; q++) acc[q] -= C * (X[i + (size_t)q * N] - T[k + (size_t)q * M]) / rho[q];
   }
+  for (int q = 1; q < Q; q++) acc[q] -= X[i + (size_t)q * N];  // the prior's gradient
   for (int q = 0; q < Q; q++) g[i + (size_t)q * N] = acc[q];
 }
 
@@ -205,8 +214,9 @@ static int place_eval(Ctx* c, PlaceBufs& pb, double* f, bool grad) {
   int rc = launch_kernel_mats(c);
   if (rc) return rc;
   if ((rc = launch_zbeta(c, c->Beta, c->scratch))) return rc;  // eta
-  k_place_resid<<<div_up(c->N, 128), 128, 0, c->stream>>>(c->N, c->ldN, c->J, c->p, c->scratch, c->Nu, c->ls,
-                                                          c->delta, c->titsias, grad ? c->W : nullptr, f, pb.wsum);
+  k_place_resid<<<div_up(c->N, 128), 128, 0, c->stream>>>(c->N, c->ldN, c->J, c->Q, c->p, c->scratch, c->Nu, c->ls,
+                                                          c->delta, c->titsias, c->X, grad ? c->W : nullptr, f,
+                                                          pb.wsum);
   GPL_LAUNCHED(c, "k_place_resid");
   if (!grad) return GPL_OK;
   if ((rc = launch_resid_gp(c, c->W, c->Beta, c->C1))) return rc;

@@ -55,6 +55,7 @@ int tune_pick(Ctx* c, const char* name, const std::vector<int>& cands, int fallb
         }
   }
   if (t->best >= 0) return t->cands[t->best];
+  if (c->capturing) return fallback;  // no timing inside a captured graph
   // the candidate with the fewest timings, counting launches whose events are not read yet
   std::vector<int> seen = t->n;
   for (auto& p : t->pending) seen[p.cand]++;
@@ -119,6 +120,16 @@ void tune_harvest(Ctx* c) {
 bool tune_settled(const Ctx* c) {
   for (auto& t : c->tun)
     if (t.best < 0 || !t.pending.empty()) return false;
+  return true;
+}
+
+// The choices made inside an evaluation (the objective's Gram, the gradient's pair contraction):
+// capture waits for these only; the IRLS tail is never part of a captured evaluation.
+bool tune_settled_for_graphs(const Ctx* c) {
+  for (auto& t : c->tun) {
+    const bool in_eval = t.name == "pair_gram" || t.name == "pair_v" || t.name == "tc_gram" || t.name == "tc_grad";
+    if (in_eval && (t.best < 0 || !t.pending.empty())) return false;
+  }
   return true;
 }
 

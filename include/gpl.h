@@ -321,9 +321,11 @@ GPL_API int gpl_wait_probe(gpl_ctx* ctx, int64_t limit_ns);
 /* Per-cell placement at a fitted model: the per-cell slice of the reference's L-BFGS phase
  * (ggplvm.cu:1214-1301) for cells whose counts and covariates this context holds, with every
  * gene's coefficients (gpl_set_beta: the fit's beta), T, rho and delta (gpl_set_params) fixed.
- * Each cell's X_i maximises its Poisson log-likelihood over all genes (getLkhdPois,
+ * Each cell's X_i maximises its Poisson log-probability over all genes (getLkhdPois,
  * ggplvm.cu:703-724, with getWForBeta's mean W = s exp(z(X_i).beta + wt delta_GP titsias_i),
- * ggplvm.cu:468-514) by its own L-BFGS under the reference's step rules (lbfgs,
+ * ggplvm.cu:468-514, and the log(y!) terms) plus the N(0, 1) prior on latent dimensions >= 1 of
+ * the reference's variance-component driver (ggplvm_delta.cu), by its own L-BFGS under the
+ * reference's step rules (lbfgs,
  * util_cuda.cu:187-232; the backtracking of ggplvm.cu:1278-1289), `iters` steps. X (N x Q,
  * column-major) is the start in and the result out; obj[N] (may be NULL) the final per-cell
  * objectives; stats[3] (may be NULL) = steps, objective evaluations, line-search tries. Uses the

@@ -113,7 +113,7 @@ def test_headline_shape_against_reference():
     bad = []
     for k, v in out.items():
         if k in ("irls_n", "fit_rc", "fit_stats"):
-            if not np.array_equal(np.asarray(v), np.asarray(g[k])):
+            if not np.array_equal(np.atleast_1d(v), np.atleast_1d(g[k])):
                 if bool(g["same_decisions"]) or k == "fit_rc":
                     bad.append(f"{k}: {v} != {g[k]}")
             continue

@@ -71,8 +71,15 @@ def test_noalloc_fills_the_whole_scratch_at_its_limit():
     torch = pytest.importorskip("torch")
     from gaspacho2_b200 import synth
 
+    import dataclasses
+
     gd = synth.make(2, 3, N=700, G=12, M=256, Q=10)
+    # 256 inducing points spread wide (N(0, 4 I) in 10 dimensions) keep Kmm well conditioned; k-means
+    # centres of 700 cells would nearly coincide and make its factor fail in both paths
+    T = 2.0 * np.random.default_rng(5).standard_normal((256, 10))
+    gd = dataclasses.replace(gd, init=dataclasses.replace(gd.init, T=T))
     ref = _through_context(gd)
+    assert np.all(np.isfinite(ref[1])), "the context path's Kmm^-1 k_n must be finite for this case"
     for _ in range(2):
         rc, got = _without_allocation(torch, gd)
         assert rc == 0, _lib.ERRORS.get(rc, rc)
