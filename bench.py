@@ -682,6 +682,21 @@ def run_ours(args):
                              "autotune": {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail")},
                              "eager_profiled_ms_per_step": eager_ms, "warmup_evaluations": warm} if batched else None,
         }
+    if rank == 0 and getattr(ds, "genotypes", None) is not None:
+        # per-(gene, variant) cis statistics at the bench state (the workload's donor genotypes)
+        D, J, V = ds.genotypes.shape
+        torch.cuda.synchronize()
+        t0 = time.time()
+        S, LR = m.cis_stats(ds.genotypes, len(ds.z.c) - 1)
+        tc = time.time() - t0
+        truth = ds.geno_truth
+        causal = LR[np.arange(J), truth["causal"]]
+        mask = np.ones_like(LR, bool)
+        mask[np.arange(J), truth["causal"]] = False
+        line["cis_statistics"] = {"genes": J, "variants_per_gene": V, "donors": D, "seconds": tc,
+                                  "median_lr_causal": float(np.median(causal)),
+                                  "median_lr_other": float(np.median(LR[mask])),
+                                  "finite": bool(np.all(np.isfinite(S)))}
     m.close()
     if rank == 0 and world == 1 and not args.no_encoder_leg:
         from gaspacho2_b200.encoder import amortised_placement

@@ -259,7 +259,7 @@ int launch_gram(Ctx* c, bool unweighted) {
   const int J = unweighted ? 1 : c->J;
   int rc = GPL_ERR_ARG;
   if (!unweighted) rc = c->precision == GPL_PREC_BF16X3 ? launch_tc_gram(c) : launch_pair_gram(c);
-  if (rc != GPL_OK && !(rc == GPL_ERR_ARG && c->precision == GPL_PREC_FP64)) return rc;
+  if (rc != GPL_OK && !(rc == GPL_ERR_ARG && (unweighted || c->precision == GPL_PREC_FP64))) return rc;
   if (rc == GPL_ERR_ARG) {
     // the unweighted Gram of one gene (GLM initialisation), or more dense columns than the
     // staged pair contraction holds

@@ -14,7 +14,9 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def fitted():
-    return synth.make(4, 1, N=1500, G=24, M=8, Q=2, init=True)
+    # 6,000 cells over 4 batches x 300 donors: at most 1,200 batch x donor cell groups, few enough
+    # (<= N/4 + 1) for the categorical variables to be handled by group sums
+    return synth.make(4, 1, N=6000, G=24, M=8, Q=2, init=True)
 
 
 def test_cis_statistics_equal_per_cell_scores(fitted):
