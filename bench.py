@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--enc-fit-lbfgs", type=int, default=60)
     ap.add_argument("--enc-epochs", type=int, default=40)
     ap.add_argument("--enc-genes", type=int, default=1000)
+    ap.add_argument("--enc-lr", type=float, default=1e-3)
+    ap.add_argument("--encoder-report", action="store_true",
+                    help="instead of the benchmark: the encoder's experiment alone, once per value of --enc-epochs-list")
+    ap.add_argument("--enc-epochs-list", default="",
+                    help="comma-separated epoch counts for --encoder-report (default: --enc-epochs)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
@@ -66,6 +71,11 @@ def parse():
     ap.add_argument("--G", type=int, default=None)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
     ap.add_argument("--irls-sweeps", type=int, default=2)
+    ap.add_argument("--option", action="append", default=[],
+                    help="name=value: a library option (gpl_set_option) for the fit-trace contexts; repeatable")
+    ap.add_argument("--eta-tc", type=int, default=None,
+                    help="option eta_tc (linear predictor and W / Nu on the FP64 tensor cores): 0 or 1; "
+                         "default: the library's")
     ap.add_argument("--cpu-genes", type=int, default=6, help="genes in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fit-config", type=int, default=1, help="configuration of the time-to-fit leg")
@@ -433,6 +443,17 @@ def irls_leg(m, ds, args, stream, torch):
                                       "FP64 GEMM rate; frac = that time / the kernel's time"}}
 
 
+def grad_blocks(g, ref, N, p, Q, M):
+    """Relative L2 error of g against ref per block of the parameter vector
+    [log Omega (N) | log delta (p) | X (N Q) | T (M Q) | log rho (rest)]."""
+    edges = np.cumsum([0, N, p, N * Q, M * Q, len(ref) - (N + p + N * Q + M * Q)])
+    out = {}
+    for name, a, b in zip(("log_omega", "log_delta", "X", "T", "log_rho"), edges[:-1], edges[1:]):
+        if b > a:
+            out[name] = float(np.linalg.norm(g[a:b] - ref[a:b]) / max(np.linalg.norm(ref[a:b]), 1e-300))
+    return out
+
+
 def precision_leg(args, ds, stream, device):
     """The precision form (tensor-core Gram and gradient contraction over whitened columns,
     FP64 elsewhere, refined solves) on the same workload and state as the FP64 line: its
@@ -456,6 +477,8 @@ def precision_leg(args, ds, stream, device):
     vbf, gbf = m.evaluate(x)
     gbf = gbf.copy()
     batched = not args.plain
+    if args.eta_tc is not None:
+        m.set_option("eta_tc", args.eta_tc)
     if batched:
         for k in ("autotune", "graph"):
             m.set_option(k, 1)
@@ -491,6 +514,7 @@ def precision_leg(args, ds, stream, device):
     return {"value": args.steps / dt, "unit": "evals/s", "ms_per_step": dt / args.steps * 1e3,
             "dtype": "bf16x3+f64", "objective_rel_err_vs_fp64": abs(vbf - v64) / abs(v64),
             "gradient_rel_l2_vs_fp64": float(np.linalg.norm(gbf - g64) / np.linalg.norm(g64)),
+            "gradient_rel_l2_by_block": grad_blocks(gbf, g64, ds.N, len(ds.init.delta), ds.Q, ds.M),
             "graph_replays_timed": int(replays), "autotune": tuning,
             "phase_ms_per_step": phases,
             "phase_note": f"per-kernel CUDA-event times of {args.profile_steps} eager evaluations after the timed region",
@@ -550,6 +574,8 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     m = GPLVM.from_dataset(ds, device=local, stream=stream.cuda_stream, precision=args.precision)
     batched = not args.plain
+    if args.eta_tc is not None:
+        m.set_option("eta_tc", args.eta_tc)
     if batched:
         # the batched form: the IRLS tail as one persistent launch, evaluations replayed from
         # captured CUDA graphs, tile orders chosen by the autotuner (all give the plain path's bits)
@@ -703,7 +729,7 @@ def run_ours(args):
 
         line["encoder"] = amortised_placement(args.enc_config, args.enc_train, args.enc_test, args.enc_fit_lbfgs,
                                               args.enc_epochs, n_genes=args.enc_genes, device=local,
-                                              stream=stream.cuda_stream)
+                                              stream=stream.cuda_stream, lr=args.enc_lr)
     if rank == 0 and args.precision == "fp64" and not args.no_precision_leg:
         line["precision_form"] = precision_leg(args, ds, stream, local)
     if rank == 0 and args.precision == "fp64" and not args.no_de_leg:
@@ -821,6 +847,11 @@ def fit_trace(args):
             if not args.plain:
                 for k in ("fused_tail", "graph"):
                     m.set_option(k, 1)
+            if args.eta_tc is not None:
+                m.set_option("eta_tc", args.eta_tc)
+            for kv in args.option:
+                k, v = kv.split("=")
+                m.set_option(k, int(v))
             m.set_params(ds.init)
             torch.cuda.synchronize()
             t0 = time.time()
@@ -850,6 +881,7 @@ def fit_trace(args):
             e.record(stream)
             torch.cuda.synchronize()
             print(json.dumps({"mode": "fit_trace", "config": args.fit_config, "precision": prec,
+                              "options": args.option,
                               "lbfgs_budget": args.fit_lbfgs, "seconds": s.elapsed_time(e) / 1e3,
                               "wall_seconds": time.time() - t0, "final_objective": outer[-1]["last"] if outer else None,
                               "outer": outer}), flush=True)
@@ -908,8 +940,27 @@ def reference_gpu(args):
     return 0
 
 
+def encoder_report(args):
+    """The encoder's experiment (gaspacho2_b200.encoder.amortised_placement) alone: one JSON line per
+    epoch count, each from a fresh fit of the training cells."""
+    import torch
+
+    from gaspacho2_b200.encoder import amortised_placement
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    epochs = [int(e) for e in args.enc_epochs_list.split(",") if e] or [args.enc_epochs]
+    for ep in epochs:
+        out = amortised_placement(args.enc_config, args.enc_train, args.enc_test, args.enc_fit_lbfgs, ep,
+                                  n_genes=args.enc_genes, device=0, stream=stream.cuda_stream, lr=args.enc_lr)
+        print(json.dumps({"mode": "encoder_report", **out}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.encoder_report:
+        return encoder_report(args)
     if args.reference_gpu:
         return reference_gpu(args)
     if args.fit_trace:

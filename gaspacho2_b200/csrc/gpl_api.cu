@@ -83,7 +83,7 @@ static int dalloc(Ctx* c, T** p, size_t n, const char* what) {
 static void free_state(Ctx* c) {
   tc_release(c);
   pair_release(c);
-  void* extra[] = {c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
+  void* extra[] = {c->cellfac, c->lvt, c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
                    c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d,
                    c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d, c->hk_pos_d, c->Wg, c->Dg, c->rOmg};
   for (void* q : extra)
@@ -93,7 +93,7 @@ static void free_state(Ctx* c) {
   c->n_hk_tiles128 = 0;
   c->part = nullptr;
   c->part_n = 0;
-  c->Dm = c->gsum = c->gT = c->HK = nullptr;
+  c->cellfac = c->lvt = c->Dm = c->gsum = c->gT = c->HK = nullptr;
   c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
   c->lvl_cc_d = c->lvl_v_d = c->lvl_ptr_d = c->lvl_grp_d = c->hk_pos_d = nullptr;
   c->Wg = c->Dg = c->rOmg = nullptr;
@@ -647,6 +647,8 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
     c->autotune = value != 0;
   } else if (s == "fused_tail") {
     c->fused_tail = value != 0;
+  } else if (s == "eta_tc") {
+    c->eta_tc = value != 0;
   } else if (s == "tail_ctas_per_sm") {
     if (value < 1 || value > 2) { c->err = "tail_ctas_per_sm must be 1 or 2"; return GPL_ERR_ARG; }
     c->tail_ctas_per_sm = (int)value;
@@ -678,6 +680,7 @@ int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
   else if (s == "pair_range_cells") *value = c->pair_range_cells;
   else if (s == "graph") *value = c->use_graph ? 1 : 0;
   else if (s == "fused_tail") *value = c->fused_tail ? 1 : 0;
+  else if (s == "eta_tc") *value = c->eta_tc ? 1 : 0;
   else if (s == "autotune") *value = c->autotune ? 1 : 0;
   else if (s == "tail_ctas_per_sm") *value = c->tail_ctas_per_sm;
   else if (s == "graph_replays") *value = c->graph_replays;
@@ -941,6 +944,7 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
   GPL_RUN(dalloc(c, &c->XX, (size_t)c->tot_max * kHist, "XX"));
   GPL_RUN(dalloc(c, &c->gdtmp, (size_t)P * J, "gdtmp"));
   GPL_RUN(dalloc(c, &c->C1, ldN * M, "C1"));
+  GPL_RUN(dalloc(c, &c->cellfac, 3 * ldN, "per-cell factors of W"));
   GPL_RUN(dalloc(c, &c->C2, (size_t)M * M, "C2"));
   GPL_RUN(dalloc(c, &c->grtmp, (size_t)M * Q, "grtmp"));
   GPL_RUN(dalloc(c, &c->red, std::max((size_t)ldN, (size_t)4096), "reduction"));
@@ -957,6 +961,8 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_RUN(dalloc(c, &c->cv_nlev_d, (size_t)ncat, "grouped variable levels"));
     GPL_RUN(dalloc(c, &c->glev_d, glev.size(), "group levels"));
     GPL_RUN(dalloc(c, &c->gcells_d, (size_t)N, "group cells"));
+    GPL_RUN(dalloc(c, &c->gid_d, (size_t)N, "cell groups"));
+    GPL_RUN(dalloc(c, &c->lvt, (size_t)J * n_grp, "level sums per group"));
     GPL_RUN(dalloc(c, &c->gstart_d, gstart.size(), "group offsets"));
     GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->hk_tiles128_d, tiles128.size(), "group tiles"));
@@ -974,6 +980,12 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_TRY(c, cudaMemcpy(c->cv_nlev_d, c->cv_nlev.data(), sizeof(int) * ncat, cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->glev_d, glev.data(), sizeof(int32_t) * glev.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->gcells_d, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    {
+      std::vector<int32_t> gid(N);
+      for (int g = 0; g < n_grp; g++)
+        for (int k = gstart[g]; k < gstart[g + 1]; k++) gid[order[k]] = g;
+      GPL_TRY(c, cudaMemcpy(c->gid_d, gid.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    }
     GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
     // per level of each grouped variable: its model column, its variable, its groups in order
     std::vector<int32_t> lvl_cc, lvl_v, lvl_ptr(1, 0), lvl_grp;

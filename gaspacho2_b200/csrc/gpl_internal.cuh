@@ -126,6 +126,8 @@ struct Ctx {
   // the IRLS sweep's per-gene tail (Cholesky, solve, coefficient update, Poisson likelihood) as
   // one persistent launch over a gene queue (option "fused_tail"), with this many CTAs per SM
   bool fused_tail = false;
+  // the linear predictor on the FP64 tensor cores (option "eta_tc", k_eta_dmma; the default)
+  bool eta_tc = true;
   int tail_ctas_per_sm = 2;
   int sm_count = 148;
   int* gene_order_d = nullptr;   // genes by decreasing matched count (the queue's order)
@@ -155,6 +157,8 @@ struct Ctx {
   std::vector<int> cv_nh, cv_nlev;  // first model column and level count of each grouped variable
   int *dcol_d = nullptr, *cv_nh_d = nullptr, *cv_nlev_d = nullptr, *gid_d = nullptr, *glev_d = nullptr;
   int *gcells_d = nullptr, *gstart_d = nullptr, *codes_d = nullptr;
+  double* lvt = nullptr;  // J x n_grp: per gene and cell group, the sum of its levels' coefficients
+  double* cellfac = nullptr;  // 3 x ldN: exp(dgp t_i wt), dgp t_i wt and log s_i of the W / Nu pass
   // levels of the grouped variables: model column, variable, and the groups at that level
   // (ascending) as offsets into a list
   int n_lvl = 0;
@@ -272,6 +276,8 @@ int launch_hk(Ctx* c);                    // HK[i] = sum_j O_ij [h_{j,g(i)} | ka
 int launch_group_order(Ctx* c, const double* src, int ncols, double* dst);  // dst[col][pos] = src[col][cell(pos)]
 // k_gemm.cu
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
+// out = z_i . B_j (ldN x J, cell fastest) on the FP64 tensor cores (k_dgemm.cu)
+int launch_eta_dmma(Ctx* c, const double* B, double* out);
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
 int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output;
                                                                       // mode 2: u is one value per cell

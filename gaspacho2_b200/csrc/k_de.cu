@@ -12,7 +12,7 @@
 //                         - sum_k log L_kk) / phi_j + P' log(2 pi') / 2
 //                  with pi' = 3.1415926535 (getLkhdPois, :667-693); P' excludes the inert GP
 //                  block of the null model.
-//   (W and nu themselves: k_w_nu with the DE flag, k_gemm.cu.)
+//   (W and nu themselves: k_eta_dmma with the DE flag, k_dgemm.cu.)
 //
 // All are per-gene (or per-coefficient) reductions over HBM-resident W, nu: bandwidth-bound
 // and small next to the Gram of each sweep.

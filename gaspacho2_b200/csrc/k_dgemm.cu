@@ -500,4 +500,208 @@ int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D) {
   return GPL_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Linear predictor over the dense columns (option eta_tc)
+// ---------------------------------------------------------------------------------------------
+// out[j * ldN + i] = D_i . B_j[dcol] + Lv[j, group(i)] for 128-cell x 128-gene tiles, where
+// Lv[j, g] is the sum of gene j's coefficients of the levels of cell group g (k_level_sums, per
+// launch): K = the dense columns in 16-deep slices (DMMA steps past n_d skipped), A = D by
+// 16-byte cp.async (cells contiguous), B = the genes' dense coefficients gathered through dcol by
+// 8-byte cp.async (k contiguous in shared memory). Persistent: one CTA per SM walks the tiles
+// cell-tile-major with a stride of the grid, so the CTAs resident at any time share a few cell
+// tiles of D and all of B through L2; the next tile's first two slices are in flight while the
+// current tile's epilogue stores (evict-first) run. The weights that follow (W, Nu) are an
+// element-wise pass of their own: inside this kernel's epilogue, at one CTA per SM, the
+// dependent FP64 operations of exp() left the tensor pipe idle for most of the launch.
+struct EtaArgs {
+  int N, ldN, P, J, n_d, n_grp;
+  const double *D, *B, *lvt;
+  const int *dcol, *gid;
+  double* out;
+};
+
+// Lv[j * n_grp + g] = sum over the grouped variables v (in order) of B[cv_nh[v] + level + j * P]
+__global__ void k_level_sums(int J, int n_grp, int n_cv, int P, const int* __restrict__ cv_nh,
+                             const int* __restrict__ glev, const double* __restrict__ B, double* __restrict__ Lv) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)J * n_grp) return;
+  const int j = (int)(e / n_grp), g = (int)(e - (int64_t)j * n_grp);
+  double s = 0.0;
+  for (int v = 0; v < n_cv; v++) s += B[cv_nh[v] + glev[(size_t)g * n_cv + v] + (size_t)j * P];
+  Lv[e] = s;
+}
+
+// One 16-deep K slice of the warp tile with only the first nkk of its four k4 steps live.
+__device__ __forceinline__ void warp_slice_live(const double* __restrict__ As, const double* __restrict__ Bs, int wm,
+                                                int wn, int g, int t, int nkk, double (&acc)[4][4][4]) {
+#pragma unroll
+  for (int kk = 0; kk < BK / 4; kk++) {
+    if (kk >= nkk) break;
+    double a[4][2], b[4];
+    const double* ar = As + (kk * 4 + t) * SA + wm * 64 + g;
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++) {
+      a[mt][0] = ar[mt * 16];
+      a[mt][1] = ar[mt * 16 + 8];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) b[nt] = Bs[(wn * 32 + nt * 8 + g) * SBT + kk * 4 + t];
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) dmma_16x8x4(acc[mt][nt], a[mt][0], a[mt][1], b[nt]);
+  }
+}
+
+size_t eta_smem_bytes(int n_d) {
+  const int KP = (n_d + BK - 1) / BK * BK;
+  return sizeof(double) * (3 * BK * SA + 3 * BN * SBT) + sizeof(int) * (size_t)KP;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
+  extern __shared__ __align__(16) double smem_d[];
+  double* As = smem_d;            // [3][BK][SA]  D rows (cells contiguous)
+  double* Bs = As + 3 * BK * SA;  // [3][BN][SBT] dense coefficients (k contiguous)
+  const int KP = (a.n_d + BK - 1) / BK * BK;
+  int* dcs = reinterpret_cast<int*>(Bs + 3 * BN * SBT);  // [KP] dcol, 0 past n_d
+  const double* __restrict__ D = a.D;
+  const double* __restrict__ B = a.B;
+  const double* __restrict__ lvt = a.lvt;
+  const int* __restrict__ gid = a.gid;
+  double* __restrict__ out = a.out;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
+  const int tm = (a.N + BM - 1) / BM, tn = (a.J + BN - 1) / BN;
+  const int tiles = tm * tn, nsl = KP / BK;
+  for (int k = tid; k < KP; k += kThreads) dcs[k] = k < a.n_d ? a.dcol[k] : 0;
+  __syncthreads();
+
+  // slice s of the tile at (m0, j0) into stage st
+  auto load = [&](int m0, int j0, int s, int st) {
+    const int kb = s * BK;
+#pragma unroll
+    for (int r = 0; r < (BM * BK / 2) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int k = ch >> 6, part = ch & 63;
+      const int col = kb + k, i = m0 + part * 2;
+      const int nb = (col < a.n_d && i < a.ldN) ? 16 : 0;  // ldN is even: a chunk is in or out whole
+      const double* src = D + (size_t)min(col, a.n_d - 1) * a.ldN + min(i, a.ldN - 2);
+      cp_async16(As + st * BK * SA + k * SA + part * 2, src, nb);
+    }
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / kThreads; r++) {
+      const int ch = tid + r * kThreads;
+      const int n = ch >> 4, k = ch & 15;
+      const int col = kb + k, j = j0 + n;
+      const int nb = (col < a.n_d && j < a.J) ? 8 : 0;
+      const double* src = B + dcs[col] + (size_t)min(j, a.J - 1) * a.P;
+      cp_async8(Bs + st * BN * SBT + n * SBT + k, src, nb);
+    }
+  };
+
+  int base = 0;  // slices issued before this tile (stage of slice s = (base + s) % 3)
+  int w = blockIdx.x;
+  if (w < tiles) {
+    const int m0 = (w / tn) * BM, j0 = (w % tn) * BN;
+    load(m0, j0, 0, 0);
+    cp_async_commit();
+    if (nsl > 1) load(m0, j0, 1, 1);
+    cp_async_commit();
+  }
+  for (; w < tiles; w += gridDim.x) {
+    const int m0 = (w / tn) * BM, j0 = (w % tn) * BN;
+    double acc[4][4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int y = 0; y < 4; y++)
+#pragma unroll
+        for (int z = 0; z < 4; z++) acc[x][y][z] = 0.0;
+    for (int s = 0; s < nsl; s++) {
+      cp_async_wait<1>();  // slice s landed
+      __syncthreads();
+      if (s + 2 < nsl) load(m0, j0, s + 2, (base + s + 2) % 3);
+      cp_async_commit();
+      const int st = (base + s) % 3;
+      const int nkk = min(BK / 4, (a.n_d - s * BK + 3) / 4);
+      warp_slice_live(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, nkk, acc);
+    }
+    // the next tile's first two slices go to the two stages that no warp reads any more
+    base += nsl;
+    const int wn2 = w + gridDim.x;
+    if (wn2 < tiles) {
+      const int m1 = (wn2 / tn) * BM, j1 = (wn2 % tn) * BN;
+      load(m1, j1, 0, base % 3);
+      cp_async_commit();
+      if (nsl > 1) load(m1, j1, 1, (base + 1) % 3);
+      cp_async_commit();
+    }
+    // the cells' level sums, then the stores
+    if (a.n_grp > 0) {
+#pragma unroll
+      for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int i = min(m0 + wm * 64 + mt * 16 + g + h * 8, a.N - 1);
+          const double* lg = lvt + gid[i];
+#pragma unroll
+          for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+              const int j = min(j0 + wn * 32 + nt * 8 + 2 * t + e, a.J - 1);
+              acc[mt][nt][h * 2 + e] += lg[(size_t)j * a.n_grp];
+            }
+        }
+    }
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int i = m0 + wm * 64 + mt * 16 + g + h * 8;
+        if (i >= a.N) continue;
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int j = j0 + wn * 32 + nt * 8 + 2 * t + e;
+            if (j < a.J) __stcs(out + (size_t)j * a.ldN + i, acc[mt][nt][h * 2 + e]);
+          }
+      }
+  }
+  cp_async_wait<0>();
+}
+
+int launch_eta_dmma(Ctx* c, const double* B, double* out) {
+  const size_t smem = eta_smem_bytes(c->n_d);
+  if (smem > 227 * 1024) {
+    c->err = "too many dense columns for the linear-predictor kernel";
+    return GPL_ERR_LIMIT;
+  }
+  if (c->n_grp > 0) {
+    const int64_t n = (int64_t)c->J * c->n_grp;
+    k_level_sums<<<(unsigned)div_up(n, 256), 256, 0, c->stream>>>(c->J, c->n_grp, c->n_cv, c->P, c->cv_nh_d,
+                                                                 c->glev_d, B, c->lvt);
+    GPL_LAUNCHED(c, "k_level_sums");
+  }
+  GPL_TRY(c, cudaFuncSetAttribute(k_eta_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EtaArgs a{};
+  a.N = c->N;
+  a.ldN = c->ldN;
+  a.P = c->P;
+  a.J = c->J;
+  a.n_d = c->n_d;
+  a.n_grp = c->n_grp;
+  a.D = c->Dm;
+  a.B = B;
+  a.lvt = c->lvt;
+  a.dcol = c->dcol_d;
+  a.gid = c->gid_d;
+  a.out = out;
+  const int tiles = div_up(c->N, BM) * div_up(c->J, BN);
+  const int grid = std::min(tiles, c->sm_count);
+  k_eta_dmma<<<grid, kThreads, smem, c->stream>>>(a);
+  GPL_LAUNCHED(c, "k_eta_dmma");
+  return GPL_OK;
+}
+
 }  // namespace gpl

@@ -5,10 +5,10 @@
 // categorical variables, so every product z_i . beta is D_i . beta[dcol] + the coefficients
 // of the cell's levels.
 //
-//   W / Nu     eta = z_i . beta_j for every cell and gene, then the getWForBeta epilogue
-//              (ggplvm.cu:468-514). The counts of the tile's genes are scattered into
-//              shared memory first: each gene's matched prefix is sorted by cell, so a
-//              binary search finds the tile's slice. Bound: FP64 FMA (N*J*n_d).
+//   W / Nu     eta = z_i . beta_j for every cell and gene (k_eta; k_eta_dmma in k_dgemm.cu on the
+//              FP64 tensor cores with option eta_tc), then the getWForBeta element-wise pass
+//              (ggplvm.cu:468-514) one block per gene (k_w_nu). Bound: FP64 FMA (N*J*n_d) for
+//              the predictor, HBM and FP64 exp() for the pass.
 //   bvec       dense rows of Z^T diag(W_j/Omega) nu_j (getZtOinvjnj, util_cuda.cu:462-487)
 //              and of the GLM initialisation right-hand sides Z^T y0_j (initBeta,
 //              init.cu:193-221); the categorical rows come from the group sums.
@@ -135,37 +135,52 @@ __device__ __forceinline__ double add_levels(double dense, int i, int j, int ldN
 }
 
 // ---- W / Nu -----------------------------------------------------------------------------
-// getWForBeta (ggplvm.cu:468-514) from the linear predictor eta = z_i . beta_j (k_eta, FFMA
-// tile GEMM with the cells' level coefficients, written to a cell x gene buffer first), one
-// block per gene: every cell gets W = exp(eta) s_i exp(dgp titsias_i wt) and the working
-// response of a zero count; then the counts that the reference's merge walk matches (the first
-// gvalid entries of the gene) replace their cells' working response. The barrier orders the
-// two writes of such a cell. The DE driver takes the Titsias factor at weight 1 and
-// nu = z.(beta - zeta) + (y - W)/W (ggplvm_de.cu:442-486); the fit driver has zeta = 0.
-__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int pvars, const double* __restrict__ E,
-                                              const double* __restrict__ ls, const double* __restrict__ delta,
-                                              const double* __restrict__ titsias, const int32_t* __restrict__ cell,
-                                              const int64_t* __restrict__ gptr, const int32_t* __restrict__ gvalid,
-                                              const double* __restrict__ cnt, int de, const double* __restrict__ e0,
-                                              double* __restrict__ W, double* __restrict__ Nu) {
+// getWForBeta (ggplvm.cu:468-514) from the linear predictor eta = z_i . beta_j (k_eta_dmma or
+// k_eta, written to a cell x gene buffer first). The per-cell factors exp(dgp titsias_i wt),
+// dgp titsias_i wt and log s_i are computed once per pass (k_cell_factors); then one block per
+// gene gives every cell W = exp(eta) s_i exp(dgp titsias_i wt) and the working response of a
+// zero count, and the counts that the reference's merge walk matches (the first gvalid entries
+// of the gene) replace their cells' working response. The barrier orders the two writes of such
+// a cell. The same expressions, in the same order, as the per-element form. The DE driver takes
+// the Titsias factor at weight 1 and nu = z.(beta - zeta) + (y - W)/W (ggplvm_de.cu:442-486);
+// the fit driver has zeta = 0.
+__global__ void k_cell_factors(int N, int ldN, int pvars, int de, const double* __restrict__ delta,
+                               const double* __restrict__ titsias, const double* __restrict__ ls,
+                               double* __restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double tt = delta[pvars - 1] * titsias[i] * (de ? 1.0 : kWt);
+  f[i] = exp(tt);
+  f[ldN + i] = tt;
+  f[2 * (size_t)ldN + i] = log(ls[i]);
+}
+
+__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, const double* __restrict__ E,
+                                              const double* __restrict__ ls, const double* __restrict__ f,
+                                              const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
+                                              const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
+                                              int de, const double* __restrict__ e0, double* __restrict__ W,
+                                              double* __restrict__ Nu) {
   const int j = blockIdx.x;
-  const double dgp = delta[pvars - 1];
-  const double wt = de ? 1.0 : kWt;
   const double* Ej = E + (size_t)j * ldN;
   double* Wj = W + (size_t)j * ldN;
   double* Nj = Nu + (size_t)j * ldN;
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const double eta = Ej[i], lsi = ls[i], tt = dgp * titsias[i] * wt;
-    Wj[i] = exp(eta) * lsi * exp(tt);
+    const double eta = Ej[i];
+    Wj[i] = exp(eta) * ls[i] * f[i];
     Nj[i] = de ? (eta - e0[i]) - 1.0 : eta - 1.0;
   }
   __syncthreads();
   const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
   for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
     const int i = cell[l];
-    const double eta = Ej[i], lsi = ls[i], tt = dgp * titsias[i] * wt, y = cnt[l];
-    const double w = exp(eta) * lsi * exp(tt);
-    Nj[i] = de ? (eta - e0[i]) + (y - w) / w : eta + exp(log(y) - (eta + log(lsi) + tt)) - 1.0;
+    const double eta = Ej[i], y = cnt[l];
+    if (de) {
+      const double w = exp(eta) * ls[i] * f[i];
+      Nj[i] = (eta - e0[i]) + (y - w) / w;
+    } else {
+      Nj[i] = eta + exp(log(y) - (eta + f[2 * (size_t)ldN + i] + f[ldN + i])) - 1.0;
+    }
   }
 }
 
@@ -174,14 +189,24 @@ __global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n
                                              const int* __restrict__ cv_nh, const int* __restrict__ codes,
                                              const double* __restrict__ B, double* __restrict__ out);
 
+// W / Nu: the linear predictor into the scratch buffer (on the FP64 tensor cores with option
+// eta_tc), the per-cell factors, then k_w_nu.
 int launch_w_nu(Ctx* c) {
   ProfScope ps(c, "w_nu");
-  dim3 g(div_up(c->N, TM), div_up(c->J, TN));
-  k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
-                                  c->codes_d, c->Beta, c->scratch);
-  GPL_LAUNCHED(c, "k_eta");
-  k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->scratch, c->ls, c->delta, c->titsias, c->cell, c->gptr,
-                                      c->gvalid, c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
+  if (c->eta_tc) {
+    const int rc = launch_eta_dmma(c, c->Beta, c->scratch);
+    if (rc) return rc;
+  } else {
+    dim3 g(div_up(c->N, TM), div_up(c->J, TN));
+    k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
+                                    c->codes_d, c->Beta, c->scratch);
+    GPL_LAUNCHED(c, "k_eta");
+  }
+  k_cell_factors<<<div_up(c->N, 256), 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->de ? 1 : 0, c->delta, c->titsias,
+                                                          c->ls, c->cellfac);
+  GPL_LAUNCHED(c, "k_cell_factors");
+  k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->scratch, c->ls, c->cellfac, c->cell, c->gptr, c->gvalid,
+                                      c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
   GPL_LAUNCHED(c, "k_w_nu");
   // W in group order for the group-sum GEMMs (W changes only here)
   if (c->Wg) return launch_group_order(c, c->W, c->J, c->Wg);
@@ -213,6 +238,7 @@ __global__ void __launch_bounds__(256) k_eta(int N, int ldN, int P, int J, int n
 
 int launch_zbeta(Ctx* c, const double* B, double* out) {
   ProfScope ps(c, "zbeta");
+  if (c->eta_tc) return launch_eta_dmma(c, B, out);
   dim3 g(div_up(c->N, TM), div_up(c->J, TN));
   k_eta<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->J, c->n_d, c->n_cv, c->Dm, c->dcol_d, c->cv_nh_d,
                                   c->codes_d, B, out);

@@ -593,7 +593,7 @@ int launch_tc_gram(Ctx* c) {
     ProfScope ps(c, "gram");
     dim3 g(t.pair_tiles, t.gram_tiles_n);
     Tunable* tu = nullptr;
-    const int grp = tune_pick(c, "tc_gram", {0, 8, 16}, 0, &tu);
+    const int grp = tune_pick(c, "tc_gram", {0, 8, 16}, 8, &tu);
     TuneScope ts(c, tu);
     k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
                                                            t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
@@ -634,7 +634,7 @@ int launch_tc_grad(Ctx* c) {
       ProfScope ps(c, "uq");
       dim3 g(t.pair_tiles, div_up(c1 - c0, kGramN));
       Tunable* tu = nullptr;
-      const int grp = tune_pick(c, "tc_grad", {0, 8, 16}, 0, &tu);
+      const int grp = tune_pick(c, "tc_grad", {0, 8, 16}, 8, &tu);
       TuneScope ts(c, c1 - c0 == c->N ? tu : nullptr);
       k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
                                                              t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,

@@ -169,11 +169,13 @@ def amortised_placement(config: int, n_train: int, n_test: int, fit_lbfgs: int, 
                         hidden: int = 256, batch: int = 1024, iters: int = 30, seed: int = 0, device: int = 0,
                         stream: Optional[int] = None, precision: str = "fp64", lr: float = 1e-3, G=None):
     """The encoder's experiment: a plain fit on n_train cells of configuration `config`, the
-    encoder trained on (profile, fitted X) of those cells, then n_test held-out cells of the same
-    generator and gene parameters placed (a) by the encoder alone, (b) by the encoder followed by
-    `iters` per-cell L-BFGS steps at the fitted model (the fallback, whose result is the judge),
-    (c) by the same steps from X = 0 (the method without the encoder). Returns a dict of the
-    per-cell objective gaps (relative to the judge), Procrustes-aligned RMSEs and timings."""
+    encoder trained on (profile, fitted X) of nine tenths of those cells for up to `epochs`
+    epochs, keeping the parameters of the 20-epoch checkpoint with the smallest RMSE on the
+    other tenth; then n_test held-out cells of the same generator and gene parameters placed
+    (a) by the encoder alone (clamped to the training targets' box), (b) by the encoder followed
+    by `iters` per-cell L-BFGS steps at the fitted model (the fallback, whose result is the
+    judge), (c) by the same steps from X = 0 (the method without the encoder). Returns a dict of
+    the per-cell objective gaps (relative to the judge), Procrustes-aligned RMSEs and timings."""
     import time
 
     from . import synth
@@ -205,19 +207,47 @@ def amortised_placement(config: int, n_train: int, n_test: int, fit_lbfgs: int, 
         Xfit, l_train, _ = place_cells(m, fit["X"].reshape(Q, N1).T.copy(), iters)
         out["target_refine_seconds"] = time.time() - t0
     genes = select_genes(train.y, train.ls, min(n_genes, full.J))
-    perm = np.random.default_rng(seed + 1).permutation(N1).astype(np.int32)
+    # a tenth of the training cells (at least one batch) held out to choose the epoch count
+    n_val = max(batch, n_train // 10)
+    rng = np.random.default_rng(seed + 1)
+    split = rng.permutation(N1)
+    tr_idx, va_idx = np.sort(split[n_val:]), np.sort(split[:n_val])
+    fit_cells = synth.cell_subset(train, tr_idx, init=False)
+    val_cells = synth.cell_subset(train, va_idx, init=False)
+    perm = rng.permutation(tr_idx.shape[0]).astype(np.int32)
     t0 = time.time()
+    chunk = max(1, min(epochs, 20))
     with Encoder(len(genes), Q, hidden=hidden, batch=batch, device=device, stream=stream, seed=seed) as enc:
-        enc.set_cells(0, train.y, train.ls, genes, perm)
-        enc.set_targets(Xfit)
-        losses = enc.train(epochs, lr=lr, seed=seed)
+        enc.set_cells(0, fit_cells.y, fit_cells.ls, genes, perm)
+        enc.set_targets(Xfit[tr_idx])
+        enc.set_cells(1, val_cells.y, val_cells.ls, genes)
+        losses, val_rmse, best, best_params, best_epochs, done = [], [], np.inf, None, 0, 0
+        while done < epochs:
+            k = min(chunk, epochs - done)
+            losses.extend(enc.train(k, lr=lr, seed=seed + done).tolist())
+            done += k
+            mv, _ = enc.predict(1)
+            r = float(np.sqrt(np.mean((mv - Xfit[va_idx]) ** 2)))
+            val_rmse.append([done, r])
+            if r < best:
+                best, best_params, best_epochs = r, enc.get_params(), done
+        if best_params is not None:
+            enc.set_params(best_params)
         out["train_seconds"] = time.time() - t0
         out["train_loss_first_last"] = [float(losses[0]), float(losses[-1])] if len(losses) else None
+        out["validation_rmse"] = val_rmse
+        out["epochs_chosen"] = best_epochs
         enc.set_cells(1, test.y, test.ls, genes)
         t0 = time.time()
         X_enc, _ = enc.predict(1)
         out["encoder_seconds"] = time.time() - t0
         out["encoder_launches"] = enc.launches()
+    # predictions outside the training targets' box (widened by a tenth of its width per
+    # dimension) are clamped to it: the encoder has seen no cell there
+    lo, hi = Xfit.min(0), Xfit.max(0)
+    lo, hi = lo - 0.1 * (hi - lo), hi + 0.1 * (hi - lo)
+    out["clamped_fraction"] = float(np.mean(np.any((X_enc < lo) | (X_enc > hi), axis=1)))
+    X_enc = np.clip(X_enc, lo, hi)
     prm = Params(np.ones(N2), fit["delta"], X_enc, fit["T"].reshape(Q, M).T, fit["rho"], fit["phi"])
     with GPLVM.from_dataset(test, device=device, stream=stream) as jm:
         jm.set_params(prm)

@@ -132,3 +132,21 @@ def test_placement_raises_objective_and_recovers_fitted_coordinates(fitted):
         gap_end = np.median((f_fit - f_end) / np.abs(f_fit))
         print(f"median objective gap to the fitted X: start {gap_start:.2e}, after 30 steps {gap_end:.2e}")
         assert gap_end < 0.2 * gap_start
+
+
+def test_amortised_placement_experiment_runs_end_to_end():
+    """The whole experiment at configuration 0 (2,000 cells): fit, validation-chosen epochs,
+    clamped predictions, placement from the encoder and from zero; every reported figure finite."""
+    from gaspacho2_b200.encoder import amortised_placement
+
+    out = amortised_placement(0, 1536, 464, 20, 40, n_genes=200, batch=256)
+    for k in ("elbo_gap_encoder", "elbo_gap_without_encoder", "validation_rmse", "epochs_chosen",
+              "clamped_fraction", "procrustes_rmse"):
+        assert k in out, k
+    assert 0 < out["epochs_chosen"] <= 40
+    assert all(np.isfinite(r) for _, r in out["validation_rmse"])
+    print({k: out[k] for k in ("elbo_gap_encoder", "elbo_gap_without_encoder", "cells_refined_above_start_from_zero",
+                               "epochs_chosen", "clamped_fraction")})
+    for k in ("elbo_gap_encoder", "elbo_gap_without_encoder"):
+        assert np.isfinite(out[k]["median"]), k
+    assert 0.0 <= out["clamped_fraction"] <= 1.0

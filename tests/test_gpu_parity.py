@@ -214,3 +214,41 @@ def test_gram_over_cell_ranges():
     e = gu.rel_err(psi[1], psi[0])
     print(f"Psi over 5 ranges vs one range: {e:.2e}")
     assert e <= 1e-13
+
+
+@pytest.mark.parametrize("name", list(gu.CASES) + ["c2_head"])
+def test_tensor_core_predictor(name):
+    """Option eta_tc (the linear predictor, W and Nu on the FP64 tensor cores, k_eta_dmma) on the
+    golden phase sequence: W and Nu of the first sweep (same Beta in both forms) within 1e-12 of the
+    FFMA form (the dense products and level coefficients are summed in other orders), and every
+    phase buffer within the golden bar (1e-8, or 20x the reference's own sub-ulp sensitivity at
+    the headline shape, whose 132 dense columns end in a slice with one live k4 step)."""
+    gd = gu.load(name)
+    outs = []
+    for flag in (0, 1):
+        with GPLVM.from_dataset(gd) as m:
+            m.set_option("eta_tc", flag)
+            assert m.get_option("eta_tc") == flag
+            outs.append(gu.run_phases(m, gd))
+    for k in ("sweep0_W", "sweep0_Nu"):
+        e = gu.rel_err(outs[1][k], outs[0][k])
+        print(f"{k}: {e:.2e} against the FFMA form")
+        assert e <= 1e-12, f"{k}: {e:.2e}"
+    g = gd.g
+    bad = []
+    for k, v in outs[1].items():
+        if k not in g or k in ("irls_n",):
+            continue
+        v = np.atleast_1d(np.asarray(v, np.float64))
+        ref = np.atleast_1d(g[k])
+        if "idx_" + k in g:
+            a = v[g["idx_" + k]]
+            e = float(np.abs(a - ref).max() / float(g["scale_" + k]))
+        else:
+            e = gu.rel_err(v, ref)
+        tol = max(TOL_PHASE, 20.0 * float(g.get("sens_" + k, 0.0)))
+        if k in ("obj0", "obj1", "sweep0_lkhd"):
+            tol = min(max(tol, TOL_PHASE), TOL_FIT)
+        if not e <= tol:
+            bad.append(f"{k}: {e:.2e} > {tol:.2e}")
+    assert not bad, "; ".join(bad)
