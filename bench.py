@@ -873,6 +873,7 @@ def fit_trace(args):
                               "first": float(tr[0]) if len(tr) else None, "last": float(tr[-1]) if len(tr) else None,
                               "ended": why, "seconds": a.elapsed_time(b) / 1e3,
                               "rejected_tries": int(st["evals"] - 1 - st["lbfgs"]),
+                              "failed_line_searches": int(np.sum(np.diff(tr) <= 0)) if len(tr) > 1 else 0,
                               "rel_gains": [float(x) for x in (np.diff(tr) / np.abs(tr[1:]))[-5:]] if len(tr) > 1
                               else []})
                 itr += 1

@@ -4,7 +4,8 @@
 //
 //   zt_u      bvec[dcol a, j] = sum_i D_ia u_ij (getZtOinvjnj util_cuda.cu:462-487 with
 //             u = W nu / Omega; initBeta init.cu:193-221 with u = y0), split over the cells
-//             into 8 ranges whose partial sums are added in order.  2*N*J*n_d flops.
+//             into 8-32 ranges (chosen to fill the last wave) whose partial sums are added in
+//             order.  2*N*J*n_d flops.
 //   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
 //   group     S[j][g][a] = sum_{i in g} w_ij D_ia, K = the group's cells, read from copies of
 //             W, D and 1/Omega in group order (each group a contiguous run of rows).
@@ -17,6 +18,7 @@
 // their arithmetic only when the slice is stored) into double-buffered shared memory laid out
 // [k][m] and [k][n] with rows padded to 4 mod 16 doubles (conflict-free fragment loads).
 #include <algorithm>
+#include <cmath>
 
 #include "dmma_common.cuh"
 #include "gpl_internal.cuh"
@@ -35,6 +37,7 @@ struct DTile {
 };
 using TileSq = DTile<2, 4, 4>;    // 128 x 128
 using TileTall = DTile<1, 9, 2>;  // 144 x 128: the dense columns (n_d <= 144) in one tile
+using TileWide = DTile<4, 2, 9>;  // 128 x 144: the dense columns (n_d <= 144) across one tile
 
 constexpr int kSplitK = 8;
 
@@ -344,6 +347,51 @@ struct EpGene {  // T_z[r + c*n]
   int n;
   __device__ void operator()(int r, int c, int z, double v) const { T[(size_t)z * n * n + r + (size_t)c * n] = v; }
 };
+// The per-gene n x n products of the whitening as two GEMMs each, over all genes at once: the
+// genes' matrices stacked as rows (A(r = z n + a, k)) against one n x n factor, or the factor
+// against the genes' matrices side by side as columns (B(k, col = z n + c)).
+struct LdGeneRows {  // A(r = z n + a, k) = G_z[a + k*n] (a contiguous)
+  static constexpr bool kFastK = false;
+  const double* G;
+  int n;
+  __device__ double operator()(int r, int k, int) const {
+    const int z = r / n, a = r - z * n;
+    return G[(size_t)z * n * n + a + (size_t)k * n];
+  }
+};
+struct LdGeneSRows {  // A(r = z n + a, k) = S_z[dcol a, dcol k] (the dense block of Psi_z^{-1})
+  static constexpr bool kFastK = false;
+  const double* S;
+  const int* dcol;
+  int n, P;
+  __device__ double operator()(int r, int k, int) const {
+    const int z = r / n, a = r - z * n;
+    return S[(size_t)z * P * P + dcol[a] + (size_t)dcol[k] * P];
+  }
+};
+struct EpGeneRows {  // T_z[a + c*n] for r = z n + a
+  double* T;
+  int n;
+  __device__ void operator()(int r, int c, int, double v) const {
+    const int z = r / n, a = r - z * n;
+    T[(size_t)z * n * n + a + (size_t)c * n] = v;
+  }
+};
+struct EpPsiDDCols {  // column col = z n + c: Psi_z at (dcol r, dcol c) and its mirror, plus DeltaInv; r <= c
+  double* Psi;
+  const double* Dinv;
+  const int* dcol;
+  int P, n;
+  __device__ void operator()(int r, int col, int, double v) const {
+    const int z = col / n, c = col - z * n;
+    if (r > c) return;
+    const size_t mk = dcol[r], ml = dcol[c];
+    const double x = v + Dinv[mk + ml * P];
+    double* Pz = Psi + (size_t)z * P * P;
+    Pz[mk + ml * P] = x;
+    Pz[ml + mk * P] = x;
+  }
+};
 struct EpPsiDD {  // Psi_z at (dcol r, dcol c) and its mirror, plus DeltaInv; r <= c only
   double* Psi;
   const double* Dinv;
@@ -397,6 +445,23 @@ static int ensure_part(Ctx* c, size_t n) {
   return GPL_OK;
 }
 
+// The number of cell ranges of a split-K launch of `tiles` output tiles at one CTA per SM: the
+// S in [8, 32] whose S x tiles CTAs fill their last wave best (the smallest such S). At config 2
+// (79 gene tiles, 148 SMs) S = 28 puts 2,212 CTAs in 14.95 waves where S = 8 gave 4.27 waves.
+static int split_count(int tiles, int sms) {
+  int best = kSplitK;
+  double best_fill = 0.0;
+  for (int s = kSplitK; s <= 32; s++) {
+    const double waves = (double)tiles * s / sms;
+    const double fill = waves / std::ceil(waves);
+    if (fill > best_fill + 1e-9) {
+      best_fill = fill;
+      best = s;
+    }
+  }
+  return best;
+}
+
 int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
   using T = TileTall;
   if (c->n_d > T::BM) return GPL_ERR_ARG;
@@ -405,15 +470,17 @@ int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
     int rc = recip_omega(c, &rOm);
     if (rc) return rc;
   }
-  int rc = ensure_part(c, (size_t)kSplitK * c->n_d * c->J);
+  const int tiles = div_up(c->J, T::BN);
+  const int S = split_count(tiles, c->sm_count);
+  int rc = ensure_part(c, (size_t)S * c->n_d * c->J);
   if (rc) return rc;
-  const int per = (c->N + kSplitK - 1) / kSplitK;
-  dim3 g(1, div_up(c->J, T::BN), kSplitK);
+  const int per = (c->N + S - 1) / S;
+  dim3 g(1, tiles, S);
   rc = launch_dgen<T>(c, g, c->n_d, c->J, LdDt{c->Dm, c->ldN}, LdU{c->W, u, rOm, c->ldN, mode},
                       KSplit{c->N, per}, EpPart{c->part, c->n_d, c->J}, "k_dgen(zt_u)");
   if (rc) return rc;
   dim3 g2(div_up(c->J, 256), c->n_d);
-  k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, kSplitK, c->dcol_d, c->part, out);
+  k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, S, c->dcol_d, c->part, out);
   GPL_LAUNCHED(c, "k_reduce_bvec");
   return GPL_OK;
 }
@@ -461,10 +528,24 @@ int dgen_hk(Ctx* c) {
                         "k_dgen(hk)");
 }
 
+// Psi_DD,j = L G~_j L^T + DeltaInv_DD for every gene: T_j = G~_j L^T as one GEMM over the stacked
+// rows of all genes (J n x n against L^T), then L T_j as one GEMM over the genes' columns side by
+// side (L against n x J n). Per gene (grid z = gene) where J n exceeds the grid's column limit.
 int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw) {
-  using T = TileTall;
   const int n = c->n_d;
-  if (n > T::BM || c->J > 65535) return GPL_ERR_ARG;
+  const int64_t Jn = (int64_t)c->J * n;
+  if (n > TileWide::BN || n > TileTall::BM) return GPL_ERR_ARG;
+  if (div_up(Jn, (int64_t)TileTall::BN) <= 65535) {
+    int rc = launch_dgen<TileWide>(c, dim3((unsigned)div_up(Jn, (int64_t)TileWide::BM), 1, 1), (int)Jn, n,
+                                   LdGeneRows{Gt, n}, LdLT{Lw, n}, KAll{n}, EpGeneRows{Tt, n},
+                                   "k_dgen(unwhiten GL^T)");
+    if (rc) return rc;
+    return launch_dgen<TileTall>(c, dim3(1, (unsigned)div_up(Jn, (int64_t)TileTall::BN), 1), n, (int)Jn,
+                                 LdL{Lw, n}, LdGeneT{Tt, n}, KAll{n},
+                                 EpPsiDDCols{c->Psi, c->DeltaInv, c->dcol_d, c->P, n}, "k_dgen(unwhiten L(GL^T))");
+  }
+  using T = TileTall;
+  if (c->J > 65535) return GPL_ERR_ARG;
   dim3 g(1, div_up(n, T::BN), c->J);
   int rc = launch_dgen<T>(c, g, n, n, LdGene{Gt, n}, LdLT{Lw, n}, KAll{n}, EpGene{Tt, n}, "k_dgen(unwhiten GL^T)");
   if (rc) return rc;
@@ -472,10 +553,22 @@ int dgen_unwhiten(Ctx* c, const double* Gt, double* Tt, const double* Lw) {
                         "k_dgen(unwhiten L(GL^T))");
 }
 
+// S~_j = L^T S_DD,j L for every gene, in the same two stacked GEMMs (S_DD,j L over the genes'
+// rows, then L^T against the genes' columns).
 int dgen_whiten_inverse(Ctx* c, const double* Lw, double* Tt, double* St) {
-  using T = TileTall;
   const int n = c->n_d;
-  if (n > T::BM || c->J > 65535) return GPL_ERR_ARG;
+  const int64_t Jn = (int64_t)c->J * n;
+  if (n > TileWide::BN || n > TileTall::BM) return GPL_ERR_ARG;
+  if (div_up(Jn, (int64_t)TileTall::BN) <= 65535) {
+    int rc = launch_dgen<TileWide>(c, dim3((unsigned)div_up(Jn, (int64_t)TileWide::BM), 1, 1), (int)Jn, n,
+                                   LdGeneSRows{c->PsiInv, c->dcol_d, n, c->P}, LdLk{Lw, n}, KAll{n},
+                                   EpGeneRows{Tt, n}, "k_dgen(S L)");
+    if (rc) return rc;
+    return launch_dgen<TileTall>(c, dim3(1, (unsigned)div_up(Jn, (int64_t)TileTall::BN), 1), n, (int)Jn,
+                                 LdLTk{Lw, n}, LdGeneT{Tt, n}, KAll{n}, EpGene{St, n}, "k_dgen(L^T S L)");
+  }
+  using T = TileTall;
+  if (c->J > 65535) return GPL_ERR_ARG;
   dim3 g(1, div_up(n, T::BN), c->J);
   int rc = launch_dgen<T>(c, g, n, n, LdGeneS{c->PsiInv, c->dcol_d, c->P}, LdLk{Lw, n}, KAll{n}, EpGene{Tt, n},
                           "k_dgen(S L)");
