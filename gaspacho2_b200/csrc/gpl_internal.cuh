@@ -53,7 +53,7 @@ struct DevBuf {
 // Column-pair FP64 GEMM state (k_dgemm.cu): the pair list (a <= b over the dense columns),
 // 1/Omega, the gathered Psi^{-1} pairs per gene and a range of V rows.
 struct PairState {
-  bool ready = false, wide = false;  // wide: more dense columns than the pair GEMMs stage
+  bool ready = false, wide = false;  // wide: a cell's V row exceeds k_v_to_u's shared memory
   int n_pairs = 0, pairs_pad = 0, cpad = 0, v_cells = 0;
   int smem_gram = 0, smem_v = 0, smem_vu = 0;
   int2* pairs = nullptr;

@@ -351,6 +351,28 @@ __global__ void __launch_bounds__(256) k_v_to_u(int N, int ldN, int n_d, int n_p
   }
 }
 
+// The same sums when a cell's V row exceeds the shared-memory budget (more than about 220 dense
+// columns): the row is read from global memory (L1 / L2) instead of staged, the dense row of
+// the cell is staged; identical operations in identical order.
+__global__ void __launch_bounds__(256) k_v_to_u_wide(int N, int ldN, int n_d, int pairs_pad, int c0, int c1,
+                                                     const double* __restrict__ D, const double* __restrict__ V,
+                                                     double* __restrict__ U) {
+  extern __shared__ __align__(16) double ds[];  // D row of the cell
+  for (int i = c0 + blockIdx.x; i < c1 && i < N; i += gridDim.x) {
+    const double* vr = V + (size_t)(i - c0) * pairs_pad;
+    for (int e = threadIdx.x; e < n_d; e += blockDim.x) ds[e] = D[(size_t)e * ldN + i];
+    __syncthreads();
+    for (int a = threadIdx.x; a < n_d; a += blockDim.x) {
+      double s = 0.0;
+      for (int b = 0; b < a; b++) s = fma(ds[b], __ldg(vr + b * n_d - b * (b - 1) / 2 + (a - b)), s);
+      const double* row = vr + a * n_d - a * (a - 1) / 2 - a;
+      for (int b = a; b < n_d; b++) s = fma(ds[b], __ldg(row + b), s);
+      U[i + (size_t)a * ldN] = s;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
@@ -374,31 +396,29 @@ int pair_prepare(Ctx* c) {
   s.smem_gram = (int)sizeof(double) * 3 * (BK * SA + BN * SBT);
   s.smem_v = (int)sizeof(double) * 3 * (BK * SA + BK * SBN);
   s.smem_vu = (int)sizeof(double) * (s.pairs_pad + n_d);
-  // more dense columns than k_v_to_u stages per cell: the pair GEMMs are not used (their
-  // callers take the FFMA forms); the pair list and 1/Omega still serve the other kernels
+  // more dense columns than k_v_to_u stages per cell: k_v_to_u_wide reads the V rows from
+  // global memory instead
   s.wide = s.smem_vu > 200 * 1024;
   if (cudaMalloc((void**)&s.pairs, sizeof(int2) * pairs.size()) != cudaSuccess ||
       cudaMalloc((void**)&s.rOm, sizeof(double) * s.cpad) != cudaSuccess ||
-      (!s.wide && cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess) ||
-      (!s.wide && cudaMalloc((void**)&s.V, sizeof(double) * (size_t)s.v_cells * s.pairs_pad) != cudaSuccess)) {
+      cudaMalloc((void**)&s.Sp, sizeof(double) * (size_t)c->J * s.pairs_pad) != cudaSuccess ||
+      cudaMalloc((void**)&s.V, sizeof(double) * (size_t)s.v_cells * s.pairs_pad) != cudaSuccess) {
     cudaGetLastError();
     pair_release(c);
     c->err = "device allocation failed: pair GEMM buffers";
     return GPL_ERR_ALLOC;
   }
   GPL_TRY(c, cudaMemcpy(s.pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
-  if (!s.wide && s.v_cells < c->N &&
+  if (s.v_cells < c->N &&
       cudaMalloc((void**)&s.Gacc, sizeof(double) * (size_t)s.n_pairs * c->J) != cudaSuccess) {
     cudaGetLastError();
     pair_release(c);
     c->err = "device allocation failed: pair Gram accumulator";
     return GPL_ERR_ALLOC;
   }
-  if (!s.wide) {
-    GPL_TRY(c, cudaFuncSetAttribute(k_pair_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_gram));
-    GPL_TRY(c, cudaFuncSetAttribute(k_pair_v, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_v));
-    GPL_TRY(c, cudaFuncSetAttribute(k_v_to_u, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_vu));
-  }
+  GPL_TRY(c, cudaFuncSetAttribute(k_pair_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_gram));
+  GPL_TRY(c, cudaFuncSetAttribute(k_pair_v, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_v));
+  if (!s.wide) GPL_TRY(c, cudaFuncSetAttribute(k_v_to_u, cudaFuncAttributeMaxDynamicSharedMemorySize, s.smem_vu));
   s.ready = true;
   return GPL_OK;
 }
@@ -433,7 +453,6 @@ int launch_pair_gram(Ctx* c) {
   int rc = pair_prepare(c);
   if (rc) return rc;
   PairState& s = c->pr;
-  if (s.wide) return GPL_ERR_ARG;
   if ((rc = launch_recip(c))) return rc;
   ProfScope ps(c, "gram");
   const bool one = s.v_cells >= c->N;
@@ -464,7 +483,6 @@ int launch_pair_gram(Ctx* c) {
 int launch_pair_uq(Ctx* c) {
   int rc = pair_prepare(c);
   if (rc) return rc;
-  if (c->pr.wide) return GPL_ERR_ARG;
   PairState& s = c->pr;
   if ((rc = launch_recip(c))) return rc;
   {
@@ -495,6 +513,12 @@ int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D) {
   PairState& s = c->pr;
   ProfScope ps(c, "v_to_u");
   const int grid = std::min(c1 - c0, 148 * 8);
+  if (s.wide) {
+    k_v_to_u_wide<<<grid, 256, sizeof(double) * c->n_d, c->stream>>>(c->N, c->ldN, c->n_d, s.pairs_pad, c0, c1, D,
+                                                                    s.V, c->U);
+    GPL_LAUNCHED(c, "k_v_to_u_wide");
+    return GPL_OK;
+  }
   k_v_to_u<<<grid, 256, s.smem_vu, c->stream>>>(c->N, c->ldN, c->n_d, s.n_pairs, s.pairs_pad, c0, c1, D, s.V, c->U);
   GPL_LAUNCHED(c, "k_v_to_u");
   return GPL_OK;
@@ -623,8 +647,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
       if (s + 2 < nsl) load(m0, j0, s + 2, (base + s + 2) % 3);
       cp_async_commit();
       const int st = (base + s) % 3;
-      const int nkk = min(BK / 4, (a.n_d - s * BK + 3) / 4);
-      warp_slice_live(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, nkk, acc);
+      if (s + 1 < nsl) {
+        warp_slice<true>(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, acc);
+      } else {  // the last slice: only the k4 steps that reach a dense column
+        const int nkk = min(BK / 4, (a.n_d - s * BK + 3) / 4);
+        warp_slice_live(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, nkk, acc);
+      }
     }
     // the next tile's first two slices go to the two stages that no warp reads any more
     base += nsl;

@@ -485,16 +485,48 @@ int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
   return GPL_OK;
 }
 
+// C1 over S gene ranges (S = 1..4, the count whose CTAs fill their last wave best: 3 at config
+// 2, 2,346 CTAs in 15.85 waves against 782 in 5.28) whose partials are added in order.
+__global__ void k_reduce_parts_ld(int m, int n, int nz, const double* __restrict__ part, double* __restrict__ out,
+                                  int64_t ld) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, cc = blockIdx.y;
+  if (r >= m) return;
+  double s = 0.0;
+  for (int z = 0; z < nz; z++) s += part[((size_t)z * m + r) * n + cc];
+  out[r + (size_t)cc * ld] = s;
+}
+
 int dgen_c1_tn(Ctx* c) {
   using T = TileSq;
   const double* rOm = nullptr;
   int rc = recip_omega(c, &rOm);
   if (rc) return rc;
   const int g0 = c->nh[c->p - 1];
-  dim3 g(div_up(c->N, T::BM), div_up(c->M, T::BN), 1);
-  return launch_dgen<T>(c, g, c->N, c->M, LdTn{c->W, c->Nu, c->scratch, rOm, c->rphi, c->ldN},
-                        LdTBetaGP{c->tBeta, c->P, g0}, KAll{c->J}, EpColMajor{c->C1, (int64_t)c->ldN},
-                        "k_dgen(c1_tn)");
+  const int tiles = div_up(c->N, T::BM) * div_up(c->M, T::BN);
+  int S = 1;
+  double best = 0.0;
+  for (int z = 1; z <= 4; z++) {
+    const double waves = (double)tiles * z / c->sm_count, fill = waves / std::ceil(waves);
+    if (fill > best + 1e-9) {
+      best = fill;
+      S = z;
+    }
+  }
+  LdTn A{c->W, c->Nu, c->scratch, rOm, c->rphi, c->ldN};
+  LdTBetaGP B{c->tBeta, c->P, g0};
+  if (S == 1) {
+    dim3 g(div_up(c->N, T::BM), div_up(c->M, T::BN), 1);
+    return launch_dgen<T>(c, g, c->N, c->M, A, B, KAll{c->J}, EpColMajor{c->C1, (int64_t)c->ldN}, "k_dgen(c1_tn)");
+  }
+  if ((rc = ensure_part(c, (size_t)S * c->N * c->M))) return rc;
+  dim3 g(div_up(c->N, T::BM), div_up(c->M, T::BN), S);
+  rc = launch_dgen<T>(c, g, c->N, c->M, A, B, KSplit{c->J, (c->J + S - 1) / S}, EpPart{c->part, c->N, c->M},
+                      "k_dgen(c1_tn)");
+  if (rc) return rc;
+  dim3 g2(div_up(c->N, 256), c->M);
+  k_reduce_parts_ld<<<g2, 256, 0, c->stream>>>(c->N, c->M, S, c->part, c->C1, (int64_t)c->ldN);
+  GPL_LAUNCHED(c, "k_reduce_parts_ld");
+  return GPL_OK;
 }
 
 int dgen_group_sums(Ctx* c, int mode) {
