@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
     ap.add_argument("--irls-sweeps", type=int, default=2)
     ap.add_argument("--option", action="append", default=[],
-                    help="name=value: a library option (gpl_set_option) for the fit-trace contexts; repeatable")
+                    help="name=value: a library option (gpl_set_option) for the benchmark's, the precision leg's "
+                         "and the fit-trace contexts; repeatable")
     ap.add_argument("--eta-tc", type=int, default=None,
                     help="option eta_tc (linear predictor and W / Nu on the FP64 tensor cores): 0 or 1; "
                          "default: the library's")
@@ -479,6 +480,9 @@ def precision_leg(args, ds, stream, device):
     batched = not args.plain
     if args.eta_tc is not None:
         m.set_option("eta_tc", args.eta_tc)
+    for kv in args.option:
+        k, v = kv.split("=")
+        m.set_option(k, int(v))
     if batched:
         for k in ("autotune", "graph"):
             m.set_option(k, 1)
@@ -576,6 +580,9 @@ def run_ours(args):
     batched = not args.plain
     if args.eta_tc is not None:
         m.set_option("eta_tc", args.eta_tc)
+    for kv in args.option:
+        k, v = kv.split("=")
+        m.set_option(k, int(v))
     if batched:
         # the batched form: the IRLS tail as one persistent launch, evaluations replayed from
         # captured CUDA graphs, tile orders chosen by the autotuner (all give the plain path's bits)

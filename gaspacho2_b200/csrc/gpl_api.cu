@@ -643,6 +643,8 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
     c->tc.run = (int)value;
   } else if (s == "tc_check") {
     c->tc_check = value != 0;
+  } else if (s == "tc_pair") {
+    c->tc_pair = value != 0;
   } else if (s == "autotune") {
     c->autotune = value != 0;
   } else if (s == "fused_tail") {
@@ -677,6 +679,7 @@ int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
   else if (s == "refine_steps") *value = c->refine_steps;
   else if (s == "tc_run") *value = c->tc_run;
   else if (s == "tc_check") *value = c->tc_check ? 1 : 0;
+  else if (s == "tc_pair") *value = c->tc_pair ? 1 : 0;
   else if (s == "pair_range_cells") *value = c->pair_range_cells;
   else if (s == "graph") *value = c->use_graph ? 1 : 0;
   else if (s == "fused_tail") *value = c->fused_tail ? 1 : 0;

@@ -65,7 +65,7 @@ struct TcState {
   bool ready = false;
   int cpad = 0, chunks_cells = 0, gram_tiles_n = 0, Jpad = 0;
   int n_pairs = 0, pair_tiles = 0;
-  int smem_gram = 0, smem_whiten = 0, run = 4;  // run: K chunks per FP32 accumulator run
+  int smem_gram = 0, smem_gram2 = 0, smem_whiten = 0, run = 4;  // run: K chunks per FP32 accumulator run
   __nv_bfloat16 *whi = nullptr, *wlo = nullptr;   // w = W/Omega, gene rows x cpad
   __nv_bfloat16 *ahi = nullptr, *alo = nullptr;   // whitened pair products, pair rows x cpad
   __nv_bfloat16 *shi = nullptr, *slo = nullptr;   // whitened inverse pairs, pair rows x Jpad
@@ -76,6 +76,7 @@ struct TcState {
   int2* pairs = nullptr;
   int* err = nullptr;
   CUtensorMap map_whi, map_wlo, map_ahi, map_alo, map_shi, map_slo, map_ohi, map_olo;
+  CUtensorMap map_whi64, map_wlo64, map_ohi64, map_olo64;  // 64-row boxes: the CTA-pair kernel's B halves
 };
 
 // One open or settled choice of the autotuner (tune.cu): candidate values, each one's best
@@ -118,6 +119,7 @@ struct Ctx {
   // options (gpl_set_option)
   bool tc_check = false;      // read the tensor-core error flag after every tensor-core launch
   int tc_run = 4;             // precision form: K chunks per FP32 accumulator run before the FP64 fold
+  bool tc_pair = false;       // precision form: the tensor-core contractions on CTA pairs (k_tc_gram2)
   int64_t pair_range_cells = 0;  // cells per range of the pair GEMMs (0: as many as 8 GiB holds)
   // CUDA graphs of one objective evaluation and of the gradient that follows it (option
   // "graph"): captured on first use, replayed after; dropped whenever a buffer they captured

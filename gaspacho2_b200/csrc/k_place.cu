@@ -5,7 +5,7 @@
 // its own L-BFGS with the reference's step rules (lbfgs, util_cuda.cu:187-232: memory 10, the
 // first step -g/1e5, the two-loop recursion with scaling s.y / y.y, every coordinate clipped to
 // [-1, 1]; the backtracking of ggplvm.cu:1278-1289: accept a rise or the 7th try, else shrink by
-// 0.1, by 0.01 after a non-finite value).
+// 0.1, by 0.01 after a non-finite value; a non-finite 7th try is not accepted here).
 //
 // Per-cell objective: the Poisson log-probability of the cell's counts over all genes, with the
 // mean of the IRLS's getLkhdPois (ggplvm.cu:703-724) and getWForBeta (ggplvm.cu:468-514), plus the
@@ -158,7 +158,10 @@ __global__ void k_place_dir(int N, int Q, int it, double* __restrict__ X, const 
 }
 
 // Line-search decision for cells still searching: accept a rise of l (or the 7th try); else
-// shrink the step (x0.1, x0.01 after a non-finite value) and move to the new trial point.
+// shrink the step (x0.1, x0.01 after a non-finite value) and move to the new trial point. One
+// departure from the reference's rule, for this per-cell use only: a 7th try whose value is not
+// finite is not accepted; the cell goes back to the step's start, where the zero step that
+// follows (a degenerate history gives no step) keeps it.
 __global__ void k_place_accept(int N, int Q, int ktr, const double* __restrict__ f_new, const double* __restrict__ f_old,
                                double* __restrict__ X, const double* __restrict__ X0, const double* __restrict__ d,
                                double* __restrict__ sr, int* __restrict__ searching, int* __restrict__ n_open) {
@@ -166,6 +169,8 @@ __global__ void k_place_accept(int N, int Q, int ktr, const double* __restrict__
   if (i >= N || !searching[i]) return;
   const double fn = f_new[i];
   if (fn > f_old[i] || ktr == 7) {
+    if (!(fn > f_old[i]) && (isnan(fn) || isinf(fn)))
+      for (int c = 0; c < Q; c++) X[i + (size_t)c * N] = X0[i + (size_t)c * N];
     searching[i] = 0;
     return;
   }

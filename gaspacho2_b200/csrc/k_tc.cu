@@ -50,7 +50,7 @@ using namespace tc;
 namespace {
 constexpr int kThreadsGram = 192;       // TMA, MMA and 4 drain warps
 constexpr int kStagesGram = 3;          // pipeline depth (192 KB of operand tiles)
-constexpr int kMaxStages = 3;
+constexpr int kMaxStages = 4;          // barriers held (the CTA-pair kernel's stages)
 constexpr int kGramN = 128;             // genes per Gram tile
 constexpr int kSBGram = 4;              // chunks per FP32 run (default; the option tc_run overrides)
 constexpr int kTileA = 128 * 128;       // 128 rows x 64 BF16
@@ -276,6 +276,198 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
+// ---------------------------------------------------------------------------------------------
+// The same contraction on CTA pairs (option tc_pair): a cluster of two CTAs computes 256 pairs x
+// 128 columns with one tcgen05.mma.cta_group::2 (M = 256) per K step, issued by the even CTA.
+// Each CTA loads its own 128 pair rows of A and half (64 rows) of B, so a CTA moves 48 KB per
+// 64-wide K chunk instead of 64 KB and four stages fit in shared memory instead of three: more
+// bytes in flight per MMA, against the single-CTA kernel's bound (bytes in flight against L2
+// latency). Each CTA's TMEM holds its 128 rows of the accumulators; both CTAs drain their own
+// rows into FP64 and write their own pairs' results, as in k_tc_gram (the same sums in the same
+// order per output: the K steps and the FP32 runs are those of k_tc_gram).
+//
+// Barriers: full[s] of the even CTA counts both CTAs' TMA bytes (the odd CTA's loads signal it
+// through its cluster address); empty[s] and accb[b] of both CTAs receive the MMA thread's
+// multicast commits; drained[b] of the even CTA counts both CTAs' 128 drain threads. Every wait is
+// bounded; both CTAs meet at the hardware cluster barrier after initialisation and before TMEM
+// is freed, on every path.
+namespace {
+constexpr int kStagesPair = 4;
+constexpr int kTileBPair = 64 * 128;  // 64 rows x 64 BF16
+constexpr uint32_t kIdescPair = idesc_bf16_f32(256, kGramN);
+}  // namespace
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreadsGram, 1)
+    k_tc_gram2(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
+               const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
+               const int2* __restrict__ pairs, int n_pairs, int chunks_total, const int* __restrict__ dcol, int P,
+               int J, const double* __restrict__ Dinv, double* __restrict__ Psi, double* __restrict__ Gt, int n_d,
+               int n_base, double* __restrict__ V, int v_ld, int run, int* __restrict__ err, int group) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* A_hi = base;
+  unsigned char* A_lo = A_hi + kStagesPair * kTileA;
+  unsigned char* B_hi = A_lo + kStagesPair * kTileA;
+  unsigned char* B_lo = B_hi + kStagesPair * kTileBPair;
+  TcShared* sh = (TcShared*)(B_lo + kStagesPair * kTileBPair);
+  int2* spairs = (int2*)(sh + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  // tile order over super tiles (two pair tiles) x column tiles, as k_tc_gram's
+  const int tm2 = gridDim.x >> 1;
+  int stile = blockIdx.x >> 1, ntile = blockIdx.y;
+  if (group > 0) {
+    const int id = blockIdx.y * tm2 + stile;
+    const int per = group * gridDim.y, grp = id / per, first = grp * group;
+    const int gm = min(tm2 - first, group), r = id - grp * per;
+    stile = first + r % gm;
+    ntile = r / gm;
+  }
+  const int ptile = 2 * stile + (int)rank;
+  const int n0 = ntile * kGramN;
+  const int nb0 = n0 + 64 * (int)rank;  // this CTA's half of the B rows
+  const int nch = chunks_total;
+  const int nsb = (nch + run - 1) / run;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStagesPair; s++) {
+      mbar_init(&sh->full[s], 1);
+      mbar_init(&sh->empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&sh->accb[b], 1);
+      mbar_init(&sh->drained[b], 256);
+    }
+    mbar_init(&sh->fin, 1);
+    sh->abort = *(const volatile int*)err != 0;
+    fence_barrier_init();
+  }
+  for (int r = threadIdx.x; r < 128; r += kThreadsGram) {
+    const int p = ptile * 128 + r;
+    spairs[r] = p < n_pairs ? pairs[p] : make_int2(-1, -1);
+  }
+  if (warp == 0) {
+    tmem_alloc_pair(&sh->tmem, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // the even CTA's barriers exist before any signal from the odd CTA
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA: this CTA's pair products (128 pairs) and half of the weights (64 genes)
+      int issued = 0;
+      for (int it = 0; it < nch; it++) {
+        const int s = it % kStagesPair;
+        if (it >= kStagesPair && !mbar_wait(&sh->empty[s], ((it / kStagesPair) - 1) & 1, err)) {
+          tc_fail(err, sh, 21);
+          break;
+        }
+        if (sh->abort) break;
+        const uint32_t fb = mapa_shared(smem_u32(&sh->full[s]), 0);
+        if (rank == 0) mbar_arrive_expect_tx(&sh->full[s], 2u * (2u * kTileA + 2u * kTileBPair));
+        const int x = it * 64;
+        tma_load_2d_pair(A_hi + s * kTileA, &map_ahi, fb, x, ptile * 128);
+        tma_load_2d_pair(A_lo + s * kTileA, &map_alo, fb, x, ptile * 128);
+        tma_load_2d_pair(B_hi + s * kTileBPair, &map_bhi, fb, x, n_base + nb0);
+        tma_load_2d_pair(B_lo + s * kTileBPair, &map_blo, fb, x, n_base + nb0);
+        issued = it + 1;
+      }
+      // the even CTA sees both CTAs' last loads land before the final cluster barrier
+      if (rank == 0)
+        for (int it = max(0, issued - kStagesPair); it < issued; it++)
+          if (!mbar_wait(&sh->full[it % kStagesPair], (it / kStagesPair) & 1, nullptr)) atomicCAS(err, 0, 22);
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {  // MMA issuer (even CTA)
+      for (int it = 0; it < nch; it++) {
+        const int s = it % kStagesPair, sb = it / run, pos = it % run, buf = sb & 1;
+        if (pos == 0 && sb >= 2 && !mbar_wait(&sh->drained[buf], ((sb >> 1) - 1) & 1, err)) {
+          tc_fail(err, sh, 26);
+          break;
+        }
+        if (!mbar_wait(&sh->full[s], (it / kStagesPair) & 1, err)) {
+          tc_fail(err, sh, 23);
+          break;
+        }
+        if (sh->abort) break;
+        tc_fence_after();
+        const uint32_t acc = tmem + buf * kGramN;
+        const uint32_t ah = smem_u32(A_hi + s * kTileA), al = smem_u32(A_lo + s * kTileA);
+        const uint32_t bh = smem_u32(B_hi + s * kTileBPair), bl = smem_u32(B_lo + s * kTileBPair);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t off = k * 32;
+          mma_bf16_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), kIdescPair, (pos | k) ? 1u : 0u);
+          mma_bf16_pair(acc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), kIdescPair, 1u);
+          mma_bf16_pair(acc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), kIdescPair, 1u);
+        }
+        mma_commit_pair_mc(&sh->empty[s], 3);
+        if (pos == run - 1 || it == nch - 1) mma_commit_pair_mc(&sh->accb[buf], 3);
+      }
+      mma_commit_pair(&sh->fin);
+      if (!mbar_wait(&sh->fin, 0, nullptr)) atomicCAS(err, 0, 27);
+    }
+  } else {
+    // drain warps (both CTAs): FP32 runs -> FP64 sum, then this CTA's results
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
+    const uint32_t drained0 = mapa_shared(smem_u32(&sh->drained[0]), 0);
+    const uint32_t drained1 = mapa_shared(smem_u32(&sh->drained[1]), 0);
+    bool ok = true;
+    for (int sb = 0; sb < nsb; sb++) {
+      const int buf = sb & 1;
+      const bool w = mbar_wait(&sh->accb[buf], (sb >> 1) & 1, err);
+      if (!warp_all(w)) {
+        if (!w) tc_fail(err, sh, 25);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      drain_f32_to_f64(lane_addr, buf * kGramN, 256, kGramN, sb == 0);
+      tc_fence_before();
+      mbar_arrive_cluster(buf ? drained1 : drained0);
+    }
+    if (warp_all(ok && !aborted(sh) && *(const volatile int*)err == 0)) {
+      tc_fence_after();
+      const int2 ab = spairs[row];
+      const bool live = ab.x >= 0;
+      const size_t mk = live ? dcol[ab.x] : 0, ml = live ? dcol[ab.y] : 0;
+      const double dv = live ? Dinv[mk + ml * P] : 0.0;
+      for (int cb = 0; cb < kGramN; cb += 16) {
+        double v[16];
+        tmem_ld_f64x16(lane_addr + 256 + 2 * cb, v);  // warp-wide: every lane loads
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+          const int j = n0 + cb + k;
+          if (live && n_base + j < J) {
+            if (V) {
+              V[(size_t)j * v_ld + ptile * 128 + row] = v[k];
+            } else if (Gt) {
+              double* Gj = Gt + (size_t)j * n_d * n_d;
+              Gj[ab.x + (size_t)ab.y * n_d] = v[k];
+              Gj[ab.y + (size_t)ab.x * n_d] = v[k];
+            } else {
+              double* Pj = Psi + (size_t)j * P * P;
+              Pj[ml + mk * P] = v[k] + dv;
+              Pj[mk + ml * P] = v[k] + dv;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // both CTAs are done with TMEM and the even CTA saw every load land
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc_pair(tmem, 512);
+}
+
 // w = W/Omega as BF16 hi/lo, gene-major with the cell dimension padded to cpad (zeros)
 __global__ void k_split_weights(int N, int ldN, int J, int cpad, const double* __restrict__ W,
                                 const double* __restrict__ Omega, __nv_bfloat16* __restrict__ whi,
@@ -491,13 +683,17 @@ int tc_prepare(Ctx* c) {
   if (!make_map(&t.map_shi, t.shi, t.Jpad, prow, 128) || !make_map(&t.map_slo, t.slo, t.Jpad, prow, 128) ||
       !make_map(&t.map_ohi, t.ohi, t.Jpad, t.cpad, 128) || !make_map(&t.map_olo, t.olo, t.Jpad, t.cpad, 128) ||
       !make_map(&t.map_ahi, t.ahi, t.cpad, prow, 128) || !make_map(&t.map_alo, t.alo, t.cpad, prow, 128) ||
-      !make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN)) {
+      !make_map(&t.map_whi, t.whi, t.cpad, J, kGramN) || !make_map(&t.map_wlo, t.wlo, t.cpad, J, kGramN) ||
+      !make_map(&t.map_whi64, t.whi, t.cpad, J, 64) || !make_map(&t.map_wlo64, t.wlo, t.cpad, J, 64) ||
+      !make_map(&t.map_ohi64, t.ohi, t.Jpad, t.cpad, 64) || !make_map(&t.map_olo64, t.olo, t.Jpad, t.cpad, 64)) {
     c->err = "cuTensorMapEncodeTiled failed";
     return GPL_ERR_CUDA;
   }
   t.run = c->tc_run > 0 ? c->tc_run : kSBGram;
   t.smem_gram = 1024 + kStagesGram * (2 * kTileA + 2 * kTileBG) + (int)sizeof(TcShared) + 128 * (int)sizeof(int2);
   GPL_TRY(c, cudaFuncSetAttribute(k_tc_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_gram));
+  t.smem_gram2 = 1024 + kStagesPair * (2 * kTileA + 2 * kTileBPair) + (int)sizeof(TcShared) + 128 * (int)sizeof(int2);
+  GPL_TRY(c, cudaFuncSetAttribute(k_tc_gram2, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_gram2));
   t.ready = true;
   return GPL_OK;
 }
@@ -595,11 +791,20 @@ int launch_tc_gram(Ctx* c) {
     Tunable* tu = nullptr;
     const int grp = tune_pick(c, "tc_gram", {0, 8, 16}, 8, &tu);
     TuneScope ts(c, tu);
-    k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
-                                                           t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
-                                                           c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.run, t.err,
-                                                           grp);
-    GPL_LAUNCHED(c, "k_tc_gram");
+    if (c->tc_pair) {
+      dim3 g2(2 * div_up(t.pair_tiles, 2), t.gram_tiles_n);
+      k_tc_gram2<<<g2, kThreadsGram, t.smem_gram2, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi64, t.map_wlo64,
+                                                                t.pairs, t.n_pairs, t.chunks_cells, c->dcol_d, c->P,
+                                                                c->J, c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr,
+                                                                0, t.run, t.err, grp);
+      GPL_LAUNCHED(c, "k_tc_gram2");
+    } else {
+      k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_ahi, t.map_alo, t.map_whi, t.map_wlo, t.pairs,
+                                                             t.n_pairs, t.chunks_cells, c->dcol_d, c->P, c->J,
+                                                             c->DeltaInv, c->Psi, t.Gt, c->n_d, 0, nullptr, 0, t.run,
+                                                             t.err, grp);
+      GPL_LAUNCHED(c, "k_tc_gram");
+    }
   }
   {
     ProfScope ps(c, "unwhiten");
@@ -636,11 +841,20 @@ int launch_tc_grad(Ctx* c) {
       Tunable* tu = nullptr;
       const int grp = tune_pick(c, "tc_grad", {0, 8, 16}, 8, &tu);
       TuneScope ts(c, c1 - c0 == c->N ? tu : nullptr);
-      k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
-                                                             t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
-                                                             c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
-                                                             s.pairs_pad, t.run, t.err, grp);
-      GPL_LAUNCHED(c, "k_tc_gram(gradient pairs)");
+      if (c->tc_pair) {
+        dim3 g2(2 * div_up(t.pair_tiles, 2), div_up(c1 - c0, kGramN));
+        k_tc_gram2<<<g2, kThreadsGram, t.smem_gram2, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi64, t.map_olo64,
+                                                                  t.pairs, t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
+                                                                  c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
+                                                                  s.pairs_pad, t.run, t.err, grp);
+        GPL_LAUNCHED(c, "k_tc_gram2(gradient pairs)");
+      } else {
+        k_tc_gram<<<g, kThreadsGram, t.smem_gram, c->stream>>>(t.map_shi, t.map_slo, t.map_ohi, t.map_olo, t.pairs,
+                                                               t.n_pairs, t.Jpad / 64, c->dcol_d, c->P, c1,
+                                                               c->DeltaInv, nullptr, nullptr, c->n_d, c0, s.V,
+                                                               s.pairs_pad, t.run, t.err, grp);
+        GPL_LAUNCHED(c, "k_tc_gram(gradient pairs)");
+      }
     }
     if ((rc = launch_v_to_u_cells(c, c0, c1, t.DwC))) return rc;
   }

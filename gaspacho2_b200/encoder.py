@@ -258,19 +258,24 @@ def amortised_placement(config: int, n_train: int, n_test: int, fit_lbfgs: int, 
         out["refine_seconds"] = time.time() - t0
         X_zero, l_zero, st_zero = place_cells(jm, np.zeros_like(X_enc), iters)
         l_true = cell_objective(jm, test.X_true)
-    rel = lambda a: (l_ref - a) / np.abs(l_ref)  # noqa: E731
+    # gaps over the cells whose objectives are finite at every point compared (the count of the
+    # others is reported)
+    ok = np.isfinite(l_ref) & np.isfinite(l_enc) & np.isfinite(l_zero)
+    out["non_finite_cells"] = int(np.sum(~ok))
+    rel = lambda a: (l_ref[ok] - a[ok]) / np.abs(l_ref[ok])  # noqa: E731
     g_enc, g_zero = rel(l_enc), rel(l_zero)
-    out["elbo_gap_encoder"] = {"median": float(np.median(g_enc)), "mean": float(np.mean(g_enc)),
-                               "p95": float(np.quantile(g_enc, 0.95))}
-    out["elbo_gap_without_encoder"] = {"median": float(np.median(g_zero)), "mean": float(np.mean(g_zero)),
-                                       "p95": float(np.quantile(g_zero, 0.95)),
-                                       "note": f"{iters} per-cell L-BFGS steps from X = 0"}
-    out["cells_refined_above_start_from_zero"] = float(np.mean(l_ref > l_zero))
+    stat = lambda g: {"median": float(np.median(g)), "mean": float(np.mean(g)),  # noqa: E731
+                      "p95": float(np.quantile(g, 0.95))} if g.size else {"median": None, "mean": None, "p95": None}
+    out["elbo_gap_encoder"] = stat(g_enc)
+    out["elbo_gap_without_encoder"] = {**stat(g_zero), "note": f"{iters} per-cell L-BFGS steps from X = 0"}
+    out["cells_refined_above_start_from_zero"] = float(np.mean(l_ref[ok] > l_zero[ok])) if ok.any() else None
     out["procrustes_rmse"] = {"encoder_vs_judge": procrustes_rmse(X_enc, X_ref),
                               "encoder_vs_truth": procrustes_rmse(X_enc, test.X_true),
                               "judge_vs_truth": procrustes_rmse(X_ref, test.X_true),
                               "without_encoder_vs_truth": procrustes_rmse(X_zero, test.X_true)}
-    out["objective_at_true_X_gap_median"] = float(np.median(rel(l_true)))
+    ok_t = ok & np.isfinite(l_true)
+    out["objective_at_true_X_gap_median"] = (float(np.median((l_ref[ok_t] - l_true[ok_t]) / np.abs(l_ref[ok_t])))
+                                             if ok_t.any() else None)
     out["placement_stats"] = {"refine": st_ref, "from_zero": st_zero}
     return out
 

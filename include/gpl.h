@@ -74,6 +74,12 @@ GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
  *                       into the FP64 sum (1..64, default 4)
  *   "tc_check"          read the tensor-core kernels' error flag after each of their launches
  *                       (1) or only when a result is read back (0, default)
+ *   "tc_pair"           precision form: the two tensor-core contractions on CTA pairs (one
+ *                       M = 256 MMA over two CTAs, each loading half of B) (1) or one CTA per
+ *                       tile (0, default); the same sums in the same order
+ *   "eta_tc"            the linear predictor z_i . beta_j of every cell and gene (W / nu, the
+ *                       gradient's predictions, the refinement) on the FP64 tensor cores (1,
+ *                       default) or as an FFMA tile GEMM (0); the two differ by rounding
  *   "pair_range_cells"  cells per range of the FP64 pair GEMMs (0, default: as many as 8 GiB
  *                       of pair products holds; smaller values exercise the multi-range path)
  *   "graph"             1: each objective evaluation and each gradient after it (in gpl_fit,
@@ -89,8 +95,9 @@ GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
  *                       by decreasing count (FP64 path, P <= 288; else the separate kernels).
  *                       Same results bit for bit. Default 0.
  *   "tail_ctas_per_sm"  CTAs per SM of that launch (1 or 2, default 2)
- *   "autotune"          1: the tile orders of the FP64 pair GEMMs and the CTAs per SM of the
- *                       fused tail are chosen by timing each candidate on the context's own
+ *   "autotune"          1: the tile orders of the FP64 pair GEMMs and of the tensor-core
+ *                       contractions and the CTAs per SM of the fused tail are chosen by timing
+ *                       each candidate on the context's own
  *                       launches (every candidate gives the same bits); the choices are kept for
  *                       the process per problem shape. Graphs are captured once all are chosen.
  *                       Default 0. */

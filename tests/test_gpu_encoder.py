@@ -147,6 +147,7 @@ def test_amortised_placement_experiment_runs_end_to_end():
     assert all(np.isfinite(r) for _, r in out["validation_rmse"])
     print({k: out[k] for k in ("elbo_gap_encoder", "elbo_gap_without_encoder", "cells_refined_above_start_from_zero",
                                "epochs_chosen", "clamped_fraction")})
+    assert out["non_finite_cells"] <= 464 // 20, "non-finite objectives at more than 5% of the held-out cells"
     for k in ("elbo_gap_encoder", "elbo_gap_without_encoder"):
         assert np.isfinite(out[k]["median"]), k
     assert 0.0 <= out["clamped_fraction"] <= 1.0

@@ -263,7 +263,9 @@ def test_wide_design_against_oracle():
 
     from gaspacho2_b200 import synth
 
-    ds = synth.make(2, 13, N=640, G=6, M=232, Q=4)
+    # 1,700 cells: the 400 batch x donor groups are few enough (<= N/4 + 1) to be handled by group
+    # sums, which leaves 1 + 3 + 232 dense columns
+    ds = synth.make(2, 13, N=1700, G=6, M=232, Q=4)
     T = 2.0 * np.random.default_rng(3).standard_normal((232, 4))
     ds = dataclasses.replace(ds, init=dataclasses.replace(ds.init, T=T))
     ref, sens = _sensitivity(ds)

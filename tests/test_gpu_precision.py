@@ -67,3 +67,35 @@ def test_precision_form_against_fp64(cfg, kw):
         if cfg != 0 and not e <= tol:
             bad.append(f"{name}: {e:.2e}")
     assert not bad, bad
+
+
+def _evaluate_opts(ds, opts):
+    with GPLVM.from_dataset(ds, precision="fp64") as m:
+        for k, v in opts.items():
+            m.set_option(k, v)
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        for j in range(3):
+            m.irls_sweep(0, j)
+        m.objective_after_irls(0)
+        m.set_precision("bf16x3")
+        v, g = m.evaluate(m.params_vector())
+        return v, g.copy()
+
+
+@pytest.mark.parametrize("cfg,kw", [(1, dict(N=6000, G=300)), (2, dict(N=6000, G=200, M=64, Q=5))])
+def test_cta_pair_contractions(cfg, kw):
+    """Option tc_pair (the Gram and the gradient contraction on CTA pairs: one M = 256
+    tcgen05.mma.cta_group::2 per K step over two CTAs' shared memory) against the single-CTA
+    kernel: the same products in the same K order per output, so the objective within 1e-12 and
+    the gradient within 1e-9 (relative). Both cases have 68 dense columns, 2,346 pairs in 19 tiles:
+    the odd CTA of the last pair has no pairs (its A rows lie past the matrix and load as zeros)."""
+    ds = synth.make(cfg, 6, init=True, **kw)
+    v0, g0 = _evaluate_opts(ds, {})
+    v1, g1 = _evaluate_opts(ds, {"tc_pair": 1})
+    rel = abs(v1 - v0) / abs(v0)
+    gr = np.linalg.norm(g1 - g0) / np.linalg.norm(g0)
+    print(f"config {cfg}: objective {rel:.2e}, gradient {gr:.2e}, bitwise {v1 == v0 and np.array_equal(g1, g0)}")
+    assert rel <= 1e-12
+    assert gr <= 1e-9
