@@ -332,6 +332,8 @@ static int gradient_run(Ctx* c) {
 // backtracking line search (rhoflag once itr > 20; a 10000-step limit on itr 30), and the
 // beta revival. lbfgs_budget > 0 caps the L-BFGS steps of this call. st = IRLS sweeps,
 // L-BFGS steps, objective evaluations, trace entries written.
+constexpr int kMaxRestarts = 8;  // line-search restarts per outer iteration (option ls_restart)
+
 static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* trace, int trace_cap) {
   int JTRMAX = (itr == 0) ? 200 : 100;
   int n = 0, ntrace = 0;
@@ -344,9 +346,14 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
   if (trace && ntrace < trace_cap) trace[ntrace++] = l0;
   const int rhoflag = itr > 20 ? 1 : 0;
   if (itr == 30) JTRMAX = 10000;
+  // option ls_restart (precision form only): after a line search whose seven tries all failed,
+  // go back to the step's start and restart the L-BFGS history there (base: the step that the
+  // history counts from) instead of accepting the last try and meeting the stop test
+  int base = 0, restarts = 0;
+  const bool restart_ok = c->ls_restart && c->precision == GPL_PREC_BF16X3;
   for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
     GPL_RUN(gradient_run(c));  // the last objective (after the IRLS or the accepted step) is here
-    GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
+    GPL_RUN(launch_lbfgs_update(c, jtr - base, rhoflag));
     double sr = 1.0;
     std::vector<double>& l = c->lkhd;
     for (int ktr = 1; ktr < 8; ktr++) {
@@ -356,9 +363,20 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
       if (l[jtr + 1] > l[jtr] || ktr == 7) break;
       else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
       else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
-      GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
+      GPL_RUN(launch_downdate(c, jtr - base, sr, rhoflag));
     }
     st[1]++;
+    if (restart_ok && !(l[jtr + 1] > l[jtr]) && restarts < kMaxRestarts) {
+      GPL_RUN(launch_downdate(c, jtr - base, 0.0, rhoflag));  // the step's start
+      GPL_RUN(objective_run(c, jtr + 1));
+      GPL_RUN(read_slot(c, jtr + 1, nullptr));
+      st[2]++;
+      base = jtr + 1;
+      restarts++;
+      if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
+      if (lbfgs_budget > 0 && st[1] >= lbfgs_budget) break;
+      continue;
+    }
     if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
     if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
     if (lbfgs_budget > 0 && st[1] >= lbfgs_budget) break;
@@ -645,6 +663,8 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
     c->tc_check = value != 0;
   } else if (s == "tc_pair") {
     c->tc_pair = value != 0;
+  } else if (s == "ls_restart") {
+    c->ls_restart = value != 0;
   } else if (s == "autotune") {
     c->autotune = value != 0;
   } else if (s == "fused_tail") {
@@ -680,6 +700,7 @@ int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
   else if (s == "tc_run") *value = c->tc_run;
   else if (s == "tc_check") *value = c->tc_check ? 1 : 0;
   else if (s == "tc_pair") *value = c->tc_pair ? 1 : 0;
+  else if (s == "ls_restart") *value = c->ls_restart ? 1 : 0;
   else if (s == "pair_range_cells") *value = c->pair_range_cells;
   else if (s == "graph") *value = c->use_graph ? 1 : 0;
   else if (s == "fused_tail") *value = c->fused_tail ? 1 : 0;

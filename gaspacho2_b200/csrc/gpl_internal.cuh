@@ -120,6 +120,7 @@ struct Ctx {
   bool tc_check = false;      // read the tensor-core error flag after every tensor-core launch
   int tc_run = 4;             // precision form: K chunks per FP32 accumulator run before the FP64 fold
   bool tc_pair = false;       // precision form: the tensor-core contractions on CTA pairs (k_tc_gram2)
+  bool ls_restart = false;    // precision form: restart the L-BFGS history after a failed line search
   int64_t pair_range_cells = 0;  // cells per range of the pair GEMMs (0: as many as 8 GiB holds)
   // CUDA graphs of one objective evaluation and of the gradient that follows it (option
   // "graph"): captured on first use, replayed after; dropped whenever a buffer they captured
