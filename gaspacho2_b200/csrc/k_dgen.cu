@@ -245,44 +245,28 @@ struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) o
   }
   __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
-// HK's tiles: grid z = tile * split + the gene range of a split-K launch
 struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the tile list
   static constexpr bool kFastK = false;
   const double* tab;
   const int2* tiles;
-  int n_grp, ld, split;
+  int n_grp, ld;
   __device__ double operator()(int r, int k, int z) const {
-    return tab[((size_t)k * n_grp + tiles[z / split].x) * ld + r];
+    return tab[((size_t)k * n_grp + tiles[z].x) * ld + r];
   }
 };
 struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell, group order
   static constexpr bool kFastK = false;
   const double *Wg, *rOmg;
   const int* pos;  // 128 slots per tile, positions in group order (-1 past the group)
-  int ldN, split;
+  int ldN;
   struct Raw {
     double w, r;
   };
   __device__ Raw load(int k, int c, int z) const {
-    const int q = pos[(size_t)(z / split) * 128 + c];
+    const int q = pos[(size_t)z * 128 + c];
     return q < 0 ? Raw{0.0, 0.0} : Raw{Wg[(size_t)k * ldN + q], rOmg[q]};
   }
   __device__ double finish(const Raw& v) const { return v.w * v.r; }
-};
-struct KSplitZ {  // gene range z % split of equal ranges of [0, K)
-  int K, per, split;
-  __device__ int2 operator()(int z) const {
-    const int q = z % split;
-    return make_int2(min(K, q * per), min(K, (q + 1) * per));
-  }
-};
-struct EpHKPart {  // partial[(q * tiles + t) * 128 * ld + c * ld + a] for z = t * split + q
-  double* part;
-  int ld, split, tiles;
-  __device__ void operator()(int a, int c, int z, double v) const {
-    const int t = z / split, q = z - t * split;
-    part[(((size_t)q * tiles + t) * 128 + c) * ld + a] = v;
-  }
 };
 
 // ---- epilogues -------------------------------------------------------------------------------
@@ -562,22 +546,6 @@ int dgen_group_sums(Ctx* c, int mode) {
                         EpGroup{c->gsum, c->n_grp, c->n_d + 1}, "k_dgen(group_sums)");
 }
 
-// HK[i, a] = sum_q partial_q over the gene ranges, in order, scattered to the tile's cells
-__global__ void k_reduce_hk(int tiles, int ld, int split, int ldN, const int* __restrict__ cells,
-                            const double* __restrict__ part, double* __restrict__ HK) {
-  const int t = blockIdx.x, c = threadIdx.x;  // 128 threads: the tile's cell slots
-  const int i = cells[(size_t)t * 128 + c];
-  if (i < 0) return;
-  for (int a = 0; a < ld; a++) {
-    double s = 0.0;
-    for (int q = 0; q < split; q++) s += part[(((size_t)q * tiles + t) * 128 + c) * ld + a];
-    HK[i + (size_t)a * ldN] = s;
-  }
-}
-
-// HK over its 128-cell group tiles, split over 1..4 gene ranges (the count whose CTAs fill their
-// last wave best: 2 at config 2, about 1,600 CTAs in 10.8 waves against 5.4) whose partials are
-// added in order.
 int dgen_hk(Ctx* c) {
   using T = TileTall;
   const int ld = c->n_d + 1;
@@ -586,32 +554,10 @@ int dgen_hk(Ctx* c) {
   int rc = recip_omega(c, &rOm);
   if (rc) return rc;
   if ((rc = launch_group_order(c, rOm, 1, c->rOmg))) return rc;
-  const int tiles = c->n_hk_tiles128;
-  int S = 1;
-  double best = 0.0;
-  for (int z = 1; z <= 4; z++) {
-    const double waves = (double)tiles * z / c->sm_count, fill = waves / std::ceil(waves);
-    if (fill > best + 1e-9) {
-      best = fill;
-      S = z;
-    }
-  }
-  if ((int64_t)tiles * S > 65535) S = 1;
-  if (S == 1) {
-    dim3 g(1, 1, tiles);
-    return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld, 1},
-                          LdTileO{c->Wg, c->rOmg, c->hk_pos_d, c->ldN, 1}, KAll{c->J},
-                          EpHK{c->HK, c->hk_cells_d, c->ldN}, "k_dgen(hk)");
-  }
-  if ((rc = ensure_part(c, (size_t)S * tiles * 128 * ld))) return rc;
-  dim3 g(1, 1, tiles * S);
-  rc = launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld, S},
-                      LdTileO{c->Wg, c->rOmg, c->hk_pos_d, c->ldN, S}, KSplitZ{c->J, (c->J + S - 1) / S, S},
-                      EpHKPart{c->part, ld, S, tiles}, "k_dgen(hk)");
-  if (rc) return rc;
-  k_reduce_hk<<<tiles, 128, 0, c->stream>>>(tiles, ld, S, c->ldN, c->hk_cells_d, c->part, c->HK);
-  GPL_LAUNCHED(c, "k_reduce_hk");
-  return GPL_OK;
+  dim3 g(1, 1, c->n_hk_tiles128);
+  return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
+                        LdTileO{c->Wg, c->rOmg, c->hk_pos_d, c->ldN}, KAll{c->J}, EpHK{c->HK, c->hk_cells_d, c->ldN},
+                        "k_dgen(hk)");
 }
 
 // Psi_DD,j = L G~_j L^T + DeltaInv_DD for every gene: T_j = G~_j L^T as one GEMM over the stacked
