@@ -41,7 +41,7 @@ PHASES = ("gram", "uq", "spair", "v_to_u", "whiten", "unwhiten", "split_weights"
           "inverse", "zt_u", "zbeta", "c1_tn", "kernel_mats", "kinvkmn", "lkhd_genes", "solve", "grad_delta", "c2",
           "grad_tau_rho", "tn_sum", "grad_omega_cell", "oinvt", "collect", "expand_delta", "chol_small", "group_sums",
           "assemble_psi", "assemble_b", "group_tables", "hk", "group_t", "refine", "unwhiten_u", "irls_tail",
-          "beta_phi", "lkhd_pois", "w_nu")
+          "beta_phi", "lkhd_pois", "w_nu", "logdet_probe")
 
 
 def parse():
@@ -892,7 +892,7 @@ def fit_trace(args):
             e.record(stream)
             torch.cuda.synchronize()
             print(json.dumps({"mode": "fit_trace", "config": args.fit_config, "precision": prec,
-                              "options": args.option,
+                              "options": args.option, "ls_fp64_steps": m.get_option("ls_fp64_steps"),
                               "lbfgs_budget": args.fit_lbfgs, "seconds": s.elapsed_time(e) / 1e3,
                               "wall_seconds": time.time() - t0, "final_objective": outer[-1]["last"] if outer else None,
                               "outer": outer}), flush=True)

@@ -332,7 +332,45 @@ static int gradient_run(Ctx* c) {
 // backtracking line search (rhoflag once itr > 20; a 10000-step limit on itr 30), and the
 // beta revival. lbfgs_budget > 0 caps the L-BFGS steps of this call. st = IRLS sweeps,
 // L-BFGS steps, objective evaluations, trace entries written.
-constexpr int kMaxRestarts = 8;  // line-search restarts per outer iteration (option ls_restart)
+// The FP64 repeat of a precision-form line search that failed (option ls_fp64): back to the step's
+// start, the FP64 objective there, the same backtracking rules against it, then the precision
+// form's objective at the accepted point into slot jtr + 1 (the next step's comparison and the
+// gradient's state). *evals = the objective evaluations made, negative if the FP64 search found
+// no rise either.
+static int ls_fp64_retry(Ctx* c, int jtr, int rhoflag, int* evals) {
+  std::vector<double>& l = c->lkhd;
+  int n = 0;
+  c->precision = GPL_PREC_FP64;
+  graph_reset(c);
+  GPL_RUN(launch_downdate(c, jtr, 0.0, rhoflag));  // the step's start
+  GPL_RUN(objective_run(c, jtr + 1));
+  GPL_RUN(read_slot(c, jtr + 1, nullptr));
+  n++;
+  const double l0 = l[jtr + 1];
+  double sr = 1.0;
+  bool rose = false;
+  for (int ktr = 1; ktr < 8; ktr++) {
+    GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
+    GPL_RUN(objective_run(c, jtr + 1));
+    GPL_RUN(read_slot(c, jtr + 1, nullptr));
+    n++;
+    if (l[jtr + 1] > l0) {
+      rose = true;
+      break;
+    }
+    if (ktr == 7) break;
+    if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
+    else sr *= 0.1;
+  }
+  c->precision = GPL_PREC_BF16X3;
+  graph_reset(c);
+  GPL_RUN(objective_run(c, jtr + 1));
+  GPL_RUN(read_slot(c, jtr + 1, nullptr));
+  n++;
+  c->ls_fp64_steps++;
+  *evals = rose ? n : -n;
+  return GPL_OK;
+}
 
 static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* trace, int trace_cap) {
   int JTRMAX = (itr == 0) ? 200 : 100;
@@ -346,14 +384,14 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
   if (trace && ntrace < trace_cap) trace[ntrace++] = l0;
   const int rhoflag = itr > 20 ? 1 : 0;
   if (itr == 30) JTRMAX = 10000;
-  // option ls_restart (precision form only): after a line search whose seven tries all failed,
-  // go back to the step's start and restart the L-BFGS history there (base: the step that the
-  // history counts from) instead of accepting the last try and meeting the stop test
-  int base = 0, restarts = 0;
-  const bool restart_ok = c->ls_restart && c->precision == GPL_PREC_BF16X3;
+  // option ls_fp64 (precision form only): a line search whose seven tries all fail is repeated
+  // with the FP64 objective (the tensor-core Gram resolves parameter changes only to about 2^-16
+  // relative, so a short step's gain can be invisible to it); the fit then goes on in the
+  // precision form from the point the FP64 search accepted
+  const bool fp64_retry = c->ls_fp64 && c->precision == GPL_PREC_BF16X3;
   for (int jtr = 0; jtr < JTRMAX && jtr + 1 < kLkhdSlots; jtr++) {
     GPL_RUN(gradient_run(c));  // the last objective (after the IRLS or the accepted step) is here
-    GPL_RUN(launch_lbfgs_update(c, jtr - base, rhoflag));
+    GPL_RUN(launch_lbfgs_update(c, jtr, rhoflag));
     double sr = 1.0;
     std::vector<double>& l = c->lkhd;
     for (int ktr = 1; ktr < 8; ktr++) {
@@ -363,22 +401,22 @@ static int fit_outer(Ctx* c, int itr, int lbfgs_budget, int32_t* st, double* tra
       if (l[jtr + 1] > l[jtr] || ktr == 7) break;
       else if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
       else if (l[jtr + 1] < l[jtr]) sr *= 0.1;
-      GPL_RUN(launch_downdate(c, jtr - base, sr, rhoflag));
+      GPL_RUN(launch_downdate(c, jtr, sr, rhoflag));
     }
     st[1]++;
-    if (restart_ok && !(l[jtr + 1] > l[jtr]) && restarts < kMaxRestarts) {
-      GPL_RUN(launch_downdate(c, jtr - base, 0.0, rhoflag));  // the step's start
-      GPL_RUN(objective_run(c, jtr + 1));
-      GPL_RUN(read_slot(c, jtr + 1, nullptr));
-      st[2]++;
-      base = jtr + 1;
-      restarts++;
-      if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
-      if (lbfgs_budget > 0 && st[1] >= lbfgs_budget) break;
-      continue;
+    bool retried = false;
+    if (fp64_retry && !(l[jtr + 1] > l[jtr])) {
+      int rs = 0;
+      GPL_RUN(ls_fp64_retry(c, jtr, rhoflag, &rs));
+      st[2] += rs > 0 ? rs : -rs;
+      retried = rs > 0;  // the FP64 search found a rise
+      if (!retried) {    // it did not either: the reference's stop
+        if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
+        break;
+      }
     }
     if (trace && ntrace < trace_cap) trace[ntrace++] = l[jtr + 1];
-    if (jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
+    if (!retried && jtr > 0 && fabs(l[jtr + 1] - l[jtr]) < fabs(l[jtr + 1]) * 1e-8) break;
     if (lbfgs_budget > 0 && st[1] >= lbfgs_budget) break;
   }
   GPL_RUN(launch_expand_delta(c));
@@ -663,8 +701,10 @@ int gpl_set_option(gpl_ctx* h, const char* name, int64_t value) {
     c->tc_check = value != 0;
   } else if (s == "tc_pair") {
     c->tc_pair = value != 0;
-  } else if (s == "ls_restart") {
-    c->ls_restart = value != 0;
+  } else if (s == "ls_fp64") {
+    c->ls_fp64 = value != 0;
+  } else if (s == "logdet_probe") {
+    c->logdet_probe = value != 0;
   } else if (s == "autotune") {
     c->autotune = value != 0;
   } else if (s == "fused_tail") {
@@ -700,7 +740,9 @@ int gpl_get_option(const gpl_ctx* h, const char* name, int64_t* value) {
   else if (s == "tc_run") *value = c->tc_run;
   else if (s == "tc_check") *value = c->tc_check ? 1 : 0;
   else if (s == "tc_pair") *value = c->tc_pair ? 1 : 0;
-  else if (s == "ls_restart") *value = c->ls_restart ? 1 : 0;
+  else if (s == "ls_fp64") *value = c->ls_fp64 ? 1 : 0;
+  else if (s == "ls_fp64_steps") *value = c->ls_fp64_steps;
+  else if (s == "logdet_probe") *value = c->logdet_probe ? 1 : 0;
   else if (s == "pair_range_cells") *value = c->pair_range_cells;
   else if (s == "graph") *value = c->use_graph ? 1 : 0;
   else if (s == "fused_tail") *value = c->fused_tail ? 1 : 0;

@@ -77,6 +77,7 @@ struct TcState {
   int* err = nullptr;
   CUtensorMap map_whi, map_wlo, map_ahi, map_alo, map_shi, map_slo, map_ohi, map_olo;
   CUtensorMap map_whi64, map_wlo64, map_ohi64, map_olo64;  // 64-row boxes: the CTA-pair kernel's B halves
+  double* probe = nullptr;  // P x J fixed Rademacher probes of the log-determinant correction
 };
 
 // One open or settled choice of the autotuner (tune.cu): candidate values, each one's best
@@ -120,7 +121,9 @@ struct Ctx {
   bool tc_check = false;      // read the tensor-core error flag after every tensor-core launch
   int tc_run = 4;             // precision form: K chunks per FP32 accumulator run before the FP64 fold
   bool tc_pair = false;       // precision form: the tensor-core contractions on CTA pairs (k_tc_gram2)
-  bool ls_restart = false;    // precision form: restart the L-BFGS history after a failed line search
+  bool ls_fp64 = false;       // precision form: repeat a failed line search with the FP64 objective
+  int64_t ls_fp64_steps = 0;  // steps so repeated
+  bool logdet_probe = true;   // precision form: the probe correction of log det Psi (k_lkhd.cu)
   int64_t pair_range_cells = 0;  // cells per range of the pair GEMMs (0: as many as 8 GiB holds)
   // CUDA graphs of one objective evaluation and of the gradient that follows it (option
   // "graph"): captured on first use, replayed after; dropped whenever a buffer they captured

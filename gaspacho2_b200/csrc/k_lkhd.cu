@@ -257,15 +257,88 @@ __global__ void __launch_bounds__(256) k_lkhd_genes(int N, int ldN, int P, const
     lkhds[j] = -((double)N) / 2.0 * log(phij) - sa / 2.0 + sld - sq / 2.0 / phij + sbx / 2.0 / phij;
 }
 
+// y_j = bx_j + DeltaInv v_j (DeltaInv as its factor L once cholDeltaInv has run: L (L^T v)), one
+// CTA per gene: the FP64 operator Psi_j applied to the probe v_j, with bx = Z^T diag(W/Omega) Z v.
+__global__ void __launch_bounds__(256) k_probe_apply(int P, const double* __restrict__ bx,
+                                                     const double* __restrict__ Dinv, int factored,
+                                                     const double* __restrict__ v, double* __restrict__ y) {
+  extern __shared__ double vs[];  // v_j, then L^T v_j
+  const int j = blockIdx.x;
+  const double* vj = v + (size_t)j * P;
+  double* ts = vs + P;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) vs[k] = vj[k];
+  __syncthreads();
+  if (factored) {
+    for (int k = threadIdx.x; k < P; k += blockDim.x) {
+      double t = 0.0;
+      for (int l = k; l < P; l++) t = fma(Dinv[l + (size_t)k * P], vs[l], t);
+      ts[k] = t;
+    }
+    __syncthreads();
+  }
+  for (int k = threadIdx.x; k < P; k += blockDim.x) {
+    double s = 0.0;
+    if (factored)
+      for (int l = 0; l <= k; l++) s = fma(Dinv[k + (size_t)l * P], ts[l], s);
+    else
+      for (int l = 0; l < P; l++) s = fma(Dinv[k <= l ? k + (size_t)l * P : l + (size_t)k * P], vs[l], s);
+    const size_t e = (size_t)j * P + k;
+    y[e] = bx[e] + s;
+  }
+}
+
+// lkhds_j -= (v_j . z_j - P) / 2 with z_j = Psi~_j^{-1} Psi_j v_j: the log-determinant correction.
+__global__ void __launch_bounds__(256) k_probe_logdet(int P, const double* __restrict__ v,
+                                                      const double* __restrict__ z, double* __restrict__ lkhds) {
+  __shared__ double sh[32];
+  const int j = blockIdx.x;
+  double s = 0.0;
+  for (int k = threadIdx.x; k < P; k += blockDim.x) s += v[(size_t)j * P + k] * z[(size_t)j * P + k];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) lkhds[j] -= 0.5 * (s - (double)P);
+}
+
+// The precision form's log det Psi_j as a smooth function of the parameters. The tensor-core Gram
+// is a staircase in them (its BF16 hi/lo operands hold 16 significant bits, so a parameter change
+// below about 2^-16 relative leaves it unchanged), and so is log det Psi~_j: an L-BFGS step too short
+// to move it sees an objective whose log-determinant part is frozen while its gradient is not. With
+// a fixed Rademacher probe v_j (v_j . v_j = P),
+//     log det Psi~_j + v_j^T Psi~_j^{-1} Psi_j v_j - P
+// equals log det Psi_j up to second order in Psi_j - Psi~_j (the expression is stationary at
+// Psi~_j = Psi_j) and moves with Psi_j, which the FP64 operator applies exactly (the refinement's
+// Z x and Z^T diag(W/Omega) E passes); the probe's own error is of the size of
+// |Psi~_j^{-1} (Psi_j - Psi~_j)|_F.
+static int probe_logdet(Ctx* c) {
+  TcState& t = c->tc;
+  if (!t.probe) {
+    c->err = "the log-determinant probe is allocated with the tensor-core buffers";
+    return GPL_ERR_STATE;
+  }
+  ProfScope ps(c, "logdet_probe");
+  const int64_t PP = (int64_t)c->P * c->P;
+  int rc;
+  if ((rc = launch_zbeta(c, t.probe, c->scratch))) return rc;            // Z v
+  if ((rc = launch_zt_u_ex(c, 0, c->scratch, c->bx))) return rc;        // Z^T diag(W/Omega) Z v
+  k_probe_apply<<<c->J, 256, 2 * sizeof(double) * c->P, c->stream>>>(c->P, c->bx, c->DeltaInv, 1, t.probe, c->rres);
+  GPL_LAUNCHED(c, "k_probe_apply");
+  if ((rc = launch_solve_batched(c, c->Psi, c->P, PP, c->rres, c->P, c->bx, c->P, c->J))) return rc;
+  k_probe_logdet<<<c->J, 256, 0, c->stream>>>(c->P, t.probe, c->bx, c->lkhds);
+  GPL_LAUNCHED(c, "k_probe_logdet");
+  return GPL_OK;
+}
+
 int launch_lkhd_genes(Ctx* c) {
   // b^T Psi^{-1} b enters as the difference q - b^T x of two large sums: in the precision form
   // x is refined against the FP64 operator (a 1e-6 error in x would survive the cancellation)
   int rc = solve_refined(c, c->bvec, c->sol, true);  // cholDeltaInv has run (ggplvm.cu:1206,1266)
   if (rc) return rc;
-  ProfScope ps(c, "lkhd_genes");
-  k_lkhd_genes<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->W, c->Nu, c->Omega, c->Psi, c->DeltaInv, c->bvec,
-                                            c->sol, c->phi, c->lkhds);
-  GPL_LAUNCHED(c, "k_lkhd_genes");
+  {
+    ProfScope ps(c, "lkhd_genes");
+    k_lkhd_genes<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->P, c->W, c->Nu, c->Omega, c->Psi, c->DeltaInv,
+                                              c->bvec, c->sol, c->phi, c->lkhds);
+    GPL_LAUNCHED(c, "k_lkhd_genes");
+  }
+  if (c->precision == GPL_PREC_BF16X3 && c->logdet_probe) return probe_logdet(c);
   return GPL_OK;
 }
 

@@ -39,6 +39,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "gpl_internal.cuh"
 #include "tc_common.cuh"
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(kThreadsGram, 1)
 //
 // Barriers: full[s] of the even CTA counts both CTAs' TMA bytes (the odd CTA's loads signal it
 // through its cluster address); empty[s] and accb[b] of both CTAs receive the MMA thread's
-// multicast commits; drained[b] of the even CTA counts both CTAs' 128 drain threads. Every wait is
+// multicast commits; drained[b] of the even CTA counts both CTAs' four drain warps. Every wait is
 // bounded; both CTAs meet at the hardware cluster barrier after initialisation and before TMEM
 // is freed, on every path.
 namespace {
@@ -337,7 +338,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreadsGram, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&sh->accb[b], 1);
-      mbar_init(&sh->drained[b], 256);
+      mbar_init(&sh->drained[b], 8);  // one arrival per drain warp of both CTAs
     }
     mbar_init(&sh->fin, 1);
     sh->abort = *(const volatile int*)err != 0;
@@ -430,7 +431,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreadsGram, 1)
       tc_fence_after();
       drain_f32_to_f64(lane_addr, buf * kGramN, 256, kGramN, sb == 0);
       tc_fence_before();
-      mbar_arrive_cluster(buf ? drained1 : drained0);
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(buf ? drained1 : drained0);
     }
     if (warp_all(ok && !aborted(sh) && *(const volatile int*)err == 0)) {
       tc_fence_after();
@@ -675,6 +677,19 @@ int tc_prepare(Ctx* c) {
   if ((rc = tc_alloc(c, &t.Lw, (size_t)n_d * n_d, "prior factor"))) return rc;
   if ((rc = tc_alloc(c, &t.Gt, (size_t)J * n_d * n_d, "whitened Gram"))) return rc;
   if ((rc = tc_alloc(c, &t.Tt, (size_t)J * n_d * n_d, "un-whitening product"))) return rc;
+  {
+    // fixed Rademacher probes (+-1) of the log-determinant correction, one P-vector per gene
+    if ((rc = tc_alloc(c, &t.probe, (size_t)c->P * J, "log-determinant probes"))) return rc;
+    std::vector<double> v((size_t)c->P * J);
+    uint64_t state = 0x9E3779B97F4A7C15ull;
+    for (size_t e = 0; e < v.size(); e++) {
+      state ^= state << 13;
+      state ^= state >> 7;
+      state ^= state << 17;
+      v[e] = (state >> 63) ? 1.0 : -1.0;
+    }
+    GPL_TRY(c, cudaMemcpy(t.probe, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+  }
   t.smem_whiten = (int)sizeof(double) * n_d * (n_d + 1) / 2;
   GPL_TRY(c, cudaFuncSetAttribute(k_whiten_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_whiten));
   GPL_TRY(c, cudaFuncSetAttribute(k_unwhiten_u, cudaFuncAttributeMaxDynamicSharedMemorySize, t.smem_whiten));
@@ -702,7 +717,7 @@ void tc_release(Ctx* c) {
   graph_reset(c);
   TcState& t = c->tc;
   void* bufs[] = {t.whi, t.wlo, t.pairs, t.err, t.Lw, t.Gt, t.Tt, t.DtC, t.DwC, t.ahi, t.alo, t.shi, t.slo,
-                  t.ohi, t.olo};
+                  t.ohi, t.olo, t.probe};
   for (void* p : bufs)
     if (p) cudaFree(p);
   t = TcState();

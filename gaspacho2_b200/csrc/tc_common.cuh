@@ -219,9 +219,11 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
       "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
       : "memory");
 }
-// Arrive on the mbarrier at the shared::cluster address `bar` (possibly in the other CTA).
+// Arrive on the mbarrier at the shared::cluster address `bar` (possibly in the other CTA), with
+// the default (CTA-scope) semantics: the arrival orders this thread's finished tcgen05 loads, not
+// memory writes the other CTA reads.
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mma_bf16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                               uint32_t accumulate) {

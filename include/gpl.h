@@ -77,11 +77,16 @@ GPL_API int gpl_set_precision(gpl_ctx* ctx, int precision);
  *   "tc_pair"           precision form: the two tensor-core contractions on CTA pairs (one
  *                       M = 256 MMA over two CTAs, each loading half of B) (1) or one CTA per
  *                       tile (0, default); the same sums in the same order
- *   "ls_restart"        precision form, in gpl_fit / gpl_fit_outer: a line search whose seven
- *                       tries all fail goes back to the step's start and restarts the L-BFGS
- *                       history there (at most 8 times per outer iteration), instead of the
- *                       reference's acceptance of the last try and its stop test (1); or the
- *                       reference's rule (0, default)
+ *   "logdet_probe"      precision form: log det Psi_j corrected with a fixed probe vector per gene
+ *                       and one application of the FP64 operator (1, default), so that the objective
+ *                       moves with parameter changes too small to change the BF16 hi/lo operands of
+ *                       the tensor-core Gram; 0: the tensor-core factor's log-determinant alone
+ *   "ls_fp64"           precision form, in gpl_fit / gpl_fit_outer: a line search whose seven
+ *                       tries all fail is repeated with the FP64 objective from the step's start
+ *                       (the tensor-core Gram does not resolve parameter changes below about 2^-16
+ *                       relative), and the fit goes on in the precision form from the point it
+ *                       accepted (1); or the reference's rule, the last try and its stop test
+ *                       (0, default). "ls_fp64_steps" (read only) counts the steps so repeated.
  *   "eta_tc"            the linear predictor z_i . beta_j of every cell and gene (W / nu, the
  *                       gradient's predictions, the refinement) on the FP64 tensor cores (1,
  *                       default) or as an FFMA tile GEMM (0); the two differ by rounding

@@ -99,3 +99,31 @@ def test_cta_pair_contractions(cfg, kw):
     print(f"config {cfg}: objective {rel:.2e}, gradient {gr:.2e}, bitwise {v1 == v0 and np.array_equal(g1, g0)}")
     assert rel <= 1e-12
     assert gr <= 1e-9
+
+
+def test_logdet_probe_and_fp64_line_search():
+    """The precision form's objective with the log-determinant probe (default) against FP64 at the
+    same state within 1e-6, and a budgeted fit with option ls_fp64 (a failed line search repeated
+    with the FP64 objective) that ends finite with the precision form restored."""
+    ds = synth.make(2, 8, init=True, N=6000, G=200, M=64, Q=5)
+    v0, _ = _evaluate_opts(ds, {"logdet_probe": 0})
+    v1, _ = _evaluate_opts(ds, {})
+    with GPLVM.from_dataset(ds, precision="fp64") as m:
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        for j in range(3):
+            m.irls_sweep(0, j)
+        m.objective_after_irls(0)
+        vf, _ = m.evaluate(m.params_vector())
+    print(f"objective vs FP64: probe {abs(v1 - vf) / abs(vf):.2e}, without {abs(v0 - vf) / abs(vf):.2e}")
+    assert abs(v1 - vf) / abs(vf) <= 1e-6
+    with GPLVM.from_dataset(ds, precision="bf16x3") as m:
+        m.set_option("ls_fp64", 1)
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        rc, st, tr = m.fit(3, 40)
+        print(f"fit: {st}, repeated steps {m.get_option('ls_fp64_steps')}, last {tr[-1]:.6e}")
+        assert np.all(np.isfinite(tr))
+        assert m.get_option("ls_fp64_steps") >= 0
