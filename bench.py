@@ -99,6 +99,11 @@ def parse():
                          "--fit-precisions")
     ap.add_argument("--fit-precisions", default="fp64,bf16x3")
     ap.add_argument("--fit-max-outer", type=int, default=1000)
+    ap.add_argument("--slope-check", action="store_true",
+                    help="instead of the benchmark: at the state after the second outer iteration's IRLS of "
+                         "--fit-config, each form's objective slope along the unit gradient direction against "
+                         "its gradient, and the precision form's errors per block, with and without the "
+                         "log-determinant probe")
     ap.add_argument("--fit-spread", action="store_true",
                     help="instead of the benchmark: the --fit-config fit's end point from starts perturbed by "
                          "1e-12 and 1e-9 (relative, X), FP64 and the precision form")
@@ -758,6 +763,64 @@ def run_ours(args):
     return 0
 
 
+def slope_check(args):
+    """The precision form's objective against its gradient: the fit of --fit-config (precision form)
+    for one outer iteration of at most 30 L-BFGS steps, the next IRLS, then at that state each form's
+    objective and gradient, and finite differences (v(x + eps d) - v(x)) / eps along the unit FP64
+    gradient direction d, taken in the gradient's coordinates (log Omega, log delta, X, T, log rho),
+    against g . d. One JSON line per setting of the log-determinant probe."""
+    import torch
+
+    from gaspacho2_b200 import GPLVM, synth
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ds = synth.make(args.fit_config, 0, init=True)
+    N, Q, M, p = ds.N, ds.Q, ds.M, len(ds.init.delta)
+    e = np.cumsum([0, N, p, N * Q, M * Q])
+    names = ("log_omega", "log_delta", "X", "T", "log_rho")
+    spans = list(zip(e[:-1], e[1:])) + [(e[-1], None)]
+
+    def move(x, d, eps):
+        y = x.copy()
+        for n, (a, b) in zip(names, spans):
+            y[a:b] = x[a:b] * np.exp(eps * d[a:b]) if n.startswith("log_") else x[a:b] + eps * d[a:b]
+        return y
+
+    with GPLVM.from_dataset(ds, stream=stream.cuda_stream, precision="bf16x3") as m:
+        m.set_params(ds.init)
+        m.kernel_mats()
+        m.glm_init()
+        m.fit_outer(0, 30)
+        m.irls(1, 100)
+        m.objective_after_irls(1)
+        x = m.params_vector()
+        m.set_precision("fp64")
+        vf, gf = m.evaluate(x)
+        gf = gf.copy()
+        d = gf / np.linalg.norm(gf)
+        for probe in (1, 0):
+            m.set_option("logdet_probe", probe)
+            m.set_precision("bf16x3")
+            vb, gb = m.evaluate(x)
+            gb = gb.copy()
+            errs = {n: float(np.linalg.norm(gb[a:b] - gf[a:b]) / max(np.linalg.norm(gf[a:b]), 1e-300))
+                    for n, (a, b) in zip(names, spans)}
+            rows = []
+            for eps in (1e-4, 1e-5, 1e-6):
+                row = {"eps": eps}
+                for prec, g in (("fp64", gf), ("bf16x3", gb)):
+                    m.set_precision(prec)
+                    v0, _ = m.evaluate(x)
+                    v1, _ = m.evaluate(move(x, d, eps))
+                    row[prec] = {"slope": (v1 - v0) / eps, "g_dot_d": float(g @ d)}
+                rows.append(row)
+            print(json.dumps({"mode": "slope_check", "config": args.fit_config, "logdet_probe": probe,
+                              "objective_rel_err": abs(vb - vf) / abs(vf), "gradient_rel_l2_by_block": errs,
+                              "slopes": rows}), flush=True)
+    return 0
+
+
 def fit_spread(args):
     """How far the fit's own discrete decisions carry rounding: the --fit-config fit to
     --fit-lbfgs steps from the seeded start and from starts whose X is scaled by (1 + eps z),
@@ -972,6 +1035,8 @@ def main():
     args = parse()
     if args.encoder_report:
         return encoder_report(args)
+    if args.slope_check:
+        return slope_check(args)
     if args.reference_gpu:
         return reference_gpu(args)
     if args.fit_trace:

@@ -335,8 +335,8 @@ static int gradient_run(Ctx* c) {
 // The FP64 repeat of a precision-form line search that failed (option ls_fp64): back to the step's
 // start, the FP64 objective there, the same backtracking rules against it, then the precision
 // form's objective at the accepted point into slot jtr + 1 (the next step's comparison and the
-// gradient's state). *evals = the objective evaluations made, negative if the FP64 search found
-// no rise either.
+// gradient's state). When the FP64 search finds no rise either, the parameters go back to the
+// step's start. *evals = the objective evaluations made, negative in that case.
 static int ls_fp64_retry(Ctx* c, int jtr, int rhoflag, int* evals) {
   std::vector<double>& l = c->lkhd;
   int n = 0;
@@ -362,6 +362,7 @@ static int ls_fp64_retry(Ctx* c, int jtr, int rhoflag, int* evals) {
     if (isnan(l[jtr + 1]) || isinf(l[jtr + 1])) sr *= 0.01;
     else sr *= 0.1;
   }
+  if (!rose) GPL_RUN(launch_downdate(c, jtr, 0.0, rhoflag));  // no rise either: back to the start
   c->precision = GPL_PREC_BF16X3;
   graph_reset(c);
   GPL_RUN(objective_run(c, jtr + 1));
