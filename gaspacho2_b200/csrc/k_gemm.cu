@@ -7,13 +7,15 @@
 //
 //   W / Nu     eta = z_i . beta_j for every cell and gene (k_eta; k_eta_dmma in k_dgemm.cu on the
 //              FP64 tensor cores with option eta_tc), then the getWForBeta element-wise pass
-//              (ggplvm.cu:468-514) one block per gene (k_w_nu). Bound: FP64 FMA (N*J*n_d) for
-//              the predictor, HBM and FP64 exp() for the pass.
+//              (ggplvm.cu:468-514): k_w_nu over cells x genes, then k_w_nu_counts. Bound:
+//              FP64 FMA (N*J*n_d) for the predictor, HBM and FP64 exp() for the pass.
 //   bvec       dense rows of Z^T diag(W_j/Omega) nu_j (getZtOinvjnj, util_cuda.cu:462-487)
 //              and of the GLM initialisation right-hand sides Z^T y0_j (initBeta,
 //              init.cu:193-221); the categorical rows come from the group sums.
 //   E          z_i . tBeta_j (cell x gene predictions used by the Omega/X gradient).
 //   C1 (part)  sum_j (tn_ij / phi_j) tBeta_j[GP] (ggplvm.cu:344).
+#include <algorithm>
+
 #include "gpl_internal.cuh"
 
 namespace gpl {
@@ -137,11 +139,11 @@ __device__ __forceinline__ double add_levels(double dense, int i, int j, int ldN
 // ---- W / Nu -----------------------------------------------------------------------------
 // getWForBeta (ggplvm.cu:468-514) from the linear predictor eta = z_i . beta_j (k_eta_dmma or
 // k_eta, written to a cell x gene buffer first). The per-cell factors exp(dgp titsias_i wt),
-// dgp titsias_i wt and log s_i are computed once per pass (k_cell_factors); then one block per
-// gene gives every cell W = exp(eta) s_i exp(dgp titsias_i wt) and the working response of a
-// zero count, and the counts that the reference's merge walk matches (the first gvalid entries
-// of the gene) replace their cells' working response. The barrier orders the two writes of such
-// a cell. The same expressions, in the same order, as the per-element form. The DE driver takes
+// dgp titsias_i wt and log s_i are computed once per pass (k_cell_factors); then every cell gets
+// W = exp(eta) s_i exp(dgp titsias_i wt) and the working response of a zero count (k_w_nu), and
+// the counts that the reference's merge walk matches (the first gvalid entries of each gene)
+// replace their cells' working response (k_w_nu_counts, after it in stream order). The same
+// expressions, in the same order, as the per-element form. The DE driver takes
 // the Titsias factor at weight 1 and nu = z.(beta - zeta) + (y - W)/W (ggplvm_de.cu:442-486);
 // the fit driver has zeta = 0.
 __global__ void k_cell_factors(int N, int ldN, int pvars, int de, const double* __restrict__ delta,
@@ -155,22 +157,45 @@ __global__ void k_cell_factors(int N, int ldN, int pvars, int de, const double* 
   f[2 * (size_t)ldN + i] = log(ls[i]);
 }
 
-__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, const double* __restrict__ E,
+// Zero-count values of every cell and gene: a 2-D grid (cell pairs x genes), two cells per thread
+// with 16-byte loads and stores (ldN is even, so a pair never straddles a column).
+__global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int J, const double* __restrict__ E,
                                               const double* __restrict__ ls, const double* __restrict__ f,
-                                              const int32_t* __restrict__ cell, const int64_t* __restrict__ gptr,
-                                              const int32_t* __restrict__ gvalid, const double* __restrict__ cnt,
                                               int de, const double* __restrict__ e0, double* __restrict__ W,
                                               double* __restrict__ Nu) {
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= N) return;
+  for (int j = blockIdx.y; j < J; j += gridDim.y) {
+    const size_t o = (size_t)j * ldN + i;
+    if (i + 1 < N) {
+      const double2 eta = *reinterpret_cast<const double2*>(E + o);
+      double2 w, nu;
+      w.x = exp(eta.x) * ls[i] * f[i];
+      w.y = exp(eta.y) * ls[i + 1] * f[i + 1];
+      nu.x = de ? (eta.x - e0[i]) - 1.0 : eta.x - 1.0;
+      nu.y = de ? (eta.y - e0[i + 1]) - 1.0 : eta.y - 1.0;
+      *reinterpret_cast<double2*>(W + o) = w;
+      *reinterpret_cast<double2*>(Nu + o) = nu;
+    } else {
+      const double eta = E[o];
+      W[o] = exp(eta) * ls[i] * f[i];
+      Nu[o] = de ? (eta - e0[i]) - 1.0 : eta - 1.0;
+    }
+  }
+}
+
+// The working response of the counts that the reference's merge walk matches (the first gvalid
+// entries of each gene), after k_w_nu wrote every cell's zero-count value (stream order).
+__global__ void __launch_bounds__(256) k_w_nu_counts(int ldN, const double* __restrict__ E,
+                                                     const double* __restrict__ ls, const double* __restrict__ f,
+                                                     const int32_t* __restrict__ cell,
+                                                     const int64_t* __restrict__ gptr,
+                                                     const int32_t* __restrict__ gvalid,
+                                                     const double* __restrict__ cnt, int de,
+                                                     const double* __restrict__ e0, double* __restrict__ Nu) {
   const int j = blockIdx.x;
   const double* Ej = E + (size_t)j * ldN;
-  double* Wj = W + (size_t)j * ldN;
   double* Nj = Nu + (size_t)j * ldN;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const double eta = Ej[i];
-    Wj[i] = exp(eta) * ls[i] * f[i];
-    Nj[i] = de ? (eta - e0[i]) - 1.0 : eta - 1.0;
-  }
-  __syncthreads();
   const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
   for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
     const int i = cell[l];
@@ -205,9 +230,15 @@ int launch_w_nu(Ctx* c) {
   k_cell_factors<<<div_up(c->N, 256), 256, 0, c->stream>>>(c->N, c->ldN, c->p, c->de ? 1 : 0, c->delta, c->titsias,
                                                           c->ls, c->cellfac);
   GPL_LAUNCHED(c, "k_cell_factors");
-  k_w_nu<<<c->J, 256, 0, c->stream>>>(c->N, c->ldN, c->scratch, c->ls, c->cellfac, c->cell, c->gptr, c->gvalid,
-                                      c->cnt, c->de ? 1 : 0, c->e0, c->W, c->Nu);
-  GPL_LAUNCHED(c, "k_w_nu");
+  {
+    dim3 g(div_up(c->N, 512), std::min(c->J, 65535));
+    k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->scratch, c->ls, c->cellfac, c->de ? 1 : 0, c->e0, c->W,
+                                     c->Nu);
+    GPL_LAUNCHED(c, "k_w_nu");
+    k_w_nu_counts<<<c->J, 256, 0, c->stream>>>(c->ldN, c->scratch, c->ls, c->cellfac, c->cell, c->gptr, c->gvalid,
+                                               c->cnt, c->de ? 1 : 0, c->e0, c->Nu);
+    GPL_LAUNCHED(c, "k_w_nu_counts");
+  }
   // W in group order for the group-sum GEMMs (W changes only here)
   if (c->Wg) return launch_group_order(c, c->W, c->J, c->Wg);
   return GPL_OK;
