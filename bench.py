@@ -518,7 +518,7 @@ def precision_leg(args, ds, stream, device):
         if n:
             phases[name] = ms / args.profile_steps
     m.profile(False)
-    tuning = {k: m.tuning(k) for k in ("tc_gram", "tc_grad")} if batched else None
+    tuning = {k: m.tuning(k) for k in ("tc_gram", "tc_grad", "eta_tile")} if batched else None
     m.close()
     return {"value": args.steps / dt, "unit": "evals/s", "ms_per_step": dt / args.steps * 1e3,
             "dtype": "bf16x3+f64", "objective_rel_err_vs_fp64": abs(vbf - v64) / abs(v64),
@@ -717,7 +717,7 @@ def run_ours(args):
             "irls_sweep": irls,
             "batched_form": {"graph": bool(m.get_option("graph")), "graph_replays_timed": int(replays),
                              "fused_tail": bool(m.get_option("fused_tail")),
-                             "autotune": {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail")},
+                             "autotune": {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail", "eta_tile")},
                              "eager_profiled_ms_per_step": eager_ms, "warmup_evaluations": warm} if batched else None,
         }
     if rank == 0 and getattr(ds, "genotypes", None) is not None:

@@ -555,37 +555,45 @@ __global__ void k_level_sums(int J, int n_grp, int n_cv, int P, const int* __res
   Lv[e] = s;
 }
 
-// One 16-deep K slice of the warp tile with only the first nkk of its four k4 steps live.
-__device__ __forceinline__ void warp_slice_live(const double* __restrict__ As, const double* __restrict__ Bs, int wm,
-                                                int wn, int g, int t, int nkk, double (&acc)[4][4][4]) {
+// One 16-deep K slice of a warp tile of MT x 16 cells x 32 genes (A rows of stride sa), with only
+// the first nkk of its four k4 steps live when kLive.
+template <int MT, bool kLive>
+__device__ __forceinline__ void warp_slice_eta(const double* __restrict__ As, const double* __restrict__ Bs, int sa,
+                                               int wm, int wn, int g, int t, int nkk, double (&acc)[MT][4][4]) {
 #pragma unroll
   for (int kk = 0; kk < BK / 4; kk++) {
-    if (kk >= nkk) break;
-    double a[4][2], b[4];
-    const double* ar = As + (kk * 4 + t) * SA + wm * 64 + g;
+    if (kLive && kk >= nkk) break;
+    double av[MT][2], b[4];
+    const double* ar = As + (kk * 4 + t) * sa + wm * (MT * 16) + g;
 #pragma unroll
-    for (int mt = 0; mt < 4; mt++) {
-      a[mt][0] = ar[mt * 16];
-      a[mt][1] = ar[mt * 16 + 8];
+    for (int mt = 0; mt < MT; mt++) {
+      av[mt][0] = ar[mt * 16];
+      av[mt][1] = ar[mt * 16 + 8];
     }
 #pragma unroll
     for (int nt = 0; nt < 4; nt++) b[nt] = Bs[(wn * 32 + nt * 8 + g) * SBT + kk * 4 + t];
 #pragma unroll
-    for (int mt = 0; mt < 4; mt++)
+    for (int mt = 0; mt < MT; mt++)
 #pragma unroll
-      for (int nt = 0; nt < 4; nt++) dmma_16x8x4(acc[mt][nt], a[mt][0], a[mt][1], b[nt]);
+      for (int nt = 0; nt < 4; nt++) dmma_16x8x4(acc[mt][nt], av[mt][0], av[mt][1], b[nt]);
   }
 }
 
+// Tiles of MT x 32 cells x 128 genes: MT = 4 (128 cells, one CTA per SM) or MT = 2 (64 cells, two
+// CTAs per SM, so that one CTA's epilogue overlaps the other's MMAs). Every output is the same
+// sum in the same order in both, so the autotuner may pick either.
+template <int MT>
 size_t eta_smem_bytes(int n_d) {
   const int KP = (n_d + BK - 1) / BK * BK;
-  return sizeof(double) * (3 * BK * SA + 3 * BN * SBT) + sizeof(int) * (size_t)KP;
+  return sizeof(double) * (3 * BK * (MT * 32 + 4) + 3 * BN * SBT) + sizeof(int) * (size_t)KP;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
+template <int MT>
+__global__ void __launch_bounds__(kThreads, MT == 2 ? 2 : 1) k_eta_dmma(const EtaArgs a) {
+  constexpr int BMt = MT * 32, SAt = BMt + 4;
   extern __shared__ __align__(16) double smem_d[];
-  double* As = smem_d;            // [3][BK][SA]  D rows (cells contiguous)
-  double* Bs = As + 3 * BK * SA;  // [3][BN][SBT] dense coefficients (k contiguous)
+  double* As = smem_d;             // [3][BK][SAt] D rows (cells contiguous)
+  double* Bs = As + 3 * BK * SAt;  // [3][BN][SBT] dense coefficients (k contiguous)
   const int KP = (a.n_d + BK - 1) / BK * BK;
   int* dcs = reinterpret_cast<int*>(Bs + 3 * BN * SBT);  // [KP] dcol, 0 past n_d
   const double* __restrict__ D = a.D;
@@ -595,7 +603,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
   double* __restrict__ out = a.out;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
-  const int tm = (a.N + BM - 1) / BM, tn = (a.J + BN - 1) / BN;
+  const int tm = (a.N + BMt - 1) / BMt, tn = (a.J + BN - 1) / BN;
   const int tiles = tm * tn, nsl = KP / BK;
   for (int k = tid; k < KP; k += kThreads) dcs[k] = k < a.n_d ? a.dcol[k] : 0;
   __syncthreads();
@@ -604,13 +612,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
   auto load = [&](int m0, int j0, int s, int st) {
     const int kb = s * BK;
 #pragma unroll
-    for (int r = 0; r < (BM * BK / 2) / kThreads; r++) {
+    for (int r = 0; r < (BMt * BK / 2) / kThreads; r++) {
       const int ch = tid + r * kThreads;
-      const int k = ch >> 6, part = ch & 63;
+      const int k = ch / (BMt / 2), part = ch % (BMt / 2);
       const int col = kb + k, i = m0 + part * 2;
       const int nb = (col < a.n_d && i < a.ldN) ? 16 : 0;  // ldN is even: a chunk is in or out whole
       const double* src = D + (size_t)min(col, a.n_d - 1) * a.ldN + min(i, a.ldN - 2);
-      cp_async16(As + st * BK * SA + k * SA + part * 2, src, nb);
+      cp_async16(As + st * BK * SAt + k * SAt + part * 2, src, nb);
     }
 #pragma unroll
     for (int r = 0; r < (BN * BK) / kThreads; r++) {
@@ -626,17 +634,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
   int base = 0;  // slices issued before this tile (stage of slice s = (base + s) % 3)
   int w = blockIdx.x;
   if (w < tiles) {
-    const int m0 = (w / tn) * BM, j0 = (w % tn) * BN;
+    const int m0 = (w / tn) * BMt, j0 = (w % tn) * BN;
     load(m0, j0, 0, 0);
     cp_async_commit();
     if (nsl > 1) load(m0, j0, 1, 1);
     cp_async_commit();
   }
   for (; w < tiles; w += gridDim.x) {
-    const int m0 = (w / tn) * BM, j0 = (w % tn) * BN;
-    double acc[4][4][4];
+    const int m0 = (w / tn) * BMt, j0 = (w % tn) * BN;
+    double acc[MT][4][4];
 #pragma unroll
-    for (int x = 0; x < 4; x++)
+    for (int x = 0; x < MT; x++)
 #pragma unroll
       for (int y = 0; y < 4; y++)
 #pragma unroll
@@ -648,17 +656,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
       cp_async_commit();
       const int st = (base + s) % 3;
       if (s + 1 < nsl) {
-        warp_slice<true>(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, acc);
+        warp_slice_eta<MT, false>(As + st * BK * SAt, Bs + st * BN * SBT, SAt, wm, wn, g, t, 4, acc);
       } else {  // the last slice: only the k4 steps that reach a dense column
         const int nkk = min(BK / 4, (a.n_d - s * BK + 3) / 4);
-        warp_slice_live(As + st * BK * SA, Bs + st * BN * SBT, wm, wn, g, t, nkk, acc);
+        warp_slice_eta<MT, true>(As + st * BK * SAt, Bs + st * BN * SBT, SAt, wm, wn, g, t, nkk, acc);
       }
     }
     // the next tile's first two slices go to the two stages that no warp reads any more
     base += nsl;
     const int wn2 = w + gridDim.x;
     if (wn2 < tiles) {
-      const int m1 = (wn2 / tn) * BM, j1 = (wn2 % tn) * BN;
+      const int m1 = (wn2 / tn) * BMt, j1 = (wn2 % tn) * BN;
       load(m1, j1, 0, base % 3);
       cp_async_commit();
       if (nsl > 1) load(m1, j1, 1, (base + 1) % 3);
@@ -667,10 +675,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
     // the cells' level sums, then the stores
     if (a.n_grp > 0) {
 #pragma unroll
-      for (int mt = 0; mt < 4; mt++)
+      for (int mt = 0; mt < MT; mt++)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const int i = min(m0 + wm * 64 + mt * 16 + g + h * 8, a.N - 1);
+          const int i = min(m0 + wm * (MT * 16) + mt * 16 + g + h * 8, a.N - 1);
           const double* lg = lvt + gid[i];
 #pragma unroll
           for (int nt = 0; nt < 4; nt++)
@@ -682,10 +690,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
         }
     }
 #pragma unroll
-    for (int mt = 0; mt < 4; mt++)
+    for (int mt = 0; mt < MT; mt++)
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int i = m0 + wm * 64 + mt * 16 + g + h * 8;
+        const int i = m0 + wm * (MT * 16) + mt * 16 + g + h * 8;
         if (i >= a.N) continue;
 #pragma unroll
         for (int nt = 0; nt < 4; nt++)
@@ -700,8 +708,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_eta_dmma(const EtaArgs a) {
 }
 
 int launch_eta_dmma(Ctx* c, const double* B, double* out) {
-  const size_t smem = eta_smem_bytes(c->n_d);
-  if (smem > 227 * 1024) {
+  if (eta_smem_bytes<4>(c->n_d) > 227 * 1024) {
     c->err = "too many dense columns for the linear-predictor kernel";
     return GPL_ERR_LIMIT;
   }
@@ -711,7 +718,6 @@ int launch_eta_dmma(Ctx* c, const double* B, double* out) {
                                                                  c->glev_d, B, c->lvt);
     GPL_LAUNCHED(c, "k_level_sums");
   }
-  GPL_TRY(c, cudaFuncSetAttribute(k_eta_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EtaArgs a{};
   a.N = c->N;
   a.ldN = c->ldN;
@@ -725,9 +731,21 @@ int launch_eta_dmma(Ctx* c, const double* B, double* out) {
   a.dcol = c->dcol_d;
   a.gid = c->gid_d;
   a.out = out;
-  const int tiles = div_up(c->N, BM) * div_up(c->J, BN);
-  const int grid = std::min(tiles, c->sm_count);
-  k_eta_dmma<<<grid, kThreads, smem, c->stream>>>(a);
+  // tile height: 128 cells (one CTA per SM) or 64 (two), the autotuner's choice (same sums)
+  Tunable* tu = nullptr;
+  const int cells = tune_pick(c, "eta_tile", {128, 64}, 128, &tu);
+  TuneScope ts(c, tu);
+  if (cells == 64) {
+    const size_t smem = eta_smem_bytes<2>(c->n_d);
+    GPL_TRY(c, cudaFuncSetAttribute(k_eta_dmma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int tiles = div_up(c->N, 64) * div_up(c->J, BN);
+    k_eta_dmma<2><<<std::min(tiles, 2 * c->sm_count), kThreads, smem, c->stream>>>(a);
+  } else {
+    const size_t smem = eta_smem_bytes<4>(c->n_d);
+    GPL_TRY(c, cudaFuncSetAttribute(k_eta_dmma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int tiles = div_up(c->N, 128) * div_up(c->J, BN);
+    k_eta_dmma<4><<<std::min(tiles, c->sm_count), kThreads, smem, c->stream>>>(a);
+  }
   GPL_LAUNCHED(c, "k_eta_dmma");
   return GPL_OK;
 }

@@ -127,7 +127,8 @@ bool tune_settled(const Ctx* c) {
 // capture waits for these only; the IRLS tail is never part of a captured evaluation.
 bool tune_settled_for_graphs(const Ctx* c) {
   for (auto& t : c->tun) {
-    const bool in_eval = t.name == "pair_gram" || t.name == "pair_v" || t.name == "tc_gram" || t.name == "tc_grad";
+    const bool in_eval = t.name == "pair_gram" || t.name == "pair_v" || t.name == "tc_gram" || t.name == "tc_grad" ||
+                         t.name == "eta_tile";
     if (in_eval && (t.best < 0 || !t.pending.empty())) return false;
   }
   return true;

@@ -115,7 +115,7 @@ GPL_API int gpl_set_option(gpl_ctx* ctx, const char* name, int64_t value);
 GPL_API int gpl_get_option(const gpl_ctx* ctx, const char* name, int64_t* value);
 
 /* The autotuner's record of one choice ("pair_gram", "pair_v", "irls_tail", "tc_gram",
- * "tc_grad"): *chosen = the chosen candidate value (-1 while open), cands[k] the candidate
+ * "tc_grad", "eta_tile"): *chosen = the chosen candidate value (-1 while open), cands[k] the candidate
  * values and best_ms[k] each one's best measured launch time (-1 untimed, -2 chosen from the
  * process-wide record without timing), up to cap entries; *n_cands the number of candidates
  * (0 if the choice never came up). No reference counterpart. */
