@@ -85,7 +85,8 @@ static void free_state(Ctx* c) {
   pair_release(c);
   void* extra[] = {c->cellfac, c->lvt, c->Dm, c->gsum, c->gT, c->HK, c->dcol_d, c->cv_nh_d, c->cv_nlev_d, c->gid_d, c->glev_d,
                    c->gcells_d, c->gstart_d, c->codes_d, c->hk_tiles_d, c->hk_tiles128_d, c->part, c->hk_cells_d,
-                   c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d, c->hk_pos_d, c->Wg, c->Dg, c->rOmg};
+                   c->lvl_cc_d, c->lvl_v_d, c->lvl_ptr_d, c->lvl_grp_d, c->hk_pos_d, c->Wg, c->Dg, c->rOmg,
+                   c->gpos_d};
   for (void* q : extra)
     if (q) cudaFree(q);
   c->hk_tiles128_d = nullptr;
@@ -97,6 +98,7 @@ static void free_state(Ctx* c) {
   c->dcol_d = c->cv_nh_d = c->cv_nlev_d = c->gid_d = c->glev_d = c->gcells_d = c->gstart_d = c->codes_d = nullptr;
   c->lvl_cc_d = c->lvl_v_d = c->lvl_ptr_d = c->lvl_grp_d = c->hk_pos_d = nullptr;
   c->Wg = c->Dg = c->rOmg = nullptr;
+  c->gpos_d = nullptr;
   c->n_lvl = 0;
   c->hk_tiles_d = nullptr;
   c->n_grp = c->n_cv = 0;
@@ -1028,8 +1030,9 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_RUN(dalloc(c, &c->cv_nlev_d, (size_t)ncat, "grouped variable levels"));
     GPL_RUN(dalloc(c, &c->glev_d, glev.size(), "group levels"));
     GPL_RUN(dalloc(c, &c->gcells_d, (size_t)N, "group cells"));
+    GPL_RUN(dalloc(c, &c->gpos_d, (size_t)N, "group positions"));
     GPL_RUN(dalloc(c, &c->gid_d, (size_t)N, "cell groups"));
-    GPL_RUN(dalloc(c, &c->lvt, (size_t)J * n_grp, "level sums per group"));
+    GPL_RUN(dalloc(c, &c->lvt, (size_t)lvt_ld(J) * n_grp, "level sums per group"));
     GPL_RUN(dalloc(c, &c->gstart_d, gstart.size(), "group offsets"));
     GPL_RUN(dalloc(c, &c->hk_tiles_d, tiles.size(), "group tiles"));
     GPL_RUN(dalloc(c, &c->hk_tiles128_d, tiles128.size(), "group tiles"));
@@ -1048,10 +1051,12 @@ int gpl_load_design(gpl_ctx* h, int N, int n_var, const int32_t* cv, const int32
     GPL_TRY(c, cudaMemcpy(c->glev_d, glev.data(), sizeof(int32_t) * glev.size(), cudaMemcpyHostToDevice));
     GPL_TRY(c, cudaMemcpy(c->gcells_d, order.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
     {
-      std::vector<int32_t> gid(N);
+      std::vector<int32_t> gid(N), gpos(N);
       for (int g = 0; g < n_grp; g++)
         for (int k = gstart[g]; k < gstart[g + 1]; k++) gid[order[k]] = g;
+      for (int k = 0; k < N; k++) gpos[order[k]] = k;
       GPL_TRY(c, cudaMemcpy(c->gid_d, gid.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+      GPL_TRY(c, cudaMemcpy(c->gpos_d, gpos.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
     }
     GPL_TRY(c, cudaMemcpy(c->gstart_d, gstart.data(), sizeof(int32_t) * gstart.size(), cudaMemcpyHostToDevice));
     // per level of each grouped variable: its model column, its variable, its groups in order

@@ -163,6 +163,7 @@ struct Ctx {
   std::vector<int> cv_nh, cv_nlev;  // first model column and level count of each grouped variable
   int *dcol_d = nullptr, *cv_nh_d = nullptr, *cv_nlev_d = nullptr, *gid_d = nullptr, *glev_d = nullptr;
   int *gcells_d = nullptr, *gstart_d = nullptr, *codes_d = nullptr;
+  int* gpos_d = nullptr;  // position of each cell in the group order (the inverse of gcells_d)
   double* lvt = nullptr;  // J x n_grp: per gene and cell group, the sum of its levels' coefficients
   double* cellfac = nullptr;  // 3 x ldN: exp(dgp t_i wt), dgp t_i wt and log s_i of the W / Nu pass
   // levels of the grouped variables: model column, variable, and the groups at that level
@@ -284,6 +285,8 @@ int launch_group_order(Ctx* c, const double* src, int ncols, double* dst);  // d
 int launch_w_nu(Ctx* c);                 // W, Nu from Beta (getWForBeta)
 // out = z_i . B_j (ldN x J, cell fastest) on the FP64 tensor cores (k_dgemm.cu)
 int launch_eta_dmma(Ctx* c, const double* B, double* out);
+// row stride of the per-group level sums (groups x genes): J rounded up to even
+inline int lvt_ld(int J) { return J + (J & 1); }
 int launch_zt_u(Ctx* c, int mode);       // bvec = Z^T u; mode 0: u = W/Omega*Nu; 1: init response
 int launch_zt_u_ex(Ctx* c, int mode, const double* u, double* out);  // the same for another u / output;
                                                                       // mode 2: u is one value per cell

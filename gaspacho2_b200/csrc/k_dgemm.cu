@@ -527,9 +527,10 @@ int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D) {
 // ---------------------------------------------------------------------------------------------
 // Linear predictor over the dense columns (option eta_tc)
 // ---------------------------------------------------------------------------------------------
-// out[j * ldN + i] = D_i . B_j[dcol] + Lv[j, group(i)] for 128-cell x 128-gene tiles, where
-// Lv[j, g] is the sum of gene j's coefficients of the levels of cell group g (k_level_sums, per
-// launch): K = the dense columns in 16-deep slices (DMMA steps past n_d skipped), A = D by
+// out[j * ldN + i] = D_i . B_j[dcol] + Lv[group(i), j] for 128-cell x 128-gene tiles, where
+// Lv[g, j] is the sum of gene j's coefficients of the levels of cell group g (k_level_sums, per
+// launch; genes contiguous in rows of ldJ, even, so that a lane reads its two genes' sums as one
+// 16-byte load and the eight cells of a quad row touch at most eight lines): K = the dense columns in 16-deep slices (DMMA steps past n_d skipped), A = D by
 // 16-byte cp.async (cells contiguous), B = the genes' dense coefficients gathered through dcol by
 // 8-byte cp.async (k contiguous in shared memory). Persistent: one CTA per SM walks the tiles
 // cell-tile-major with a stride of the grid, so the CTAs resident at any time share a few cell
@@ -538,21 +539,21 @@ int launch_v_to_u_cells(Ctx* c, int c0, int c1, const double* D) {
 // element-wise pass of their own: inside this kernel's epilogue, at one CTA per SM, the
 // dependent FP64 operations of exp() left the tensor pipe idle for most of the launch.
 struct EtaArgs {
-  int N, ldN, P, J, n_d, n_grp;
+  int N, ldN, P, J, ldJ, n_d, n_grp;
   const double *D, *B, *lvt;
   const int *dcol, *gid;
   double* out;
 };
 
-// Lv[j * n_grp + g] = sum over the grouped variables v (in order) of B[cv_nh[v] + level + j * P]
-__global__ void k_level_sums(int J, int n_grp, int n_cv, int P, const int* __restrict__ cv_nh,
+// Lv[g * ldJ + j] = sum over the grouped variables v (in order) of B[cv_nh[v] + level + j * P]
+__global__ void k_level_sums(int J, int ldJ, int n_grp, int n_cv, int P, const int* __restrict__ cv_nh,
                              const int* __restrict__ glev, const double* __restrict__ B, double* __restrict__ Lv) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (int64_t)J * n_grp) return;
-  const int j = (int)(e / n_grp), g = (int)(e - (int64_t)j * n_grp);
+  const int g = (int)(e / J), j = (int)(e - (int64_t)g * J);
   double s = 0.0;
   for (int v = 0; v < n_cv; v++) s += B[cv_nh[v] + glev[(size_t)g * n_cv + v] + (size_t)j * P];
-  Lv[e] = s;
+  Lv[(size_t)g * ldJ + j] = s;
 }
 
 // One 16-deep K slice of a warp tile of MT x 16 cells x 32 genes (A rows of stride sa), with only
@@ -679,14 +680,15 @@ __global__ void __launch_bounds__(kThreads, MT == 2 ? 2 : 1) k_eta_dmma(const Et
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int i = min(m0 + wm * (MT * 16) + mt * 16 + g + h * 8, a.N - 1);
-          const double* lg = lvt + gid[i];
+          const double* lg = lvt + (size_t)gid[i] * a.ldJ;
 #pragma unroll
-          for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-              const int j = min(j0 + wn * 32 + nt * 8 + 2 * t + e, a.J - 1);
-              acc[mt][nt][h * 2 + e] += lg[(size_t)j * a.n_grp];
-            }
+          for (int nt = 0; nt < 4; nt++) {
+            // genes j, j + 1 (j even); past J only columns that are never stored
+            const int j = min(j0 + wn * 32 + nt * 8 + 2 * t, a.ldJ - 2);
+            const double2 v = *reinterpret_cast<const double2*>(lg + j);
+            acc[mt][nt][h * 2] += v.x;
+            acc[mt][nt][h * 2 + 1] += v.y;
+          }
         }
     }
 #pragma unroll
@@ -714,8 +716,8 @@ int launch_eta_dmma(Ctx* c, const double* B, double* out) {
   }
   if (c->n_grp > 0) {
     const int64_t n = (int64_t)c->J * c->n_grp;
-    k_level_sums<<<(unsigned)div_up(n, 256), 256, 0, c->stream>>>(c->J, c->n_grp, c->n_cv, c->P, c->cv_nh_d,
-                                                                 c->glev_d, B, c->lvt);
+    k_level_sums<<<(unsigned)div_up(n, 256), 256, 0, c->stream>>>(c->J, lvt_ld(c->J), c->n_grp, c->n_cv, c->P,
+                                                                 c->cv_nh_d, c->glev_d, B, c->lvt);
     GPL_LAUNCHED(c, "k_level_sums");
   }
   EtaArgs a{};
@@ -723,6 +725,7 @@ int launch_eta_dmma(Ctx* c, const double* B, double* out) {
   a.ldN = c->ldN;
   a.P = c->P;
   a.J = c->J;
+  a.ldJ = lvt_ld(c->J);
   a.n_d = c->n_d;
   a.n_grp = c->n_grp;
   a.D = c->Dm;

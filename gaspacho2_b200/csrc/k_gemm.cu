@@ -157,29 +157,50 @@ __global__ void k_cell_factors(int N, int ldN, int pvars, int de, const double* 
   f[2 * (size_t)ldN + i] = log(ls[i]);
 }
 
-// Zero-count values of every cell and gene: a 2-D grid (cell pairs x genes), two cells per thread
-// with 16-byte loads and stores (ldN is even, so a pair never straddles a column).
+// Zero-count values of every cell and gene: a 2-D grid (cell pairs x gene quads), two cells and
+// up to kWnuGenes genes per thread with 16-byte loads and stores (ldN is even, so a pair never
+// straddles a column; past N the pair's second value is read from the column's padding and
+// dropped). The quad's loads are issued before any exp(), so 64 bytes per thread are in flight.
+// With a group order (gpos: each cell's position in it) W's group-ordered copy for the group-sum
+// GEMMs is written here too, one 8-byte store per value, in place of a gather pass over W.
+constexpr int kWnuGenes = 4;
 __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int J, const double* __restrict__ E,
                                               const double* __restrict__ ls, const double* __restrict__ f,
-                                              int de, const double* __restrict__ e0, double* __restrict__ W,
-                                              double* __restrict__ Nu) {
+                                              int de, const double* __restrict__ e0,
+                                              const int* __restrict__ gpos, double* __restrict__ W,
+                                              double* __restrict__ Nu, double* __restrict__ Wg) {
   const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= N) return;
-  for (int j = blockIdx.y; j < J; j += gridDim.y) {
-    const size_t o = (size_t)j * ldN + i;
-    if (i + 1 < N) {
-      const double2 eta = *reinterpret_cast<const double2*>(E + o);
+  const bool two = i + 1 < N;
+  const double l0 = ls[i], f0 = f[i], l1 = two ? ls[i + 1] : 0.0, f1 = two ? f[i + 1] : 0.0;
+  const double z0 = de ? e0[i] : 0.0, z1 = de && two ? e0[i + 1] : 0.0;
+  const int p0 = Wg ? gpos[i] : 0, p1 = Wg && two ? gpos[i + 1] : 0;
+  for (int jb = blockIdx.y * kWnuGenes; jb < J; jb += gridDim.y * kWnuGenes) {
+    double2 eta[kWnuGenes];
+#pragma unroll
+    for (int u = 0; u < kWnuGenes; u++)
+      if (jb + u < J) eta[u] = *reinterpret_cast<const double2*>(E + (size_t)(jb + u) * ldN + i);
+#pragma unroll
+    for (int u = 0; u < kWnuGenes; u++) {
+      const int j = jb + u;
+      if (j >= J) break;
+      const size_t o = (size_t)j * ldN + i;
       double2 w, nu;
-      w.x = exp(eta.x) * ls[i] * f[i];
-      w.y = exp(eta.y) * ls[i + 1] * f[i + 1];
-      nu.x = de ? (eta.x - e0[i]) - 1.0 : eta.x - 1.0;
-      nu.y = de ? (eta.y - e0[i + 1]) - 1.0 : eta.y - 1.0;
-      *reinterpret_cast<double2*>(W + o) = w;
-      *reinterpret_cast<double2*>(Nu + o) = nu;
-    } else {
-      const double eta = E[o];
-      W[o] = exp(eta) * ls[i] * f[i];
-      Nu[o] = de ? (eta - e0[i]) - 1.0 : eta - 1.0;
+      w.x = exp(eta[u].x) * l0 * f0;
+      nu.x = de ? (eta[u].x - z0) - 1.0 : eta[u].x - 1.0;
+      if (two) {
+        w.y = exp(eta[u].y) * l1 * f1;
+        nu.y = de ? (eta[u].y - z1) - 1.0 : eta[u].y - 1.0;
+        *reinterpret_cast<double2*>(W + o) = w;
+        *reinterpret_cast<double2*>(Nu + o) = nu;
+      } else {
+        W[o] = w.x;
+        Nu[o] = nu.x;
+      }
+      if (Wg) {
+        Wg[(size_t)j * ldN + p0] = w.x;
+        if (two) Wg[(size_t)j * ldN + p1] = w.y;
+      }
     }
   }
 }
@@ -231,16 +252,15 @@ int launch_w_nu(Ctx* c) {
                                                           c->ls, c->cellfac);
   GPL_LAUNCHED(c, "k_cell_factors");
   {
-    dim3 g(div_up(c->N, 512), std::min(c->J, 65535));
-    k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->scratch, c->ls, c->cellfac, c->de ? 1 : 0, c->e0, c->W,
-                                     c->Nu);
+    // W's group-ordered copy for the group-sum GEMMs is written by k_w_nu (W changes only here)
+    dim3 g(div_up(c->N, 512), std::min(div_up(c->J, kWnuGenes), 65535));
+    k_w_nu<<<g, 256, 0, c->stream>>>(c->N, c->ldN, c->J, c->scratch, c->ls, c->cellfac, c->de ? 1 : 0, c->e0,
+                                     c->gpos_d, c->W, c->Nu, c->Wg);
     GPL_LAUNCHED(c, "k_w_nu");
     k_w_nu_counts<<<c->J, 256, 0, c->stream>>>(c->ldN, c->scratch, c->ls, c->cellfac, c->cell, c->gptr, c->gvalid,
                                                c->cnt, c->de ? 1 : 0, c->e0, c->Nu);
     GPL_LAUNCHED(c, "k_w_nu_counts");
   }
-  // W in group order for the group-sum GEMMs (W changes only here)
-  if (c->Wg) return launch_group_order(c, c->W, c->J, c->Wg);
   return GPL_OK;
 }
 

@@ -54,7 +54,7 @@ def _fit(gd, budget=12, **opts):
         out["trace"] = tr
         out["stats"] = np.array([st["outer"], st["irls"], st["lbfgs"], st["evals"]])
         info = {k: m.get_option(k) for k in ("graph", "graph_replays", "autotune")}
-        tun = {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail")}
+        tun = {k: m.tuning(k) for k in ("pair_gram", "pair_v", "irls_tail", "eta_tile")}
     return out, info, tun
 
 
@@ -81,7 +81,7 @@ def test_autotuned_fit_same_bits_and_records():
     b, info, tun = _fit(gd, autotune=1, graph=1, fused_tail=1)
     for k in a:
         assert np.array_equal(a[k], b[k]), f"{k}: autotuned fit differs"
-    for name in ("pair_gram", "irls_tail", "pair_v"):
+    for name in ("pair_gram", "irls_tail", "pair_v", "eta_tile"):
         t = tun[name]
         assert t["chosen"] is not None, f"{name}: never settled"
         assert t["chosen"] in t["candidates_ms"]
