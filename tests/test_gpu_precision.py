@@ -69,6 +69,36 @@ def test_precision_form_against_fp64(cfg, kw):
     assert not bad, bad
 
 
+@pytest.mark.parametrize("name", ["c2_head", "c2_cats"])
+def test_precision_form_against_reference_golden(name):
+    """The precision form's phases against the reference's own kernels (the golden vectors, FP64
+    on the host): at the benchmark's model shape (c2_head: M = 128, Q = 10, P = 236) and with an
+    empty donor level (c2_cats). The objective values within 1e-6 relative, the gradient blocks
+    within 1e-4 (T within 1e-3) relative L2 (measured: objective 4.7e-9 and 3.8e-8, gradient
+    blocks 7.4e-8 to 4.3e-6, T 9.3e-6 and 2.5e-5)."""
+    from tests import golden_util as gu
+
+    gd = gu.load(name)
+    with GPLVM.from_dataset(gd, precision="bf16x3") as m:
+        out = gu.run_phases(m, gd)
+        dims = (m.N, m.Q, m.M)
+    ref = gd.g
+    bad = []
+    for k in ("sweep0_lkhd", "obj0", "obj1"):
+        e = abs(float(out[k]) - float(ref[k])) / abs(float(ref[k]))
+        print(f"{name}: {k} rel err {e:.2e}")
+        if not e <= 1e-6:
+            bad.append(f"{k}: {e:.2e}")
+    b0, b1 = _blocks(np.asarray(ref["grad0"]), dims), _blocks(np.asarray(out["grad0"]), dims)
+    for blk in b0:
+        e = np.linalg.norm(b1[blk] - b0[blk]) / max(np.linalg.norm(b0[blk]), 1e-300)
+        tol = 1e-3 if blk == "T" else 1e-4
+        print(f"{name}: grad {blk:5s} rel-l2 {e:.2e} (tol {tol:.0e})")
+        if not e <= tol:
+            bad.append(f"grad {blk}: {e:.2e}")
+    assert not bad, bad
+
+
 def _evaluate_opts(ds, opts):
     with GPLVM.from_dataset(ds, precision="fp64") as m:
         for k, v in opts.items():
