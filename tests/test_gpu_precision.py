@@ -85,7 +85,8 @@ def test_precision_form_against_reference_golden(name):
     ref = gd.g
     bad = []
     for k in ("sweep0_lkhd", "obj0", "obj1"):
-        e = abs(float(out[k]) - float(ref[k])) / abs(float(ref[k]))
+        a, b = float(np.ravel(out[k])[0]), float(np.ravel(ref[k])[0])
+        e = abs(a - b) / abs(b)
         print(f"{name}: {k} rel err {e:.2e}")
         if not e <= 1e-6:
             bad.append(f"{k}: {e:.2e}")
