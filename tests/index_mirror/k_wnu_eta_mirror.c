@@ -1,0 +1,290 @@
+/*
+ * CPU mirror of the memory indexing of the linear predictor and the W / nu pass:
+ * k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu) and k_w_nu
+ * (gaspacho2_b200/csrc/k_gemm.cu).
+ *
+ * The kernels' own index expressions are replayed for every block and thread of a launch
+ * (256 threads; lane = 4 g + t as in the DMMA fragments), over a sweep of sizes: cell counts
+ * around the tile heights and the padded column length (ldN = N rounded up to 32), gene counts
+ * around the tile width and odd ones, dense-column counts with ragged last slices, with and
+ * without cell groups, and persistent grids smaller than the tile count. Each global index is
+ * checked against its allocation (the sizes gaspacho2_b200/csrc/gpl_api.cu allocates), each
+ * shared index against the launch's dynamic shared memory, including the source of a
+ * zero-byte (zero-fill) cp.async; outputs are counted: every (cell, gene) of the predictor and
+ * of W, nu and W's group-ordered copy is written exactly once, every persistent tile visited
+ * once.
+ *
+ *   k_wnu_eta_mirror        prints "ok eta4 <sizes>", "ok eta2 <sizes>", "ok levels <sizes>",
+ *                           "ok w_nu <sizes>" and exits 0, or lists the first faults, exits 1.
+ *   k_wnu_eta_mirror plant  the same with the level sums' rows left unpadded (J instead of J
+ *                           rounded up to even): must fail on an odd gene count.
+ *
+ * Compiled and run by tests/test_index_mirror.py. Keep it in step with the two kernels.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define BN 128
+#define BK 16
+#define SBT (BK + 4)
+#define NT 256
+#define WNU_GENES 4
+
+static long faults = 0;
+static void fault(const char* what, const char* ctx, long idx, long lim) {
+  if (faults < 20) fprintf(stderr, "%s: %s index %ld outside [0, %ld)\n", ctx, what, idx, lim);
+  faults++;
+}
+#define CHK(what, i, lim) do { long i_ = (long)(i), l_ = (long)(lim); if (i_ < 0 || i_ >= l_) fault(what, ctx, i_, l_); } while (0)
+
+static int imin(int a, int b) { return a < b ? a : b; }
+static int div_up(int a, int b) { return (a + b - 1) / b; }
+static int ld_cells(int N) { return (N + 31) / 32 * 32; }
+static int plant_unpadded = 0; /* "plant": the level sums' rows left at J (unpadded) */
+static int lvt_ld(int J) { return plant_unpadded ? J : J + (J & 1); }
+
+/* k_eta_dmma<MT>: loads, fragment reads, level sums and stores of every tile a grid of
+ * `grid` persistent CTAs walks. */
+static void mirror_eta(int MT, int N, int J, int n_d, int n_grp, int grid) {
+  char ctx[96];
+  snprintf(ctx, sizeof ctx, "eta%d N=%d J=%d n_d=%d n_grp=%d grid=%d", MT, N, J, n_d, n_grp, grid);
+  const int ldN = ld_cells(N), P = n_d + 3 + (n_grp ? 4 : 0), ldJ = lvt_ld(J);
+  const int BMt = MT * 32, SAt = BMt + 4;
+  const int KP = (n_d + BK - 1) / BK * BK, nsl = KP / BK;
+  /* shared memory in doubles: As [3][BK][SAt], Bs [3][BN][SBT], then KP ints */
+  const long as_n = 3L * BK * SAt, bs_n = 3L * BN * SBT;
+  const long D_n = (long)n_d * ldN, B_n = (long)P * J, lvt_n = (long)n_grp * ldJ, out_n = (long)ldN * J;
+  int* dcol = malloc(sizeof(int) * (n_d ? n_d : 1));
+  for (int k = 0; k < n_d; k++) dcol[k] = 1 + (k * 7) % (P - 1); /* any column of the P model columns */
+  int* gid = malloc(sizeof(int) * N);
+  for (int i = 0; i < N; i++) gid[i] = n_grp ? (i * 5 + 1) % n_grp : 0;
+  int* dcs = malloc(sizeof(int) * KP);
+  for (int k = 0; k < KP; k++) dcs[k] = k < n_d ? dcol[k] : 0;
+  unsigned char* written = calloc((size_t)out_n, 1);
+  const int tm = (N + BMt - 1) / BMt, tn = (J + BN - 1) / BN, tiles = tm * tn;
+  int* visits = calloc((size_t)tiles, sizeof(int));
+
+  for (int b = 0; b < grid; b++) {
+    /* the persistent walk and the next tile's prefetch */
+    for (int w = b; w < tiles; w += grid) {
+      visits[w]++;
+      const int m0 = (w / tn) * BMt, j0 = (w % tn) * BN;
+      for (int s = 0; s < nsl; s++) {
+        const int kb = s * BK;
+        for (int st = 0; st < 3; st += 2) { /* any stage: check stages 0 and 2 */
+          for (int tid = 0; tid < NT; tid++) {
+            for (int r = 0; r < (BMt * BK / 2) / NT; r++) {
+              const int ch = tid + r * NT;
+              const int k = ch / (BMt / 2), part = ch % (BMt / 2);
+              const int col = kb + k, i = m0 + part * 2;
+              const long src = (long)imin(col, n_d - 1) * ldN + imin(i, ldN - 2);
+              CHK("A source", src, D_n);
+              CHK("A source + 1", src + 1, D_n);
+              const long dst = (long)st * BK * SAt + (long)k * SAt + part * 2;
+              CHK("A stage", dst, as_n);
+              CHK("A stage + 1", dst + 1, as_n);
+            }
+            for (int r = 0; r < (BN * BK) / NT; r++) {
+              const int ch = tid + r * NT;
+              const int n = ch >> 4, k = ch & 15;
+              const int col = kb + k, j = j0 + n;
+              CHK("dcol slot", col, KP);
+              const long src = (long)dcs[col] + (long)imin(j, J - 1) * P;
+              CHK("B source", src, B_n);
+              CHK("B stage", (long)st * BN * SBT + (long)n * SBT + k, bs_n);
+            }
+          }
+        }
+      }
+      /* fragment reads of one stage (warp_slice_eta), every k4 step */
+      for (int tid = 0; tid < NT; tid++) {
+        const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3, wm = warp >> 2, wn = warp & 3;
+        for (int kk = 0; kk < BK / 4; kk++) {
+          for (int mt = 0; mt < MT; mt++) {
+            const long a = (long)(kk * 4 + t) * SAt + wm * (MT * 16) + g + mt * 16;
+            CHK("A fragment", a, (long)BK * SAt);
+            CHK("A fragment + 8", a + 8, (long)BK * SAt);
+          }
+          for (int nt = 0; nt < 4; nt++) CHK("B fragment", (long)(wn * 32 + nt * 8 + g) * SBT + kk * 4 + t, (long)BN * SBT);
+        }
+        /* level sums, then the stores */
+        for (int mt = 0; mt < MT; mt++)
+          for (int h = 0; h < 2; h++) {
+            if (n_grp > 0) {
+              const int ic = imin(m0 + wm * (MT * 16) + mt * 16 + g + h * 8, N - 1);
+              CHK("gid", ic, N);
+              const long lg = (long)gid[ic] * ldJ;
+              for (int nt = 0; nt < 4; nt++) {
+                const int j = imin(j0 + wn * 32 + nt * 8 + 2 * t, ldJ - 2);
+                CHK("level sum", lg + j, lvt_n);
+                CHK("level sum + 1", lg + j + 1, lvt_n);
+                if ((lg + j) % 2) fault("level sum alignment", ctx, lg + j, 2);
+              }
+            }
+            const int i = m0 + wm * (MT * 16) + mt * 16 + g + h * 8;
+            if (i >= N) continue;
+            for (int nt = 0; nt < 4; nt++)
+              for (int e = 0; e < 2; e++) {
+                const int j = j0 + wn * 32 + nt * 8 + 2 * t + e;
+                if (j < J) {
+                  const long o = (long)j * ldN + i;
+                  CHK("out", o, out_n);
+                  if (o >= 0 && o < out_n) written[o]++;
+                }
+              }
+          }
+      }
+      const int w2 = w + grid;
+      if (w2 < tiles) {
+        const int m1 = (w2 / tn) * BMt, j1 = (w2 % tn) * BN;
+        CHK("next tile row", m1, tm * BMt);
+        CHK("next tile column", j1, tn * BN);
+      }
+    }
+  }
+  for (int w = 0; w < tiles; w++)
+    if (visits[w] != 1) fault("tile visit count", ctx, visits[w], 1);
+  for (int j = 0; j < J; j++)
+    for (int i = 0; i < N; i++)
+      if (written[(long)j * ldN + i] != 1) {
+        fault("output write count", ctx, written[(long)j * ldN + i], 1);
+        j = J;
+        break;
+      }
+  free(dcol);
+  free(gid);
+  free(dcs);
+  free(written);
+  free(visits);
+}
+
+/* k_level_sums: one thread per (group, gene), Lv[g * ldJ + j]. */
+static void mirror_levels(int J, int n_grp) {
+  char ctx[64];
+  snprintf(ctx, sizeof ctx, "levels J=%d n_grp=%d", J, n_grp);
+  const int ldJ = lvt_ld(J);
+  const long n = (long)J * n_grp, lvt_n = (long)n_grp * ldJ;
+  unsigned char* written = calloc((size_t)(lvt_n ? lvt_n : 1), 1);
+  const long blocks = (n + 255) / 256;
+  for (long b = 0; b < blocks; b++)
+    for (int tx = 0; tx < 256; tx++) {
+      const long e = b * 256 + tx;
+      if (e >= n) continue;
+      const int g = (int)(e / J), j = (int)(e - (long)g * J);
+      const long o = (long)g * ldJ + j;
+      CHK("Lv", o, lvt_n);
+      if (o >= 0 && o < lvt_n) written[o]++;
+    }
+  for (int g = 0; g < n_grp; g++)
+    for (int j = 0; j < J; j++)
+      if (written[(long)g * ldJ + j] != 1) fault("Lv write count", ctx, written[(long)g * ldJ + j], 1);
+  free(written);
+}
+
+/* k_w_nu over the launcher's 2-D grid (cell pairs x gene quads, the y extent capped at
+ * 65535 so that larger gene counts take a stride); gridy_cap lets a small case take it. */
+static void mirror_w_nu(int N, int J, int groups, int gridy_cap) {
+  char ctx[80];
+  snprintf(ctx, sizeof ctx, "w_nu N=%d J=%d groups=%d ycap=%d", N, J, groups, gridy_cap);
+  const int ldN = ld_cells(N);
+  const long E_n = (long)ldN * J, W_n = (long)ldN * (J + 1), Nu_n = (long)ldN * J, Wg_n = (long)ldN * J;
+  int* gpos = malloc(sizeof(int) * N);
+  for (int k = 0; k < N; k++) gpos[k] = (int)(((long)k * 7919) % N); /* a permutation when N is not a multiple of 7919 */
+  unsigned char* wr_w = calloc((size_t)W_n, 1);
+  unsigned char* wr_nu = calloc((size_t)Nu_n, 1);
+  unsigned char* wr_g = calloc((size_t)Wg_n, 1);
+  const int gx = div_up(N, 512), gy = imin(div_up(J, WNU_GENES), gridy_cap);
+  for (int by = 0; by < gy; by++)
+    for (int bx = 0; bx < gx; bx++)
+      for (int tx = 0; tx < 256; tx++) {
+        const int i = 2 * (bx * 256 + tx);
+        if (i >= N) continue;
+        const int two = i + 1 < N;
+        CHK("ls / e0 / gpos", i, N);
+        CHK("cell factors", i, 3L * ldN);
+        if (two) CHK("ls / e0 / gpos + 1", i + 1, N);
+        const int p0 = groups ? gpos[i] : 0, p1 = groups && two ? gpos[i + 1] : 0;
+        for (int jb = by * WNU_GENES; jb < J; jb += gy * WNU_GENES)
+          for (int u = 0; u < WNU_GENES; u++) {
+            const int j = jb + u;
+            if (j >= J) break;
+            const long o = (long)j * ldN + i;
+            CHK("eta pair", o, E_n);
+            CHK("eta pair + 1", o + 1, E_n);
+            if (o % 2) fault("pair alignment", ctx, o, 2);
+            if (two) {
+              CHK("W pair", o + 1, W_n);
+              CHK("Nu pair", o + 1, Nu_n);
+              wr_w[o]++, wr_w[o + 1]++, wr_nu[o]++, wr_nu[o + 1]++;
+            } else {
+              CHK("W", o, W_n);
+              CHK("Nu", o, Nu_n);
+              wr_w[o]++, wr_nu[o]++;
+            }
+            if (groups) {
+              const long q0 = (long)j * ldN + p0;
+              CHK("Wg", q0, Wg_n);
+              wr_g[q0]++;
+              if (two) {
+                const long q1 = (long)j * ldN + p1;
+                CHK("Wg", q1, Wg_n);
+                wr_g[q1]++;
+              }
+            }
+          }
+      }
+  for (int j = 0; j < J; j++)
+    for (int i = 0; i < N; i++) {
+      const long o = (long)j * ldN + i;
+      if (wr_w[o] != 1 || wr_nu[o] != 1 || (groups && wr_g[o] != 1)) {
+        fault("W / nu / Wg write count", ctx, o, 1);
+        j = J;
+        break;
+      }
+    }
+  free(gpos);
+  free(wr_w);
+  free(wr_nu);
+  free(wr_g);
+}
+
+int main(int argc, char** argv) {
+  plant_unpadded = argc > 1 && strcmp(argv[1], "plant") == 0;
+  static const int Ns[] = {1, 2, 3, 31, 32, 33, 63, 64, 65, 127, 128, 129, 130, 255, 257, 511, 512, 513, 1001};
+  static const int Js[] = {1, 2, 3, 5, 127, 128, 129, 131, 256, 257};
+  static const int nds[] = {1, 2, 4, 15, 16, 17, 33, 132, 144, 260};
+  static const int grps[] = {0, 1, 3};
+  const int nN = sizeof Ns / sizeof *Ns, nJ = sizeof Js / sizeof *Js, nD = sizeof nds / sizeof *nds;
+  for (int MT = 4; MT >= 2; MT -= 2) {
+    long sizes = 0;
+    for (int a = 0; a < nN; a++)
+      for (int b = 0; b < nJ; b++)
+        for (int d = 0; d < nD; d++)
+          for (int q = 0; q < 3; q++) {
+            const int N = Ns[a], J = Js[b], tiles = ((N + MT * 32 - 1) / (MT * 32)) * ((J + BN - 1) / BN);
+            /* the launcher's grid (148 SMs, one or two CTAs each) and a small one that strides */
+            const int full = imin(tiles, (MT == 2 ? 2 : 1) * 148);
+            mirror_eta(MT, N, J, nds[d], grps[q], full);
+            if (tiles > 3) mirror_eta(MT, N, J, nds[d], grps[q], 3);
+            sizes++;
+          }
+    if (faults) return 1;
+    printf("ok eta%d %ld\n", MT, sizes);
+  }
+  long sizes = 0;
+  for (int b = 0; b < nJ; b++)
+    for (int q = 0; q < 3; q++, sizes++) mirror_levels(Js[b], grps[q]);
+  if (faults) return 1;
+  printf("ok levels %ld\n", sizes);
+  sizes = 0;
+  for (int a = 0; a < nN; a++)
+    for (int b = 0; b < nJ; b++)
+      for (int grp = 0; grp < 2; grp++, sizes++) {
+        mirror_w_nu(Ns[a], Js[b], grp, 65535);
+        mirror_w_nu(Ns[a], Js[b], grp, 2); /* the y stride */
+      }
+  if (faults) return 1;
+  printf("ok w_nu %ld\n", sizes);
+  return 0;
+}

@@ -1,10 +1,16 @@
-"""CPU replay of the memory indexing of the batched Cholesky and inverse panel kernels.
+"""CPU replay of the memory indexing of the batched Cholesky and inverse panel kernels, and of the
+linear predictor and the W / nu pass.
 
 tests/index_mirror/k_inv_mirror.c mirrors every shared- and global-memory index of
 k_potrf_panel, k_trtri_panel and k_lauum_panel (gaspacho2_b200/csrc/k_inv.cu) and counts the
 outputs each must write. It runs here for every P from 1 up to the largest P the launchers
 admit (read from k_inv.cu), so no size the GPU path can reach goes unchecked; one P past the
 Cholesky panel's limit shows that the mirror does catch the rows its update would leave out.
+
+tests/index_mirror/k_wnu_eta_mirror.c mirrors k_eta_dmma (both tile heights), k_level_sums and
+k_w_nu over a sweep of cell, gene, dense-column and group counts (odd sizes, ragged slices,
+persistent grids that stride) and counts every output; with the level sums' rows planted
+unpadded it must fail.
 """
 import os
 import re
@@ -56,3 +62,25 @@ def test_mirror_flags_rows_the_cholesky_update_misses(mirror):
     r = subprocess.run([mirror, "potrf", str(top + 1), str(top + 1)], capture_output=True, text=True)
     assert r.returncode == 1
     assert "updated 0 times" in r.stderr
+
+
+@pytest.fixture(scope="module")
+def wnu_mirror(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("mirror") / "k_wnu_eta_mirror")
+    subprocess.run(["gcc", "-O2", "-std=c11", "-o", exe, os.path.join(HERE, "index_mirror", "k_wnu_eta_mirror.c")],
+                   check=True)
+    return exe
+
+
+def test_predictor_and_w_nu_stay_in_bounds(wnu_mirror):
+    r = subprocess.run([wnu_mirror], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.split()
+    for name in ("eta4", "eta2", "levels", "w_nu"):
+        assert name in lines, r.stdout
+
+
+def test_mirror_flags_unpadded_level_sums(wnu_mirror):
+    r = subprocess.run([wnu_mirror, "plant"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 1
+    assert "level sum alignment" in r.stderr
