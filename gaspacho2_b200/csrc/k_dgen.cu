@@ -5,7 +5,8 @@
 //   zt_u      bvec[dcol a, j] = sum_i D_ia u_ij (getZtOinvjnj util_cuda.cu:462-487 with
 //             u = W nu / Omega; initBeta init.cu:193-221 with u = y0), split over the cells
 //             into 8-32 ranges (chosen to fill the last wave) whose partial sums are added in
-//             order.  2*N*J*n_d flops.
+//             order; its own kernel (k_zt_u), whose raw operands arrive by cp.async.
+//             2*N*J*n_d flops.
 //   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
 //   group     S[j][g][a] = sum_{i in g} w_ij D_ia, K = the group's cells, read from copies of
 //             W, D and 1/Omega in group order (each group a contiguous run of rows).
@@ -181,26 +182,6 @@ struct KGroup {  // the cells of group z
   __device__ int2 operator()(int z) const { return make_int2(0, gstart[z + 1] - gstart[z]); }
 };
 
-struct LdDt {  // A(r = dense column, k = cell) = D[r*ldN + k]
-  static constexpr bool kFastK = true;
-  const double* D;
-  int ldN;
-  __device__ double operator()(int r, int k, int) const { return D[(size_t)r * ldN + k]; }
-};
-struct LdU {  // B(k = cell, c = gene): mode 0 W u / Omega, 1 u (y0), 2 W g / Omega with g per cell
-  static constexpr bool kFastK = true;
-  const double *W, *Nu, *rOm;
-  int ldN, mode;
-  struct Raw {
-    double w, r, u;
-  };
-  __device__ Raw load(int k, int c, int) const {
-    const size_t e = (size_t)c * ldN + k;
-    if (mode == 1) return Raw{1.0, 1.0, Nu[e]};
-    return Raw{W[e], rOm[k], mode == 0 ? Nu[e] : Nu[k]};
-  }
-  __device__ double finish(const Raw& v) const { return v.w * v.r * v.u; }
-};
 struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega (1/phi given)
   static constexpr bool kFastK = false;
   const double *W, *Nu, *E, *rOm, *rphi;
@@ -462,23 +443,138 @@ static int split_count(int tiles, int sms) {
   return best;
 }
 
+// Z^T u with the operands' raw values copied by cp.async: a three-stage pipeline of 16-cell
+// slices (the dense columns [a][cell], W and u [gene][cell], cells contiguous in rows of kZtS;
+// 1/Omega and a per-cell u [cell]) with one barrier per slice, the B operand w * (1/Omega) * u
+// formed as its fragments are read (the same product, in the same order, as the register-staged
+// form, so the sums are those of TileTall's k_dgen over the same cell ranges). Tile: all dense
+// columns (<= 144) x 128 genes, 8 warps along the genes, each 9 x 2 DMMA tiles of 16 x 8; CTA
+// (gene tile, cell range z) writes its partial sums to part[z][a][j]. MODE 0: B = W u / Omega
+// (u cells x genes); 1: B = u; 2: B = W g / Omega with g one value per cell. The cell ranges
+// start at even cells, so every 16-byte copy is aligned (ldN is a multiple of 32).
+namespace {
+constexpr int kZtBK = 16, kZtS = kZtBK + 4;  // slice depth; row stride, 4 mod 16 doubles
+constexpr int kZtBM = 144, kZtBN = 128, kZtStages = 3;
+constexpr int kZtStage = kZtBM * kZtS + 2 * kZtBN * kZtS + 2 * kZtBK;  // doubles per stage
+constexpr int kZtSmem = (int)sizeof(double) * kZtStages * kZtStage;
+}  // namespace
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 1)
+    k_zt_u(int m, int n, int N, int ldN, int per, const double* __restrict__ D, const double* __restrict__ W,
+           const double* __restrict__ U, const double* __restrict__ rOm, double* __restrict__ part) {
+  extern __shared__ __align__(16) double zs[];
+  const int tid = threadIdx.x, wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int n0 = blockIdx.y * kZtBN, z = blockIdx.z;
+  const int kbeg = min(N, z * per), kend = min(N, (z + 1) * per);
+  const int nsl = kend > kbeg ? (kend - kbeg + kZtBK - 1) / kZtBK : 0;
+
+  // slice s into stage st; a pair of cells past the range is zero-filled (8 bytes of a pair
+  // whose second cell is past it), its source clamped into the matrix
+  auto load = [&](int s, int st) {
+    double* As = zs + st * kZtStage;
+    double* Ws = As + kZtBM * kZtS;
+    double* Us = Ws + kZtBN * kZtS;
+    double* Rs = Us + kZtBN * kZtS;
+    double* Vs = Rs + kZtBK;
+    const int k0 = kbeg + s * kZtBK;
+    for (int ch = tid; ch < kZtBM * (kZtBK / 2); ch += 256) {
+      const int r = ch >> 3, kc = (ch & 7) * 2, k = k0 + kc;
+      const int nb = (r < m && k < kend) ? (k + 1 < kend ? 16 : 8) : 0;
+      cp_async16(As + r * kZtS + kc, D + (size_t)min(r, m - 1) * ldN + min(k, ldN - 2), nb);
+    }
+#pragma unroll
+    for (int q = 0; q < (kZtBN * (kZtBK / 2)) / 256; q++) {
+      const int ch = tid + q * 256;
+      const int cc = ch >> 3, kc = (ch & 7) * 2, k = k0 + kc;
+      const int nb = (n0 + cc < n && k < kend) ? (k + 1 < kend ? 16 : 8) : 0;
+      const size_t src = (size_t)min(n0 + cc, n - 1) * ldN + min(k, ldN - 2);
+      if (MODE != 1) cp_async16(Ws + cc * kZtS + kc, W + src, nb);
+      if (MODE != 2) cp_async16(Us + cc * kZtS + kc, U + src, nb);
+    }
+    if (tid < kZtBK) {
+      const int k = k0 + tid, nb = k < kend ? 8 : 0;
+      if (MODE != 1) cp_async8(Rs + tid, rOm + min(k, N - 1), nb);
+      if (MODE == 2) cp_async8(Vs + tid, U + min(k, N - 1), nb);
+    }
+  };
+
+  double acc[9][2][4];
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int y = 0; y < 2; y++)
+#pragma unroll
+      for (int w = 0; w < 4; w++) acc[x][y][w] = 0.0;
+  if (nsl > 0) load(0, 0);
+  cp_async_commit();
+  if (nsl > 1) load(1, 1);
+  cp_async_commit();
+  for (int s = 0; s < nsl; s++) {
+    cp_async_wait<1>();  // slice s landed
+    __syncthreads();     // and every warp is done with slice s - 1, whose stage is refilled next
+    if (s + 2 < nsl) load(s + 2, (s + 2) % kZtStages);
+    cp_async_commit();
+    const double* As = zs + (s % kZtStages) * kZtStage;
+    const double* Ws = As + kZtBM * kZtS;
+    const double* Us = Ws + kZtBN * kZtS;
+    const double* Rs = Us + kZtBN * kZtS;
+    const double* Vs = Rs + kZtBK;
+#pragma unroll
+    for (int k4 = 0; k4 < kZtBK / 4; k4++) {
+      const int kk = k4 * 4 + t;
+      double a[9][2], b[2];
+#pragma unroll
+      for (int x = 0; x < 9; x++) {
+        a[x][0] = As[(x * 16 + g) * kZtS + kk];
+        a[x][1] = As[(x * 16 + g + 8) * kZtS + kk];
+      }
+#pragma unroll
+      for (int y = 0; y < 2; y++) {
+        const int e = (wn * 16 + y * 8 + g) * kZtS + kk;
+        b[y] = MODE == 1 ? Us[e] : MODE == 0 ? Ws[e] * Rs[kk] * Us[e] : Ws[e] * Rs[kk] * Vs[kk];
+      }
+#pragma unroll
+      for (int x = 0; x < 9; x++)
+#pragma unroll
+        for (int y = 0; y < 2; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = x * 16 + g + 8 * h;
+      if (r >= m) continue;
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int cc = n0 + wn * 16 + y * 8 + 2 * t + e;
+          if (cc < n) part[((size_t)z * m + r) * n + cc] = acc[x][y][2 * h + e];
+        }
+    }
+}
+
 int dgen_zt_u(Ctx* c, int mode, const double* u, double* out) {
-  using T = TileTall;
-  if (c->n_d > T::BM) return GPL_ERR_ARG;
+  if (c->n_d > kZtBM) return GPL_ERR_ARG;
   const double* rOm = nullptr;
   if (mode != 1) {
     int rc = recip_omega(c, &rOm);
     if (rc) return rc;
   }
-  const int tiles = div_up(c->J, T::BN);
+  const int tiles = div_up(c->J, kZtBN);
   const int S = split_count(tiles, c->sm_count);
   int rc = ensure_part(c, (size_t)S * c->n_d * c->J);
   if (rc) return rc;
-  const int per = (c->N + S - 1) / S;
+  int per = (c->N + S - 1) / S;
+  per += per & 1;  // even range starts: aligned 16-byte copies
   dim3 g(1, tiles, S);
-  rc = launch_dgen<T>(c, g, c->n_d, c->J, LdDt{c->Dm, c->ldN}, LdU{c->W, u, rOm, c->ldN, mode},
-                      KSplit{c->N, per}, EpPart{c->part, c->n_d, c->J}, "k_dgen(zt_u)");
-  if (rc) return rc;
+  auto* fn = mode == 0 ? k_zt_u<0> : mode == 1 ? k_zt_u<1> : k_zt_u<2>;
+  GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kZtSmem));
+  fn<<<g, 256, kZtSmem, c->stream>>>(c->n_d, c->J, c->N, c->ldN, per, c->Dm, c->W, u, rOm, c->part);
+  GPL_LAUNCHED(c, "k_zt_u");
   dim3 g2(div_up(c->J, 256), c->n_d);
   k_reduce_bvec<<<g2, 256, 0, c->stream>>>(c->n_d, c->J, c->P, S, c->dcol_d, c->part, out);
   GPL_LAUNCHED(c, "k_reduce_bvec");

@@ -206,7 +206,10 @@ __global__ void __launch_bounds__(256) k_w_nu(int N, int ldN, int J, const doubl
 }
 
 // The working response of the counts that the reference's merge walk matches (the first gvalid
-// entries of each gene), after k_w_nu wrote every cell's zero-count value (stream order).
+// entries of each gene), after k_w_nu wrote every cell's zero-count value (stream order). Each
+// thread takes kCountsIlp entries per round, their index, count and eta loads issued before any
+// exp(), so that the dependent gathers of several entries are in flight at once.
+constexpr int kCountsIlp = 4;
 __global__ void __launch_bounds__(256) k_w_nu_counts(int ldN, const double* __restrict__ E,
                                                      const double* __restrict__ ls, const double* __restrict__ f,
                                                      const int32_t* __restrict__ cell,
@@ -218,14 +221,27 @@ __global__ void __launch_bounds__(256) k_w_nu_counts(int ldN, const double* __re
   const double* Ej = E + (size_t)j * ldN;
   double* Nj = Nu + (size_t)j * ldN;
   const int64_t b = gptr[j], e = gptr[j] + gvalid[j];
-  for (int64_t l = b + threadIdx.x; l < e; l += blockDim.x) {
-    const int i = cell[l];
-    const double eta = Ej[i], y = cnt[l];
-    if (de) {
-      const double w = exp(eta) * ls[i] * f[i];
-      Nj[i] = (eta - e0[i]) + (y - w) / w;
-    } else {
-      Nj[i] = eta + exp(log(y) - (eta + f[2 * (size_t)ldN + i] + f[ldN + i])) - 1.0;
+  for (int64_t l0 = b + threadIdx.x; l0 < e; l0 += (int64_t)kCountsIlp * blockDim.x) {
+    int ic[kCountsIlp];
+    double y[kCountsIlp], eta[kCountsIlp];
+#pragma unroll
+    for (int u = 0; u < kCountsIlp; u++) {
+      const int64_t l = l0 + (int64_t)u * blockDim.x;
+      ic[u] = l < e ? cell[l] : -1;
+      y[u] = l < e ? cnt[l] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kCountsIlp; u++) eta[u] = ic[u] >= 0 ? Ej[ic[u]] : 0.0;
+#pragma unroll
+    for (int u = 0; u < kCountsIlp; u++) {
+      const int i = ic[u];
+      if (i < 0) continue;
+      if (de) {
+        const double w = exp(eta[u]) * ls[i] * f[i];
+        Nj[i] = (eta[u] - e0[i]) + (y[u] - w) / w;
+      } else {
+        Nj[i] = eta[u] + exp(log(y[u]) - (eta[u] + f[2 * (size_t)ldN + i] + f[ldN + i])) - 1.0;
+      }
     }
   }
 }

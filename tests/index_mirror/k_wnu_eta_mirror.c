@@ -1,7 +1,7 @@
 /*
- * CPU mirror of the memory indexing of the linear predictor and the W / nu pass:
- * k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu) and k_w_nu
- * (gaspacho2_b200/csrc/k_gemm.cu).
+ * CPU mirror of the memory indexing of the linear predictor, the W / nu pass and Z^T u:
+ * k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu), k_w_nu and k_w_nu_counts
+ * (gaspacho2_b200/csrc/k_gemm.cu) and k_zt_u<MODE> (gaspacho2_b200/csrc/k_dgen.cu).
  *
  * The kernels' own index expressions are replayed for every block and thread of a launch
  * (256 threads; lane = 4 g + t as in the DMMA fragments), over a sweep of sizes: cell counts
@@ -15,9 +15,12 @@
  * once.
  *
  *   k_wnu_eta_mirror        prints "ok eta4 <sizes>", "ok eta2 <sizes>", "ok levels <sizes>",
- *                           "ok w_nu <sizes>" and exits 0, or lists the first faults, exits 1.
+ *                           "ok w_nu <sizes>", "ok counts <sizes>", "ok zt_u <sizes>" and exits 0,
+ *                           or lists the first faults and exits 1.
  *   k_wnu_eta_mirror plant  the same with the level sums' rows left unpadded (J instead of J
  *                           rounded up to even): must fail on an odd gene count.
+ *   k_wnu_eta_mirror plant-odd  Z^T u alone with its cell ranges left at ceil(N / S) cells
+ *                           (not rounded up to even): must fail on a misaligned 16-byte copy.
  *
  * Compiled and run by tests/test_index_mirror.py. Keep it in step with the two kernels.
  */
@@ -42,6 +45,7 @@ static int imin(int a, int b) { return a < b ? a : b; }
 static int div_up(int a, int b) { return (a + b - 1) / b; }
 static int ld_cells(int N) { return (N + 31) / 32 * 32; }
 static int plant_unpadded = 0; /* "plant": the level sums' rows left at J (unpadded) */
+static int plant_odd = 0;      /* "plant-odd": Z^T u's cell ranges not rounded to even */
 static int lvt_ld(int J) { return plant_unpadded ? J : J + (J & 1); }
 
 /* k_eta_dmma<MT>: loads, fragment reads, level sums and stores of every tile a grid of
@@ -249,14 +253,174 @@ static void mirror_w_nu(int N, int J, int groups, int gridy_cap) {
   free(wr_g);
 }
 
+/* k_w_nu_counts: one block of 256 threads per gene, kCountsIlp entries per thread per round. */
+static void mirror_counts(int N, int J, int dens) {
+  char ctx[64];
+  snprintf(ctx, sizeof ctx, "counts N=%d J=%d dens=%d", N, J, dens);
+  const int ldN = ld_cells(N), ILP = 4;
+  /* CSR with a matched prefix of increasing cells per gene: every dens-th cell */
+  long* gptr = malloc(sizeof(long) * (J + 1));
+  int* gvalid = malloc(sizeof(int) * J);
+  gptr[0] = 0;
+  for (int j = 0; j < J; j++) {
+    const int cnt = (N + dens - 1 - (j % dens)) / dens;
+    gvalid[j] = cnt > 0 ? cnt : 0;
+    gptr[j + 1] = gptr[j] + gvalid[j] + (j % 3); /* unmatched tail entries after the prefix */
+  }
+  const long L = gptr[J];
+  int* cell = malloc(sizeof(int) * (L ? L : 1));
+  for (int j = 0; j < J; j++) {
+    long l = gptr[j];
+    for (int i = j % dens; i < N; i += dens) cell[l++] = i;
+    for (; l < gptr[j + 1]; l++) cell[l] = 0; /* past the prefix: never read */
+  }
+  unsigned char* wr = calloc((size_t)ldN * J, 1);
+  for (int j = 0; j < J; j++)
+    for (int tx = 0; tx < 256; tx++) {
+      const long b = gptr[j], e = gptr[j] + gvalid[j];
+      for (long l0 = b + tx; l0 < e; l0 += (long)ILP * 256)
+        for (int u = 0; u < ILP; u++) {
+          const long l = l0 + (long)u * 256;
+          if (l >= e) continue;
+          CHK("CSR entry", l, L);
+          const int i = cell[l];
+          CHK("cell", i, N);
+          CHK("eta / nu", (long)j * ldN + i, (long)ldN * J);
+          CHK("cell factors", 2L * ldN + i, 3L * ldN);
+          wr[(long)j * ldN + i]++;
+        }
+    }
+  for (int j = 0; j < J; j++)
+    for (long l = gptr[j]; l < gptr[j] + gvalid[j]; l++)
+      if (wr[(long)j * ldN + cell[l]] != 1) {
+        fault("matched count write count", ctx, wr[(long)j * ldN + cell[l]], 1);
+        break;
+      }
+  free(gptr);
+  free(gvalid);
+  free(cell);
+  free(wr);
+}
+
+/* k_zt_u<MODE>: grid (1, gene tiles, S cell ranges); three stages of 16-cell slices. */
+#define ZT_BK 16
+#define ZT_S (ZT_BK + 4)
+#define ZT_BM 144
+#define ZT_BN 128
+#define ZT_STAGE (ZT_BM * ZT_S + 2 * ZT_BN * ZT_S + 2 * ZT_BK)
+static void mirror_zt_u(int mode, int N, int J, int m, int S) {
+  char ctx[80];
+  snprintf(ctx, sizeof ctx, "zt_u mode=%d N=%d J=%d n_d=%d S=%d", mode, N, J, m, S);
+  const int ldN = ld_cells(N), n = J;
+  int per = (N + S - 1) / S;
+  if (!plant_odd) per += per & 1;
+  const long D_n = (long)m * ldN, U_n = mode == 2 ? (long)N : (long)ldN * J, W_n = (long)ldN * (J + 1);
+  const long R_n = N, part_n = (long)S * m * n, sm_n = 3L * ZT_STAGE;
+  const int tiles = (J + ZT_BN - 1) / ZT_BN;
+  unsigned char* wr = calloc((size_t)part_n, 1);
+  unsigned char* cellhit = calloc((size_t)N, 1);
+  for (int z = 0; z < S; z++) {
+    const int kbeg = imin(N, z * per), kend = imin(N, (z + 1) * per);
+    const int nsl = kend > kbeg ? (kend - kbeg + ZT_BK - 1) / ZT_BK : 0;
+    if (kbeg < kend && kbeg % 2) fault("odd range start", ctx, kbeg, 2); /* an empty range loads nothing */
+    for (int by = 0; by < tiles; by++) {
+      const int n0 = by * ZT_BN;
+      for (int s = 0; s < nsl; s++) {
+        const int st = s % 3, k0 = kbeg + s * ZT_BK;
+        const long As = (long)st * ZT_STAGE, Ws = As + ZT_BM * ZT_S, Us = Ws + ZT_BN * ZT_S, Rs = Us + ZT_BN * ZT_S,
+                   Vs = Rs + ZT_BK;
+        for (int tid = 0; tid < 256; tid++) {
+          for (int ch = tid; ch < ZT_BM * (ZT_BK / 2); ch += 256) {
+            const int r = ch >> 3, kc = (ch & 7) * 2, k = k0 + kc;
+            const int nb = (r < m && k < kend) ? (k + 1 < kend ? 16 : 8) : 0;
+            const long src = (long)imin(r, m - 1) * ldN + imin(k, ldN - 2);
+            CHK("D", src, D_n);
+            CHK("D + 1", src + 1, D_n);
+            if (src % 2) fault("D alignment", ctx, src, 2);
+            CHK("A stage", As + r * ZT_S + kc + 1, Ws);
+            if ((As + r * ZT_S + kc) % 2) fault("A stage alignment", ctx, As + r * ZT_S + kc, 2);
+            if (nb && by == 0 && r == 0) {
+              cellhit[k]++;
+              if (nb == 16) cellhit[k + 1]++;
+            }
+          }
+          for (int q = 0; q < (ZT_BN * (ZT_BK / 2)) / 256; q++) {
+            const int ch = tid + q * 256;
+            const int cc = ch >> 3, kc = (ch & 7) * 2, k = k0 + kc;
+            const long src = (long)imin(n0 + cc, n - 1) * ldN + imin(k, ldN - 2);
+            if (src % 2) fault("W / u alignment", ctx, src, 2);
+            if (mode != 1) CHK("W", src + 1, W_n);
+            if (mode != 2) CHK("u", src + 1, U_n);
+            CHK("W stage", Ws + cc * ZT_S + kc + 1, Us);
+            CHK("u stage", Us + cc * ZT_S + kc + 1, Rs);
+          }
+          if (tid < ZT_BK) {
+            const int k = k0 + tid;
+            if (mode != 1) CHK("1/Omega", imin(k, N - 1), R_n);
+            if (mode == 2) CHK("per-cell u", imin(k, N - 1), U_n);
+            CHK("1/Omega stage", Rs + tid, Vs);
+            CHK("per-cell u stage", Vs + tid, (long)(st + 1) * ZT_STAGE);
+          }
+          /* fragment reads of this stage */
+          const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+          for (int k4 = 0; k4 < ZT_BK / 4; k4++) {
+            const int kk = k4 * 4 + t;
+            for (int x = 0; x < 9; x++) {
+              CHK("A fragment", As + (x * 16 + g) * ZT_S + kk, Ws);
+              CHK("A fragment + 8", As + (x * 16 + g + 8) * ZT_S + kk, Ws);
+            }
+            for (int y = 0; y < 2; y++) {
+              const long e = (long)(wn * 16 + y * 8 + g) * ZT_S + kk;
+              CHK("W fragment", Ws + e, Us);
+              CHK("u fragment", Us + e, Rs);
+            }
+            CHK("1/Omega fragment", Rs + kk, Vs);
+            CHK("stage end", Vs + kk, sm_n);
+          }
+        }
+      }
+      /* the partial sums */
+      for (int tid = 0; tid < 256; tid++) {
+        const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+        for (int x = 0; x < 9; x++)
+          for (int h = 0; h < 2; h++) {
+            const int r = x * 16 + g + 8 * h;
+            if (r >= m) continue;
+            for (int y = 0; y < 2; y++)
+              for (int e = 0; e < 2; e++) {
+                const int cc = n0 + wn * 16 + y * 8 + 2 * t + e;
+                if (cc >= n) continue;
+                const long o = ((long)z * m + r) * n + cc;
+                CHK("part", o, part_n);
+                if (o >= 0 && o < part_n) wr[o]++;
+              }
+          }
+      }
+    }
+  }
+  for (long o = 0; o < part_n; o++)
+    if (wr[o] != 1) {
+      fault("partial write count", ctx, wr[o], 1);
+      break;
+    }
+  for (int k = 0; k < N; k++)
+    if (cellhit[k] != 1) {
+      fault("cell load count", ctx, cellhit[k], 1);
+      break;
+    }
+  free(wr);
+  free(cellhit);
+}
+
 int main(int argc, char** argv) {
   plant_unpadded = argc > 1 && strcmp(argv[1], "plant") == 0;
+  plant_odd = argc > 1 && strcmp(argv[1], "plant-odd") == 0;
   static const int Ns[] = {1, 2, 3, 31, 32, 33, 63, 64, 65, 127, 128, 129, 130, 255, 257, 511, 512, 513, 1001};
   static const int Js[] = {1, 2, 3, 5, 127, 128, 129, 131, 256, 257};
   static const int nds[] = {1, 2, 4, 15, 16, 17, 33, 132, 144, 260};
   static const int grps[] = {0, 1, 3};
   const int nN = sizeof Ns / sizeof *Ns, nJ = sizeof Js / sizeof *Js, nD = sizeof nds / sizeof *nds;
-  for (int MT = 4; MT >= 2; MT -= 2) {
+  for (int MT = 4; MT >= 2 && !plant_odd; MT -= 2) {
     long sizes = 0;
     for (int a = 0; a < nN; a++)
       for (int b = 0; b < nJ; b++)
@@ -273,12 +437,12 @@ int main(int argc, char** argv) {
     printf("ok eta%d %ld\n", MT, sizes);
   }
   long sizes = 0;
-  for (int b = 0; b < nJ; b++)
+  for (int b = 0; b < nJ && !plant_odd; b++)
     for (int q = 0; q < 3; q++, sizes++) mirror_levels(Js[b], grps[q]);
   if (faults) return 1;
   printf("ok levels %ld\n", sizes);
   sizes = 0;
-  for (int a = 0; a < nN; a++)
+  for (int a = 0; a < nN && !plant_odd; a++)
     for (int b = 0; b < nJ; b++)
       for (int grp = 0; grp < 2; grp++, sizes++) {
         mirror_w_nu(Ns[a], Js[b], grp, 65535);
@@ -286,5 +450,23 @@ int main(int argc, char** argv) {
       }
   if (faults) return 1;
   printf("ok w_nu %ld\n", sizes);
+  sizes = 0;
+  for (int a = 0; a < nN && !plant_odd; a++)
+    for (int b = 0; b < nJ; b++)
+      for (int dens = 1; dens <= 7; dens += 3, sizes++) mirror_counts(Ns[a], Js[b], dens);
+  if (faults) return 1;
+  printf("ok counts %ld\n", sizes);
+  static const int zN[] = {1, 2, 3, 17, 31, 33, 100, 255, 1001, 3001};
+  static const int zJ[] = {1, 3, 128, 129, 257};
+  static const int zM[] = {1, 2, 17, 132, 144};
+  static const int zS[] = {1, 2, 8, 28, 32};
+  sizes = 0;
+  for (int mode = 0; mode < 3; mode++)
+    for (int a = 0; a < 10; a++)
+      for (int b = 0; b < 5; b++)
+        for (int d = 0; d < 5; d++)
+          for (int q = 0; q < 5; q++, sizes++) mirror_zt_u(mode, zN[a], zJ[b], zM[d], zS[q]);
+  if (faults) return 1;
+  printf("ok zt_u %ld\n", sizes);
   return 0;
 }
