@@ -11,7 +11,8 @@
 //   group     S[j][g][a] = sum_{i in g} w_ij D_ia, K = the group's cells, read from copies of
 //             W, D and 1/Omega in group order (each group a contiguous run of rows).
 //   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for 128-cell tiles of each group, O read
-//             from the group-ordered copies and HK scattered back to the cells.
+//             from the group-ordered copies and HK scattered back to the cells; its own kernel
+//             (k_hk), whose raw operands arrive by cp.async.
 //
 // Tile: 8 warps as WARPS_M x WARPS_N, each warp WM x WN DMMA tiles of 16 x 8, K slices of 16
 // staged through registers (the next slice's global loads are in flight during the current
@@ -226,29 +227,6 @@ struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) o
   }
   __device__ double finish(const Raw& v) const { return v.w * v.r; }
 };
-struct LdTab {  // A(r = a, k = gene) = tab[(k*n_grp + g)*ld + r], g from the tile list
-  static constexpr bool kFastK = false;
-  const double* tab;
-  const int2* tiles;
-  int n_grp, ld;
-  __device__ double operator()(int r, int k, int z) const {
-    return tab[((size_t)k * n_grp + tiles[z].x) * ld + r];
-  }
-};
-struct LdTileO {  // B(k = gene, c = cell slot) = W/Omega of the tile's c-th cell, group order
-  static constexpr bool kFastK = false;
-  const double *Wg, *rOmg;
-  const int* pos;  // 128 slots per tile, positions in group order (-1 past the group)
-  int ldN;
-  struct Raw {
-    double w, r;
-  };
-  __device__ Raw load(int k, int c, int z) const {
-    const int q = pos[(size_t)z * 128 + c];
-    return q < 0 ? Raw{0.0, 0.0} : Raw{Wg[(size_t)k * ldN + q], rOmg[q]};
-  }
-  __device__ double finish(const Raw& v) const { return v.w * v.r; }
-};
 
 // ---- epilogues -------------------------------------------------------------------------------
 struct EpPart {  // split-K partials part[z][r][c]
@@ -265,15 +243,6 @@ struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
   double* S;
   int n_grp, ld;
   __device__ void operator()(int a, int j, int g, double v) const { S[((size_t)j * n_grp + g) * ld + a] = v; }
-};
-struct EpHK {  // HK[cell + a*ldN] with r = a, c = cell slot of tile z
-  double* HK;
-  const int* cells;
-  int ldN;
-  __device__ void operator()(int a, int c, int z, double v) const {
-    const int i = cells[(size_t)z * 128 + c];
-    if (i >= 0) HK[i + (size_t)a * ldN] = v;
-  }
 };
 
 // Un-whitening of the precision form's Gram, one gene per z: T = G L^T, then L T.
@@ -642,18 +611,118 @@ int dgen_group_sums(Ctx* c, int mode) {
                         EpGroup{c->gsum, c->n_grp, c->n_d + 1}, "k_dgen(group_sums)");
 }
 
+// HK[i, a] = sum_j O_ij tab[j][g(i)][a] for the 128 cell slots of each group tile (grid z =
+// tile), the genes in 16-deep slices through a four-stage cp.async pipeline of the raw operands:
+// the group's table rows tab[j][g][0..ld) ([gene][a]) and W's group-ordered values of the tile's
+// slots ([gene][slot]), by 8-byte copies (neither row starts at an even offset in general);
+// 1/Omega of the slots is read once. The B operand W (1/Omega) is formed at the fragment loads,
+// the same product in the same order as the register-staged form, so the sums are TileTall's.
+namespace {
+constexpr int kHkBK = 16, kHkSA = 148, kHkSB = 132, kHkStages = 4;  // row strides 4 mod 16
+constexpr int kHkStage = kHkBK * kHkSA + kHkBK * kHkSB;             // doubles per stage
+constexpr int kHkSmem = (int)sizeof(double) * (kHkStages * kHkStage + 128);
+}  // namespace
+
+__global__ void __launch_bounds__(256, 1)
+    k_hk(int ld, int J, int n_grp, int ldN, const double* __restrict__ tab, const int2* __restrict__ tiles,
+         const double* __restrict__ Wg, const double* __restrict__ rOmg, const int* __restrict__ pos,
+         const int* __restrict__ cells, double* __restrict__ HK) {
+  extern __shared__ __align__(16) double hs[];
+  double* Rs = hs + kHkStages * kHkStage;  // [128] 1/Omega of the slots, 0 past the group
+  const int tid = threadIdx.x, wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int z = blockIdx.z, grp = tiles[z].x;
+  const int myq = pos[(size_t)z * 128 + (tid & 127)];  // this thread's slot in every B copy
+  if (tid < 128) Rs[tid] = myq < 0 ? 0.0 : rOmg[myq];
+  const int nsl = (J + kHkBK - 1) / kHkBK;
+
+  auto load = [&](int s, int st) {
+    double* As = hs + st * kHkStage;
+    double* Bs = As + kHkBK * kHkSA;
+    const int k0 = s * kHkBK;
+    for (int e = tid; e < kHkBK * 144; e += 256) {
+      const int k = e / 144, r = e - k * 144, j = k0 + k;
+      const int nb = (r < ld && j < J) ? 8 : 0;
+      cp_async8(As + k * kHkSA + r, tab + ((size_t)min(j, J - 1) * n_grp + grp) * ld + min(r, ld - 1), nb);
+    }
+#pragma unroll
+    for (int q = 0; q < (kHkBK * 128) / 256; q++) {
+      const int k = (tid >> 7) + 2 * q, j = k0 + k;
+      const int nb = (myq >= 0 && j < J) ? 8 : 0;
+      cp_async8(Bs + k * kHkSB + (tid & 127), Wg + (size_t)min(j, J - 1) * ldN + max(myq, 0), nb);
+    }
+  };
+
+  double acc[9][2][4];
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int y = 0; y < 2; y++)
+#pragma unroll
+      for (int w = 0; w < 4; w++) acc[x][y][w] = 0.0;
+#pragma unroll
+  for (int s = 0; s < kHkStages - 1; s++) {
+    if (s < nsl) load(s, s);
+    cp_async_commit();
+  }
+  for (int s = 0; s < nsl; s++) {
+    cp_async_wait<kHkStages - 2>();  // slice s landed
+    __syncthreads();                 // and every warp is done with slice s - 1, whose stage is refilled next
+    if (s + kHkStages - 1 < nsl) load(s + kHkStages - 1, (s + kHkStages - 1) % kHkStages);
+    cp_async_commit();
+    const double* As = hs + (s % kHkStages) * kHkStage;
+    const double* Bs = As + kHkBK * kHkSA;
+#pragma unroll
+    for (int k4 = 0; k4 < kHkBK / 4; k4++) {
+      const int kk = k4 * 4 + t;
+      double a[9][2], b[2];
+#pragma unroll
+      for (int x = 0; x < 9; x++) {
+        a[x][0] = As[kk * kHkSA + x * 16 + g];
+        a[x][1] = As[kk * kHkSA + x * 16 + g + 8];
+      }
+#pragma unroll
+      for (int y = 0; y < 2; y++) {
+        const int cs = wn * 16 + y * 8 + g;
+        b[y] = Bs[kk * kHkSB + cs] * Rs[cs];
+      }
+#pragma unroll
+      for (int x = 0; x < 9; x++)
+#pragma unroll
+        for (int y = 0; y < 2; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
+    }
+  }
+  cp_async_wait<0>();
+  const int* cz = cells + (size_t)z * 128;
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = x * 16 + g + 8 * h;
+      if (r >= ld) continue;
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int i = cz[wn * 16 + y * 8 + 2 * t + e];
+          if (i >= 0) HK[i + (size_t)r * ldN] = acc[x][y][2 * h + e];
+        }
+    }
+}
+
 int dgen_hk(Ctx* c) {
-  using T = TileTall;
   const int ld = c->n_d + 1;
-  if (ld > T::BM) return GPL_ERR_ARG;
+  if (ld > 144) return GPL_ERR_ARG;
   const double* rOm = nullptr;
   int rc = recip_omega(c, &rOm);
   if (rc) return rc;
   if ((rc = launch_group_order(c, rOm, 1, c->rOmg))) return rc;
-  dim3 g(1, 1, c->n_hk_tiles128);
-  return launch_dgen<T>(c, g, ld, T::BN, LdTab{c->gsum, c->hk_tiles128_d, c->n_grp, ld},
-                        LdTileO{c->Wg, c->rOmg, c->hk_pos_d, c->ldN}, KAll{c->J}, EpHK{c->HK, c->hk_cells_d, c->ldN},
-                        "k_dgen(hk)");
+  if (c->n_hk_tiles128 == 0) return GPL_OK;
+  GPL_TRY(c, cudaFuncSetAttribute(k_hk, cudaFuncAttributeMaxDynamicSharedMemorySize, kHkSmem));
+  k_hk<<<dim3(1, 1, c->n_hk_tiles128), 256, kHkSmem, c->stream>>>(ld, c->J, c->n_grp, c->ldN, c->gsum,
+                                                                   c->hk_tiles128_d, c->Wg, c->rOmg, c->hk_pos_d,
+                                                                   c->hk_cells_d, c->HK);
+  GPL_LAUNCHED(c, "k_hk");
+  return GPL_OK;
 }
 
 // Psi_DD,j = L G~_j L^T + DeltaInv_DD for every gene: T_j = G~_j L^T as one GEMM over the stacked

@@ -1,7 +1,7 @@
 /*
- * CPU mirror of the memory indexing of the linear predictor, the W / nu pass and Z^T u:
+ * CPU mirror of the memory indexing of the linear predictor, the W / nu pass, Z^T u and HK:
  * k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu), k_w_nu and k_w_nu_counts
- * (gaspacho2_b200/csrc/k_gemm.cu) and k_zt_u<MODE> (gaspacho2_b200/csrc/k_dgen.cu).
+ * (gaspacho2_b200/csrc/k_gemm.cu), k_zt_u<MODE> and k_hk (gaspacho2_b200/csrc/k_dgen.cu).
  *
  * The kernels' own index expressions are replayed for every block and thread of a launch
  * (256 threads; lane = 4 g + t as in the DMMA fragments), over a sweep of sizes: cell counts
@@ -15,8 +15,8 @@
  * once.
  *
  *   k_wnu_eta_mirror        prints "ok eta4 <sizes>", "ok eta2 <sizes>", "ok levels <sizes>",
- *                           "ok w_nu <sizes>", "ok counts <sizes>", "ok zt_u <sizes>" and exits 0,
- *                           or lists the first faults and exits 1.
+ *                           "ok w_nu <sizes>", "ok counts <sizes>", "ok zt_u <sizes>",
+ *                           "ok hk <sizes>" and exits 0, or lists the first faults and exits 1.
  *   k_wnu_eta_mirror plant  the same with the level sums' rows left unpadded (J instead of J
  *                           rounded up to even): must fail on an odd gene count.
  *   k_wnu_eta_mirror plant-odd  Z^T u alone with its cell ranges left at ceil(N / S) cells
@@ -412,6 +412,104 @@ static void mirror_zt_u(int mode, int N, int J, int m, int S) {
   free(cellhit);
 }
 
+/* k_hk: grid z = the 128-slot tiles of every group (gpl_api.cu's tile list), four stages of
+ * 16-gene slices; groups of the given sizes, the cells in group order a permutation. */
+#define HK_BK 16
+#define HK_SA 148
+#define HK_SB 132
+#define HK_STAGE (HK_BK * HK_SA + HK_BK * HK_SB)
+static void mirror_hk(int n_d, int J, const int* sizes, int n_grp) {
+  char ctx[80];
+  int N = 0;
+  for (int q = 0; q < n_grp; q++) N += sizes[q];
+  snprintf(ctx, sizeof ctx, "hk n_d=%d J=%d n_grp=%d N=%d", n_d, J, n_grp, N);
+  if (N == 0) return;
+  const int ld = n_d + 1, ldN = ld_cells(N);
+  const long tab_n = (long)J * n_grp * ld, Wg_n = (long)ldN * J, HK_n = (long)ldN * ld;
+  const long sm_n = 4L * HK_STAGE + 128;
+  int* gstart = malloc(sizeof(int) * (n_grp + 1));
+  gstart[0] = 0;
+  for (int q = 0; q < n_grp; q++) gstart[q + 1] = gstart[q] + sizes[q];
+  int* order = malloc(sizeof(int) * N);
+  for (int k = 0; k < N; k++) order[k] = (int)(((long)k * 7919) % N);
+  int ntiles = 0;
+  for (int q = 0; q < n_grp; q++) ntiles += (sizes[q] + 127) / 128;
+  int* tg = malloc(sizeof(int) * (ntiles ? ntiles : 1));
+  int* tcell = malloc(sizeof(int) * 128 * (ntiles ? ntiles : 1));
+  int* tpos = malloc(sizeof(int) * 128 * (ntiles ? ntiles : 1));
+  int nt = 0;
+  for (int q = 0; q < n_grp; q++)
+    for (int r0 = 0; r0 < sizes[q]; r0 += 128, nt++) {
+      tg[nt] = q;
+      for (int c = 0; c < 128; c++) {
+        const int in = r0 + c < sizes[q];
+        tcell[nt * 128 + c] = in ? order[gstart[q] + r0 + c] : -1;
+        tpos[nt * 128 + c] = in ? gstart[q] + r0 + c : -1;
+      }
+    }
+  unsigned char* wr = calloc((size_t)HK_n, 1);
+  const int nsl = (J + HK_BK - 1) / HK_BK;
+  for (int z = 0; z < ntiles; z++) {
+    const int grp = tg[z];
+    CHK("group", grp, n_grp);
+    for (int tid = 0; tid < 256; tid++) {
+      const int myq = tpos[z * 128 + (tid & 127)];
+      if (myq >= 0) CHK("1/Omega slot", myq, N);
+      if (tid < 128) CHK("1/Omega stage", 4L * HK_STAGE + tid, sm_n);
+      for (int s = 0; s < nsl; s++) {
+        const int st = s % 4, k0 = s * HK_BK;
+        const long As = (long)st * HK_STAGE, Bs = As + HK_BK * HK_SA;
+        for (int e = tid; e < HK_BK * 144; e += 256) {
+          const int k = e / 144, r = e - k * 144, j = k0 + k;
+          CHK("table", ((long)imin(j, J - 1) * n_grp + grp) * ld + imin(r, ld - 1), tab_n);
+          CHK("table stage", As + (long)k * HK_SA + r, Bs);
+        }
+        for (int q = 0; q < (HK_BK * 128) / 256; q++) {
+          const int k = (tid >> 7) + 2 * q, j = k0 + k;
+          CHK("W group order", (long)imin(j, J - 1) * ldN + (myq > 0 ? myq : 0), Wg_n);
+          CHK("W stage", Bs + (long)k * HK_SB + (tid & 127), (long)(st + 1) * HK_STAGE);
+        }
+        const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+        for (int k4 = 0; k4 < HK_BK / 4; k4++) {
+          const int kk = k4 * 4 + t;
+          for (int x = 0; x < 9; x++) CHK("table fragment", As + (long)kk * HK_SA + x * 16 + g + 8, Bs);
+          for (int y = 0; y < 2; y++) {
+            const int cs = wn * 16 + y * 8 + g;
+            CHK("W fragment", Bs + (long)kk * HK_SB + cs, (long)(st + 1) * HK_STAGE);
+            CHK("slot", cs, 128);
+          }
+        }
+      }
+      const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+      for (int x = 0; x < 9; x++)
+        for (int h = 0; h < 2; h++) {
+          const int r = x * 16 + g + 8 * h;
+          if (r >= ld) continue;
+          for (int y = 0; y < 2; y++)
+            for (int e = 0; e < 2; e++) {
+              const int i = tcell[z * 128 + wn * 16 + y * 8 + 2 * t + e];
+              if (i < 0) continue;
+              CHK("HK", i + (long)r * ldN, HK_n);
+              wr[i + (long)r * ldN]++;
+            }
+        }
+    }
+  }
+  for (int r = 0; r < ld; r++)
+    for (int i = 0; i < N; i++)
+      if (wr[i + (long)r * ldN] != 1) {
+        fault("HK write count", ctx, wr[i + (long)r * ldN], 1);
+        r = ld;
+        break;
+      }
+  free(gstart);
+  free(order);
+  free(tg);
+  free(tcell);
+  free(tpos);
+  free(wr);
+}
+
 int main(int argc, char** argv) {
   plant_unpadded = argc > 1 && strcmp(argv[1], "plant") == 0;
   plant_odd = argc > 1 && strcmp(argv[1], "plant-odd") == 0;
@@ -468,5 +566,20 @@ int main(int argc, char** argv) {
           for (int q = 0; q < 5; q++, sizes++) mirror_zt_u(mode, zN[a], zJ[b], zM[d], zS[q]);
   if (faults) return 1;
   printf("ok zt_u %ld\n", sizes);
+  if (plant_odd) return 0;
+  static const int g1[] = {1};
+  static const int g2[] = {127, 128, 129, 0, 255, 3};
+  static const int g3[] = {300, 1, 1, 2, 513, 64, 0, 77};
+  static const int hd[] = {1, 2, 17, 100, 132, 143};
+  static const int hJ[] = {1, 3, 16, 17, 100};
+  sizes = 0;
+  for (int d = 0; d < 6; d++)
+    for (int b = 0; b < 5; b++, sizes += 3) {
+      mirror_hk(hd[d], hJ[b], g1, 1);
+      mirror_hk(hd[d], hJ[b], g2, 6);
+      mirror_hk(hd[d], hJ[b], g3, 8);
+    }
+  if (faults) return 1;
+  printf("ok hk %ld\n", sizes);
   return 0;
 }
