@@ -9,7 +9,8 @@
 //             2*N*J*n_d flops.
 //   c1_tn     C1[i, a] = sum_j (tn_ij / phi_j) tBeta_j[GP a] (ggplvm.cu:344).  2*N*J*M flops.
 //   group     S[j][g][a] = sum_{i in g} w_ij D_ia, K = the group's cells, read from copies of
-//             W, D and 1/Omega in group order (each group a contiguous run of rows).
+//             W, D and 1/Omega in group order (each group a contiguous run of rows); its own
+//             kernel (k_group_sums_dmma), whose raw operands arrive by cp.async.
 //   hk        HK[i, a] = sum_j O_ij tab[j][g(i)][a] for 128-cell tiles of each group, O read
 //             from the group-ordered copies and HK scattered back to the cells; its own kernel
 //             (k_hk), whose raw operands arrive by cp.async.
@@ -178,10 +179,6 @@ struct KAll {
   int K;
   __device__ int2 operator()(int) const { return make_int2(0, K); }
 };
-struct KGroup {  // the cells of group z
-  const int* gstart;
-  __device__ int2 operator()(int z) const { return make_int2(0, gstart[z + 1] - gstart[z]); }
-};
 
 struct LdTn {  // A(r = cell, k = gene) = (O nu - O E) / phi, O = W / Omega (1/phi given)
   static constexpr bool kFastK = false;
@@ -205,28 +202,6 @@ struct LdTBetaGP {  // B(k = gene, c = a) = tBeta[g0 + c + k*P]
   int P, g0;
   __device__ double operator()(int k, int c, int) const { return tB[g0 + c + (size_t)k * P]; }
 };
-struct LdGroupD {  // A(r = dense column, k = k-th cell of group z) = Dg[r*ldN + gstart[z] + k] (group order)
-  static constexpr bool kFastK = true;
-  const double* Dg;
-  const int* gstart;
-  int ldN;
-  __device__ double operator()(int r, int k, int z) const { return Dg[(size_t)r * ldN + gstart[z] + k]; }
-};
-struct LdGroupW {  // B(k = k-th cell of group z, c = gene) = W/Omega (mode 0) or 1 (mode 1), group order
-  static constexpr bool kFastK = true;
-  const double *Wg, *rOmg;
-  const int* gstart;
-  int ldN, mode;
-  struct Raw {
-    double w, r;
-  };
-  __device__ Raw load(int k, int c, int z) const {
-    if (mode == 1) return Raw{1.0, 1.0};
-    const int pos = gstart[z] + k;
-    return Raw{Wg[(size_t)c * ldN + pos], rOmg[pos]};
-  }
-  __device__ double finish(const Raw& v) const { return v.w * v.r; }
-};
 
 // ---- epilogues -------------------------------------------------------------------------------
 struct EpPart {  // split-K partials part[z][r][c]
@@ -238,11 +213,6 @@ struct EpColMajor {  // out[r + c*ld]
   double* out;
   int64_t ld;
   __device__ void operator()(int r, int c, int, double v) const { out[r + (size_t)c * ld] = v; }
-};
-struct EpGroup {  // S[(j*n_grp + g)*ld + a] with r = a, c = j, z = g
-  double* S;
-  int n_grp, ld;
-  __device__ void operator()(int a, int j, int g, double v) const { S[((size_t)j * n_grp + g) * ld + a] = v; }
 };
 
 // Un-whitening of the precision form's Gram, one gene per z: T = G L^T, then L T.
@@ -594,9 +564,106 @@ int dgen_c1_tn(Ctx* c) {
   return GPL_OK;
 }
 
+// S[j][g][a] = sum over group g's cells of w_ij D_ia (w = W/Omega, MODE 0; 1, MODE 1): grid
+// (gene tiles, groups), the group's cells (a contiguous run in group order) in 16-cell slices
+// through a three-stage cp.async pipeline of the raw operands, 8-byte copies (a group starts at
+// any cell): the dense columns [a][cell] from their group-ordered copy, W's group-ordered values
+// [gene][cell] and 1/Omega [cell]; w formed at the fragment loads, the same product in the same
+// order as the register-staged form, so the sums are TileTall's.
+template <int MODE>
+__global__ void __launch_bounds__(256, 1)
+    k_group_sums_dmma(int m, int n, int n_grp, int ldN, const int* __restrict__ gstart, const double* __restrict__ Dg,
+                      const double* __restrict__ Wg, const double* __restrict__ rOmg, double* __restrict__ S) {
+  extern __shared__ __align__(16) double zs[];
+  const int tid = threadIdx.x, wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int n0 = blockIdx.y * kZtBN, z = blockIdx.z;
+  const int kbeg = gstart[z], kend = gstart[z + 1];
+  const int nsl = kend > kbeg ? (kend - kbeg + kZtBK - 1) / kZtBK : 0;
+  const int last = max(kend - 1, 0);  // a cell of the matrix, for the sources of zero-fill copies
+
+  auto load = [&](int s, int st) {
+    double* As = zs + st * kZtStage;
+    double* Ws = As + kZtBM * kZtS;
+    double* Rs = Ws + 2 * kZtBN * kZtS;
+    const int k0 = kbeg + s * kZtBK;
+    for (int e = tid; e < kZtBM * kZtBK; e += 256) {
+      const int r = e >> 4, kc = e & 15, k = k0 + kc;
+      const int nb = (r < m && k < kend) ? 8 : 0;
+      cp_async8(As + r * kZtS + kc, Dg + (size_t)min(r, m - 1) * ldN + min(k, last), nb);
+    }
+    if (MODE == 0) {
+#pragma unroll
+      for (int q = 0; q < (kZtBN * kZtBK) / 256; q++) {
+        const int e = tid + q * 256, cc = e >> 4, kc = e & 15, k = k0 + kc;
+        const int nb = (n0 + cc < n && k < kend) ? 8 : 0;
+        cp_async8(Ws + cc * kZtS + kc, Wg + (size_t)min(n0 + cc, n - 1) * ldN + min(k, last), nb);
+      }
+      if (tid < kZtBK) {
+        const int k = k0 + tid;
+        cp_async8(Rs + tid, rOmg + min(k, last), k < kend ? 8 : 0);
+      }
+    }
+  };
+
+  double acc[9][2][4];
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int y = 0; y < 2; y++)
+#pragma unroll
+      for (int w = 0; w < 4; w++) acc[x][y][w] = 0.0;
+  if (nsl > 0) load(0, 0);
+  cp_async_commit();
+  if (nsl > 1) load(1, 1);
+  cp_async_commit();
+  for (int s = 0; s < nsl; s++) {
+    cp_async_wait<1>();  // slice s landed
+    __syncthreads();     // and every warp is done with slice s - 1, whose stage is refilled next
+    if (s + 2 < nsl) load(s + 2, (s + 2) % kZtStages);
+    cp_async_commit();
+    const double* As = zs + (s % kZtStages) * kZtStage;
+    const double* Ws = As + kZtBM * kZtS;
+    const double* Rs = Ws + 2 * kZtBN * kZtS;
+    const int live = kend - (kbeg + s * kZtBK);  // cells of this slice in the group
+#pragma unroll
+    for (int k4 = 0; k4 < kZtBK / 4; k4++) {
+      const int kk = k4 * 4 + t;
+      double a[9][2], b[2];
+#pragma unroll
+      for (int x = 0; x < 9; x++) {
+        a[x][0] = As[(x * 16 + g) * kZtS + kk];
+        a[x][1] = As[(x * 16 + g + 8) * kZtS + kk];
+      }
+#pragma unroll
+      for (int y = 0; y < 2; y++) {
+        const int e = (wn * 16 + y * 8 + g) * kZtS + kk;
+        b[y] = MODE == 0 ? Ws[e] * Rs[kk] : (kk < live && n0 + wn * 16 + y * 8 + g < n ? 1.0 * 1.0 : 0.0);
+      }
+#pragma unroll
+      for (int x = 0; x < 9; x++)
+#pragma unroll
+        for (int y = 0; y < 2; y++) dmma_16x8x4(acc[x][y], a[x][0], a[x][1], b[y]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int x = 0; x < 9; x++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = x * 16 + g + 8 * h;
+      if (r >= m) continue;
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int j = n0 + wn * 16 + y * 8 + 2 * t + e;
+          if (j < n) S[((size_t)j * n_grp + z) * (m + 1) + r] = acc[x][y][2 * h + e];
+        }
+    }
+}
+
 int dgen_group_sums(Ctx* c, int mode) {
-  using T = TileTall;
-  if (c->n_d > T::BM) return GPL_ERR_ARG;
+  if (c->n_d > kZtBM) return GPL_ERR_ARG;
   int rc;
   if (mode == 0) {
     const double* rOm = nullptr;
@@ -605,10 +672,12 @@ int dgen_group_sums(Ctx* c, int mode) {
   }
   if ((rc = launch_group_order(c, c->Dm, c->n_d, c->Dg))) return rc;
   const int J = mode == 1 ? 1 : c->J;
-  dim3 g(1, div_up(J, T::BN), c->n_grp);
-  return launch_dgen<T>(c, g, c->n_d, J, LdGroupD{c->Dg, c->gstart_d, c->ldN},
-                        LdGroupW{c->Wg, c->rOmg, c->gstart_d, c->ldN, mode}, KGroup{c->gstart_d},
-                        EpGroup{c->gsum, c->n_grp, c->n_d + 1}, "k_dgen(group_sums)");
+  dim3 g(1, div_up(J, kZtBN), c->n_grp);
+  auto* fn = mode == 0 ? k_group_sums_dmma<0> : k_group_sums_dmma<1>;
+  GPL_TRY(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kZtSmem));
+  fn<<<g, 256, kZtSmem, c->stream>>>(c->n_d, J, c->n_grp, c->ldN, c->gstart_d, c->Dg, c->Wg, c->rOmg, c->gsum);
+  GPL_LAUNCHED(c, "k_group_sums_dmma");
+  return GPL_OK;
 }
 
 // HK[i, a] = sum_j O_ij tab[j][g(i)][a] for the 128 cell slots of each group tile (grid z =

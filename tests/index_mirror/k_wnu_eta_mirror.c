@@ -1,7 +1,8 @@
 /*
- * CPU mirror of the memory indexing of the linear predictor, the W / nu pass, Z^T u and HK:
- * k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu), k_w_nu and k_w_nu_counts
- * (gaspacho2_b200/csrc/k_gemm.cu), k_zt_u<MODE> and k_hk (gaspacho2_b200/csrc/k_dgen.cu).
+ * CPU mirror of the memory indexing of the linear predictor, the W / nu pass, Z^T u, HK and
+ * the group sums: k_eta_dmma<MT> and k_level_sums (gaspacho2_b200/csrc/k_dgemm.cu), k_w_nu and
+ * k_w_nu_counts (gaspacho2_b200/csrc/k_gemm.cu), k_zt_u<MODE>, k_hk and k_group_sums_dmma<MODE>
+ * (gaspacho2_b200/csrc/k_dgen.cu).
  *
  * The kernels' own index expressions are replayed for every block and thread of a launch
  * (256 threads; lane = 4 g + t as in the DMMA fragments), over a sweep of sizes: cell counts
@@ -16,7 +17,8 @@
  *
  *   k_wnu_eta_mirror        prints "ok eta4 <sizes>", "ok eta2 <sizes>", "ok levels <sizes>",
  *                           "ok w_nu <sizes>", "ok counts <sizes>", "ok zt_u <sizes>",
- *                           "ok hk <sizes>" and exits 0, or lists the first faults and exits 1.
+ *                           "ok hk <sizes>", "ok group_sums <sizes>" and exits 0, or lists the
+ *                           first faults and exits 1.
  *   k_wnu_eta_mirror plant  the same with the level sums' rows left unpadded (J instead of J
  *                           rounded up to even): must fail on an odd gene count.
  *   k_wnu_eta_mirror plant-odd  Z^T u alone with its cell ranges left at ceil(N / S) cells
@@ -510,6 +512,94 @@ static void mirror_hk(int n_d, int J, const int* sizes, int n_grp) {
   free(wr);
 }
 
+/* k_group_sums_dmma<MODE>: grid (gene tiles, groups); three stages of 16-cell slices of the
+ * group's run of cells in group order, the stage layout of k_zt_u. */
+static void mirror_group_sums(int mode, int m, int J, const int* sizes, int n_grp) {
+  char ctx[80];
+  int N = 0;
+  for (int q = 0; q < n_grp; q++) N += sizes[q];
+  snprintf(ctx, sizeof ctx, "group_sums mode=%d n_d=%d J=%d n_grp=%d N=%d", mode, m, J, n_grp, N);
+  if (N == 0) return;
+  const int ldN = ld_cells(N), n = mode == 1 ? 1 : J;
+  const long Dg_n = (long)m * ldN, Wg_n = (long)ldN * J, R_n = ldN, S_n = (long)J * n_grp * (m + 1);
+  int* gstart = malloc(sizeof(int) * (n_grp + 1));
+  gstart[0] = 0;
+  for (int q = 0; q < n_grp; q++) gstart[q + 1] = gstart[q] + sizes[q];
+  unsigned char* wr = calloc((size_t)S_n, 1);
+  const int tiles = (n + ZT_BN - 1) / ZT_BN;
+  for (int z = 0; z < n_grp; z++) {
+    const int kbeg = gstart[z], kend = gstart[z + 1];
+    const int nsl = kend > kbeg ? (kend - kbeg + ZT_BK - 1) / ZT_BK : 0;
+    const int last = kend - 1 > 0 ? kend - 1 : 0;
+    unsigned char* hit = calloc((size_t)(kend - kbeg + 1), 1);
+    for (int by = 0; by < tiles; by++) {
+      const int n0 = by * ZT_BN;
+      for (int s = 0; s < nsl; s++) {
+        const int st = s % 3, k0 = kbeg + s * ZT_BK;
+        const long As = (long)st * ZT_STAGE, Ws = As + ZT_BM * ZT_S, Rs = Ws + 2L * ZT_BN * ZT_S;
+        for (int tid = 0; tid < 256; tid++) {
+          for (int e = tid; e < ZT_BM * ZT_BK; e += 256) {
+            const int r = e >> 4, kc = e & 15, k = k0 + kc;
+            CHK("Dg", (long)imin(r, m - 1) * ldN + imin(k, last), Dg_n);
+            CHK("A stage", As + r * ZT_S + kc, Ws);
+            if (r < m && k < kend && by == 0 && r == 0) hit[k - kbeg]++;
+          }
+          if (mode == 0) {
+            for (int q = 0; q < (ZT_BN * ZT_BK) / 256; q++) {
+              const int e = tid + q * 256, cc = e >> 4, kc = e & 15, k = k0 + kc;
+              CHK("Wg", (long)imin(n0 + cc, n - 1) * ldN + imin(k, last), Wg_n);
+              CHK("W stage", Ws + cc * ZT_S + kc, Ws + ZT_BN * ZT_S);
+            }
+            if (tid < ZT_BK) {
+              CHK("1/Omega", imin(k0 + tid, last), R_n);
+              CHK("1/Omega stage", Rs + tid, (long)(st + 1) * ZT_STAGE);
+            }
+          }
+          const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+          for (int k4 = 0; k4 < ZT_BK / 4; k4++) {
+            const int kk = k4 * 4 + t;
+            for (int x = 0; x < 9; x++) CHK("A fragment", As + (x * 16 + g + 8) * ZT_S + kk, Ws);
+            for (int y = 0; y < 2; y++) CHK("W fragment", Ws + (long)(wn * 16 + y * 8 + g) * ZT_S + kk, Ws + ZT_BN * ZT_S);
+            CHK("1/Omega fragment", Rs + kk, (long)(st + 1) * ZT_STAGE);
+          }
+        }
+      }
+      for (int tid = 0; tid < 256; tid++) {
+        const int wn = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+        for (int x = 0; x < 9; x++)
+          for (int h = 0; h < 2; h++) {
+            const int r = x * 16 + g + 8 * h;
+            if (r >= m) continue;
+            for (int y = 0; y < 2; y++)
+              for (int e = 0; e < 2; e++) {
+                const int j = n0 + wn * 16 + y * 8 + 2 * t + e;
+                if (j >= n) continue;
+                const long o = ((long)j * n_grp + z) * (m + 1) + r;
+                CHK("S", o, S_n);
+                if (o >= 0 && o < S_n) wr[o]++;
+              }
+          }
+      }
+    }
+    for (int k = 0; k < kend - kbeg; k++)
+      if (hit[k] != 1) {
+        fault("group cell load count", ctx, hit[k], 1);
+        break;
+      }
+    free(hit);
+  }
+  for (int j = 0; j < n; j++)
+    for (int z = 0; z < n_grp; z++)
+      for (int r = 0; r < m; r++)
+        if (wr[((long)j * n_grp + z) * (m + 1) + r] != 1) {
+          fault("S write count", ctx, wr[((long)j * n_grp + z) * (m + 1) + r], 1);
+          j = n, z = n_grp;
+          break;
+        }
+  free(gstart);
+  free(wr);
+}
+
 int main(int argc, char** argv) {
   plant_unpadded = argc > 1 && strcmp(argv[1], "plant") == 0;
   plant_odd = argc > 1 && strcmp(argv[1], "plant-odd") == 0;
@@ -581,5 +671,15 @@ int main(int argc, char** argv) {
     }
   if (faults) return 1;
   printf("ok hk %ld\n", sizes);
+  sizes = 0;
+  for (int mode = 0; mode < 2; mode++)
+    for (int d = 0; d < 6; d++)
+      for (int b = 0; b < 5; b++, sizes += 3) {
+        mirror_group_sums(mode, hd[d] < 144 ? hd[d] : 144, hJ[b] * 3, g1, 1);
+        mirror_group_sums(mode, hd[d], hJ[b] * 3, g2, 6);
+        mirror_group_sums(mode, hd[d], hJ[b] * 3, g3, 8);
+      }
+  if (faults) return 1;
+  printf("ok group_sums %ld\n", sizes);
   return 0;
 }

@@ -8,7 +8,7 @@ admit (read from k_inv.cu), so no size the GPU path can reach goes unchecked; on
 Cholesky panel's limit shows that the mirror does catch the rows its update would leave out.
 
 tests/index_mirror/k_wnu_eta_mirror.c mirrors k_eta_dmma (both tile heights), k_level_sums,
-k_w_nu, k_w_nu_counts, k_zt_u (its three modes) and k_hk over a sweep of cell, gene, dense-column,
+k_w_nu, k_w_nu_counts, k_zt_u (its three modes), k_hk and k_group_sums_dmma over a sweep of cell, gene, dense-column,
 group and cell-range counts (odd sizes, ragged slices, persistent grids that stride, empty
 ranges) and counts every output and every loaded cell; with the level sums' rows planted
 unpadded, or Z^T u's cell ranges planted at odd starts, it must fail.
@@ -77,7 +77,7 @@ def test_predictor_and_w_nu_stay_in_bounds(wnu_mirror):
     r = subprocess.run([wnu_mirror], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = r.stdout.split()
-    for name in ("eta4", "eta2", "levels", "w_nu", "counts", "zt_u", "hk"):
+    for name in ("eta4", "eta2", "levels", "w_nu", "counts", "zt_u", "hk", "group_sums"):
         assert name in lines, r.stdout
 
 
